@@ -1,0 +1,301 @@
+"""Benchmark of the B200 helium engine (one JSON line on stdout from rank 0).
+
+Step = one two-electron H·psi application on the H·psi microbenchmark grid (coupled
+l1,l2<=5, L<=3, M=0: nc=43; 60 FE elements of order 9 + 20-point ECS tail: n=560;
+N=13,484,800 amplitudes), length gauge, z field 0.02 a.u., complex128 arithmetic.
+`value` = H·psi GB/s = algorithmic bytes (read psi + write H·psi = 2 N 16 B) per
+application / device time, summed over ranks.  The complex64 mode, the end-to-end
+host-buffer figure, the roofline of the kernel and the CPU oracle baseline are
+reported beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Multi-GPU runs are independent replicas (one instance per GPU, no collective on
+the data path); timing is the max over ranks of CUDA-event time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = 'H·ψ HBM GB/s (3D He steps/s & H·ψ HBM GB/s: FP64 vs mixed/batched at ≤1e-6 spectrum err)'
+WORKLOAD = 'H·ψ microbenchmark: coupled l1,l2<=5 L<=3 M=0 (nc=43), 60 FE x order 9 + 20-pt ECS tail (n=560), N=13.48M'
+L2_BYTES = 126 * 2 ** 20
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument('--gpus', type=int, default=1)
+    p.add_argument('--steps', type=int, default=200)
+    p.add_argument('--warmup', type=int, default=5)
+    p.add_argument('--impl', choices=['b200', 'reference'], default='b200')
+    p.add_argument('--no-cpu-baseline', action='store_true')
+    p.add_argument('--profile', choices=['c128', 'c64'], default=None,
+                   help='run only W+K applications of one precision (for ncu captures); prints no JSON')
+    return p.parse_args()
+
+
+def peaks():
+    path = REPO / 'MEASURED_PEAKS.json'
+    if path.exists():
+        data = json.loads(path.read_text())
+        return float(data['hbm_gbs']), float(data['bf16_tflops']), 'measured'
+    return 6650.0, 1590.0, 'fallback'
+
+
+def profile_traffic(name):
+    """dram bytes per launch recorded in a committed ncu summary (profiles/<name>.md)."""
+    path = REPO / 'profiles' / f'{name}.md'
+    if not path.exists():
+        return None
+    for line in path.read_text().splitlines():
+        if line.strip().startswith('traffic_bytes_per_launch:'):
+            try:
+                return float(line.split(':', 1)[1])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling while the timed region runs."""
+    QUERY = ('clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,'
+             'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,'
+             'clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, gpu_id):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.gpu_id), f'--query-gpu={self.QUERY}',
+                                          '--format=csv,noheader,nounits', '-lms', '50'],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(',')]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[4:8]):
+                if flag.lower() in ('active', '1'):
+                    reasons.add(name)
+        return {'sm_mhz': float(np.median(sm)) if sm else None, 'sm_max_mhz': mx, 'samples': len(sm),
+                'reasons': sorted(reasons)}
+
+
+def gpu_identifier(torch, device):
+    props = torch.cuda.get_device_properties(device)
+    uuid = getattr(props, 'uuid', None)
+    if uuid is not None:
+        text = str(uuid)
+        return text if text.startswith('GPU-') else 'GPU-' + text
+    visible = os.environ.get('CUDA_VISIBLE_DEVICES')
+    return visible.split(',')[device.index or 0] if visible else device.index or 0
+
+
+def cpu_oracle_rate(h, psi, field, budget_s):
+    """Oracle (C/OpenMP restatement of kernels.f90:119-176) on a bounded channel sample.
+    Returns (GB/s of the full-operator equivalent, threads, sample description)."""
+    from oracle import cpu
+    tables = cpu.host_tables(h)
+    start = time.perf_counter()
+    cpu.tensor_apply(h, psi, field, False, channels=(0, 1), tables=tables)
+    per_channel = max(time.perf_counter() - start, 1e-6)
+    count = int(min(h.nc, max(1, budget_s / per_channel)))
+    start = time.perf_counter()
+    cpu.tensor_apply(h, psi, field, False, channels=(0, count), tables=tables)
+    elapsed = time.perf_counter() - start
+    gbs = 2 * h.size * 16 * (count / h.nc) / elapsed / 1e9
+    return gbs, cpu.threads(), f'output channels 0..{count - 1} of {h.nc} (one H.psi over {count / h.nc:.3f} of the state), {elapsed:.1f} s'
+
+
+def run_reference(args, rank):
+    """--impl reference: the CPU oracle of the reference's native H·psi on host cores."""
+    if rank != 0:
+        return 0
+    os.environ.setdefault('OMP_NUM_THREADS', str(os.cpu_count()))
+    from laqphysics_b200 import workloads
+    from oracle import cpu
+    h = workloads.hpsi_microbench()
+    psi = workloads.seeded_state(h.size, 1234)
+    field = (0., 0., .02)
+    tables = cpu.host_tables(h)
+    start = time.perf_counter()
+    cpu.tensor_apply(h, psi, field, False, channels=(0, 1), tables=tables)
+    per_channel = max(time.perf_counter() - start, 1e-6)
+    budget = 150.0 / max(1, args.steps + args.warmup)
+    count = int(min(h.nc, max(1, budget / per_channel)))
+    for _ in range(args.warmup):
+        cpu.tensor_apply(h, psi, field, False, channels=(0, count), tables=tables)
+    start = time.perf_counter()
+    for _ in range(args.steps):
+        cpu.tensor_apply(h, psi, field, False, channels=(0, count), tables=tables)
+    elapsed = time.perf_counter() - start
+    frac = count / h.nc
+    gbs = 2 * h.size * 16 * frac * args.steps / elapsed / 1e9
+    sample = f'each step: output channels 0..{count - 1} of {h.nc} ({frac:.3f} of one H.psi), complex128'
+    line = {'impl': 'reference', 'metric': METRIC, 'value': gbs, 'unit': 'GB/s', 'n_gpus': args.gpus,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': elapsed / args.steps * 1e3 / frac,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'complex128',
+            'data': 'synthetic (seeded complex Gaussian state)',
+            'config': {'workload': WORKLOAD, 'field': 'length gauge, Ez=0.02', 'parallelism': 'replicas'},
+            'cpu_baseline': {'value': gbs, 'unit': 'GB/s', 'cores': cpu.threads(), 'kind': 'port', 'sample': sample},
+            'e2e': {'value': gbs, 'unit': 'GB/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get('RANK', 0))
+    world = int(os.environ.get('WORLD_SIZE', 1))
+    local = int(os.environ.get('LOCAL_RANK', 0))
+    if args.impl == 'reference':
+        return run_reference(args, rank)
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    if world > 1:
+        dist.init_process_group('nccl', timeout=timedelta(seconds=300), device_id=torch.device('cuda', local))
+    device = torch.device('cuda', local)
+    torch.cuda.set_device(device)
+    from laqphysics_b200 import workloads
+    from laqphysics_b200.engine import B200Hamiltonian
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    h = workloads.hpsi_microbench()
+    engine = B200Hamiltonian(h, device)
+    field = (0., 0., .02)
+    N = h.size
+    bytes128 = 2 * N * 16
+    inputs = [torch.as_tensor(workloads.seeded_state(N, 1234 + 7 * rank + k), device=device) for k in range(2)]
+    out = torch.empty_like(inputs[0])
+    in64 = [x.to(torch.complex64) for x in inputs]
+    out64 = torch.empty_like(in64[0])
+    stream = torch.cuda.current_stream(device)
+
+    def timed(fn, steps):
+        barrier()
+        torch.cuda.synchronize(device)
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for k in range(steps):
+            fn(k)
+        stop.record(stream)
+        torch.cuda.synchronize(device)
+        barrier()
+        ms = start.elapsed_time(stop)
+        if world > 1:
+            t = torch.tensor([ms], device=device, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    step128 = lambda k: engine.apply(inputs[k % 2], field, False, out=out)
+    step64 = lambda k: engine.apply(in64[k % 2], field, False, out=out64)
+    host_in = torch.empty(N, dtype=torch.complex128).pin_memory()
+    host_in.copy_(inputs[0].cpu())
+    host_out = torch.empty_like(host_in).pin_memory()
+    dev_in = torch.empty_like(inputs[0])
+
+    def step_e2e(k):
+        dev_in.copy_(host_in, non_blocking=True)
+        engine.apply(dev_in, field, False, out=out)
+        host_out.copy_(out, non_blocking=True)
+
+    if args.profile:
+        step = step128 if args.profile == 'c128' else step64
+        for k in range(args.warmup + args.steps):
+            step(k)
+        torch.cuda.synchronize(device)
+        return 0
+    for k in range(max(3, args.warmup)):
+        step128(k); step64(k); step_e2e(k)
+    torch.cuda.synchronize(device)
+    launches0 = engine.apply_count
+    with ClockSampler(gpu_identifier(torch, device)) as clocks:
+        ms128 = timed(step128, args.steps)
+        launches = engine.apply_count - launches0
+        ms64 = timed(step64, args.steps)
+        e2e_steps = max(3, min(args.steps, 20))
+        ms_e2e = timed(step_e2e, e2e_steps)
+    per128 = ms128 / args.steps
+    per64 = ms64 / args.steps
+    per_e2e = ms_e2e / e2e_steps
+    value = world * bytes128 / (per128 * 1e-3) / 1e9
+    value64 = world * (2 * N * 8) / (per64 * 1e-3) / 1e9
+    e2e = world * bytes128 / (per_e2e * 1e-3) / 1e9
+    hbm, _, peak_kind = peaks()
+    flops = workloads.hpsi_flops(h)
+    achieved = bytes128 / (per128 * 1e-3) / 1e9
+    line = {
+        'metric': METRIC, 'value': value, 'unit': 'GB/s', 'n_gpus': world, 'steps': args.steps,
+        'warmup': args.warmup, 'ms_per_step': per128, 'higher_is_better': True, 'scaling': 'weak',
+        'vs_baseline': None, 'dtype': 'complex128', 'data': 'synthetic (seeded complex Gaussian state)',
+        'config': {'workload': WORKLOAD, 'field': 'length gauge, Ez=0.02', 'parallelism': f'replicas x{world}',
+                   'l2': 'two rotating 216 MB input states (> 126 MB L2)'},
+        'gpu_launches': launches,
+        'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': hbm, 'unit': 'GB/s', 'frac': achieved / hbm,
+                     'traffic': profile_traffic('hpsi_c128_microbench'), 'peak_kind': peak_kind,
+                     'kernel': 'hpsi_gather_kernel<double>',
+                     'fp64_tflops': flops / (per128 * 1e-3) / 1e12, 'flops_per_apply': flops},
+        'complex64': {'value': value64, 'unit': 'GB/s', 'ms_per_step': per64,
+                      'frac': value64 / world / hbm, 'speedup_vs_complex128': per128 / per64},
+        'e2e': {'value': e2e, 'unit': 'GB/s', 'ms_per_step': per_e2e, 'steps': e2e_steps,
+                'h2d_bytes_per_step': N * 16, 'd2h_bytes_per_step': N * 16,
+                'path': 'pinned host psi -> H2D -> B200Hamiltonian.apply -> D2H pinned host'},
+        'clocks': clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        os.environ.setdefault('OMP_NUM_THREADS', str(os.cpu_count()))
+        gbs, cores, sample = cpu_oracle_rate(h, workloads.seeded_state(N, 1234), field, 15.0)
+        line['cpu_baseline'] = {'value': gbs, 'unit': 'GB/s', 'cores': cores, 'kind': 'port', 'sample': sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == '__main__':
+    sys.exit(main())

@@ -1,0 +1,105 @@
+/*
+ * helium_b200.h — C-ABI of the B200 (sm_100a) two-electron helium propagation engine.
+ *
+ * Plain C types only: integers, doubles, raw pointers and sizes.  Complex arrays are
+ * interleaved (re, im) pairs — the memory layout of numpy complex128 / C99 double
+ * complex / torch.complex128 (and of complex64 when `precision` = HE_C64).  Wave
+ * functions use the reference's Fortran order psi(i, j, c): r1 index fastest, then r2,
+ * then channel (src/kernels.f90:125, python/native.py:25).  Device pointers and
+ * `stream` (a cudaStream_t passed as void*) belong to the caller.  Every he_* entry
+ * returns an int status (HE_OK = 0); he_last_error() gives the message of the last
+ * failure on the calling thread.  Nothing here traps: device-side failures (e.g. a
+ * Krylov or GMRES non-convergence) come back as status words.
+ */
+#ifndef HELIUM_B200_H
+#define HELIUM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    HE_OK = 0,
+    HE_ERR_ARG = 1,        /* bad argument (null pointer, negative size, bad enum)        */
+    HE_ERR_SHAPE = 2,      /* table inconsistent with its sizes (index out of range ...)  */
+    HE_ERR_CUDA = 3,       /* CUDA runtime error; see he_last_error()                     */
+    HE_ERR_NOCONV = 4,     /* Arnoldi or GMRES did not converge within its limits         */
+    HE_ERR_UNSUPPORTED = 5 /* requested combination not built (e.g. no complex64 tables)  */
+};
+
+enum { HE_C128 = 0, HE_C64 = 1 };   /* arithmetic of an apply: complex128 or complex64 */
+
+/* ------------------------------------------------------------------------------------
+ * Drop-in native symbol.
+ * Replaces `tensor_apply` of the reference's Fortran library: src/kernels.f90:119-127
+ * (bind(C) signature), loaded by python/native.py:8 and called at python/native.py:31-38
+ * (callers python/helium3d.py:79-80, python/ground_s.py:46).  Same argument order and
+ * meaning: scalars by value, zero-based CSR/edge indices, host column-major arrays,
+ * `out` preallocated by the caller.  The work runs on the current CUDA device: the
+ * tables and psi are staged to device memory, H·psi is computed in complex128 by the
+ * sm_100a kernel and copied back.  The reference has no error channel; here a failure
+ * leaves `out` untouched and is reported by he_last_status()/he_last_error().
+ * ---------------------------------------------------------------------------------- */
+void tensor_apply(int n, int nc, int nt, const int *ptr, const int *col, const double *tv,
+                  const double *diag, int nv, const int *vptr, const int *vc, const int *vl,
+                  const double *vcoef, const double *rad, int nd, const int *dptr, const int *dc,
+                  const int *de, const double *dcoef, const double *ldiff, const double *r,
+                  const double *field, int velocity, const double *psi, double *out);
+
+int he_last_status(void);
+const char *he_last_error(void);
+int he_version(void);
+
+/* ------------------------------------------------------------------------------------
+ * Device operator handle.
+ * Replaces the construction half of the reference's TorchHamiltonian
+ * (python/torch_backend.py:12-75): host tables in, device-resident tables out.
+ * Tables are the arrays of python/helium3d.py:12-50 (or of CoupledHelium,
+ * python/coupled_angular.py:13-55): kinetic CSR (ptr, col, tv), diagonal `diag`
+ * (n*n*nc; may be NULL when the separable parts d1(n,nc), d2(n,nc) with
+ * diag(i,j,c) = d1(i,c) + d2(j,c) are given), Coulomb edges (vptr, vc, vl, vcoef),
+ * multipole radial table rad(n, n, nlam), dipole edges (dptr, dc, de, dcoef(3,nd),
+ * ldiff) and nodes r(n).  flags: bit 0 = also build complex64 tables.
+ * ---------------------------------------------------------------------------------- */
+typedef struct he_operator *he_handle;
+
+int he_create(he_handle *out, int n, int nc, int nt, const int *ptr, const int *col, const double *tv,
+              const double *diag, const double *d1, const double *d2,
+              int nv, const int *vptr, const int *vc, const int *vl, const double *vcoef,
+              const double *rad, int nlam,
+              int nd, const int *dptr, const int *dc, const int *de, const double *dcoef,
+              const double *ldiff, const double *r, int flags);
+int he_destroy(he_handle h);
+int he_info(he_handle h, long long *values, int count);
+
+/* out = H(field, gauge) psi.  Replaces TorchHamiltonian.apply
+ * (python/torch_backend.py:109-131) and, bit for bit in meaning, kernels.f90:119-176.
+ * velocity = 0: length gauge (field = E), 1: velocity gauge (field = A, adds |A|^2). */
+int he_apply(he_handle h, const void *psi, void *out, const double *field, int velocity,
+             int precision, void *stream);
+
+/* out = psi + i*alpha*(H(field) psi - e_ref psi): the shifted Pade operator of
+ * python/implicit.py:77-84 (K = H - E_ref, A(y) = y + i alpha K y), alpha complex. */
+int he_apply_shifted(he_handle h, const void *psi, void *out, const double *field, int velocity,
+                     double alpha_re, double alpha_im, double e_ref, int precision, void *stream);
+
+/* Jacobi diagonal of H at zero field: diag + kinetic diagonals + same-channel Coulomb
+ * (python/torch_backend.py:24-31).  out: n*n*nc complex128, device. */
+int he_diagonal(he_handle h, void *out, void *stream);
+
+/* ------------------------------------------------------------------------------------
+ * tSURFF surface flux frame.  Replaces Helium.flux / TorchHamiltonian.flux
+ * (python/helium3d.py:68-77, python/torch_backend.py:133-138):
+ * frame(a, s, c) = sum_b J(s, lo+b) psi(a, lo+b, c)
+ *   + sum_{electron-2 dipole edges k of c, |coef_k| > 1e-15} coef_k sum_b JP(s, lo+b) psi(a, lo+b, dc_k).
+ * J, JP: ns x width complex128 row-major device arrays holding columns [lo, lo+width)
+ * of surface_T and surface_P (python/helium3d.py:65-66); frame: (n, ns, nc) Fortran
+ * order, complex128, device.
+ * ---------------------------------------------------------------------------------- */
+int he_flux(he_handle h, const void *psi, void *frame, int ns, int lo, int width, const void *J,
+            const void *JP, const double *field, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HELIUM_B200_H */

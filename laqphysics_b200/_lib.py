@@ -1,0 +1,61 @@
+"""ctypes binding of libhelium_b200.so (the C-ABI declared in include/helium_b200.h).
+
+The library is required: importing this module without it raises, so no code path
+can silently run without the CUDA kernels.  Build it with
+``python -m laqphysics_b200.build``.
+"""
+import ctypes as ct
+import os
+from pathlib import Path
+
+LIBRARY = Path(os.environ.get('HELIUM_B200_LIBRARY', Path(__file__).resolve().parent / '_lib' / 'libhelium_b200.so'))
+if not LIBRARY.exists():
+    raise ImportError(f'{LIBRARY} is missing: build it with `python -m laqphysics_b200.build`')
+LIB = ct.CDLL(str(LIBRARY))
+
+HE_OK, HE_ERR_ARG, HE_ERR_SHAPE, HE_ERR_CUDA, HE_ERR_NOCONV, HE_ERR_UNSUPPORTED = range(6)
+HE_C128, HE_C64 = 0, 1
+
+P = ct.c_void_p
+I = ct.c_int
+D = ct.c_double
+
+# Every exported symbol and its argument types: (name, restype, argtypes).
+SIGNATURES = {
+    'tensor_apply': (None, [I, I, I, P, P, P, P, I, P, P, P, P, P, I, P, P, P, P, P, P, P, I, P, P]),
+    'he_last_status': (I, []),
+    'he_last_error': (ct.c_char_p, []),
+    'he_version': (I, []),
+    'he_create': (I, [ct.POINTER(P), I, I, I, P, P, P, P, P, P, I, P, P, P, P, P, I, I, P, P, P, P, P, P, I]),
+    'he_destroy': (I, [P]),
+    'he_info': (I, [P, ct.POINTER(ct.c_longlong), I]),
+    'he_apply': (I, [P, P, P, P, I, I, P]),
+    'he_apply_shifted': (I, [P, P, P, P, I, D, D, D, I, P]),
+    'he_diagonal': (I, [P, P, P]),
+    'he_flux': (I, [P, P, P, I, I, I, P, P, P, P]),
+}
+
+for _name, (_res, _args) in SIGNATURES.items():
+    _fn = getattr(LIB, _name)
+    _fn.restype = _res
+    _fn.argtypes = _args
+
+
+class HeliumError(RuntimeError):
+    """A C-ABI call returned a non-zero status."""
+
+    def __init__(self, status, message):
+        super().__init__(f'{message} (status {status})')
+        self.status = status
+
+
+def check(status, what=''):
+    if status != HE_OK:
+        message = LIB.he_last_error().decode(errors='replace')
+        raise HeliumError(status, f'{what}: {message}' if what else message)
+    return status
+
+
+def ptr(array):
+    """Address of a numpy array's data as a ctypes void pointer."""
+    return ct.c_void_p(array.ctypes.data)

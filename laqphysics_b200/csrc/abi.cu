@@ -1,0 +1,268 @@
+// extern "C" entry points of libhelium_b200.so: operator handles, the drop-in
+// host-pointer `tensor_apply`, and error reporting.
+#include <algorithm>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "hamiltonian.cuh"
+#include "operator.cuh"
+
+namespace {
+thread_local char g_error[512] = "";
+thread_local int g_status = HE_OK;
+}  // namespace
+
+void he_set_error(const char *what, const char *file, int line)
+{
+    const char *base = strrchr(file, '/');
+    snprintf(g_error, sizeof(g_error), "%s (%s:%d)", what, base ? base + 1 : file, line);
+}
+
+int he_fail(int status, const char *what, const char *file, int line)
+{
+    he_set_error(what, file, line);
+    g_status = status;
+    return status;
+}
+
+extern "C" const char *he_last_error(void) { return g_error; }
+extern "C" int he_last_status(void) { return g_status; }
+extern "C" int he_version(void) { return 1; }
+
+// ---------------------------------------------------------------------------------
+// Table upload
+// ---------------------------------------------------------------------------------
+namespace {
+
+template <typename T> int upload(he_operator *h, const T *src, size_t count, const T **dst)
+{
+    *dst = nullptr;
+    if (count == 0) return HE_OK;
+    void *p = nullptr;
+    HE_CUDA_TRY(cudaMalloc(&p, count * sizeof(T)));
+    h->allocations.push_back(p);
+    HE_CUDA_TRY(cudaMemcpy(p, src, count * sizeof(T), cudaMemcpyHostToDevice));
+    *dst = static_cast<const T *>(p);
+    return HE_OK;
+}
+
+// complex128 host array -> device complex of precision R
+template <typename R> int upload_c(he_operator *h, const double *src, size_t count, const cplx<R> **dst)
+{
+    std::vector<cplx<R>> tmp(count);
+    for (size_t k = 0; k < count; ++k) tmp[k] = mk<R>((R)src[2 * k], (R)src[2 * k + 1]);
+    return upload(h, tmp.data(), count, dst);
+}
+
+template <typename R> int upload_r(he_operator *h, const double *src, size_t count, const R **dst)
+{
+    std::vector<R> tmp(src, src + count);
+    return upload(h, tmp.data(), count, dst);
+}
+
+int check_csr(const int *ptr, int rows, const int *col, int nnz, int ncol, const char *name)
+{
+    if (ptr[0] != 0 || ptr[rows] != nnz) return he_fail(HE_ERR_SHAPE, name, __FILE__, __LINE__);
+    for (int i = 0; i < rows; ++i)
+        if (ptr[i + 1] < ptr[i]) return he_fail(HE_ERR_SHAPE, name, __FILE__, __LINE__);
+    for (int k = 0; k < nnz; ++k)
+        if (col[k] < 0 || col[k] >= ncol) return he_fail(HE_ERR_SHAPE, name, __FILE__, __LINE__);
+    return HE_OK;
+}
+
+template <typename R>
+int build_tables(he_operator *h, he::DeviceTables<R> *t, const int *ptr, const int *col, const double *tv,
+                 const double *diag, const double *d1, const double *d2, const int *vptr, const int *vc,
+                 const int *vl, const double *vcoef, const double *rad, const int *dptr, const int *dc,
+                 const int *de, const double *dcoef, const double *ldiff, const double *r,
+                 const double *hinv)
+{
+    const size_t n = h->n, nc = h->nc;
+    t->n = h->n; t->nc = h->nc; t->nt = h->nt; t->nv = h->nv; t->nd = h->nd; t->nlam = h->nlam;
+    t->diag_separable = h->separable;
+    int s;
+    if ((s = upload(h, ptr, n + 1, &t->ptr))) return s;
+    if ((s = upload(h, col, (size_t)h->nt, &t->col))) return s;
+    if ((s = upload_c<R>(h, tv, (size_t)h->nt, &t->tv))) return s;
+    t->diag = nullptr; t->d1 = nullptr; t->d2 = nullptr;
+    if (h->separable) {
+        if ((s = upload_c<R>(h, d1, n * nc, &t->d1))) return s;
+        if ((s = upload_c<R>(h, d2, n * nc, &t->d2))) return s;
+    } else {
+        if ((s = upload_c<R>(h, diag, n * n * nc, &t->diag))) return s;
+    }
+    if ((s = upload(h, vptr, nc + 1, &t->vptr))) return s;
+    if ((s = upload(h, vc, (size_t)h->nv, &t->vc))) return s;
+    if ((s = upload(h, vl, (size_t)h->nv, &t->vl))) return s;
+    if ((s = upload_c<R>(h, vcoef, (size_t)h->nv, &t->vcoef))) return s;
+    if ((s = upload_c<R>(h, rad, n * n * (size_t)h->nlam, &t->rad))) return s;
+    if ((s = upload(h, dptr, nc + 1, &t->dptr))) return s;
+    if ((s = upload(h, dc, (size_t)h->nd, &t->dc))) return s;
+    if ((s = upload(h, de, (size_t)h->nd, &t->de))) return s;
+    if ((s = upload_c<R>(h, dcoef, 3 * (size_t)h->nd, &t->dcoef))) return s;
+    if ((s = upload_r<R>(h, ldiff, (size_t)h->nd, &t->ldiff))) return s;
+    if ((s = upload_c<R>(h, r, n, &t->r))) return s;
+    if ((s = upload_c<R>(h, hinv, n, &t->hinv))) return s;
+    return HE_OK;
+}
+
+}  // namespace
+
+he_operator::~he_operator()
+{
+    for (void *p : allocations) cudaFree(p);
+}
+
+extern "C" int he_create(he_handle *out, int n, int nc, int nt, const int *ptr, const int *col, const double *tv,
+                         const double *diag, const double *d1, const double *d2, int nv, const int *vptr,
+                         const int *vc, const int *vl, const double *vcoef, const double *rad, int nlam, int nd,
+                         const int *dptr, const int *dc, const int *de, const double *dcoef, const double *ldiff,
+                         const double *r, int flags)
+{
+    g_status = HE_OK;
+    if (!out) return he_fail(HE_ERR_ARG, "null handle pointer", __FILE__, __LINE__);
+    *out = nullptr;
+    if (n < 1 || nc < 1 || nt < 0 || nv < 0 || nd < 0 || nlam < 1)
+        return he_fail(HE_ERR_ARG, "sizes must be positive", __FILE__, __LINE__);
+    if (!ptr || (nt && (!col || !tv)) || !vptr || (nv && (!vc || !vl || !vcoef)) || !rad || !dptr ||
+        (nd && (!dc || !de || !dcoef || !ldiff)) || !r)
+        return he_fail(HE_ERR_ARG, "null table pointer", __FILE__, __LINE__);
+    const bool separable = d1 && d2;
+    if (!separable && !diag) return he_fail(HE_ERR_ARG, "need diag or (d1, d2)", __FILE__, __LINE__);
+    int s;
+    if ((s = check_csr(ptr, n, col, nt, n, "kinetic CSR inconsistent"))) return s;
+    if ((s = check_csr(vptr, nc, vc, nv, nc, "Coulomb edge list inconsistent"))) return s;
+    if ((s = check_csr(dptr, nc, dc, nd, nc, "dipole edge list inconsistent"))) return s;
+    for (int k = 0; k < nv; ++k)
+        if (vl[k] < 0 || vl[k] >= nlam) return he_fail(HE_ERR_SHAPE, "multipole order outside rad table", __FILE__, __LINE__);
+    for (int k = 0; k < nd; ++k)
+        if (de[k] != 1 && de[k] != 2) return he_fail(HE_ERR_SHAPE, "dipole electron must be 1 or 2", __FILE__, __LINE__);
+    for (int i = 0; i < n; ++i)
+        if (r[2 * i] == 0.0 && r[2 * i + 1] == 0.0) return he_fail(HE_ERR_SHAPE, "radial node at r=0", __FILE__, __LINE__);
+
+    he_operator *h = new he_operator();
+    h->n = n; h->nc = nc; h->nt = nt; h->nv = nv; h->nd = nd; h->nlam = nlam;
+    h->separable = separable;
+    h->has32 = (flags & 1) != 0;
+    HE_CUDA_TRY(cudaGetDevice(&h->device));
+    std::vector<double> hinv(2 * (size_t)n), tdiag(2 * (size_t)n, 0.0);
+    for (int i = 0; i < n; ++i) {
+        const std::complex<double> v = 1.0 / (2.0 * std::complex<double>(r[2 * i], r[2 * i + 1]));
+        hinv[2 * i] = v.real(); hinv[2 * i + 1] = v.imag();
+        for (int k = ptr[i]; k < ptr[i + 1]; ++k)
+            if (col[k] == i) { tdiag[2 * i] += tv[2 * k]; tdiag[2 * i + 1] += tv[2 * k + 1]; }
+    }
+    s = build_tables<double>(h, &h->t64, ptr, col, tv, diag, d1, d2, vptr, vc, vl, vcoef, rad, dptr, dc, de, dcoef,
+                             ldiff, r, hinv.data());
+    if (!s && h->has32)
+        s = build_tables<float>(h, &h->t32, ptr, col, tv, diag, d1, d2, vptr, vc, vl, vcoef, rad, dptr, dc, de,
+                                dcoef, ldiff, r, hinv.data());
+    if (!s) {
+        const double2 *td = nullptr;
+        s = upload_c<double>(h, tdiag.data(), (size_t)n, &td);
+        h->tdiag = td;
+    }
+    if (s) { delete h; g_status = s; return s; }
+    *out = h;
+    return HE_OK;
+}
+
+extern "C" int he_destroy(he_handle h)
+{
+    delete h;
+    return HE_OK;
+}
+
+extern "C" int he_info(he_handle h, long long *values, int count)
+{
+    if (!h || !values) return he_fail(HE_ERR_ARG, "null argument", __FILE__, __LINE__);
+    const long long all[] = {h->n, h->nc, h->nt, h->nv, h->nd, h->nlam, h->separable, h->has32, h->device};
+    for (int k = 0; k < count && k < (int)(sizeof(all) / sizeof(all[0])); ++k) values[k] = all[k];
+    return HE_OK;
+}
+
+namespace {
+int apply_common(he_handle h, const void *psi, void *out, const double *field, int velocity, int precision,
+                 double beta_re, double beta_im, double gamma_re, double gamma_im, void *stream)
+{
+    g_status = HE_OK;
+    if (!h || !psi || !out || !field) return he_fail(HE_ERR_ARG, "null argument", __FILE__, __LINE__);
+    if (velocity != 0 && velocity != 1) return he_fail(HE_ERR_ARG, "velocity must be 0 or 1", __FILE__, __LINE__);
+    if (psi == out) return he_fail(HE_ERR_ARG, "H·psi cannot run in place", __FILE__, __LINE__);
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int s;
+    if (precision == HE_C128) {
+        s = he::launch_hpsi<double>(h->t64, static_cast<const double2 *>(psi), static_cast<double2 *>(out), field,
+                                    velocity, mk<double>(beta_re, beta_im), mk<double>(gamma_re, gamma_im), st);
+    } else if (precision == HE_C64) {
+        if (!h->has32) return he_fail(HE_ERR_UNSUPPORTED, "handle built without complex64 tables", __FILE__, __LINE__);
+        s = he::launch_hpsi<float>(h->t32, static_cast<const float2 *>(psi), static_cast<float2 *>(out), field,
+                                   velocity, mk<float>((float)beta_re, (float)beta_im),
+                                   mk<float>((float)gamma_re, (float)gamma_im), st);
+    } else {
+        return he_fail(HE_ERR_ARG, "precision must be HE_C128 or HE_C64", __FILE__, __LINE__);
+    }
+    g_status = s;
+    return s;
+}
+}  // namespace
+
+extern "C" int he_apply(he_handle h, const void *psi, void *out, const double *field, int velocity, int precision,
+                        void *stream)
+{
+    return apply_common(h, psi, out, field, velocity, precision, 0.0, 0.0, 1.0, 0.0, stream);
+}
+
+extern "C" int he_apply_shifted(he_handle h, const void *psi, void *out, const double *field, int velocity,
+                                double alpha_re, double alpha_im, double e_ref, int precision, void *stream)
+{
+    // psi + i alpha (H psi - e_ref psi) = (1 - i alpha e_ref) psi + (i alpha) H psi
+    const double ga_re = -alpha_im, ga_im = alpha_re;     // i*alpha
+    return apply_common(h, psi, out, field, velocity, precision, 1.0 - ga_re * e_ref, -ga_im * e_ref, ga_re, ga_im,
+                        stream);
+}
+
+extern "C" int he_diagonal(he_handle h, void *out, void *stream)
+{
+    g_status = HE_OK;
+    if (!h || !out) return he_fail(HE_ERR_ARG, "null argument", __FILE__, __LINE__);
+    return g_status = he::launch_diagonal(h->t64, h->tdiag, static_cast<double2 *>(out), static_cast<cudaStream_t>(stream));
+}
+
+// ---------------------------------------------------------------------------------
+// Drop-in host-pointer tensor_apply (src/kernels.f90:119-127 signature).
+// ---------------------------------------------------------------------------------
+extern "C" void tensor_apply(int n, int nc, int nt, const int *ptr, const int *col, const double *tv,
+                             const double *diag, int nv, const int *vptr, const int *vc, const int *vl,
+                             const double *vcoef, const double *rad, int nd, const int *dptr, const int *dc,
+                             const int *de, const double *dcoef, const double *ldiff, const double *r,
+                             const double *field, int velocity, const double *psi, double *out)
+{
+    g_status = HE_OK;
+    if (!psi || !out || !field || n < 1 || nc < 1) { he_fail(HE_ERR_ARG, "bad tensor_apply argument", __FILE__, __LINE__); return; }
+    int nlam = 1;
+    for (int k = 0; k < nv; ++k) nlam = std::max(nlam, vl[k] + 1);
+    he_handle h = nullptr;
+    if (he_create(&h, n, nc, nt, ptr, col, tv, diag, nullptr, nullptr, nv, vptr, vc, vl, vcoef, rad, nlam, nd, dptr,
+                  dc, de, dcoef, ldiff, r, 0) != HE_OK)
+        return;
+    const size_t bytes = (size_t)n * n * nc * 2 * sizeof(double);
+    void *dpsi = nullptr, *dout = nullptr;
+    cudaError_t e = cudaMalloc(&dpsi, bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&dout, bytes);
+    if (e == cudaSuccess) e = cudaMemcpy(dpsi, psi, bytes, cudaMemcpyHostToDevice);
+    int s = HE_ERR_CUDA;
+    if (e == cudaSuccess) s = he_apply(h, dpsi, dout, field, velocity, HE_C128, nullptr);
+    if (s == HE_OK) {
+        e = cudaMemcpy(out, dout, bytes, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) s = HE_ERR_CUDA;
+    }
+    if (e != cudaSuccess) he_set_error(cudaGetErrorString(e), __FILE__, __LINE__);
+    cudaFree(dpsi);
+    cudaFree(dout);
+    he_destroy(h);
+    g_status = s;
+}

@@ -1,0 +1,160 @@
+"""Device engine with the reference's ``TorchHamiltonian`` duck-type.
+
+``B200Hamiltonian(h, device, coulomb_backend=...)`` can stand where the reference
+constructs ``TorchHamiltonian(h, device, coulomb_backend=...)``
+(python/run3d.py:189, python/torch_backend.py:11-138): the same attributes
+(``n, nc, size, device, dtype, h, diagonal, coulomb_backend,
+coulomb_block_bytes, a2_coefficient``) and methods (``state, host, synchronize,
+apply, flux``), complex128 1-D contiguous states in the reference's Fortran order.
+All arithmetic on states runs in this package's sm_100a kernels through the C-ABI
+(include/helium_b200.h); torch only owns the device memory and the stream.
+"""
+import ctypes as ct
+
+import numpy as np
+import torch
+
+from ._lib import HE_C64, HE_C128, LIB, HeliumError, check, ptr
+
+PRECISIONS = {'complex128': (HE_C128, torch.complex128), 'complex64': (HE_C64, torch.complex64)}
+
+
+def _host_tables(h):
+    def arr(name, dtype):
+        return np.ascontiguousarray(np.asarray(getattr(h, name)).ravel(order='F'), dtype=dtype)
+    t = {name: arr(name, np.int32) for name in ('ptr', 'col', 'vptr', 'vc', 'vl', 'dptr', 'dc', 'de')}
+    for name in ('tv', 'vcoef', 'r'):
+        t[name] = arr(name, np.complex128)
+    t['ldiff'] = arr('ldiff', np.float64)
+    t['dcoef'] = np.ascontiguousarray(np.asarray(h.dcoef).reshape(3, -1).T, dtype=np.complex128)  # (nd, 3) rows
+    t['rad'] = arr('rad', np.complex128)
+    parts = getattr(h, 'diag_parts', None)
+    if parts is not None:
+        t['d1'] = np.ascontiguousarray(np.asarray(parts[0]).ravel(order='F'), dtype=np.complex128)
+        t['d2'] = np.ascontiguousarray(np.asarray(parts[1]).ravel(order='F'), dtype=np.complex128)
+        t['diag'] = None
+    else:
+        t['diag'] = arr('diag', np.complex128)
+        t['d1'] = t['d2'] = None
+    t['nlam'] = int(np.asarray(h.rad).shape[2]) if np.ndim(h.rad) == 3 else int(max(t['vl'], default=0) + 1)
+    return t
+
+
+class OperatorHandle:
+    """Owns one ``he_handle`` (device tables) for a Hamiltonian table object ``h``."""
+
+    def __init__(self, h, device, complex64=True):
+        self.device = torch.device(device)
+        if self.device.type != 'cuda':
+            raise ValueError('the B200 engine runs on CUDA devices only')
+        t = _host_tables(h)
+        self._keep = t
+        n, nc = int(h.n), int(h.nc)
+        handle = ct.c_void_p()
+        opt = lambda a: ptr(a) if a is not None else None
+        with torch.cuda.device(self.device):
+            status = LIB.he_create(ct.byref(handle), n, nc, len(t['tv']), ptr(t['ptr']), ptr(t['col']), ptr(t['tv']),
+                                   opt(t['diag']), opt(t['d1']), opt(t['d2']), len(t['vc']), ptr(t['vptr']),
+                                   ptr(t['vc']), ptr(t['vl']), ptr(t['vcoef']), ptr(t['rad']), t['nlam'],
+                                   len(t['dc']), ptr(t['dptr']), ptr(t['dc']), ptr(t['de']), ptr(t['dcoef']),
+                                   ptr(t['ldiff']), ptr(t['r']), 1 if complex64 else 0)
+        check(status, 'he_create')
+        self.handle = handle
+        self.n, self.nc = n, nc
+
+    def __del__(self):
+        handle = getattr(self, 'handle', None)
+        if handle is not None and handle.value:
+            LIB.he_destroy(handle)
+            self.handle = None
+
+
+def _stream(device):
+    return ct.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+class B200Hamiltonian:
+    """complex128 (or complex64) H·psi on one GPU with the TorchHamiltonian interface."""
+
+    def __init__(self, h, device='cuda:0', angular_sparse=True, coulomb_backend='sparse', precision='complex128'):
+        if coulomb_backend not in ('sparse', 'blocks'):
+            raise ValueError('unknown Coulomb contraction')
+        if precision not in PRECISIONS:
+            raise ValueError('precision must be complex128 or complex64')
+        self.h = h
+        self.device = torch.device(device)
+        self.n, self.nc, self.size = int(h.n), int(h.nc), int(h.size)
+        self.dtype = torch.complex128
+        self.precision = precision
+        self.angular_sparse = angular_sparse
+        # Multipoles are contracted on the fly in every mode: nothing is precomputed.
+        self.coulomb_backend = coulomb_backend
+        self.coulomb_block_bytes = 0
+        self.a2_coefficient = 1.0
+        self.op = OperatorHandle(h, self.device)
+        self.diagonal = torch.empty(self.size, dtype=torch.complex128, device=self.device)
+        check(LIB.he_diagonal(self.op.handle, ct.c_void_p(self.diagonal.data_ptr()), _stream(self.device)), 'he_diagonal')
+        self.apply_count = 0
+        if hasattr(h, 'surface_indices'):
+            self._prepare_flux()
+
+    # --- state transfer -------------------------------------------------------------
+    def state(self, x):
+        return torch.as_tensor(np.array(np.asarray(x).ravel(), dtype=np.complex128, copy=True), device=self.device)
+
+    def host(self, x):
+        return x.detach().cpu().numpy()
+
+    def synchronize(self):
+        torch.cuda.synchronize(self.device)
+
+    def _check(self, x, dtype):
+        if x.device != self.device or x.dtype != dtype or not x.is_contiguous() or x.numel() != self.size:
+            raise ValueError(f'state must be a contiguous {dtype} tensor of {self.size} elements on {self.device}')
+
+    # --- operator -------------------------------------------------------------------
+    @torch.no_grad()
+    def apply(self, x, field=(0., 0., 0.), velocity=True, out=None, precision=None):
+        """out = H(field) x; complex128 unless ``precision='complex64'`` (then x, out are complex64)."""
+        code, dtype = PRECISIONS[precision or ('complex128' if x.dtype == torch.complex128 else 'complex64')]
+        self._check(x, dtype)
+        if out is None:
+            out = torch.empty_like(x)
+        f = np.ascontiguousarray(field, dtype=np.float64)
+        if f.shape != (3,):
+            raise ValueError('field must have three Cartesian components')
+        check(LIB.he_apply(self.op.handle, ct.c_void_p(x.data_ptr()), ct.c_void_p(out.data_ptr()), ptr(f),
+                           int(bool(velocity)), code, _stream(self.device)), 'he_apply')
+        self.apply_count += 1
+        return out
+
+    @torch.no_grad()
+    def apply_shifted(self, x, field, alpha, reference_energy=0., velocity=True, out=None):
+        """out = x + i*alpha*(H(field) x - E_ref x): the Pade operator of python/implicit.py:77-84."""
+        code, dtype = PRECISIONS['complex128' if x.dtype == torch.complex128 else 'complex64']
+        self._check(x, dtype)
+        if out is None:
+            out = torch.empty_like(x)
+        f = np.ascontiguousarray(field, dtype=np.float64)
+        alpha = complex(alpha)
+        check(LIB.he_apply_shifted(self.op.handle, ct.c_void_p(x.data_ptr()), ct.c_void_p(out.data_ptr()), ptr(f),
+                                   int(bool(velocity)), alpha.real, alpha.imag, float(reference_energy), code,
+                                   _stream(self.device)), 'he_apply_shifted')
+        self.apply_count += 1
+        return out
+
+    # --- surface flux ---------------------------------------------------------------
+    def _prepare_flux(self):
+        from .surface import SurfaceFlux
+        self.surface = SurfaceFlux(self)
+
+    @torch.no_grad()
+    def flux(self, x, field):
+        if not hasattr(self, 'surface'):
+            if not hasattr(self.h, 'surface_indices'):
+                raise HeliumError(1, 'prepare_surface() was not called on the Hamiltonian tables')
+            self._prepare_flux()
+        return self.host(self.surface.frame(x, field))
+
+
+TorchHamiltonian = B200Hamiltonian

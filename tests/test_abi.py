@@ -1,0 +1,97 @@
+"""The C-ABI library loads, exports every symbol include/*.h declares, and validates
+its inputs on the host (no GPU needed for any of these checks)."""
+import ctypes as ct
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import REPO, Tables, golden
+
+HEADERS = sorted((REPO / 'include').glob('*.h'))
+
+
+def declared_functions():
+    names = set()
+    for header in HEADERS:
+        text = re.sub(r'/\*.*?\*/', '', header.read_text(), flags=re.S)
+        for match in re.finditer(r'^[A-Za-z_][\w\s\*]*?\b([a-z_][a-z0-9_]*)\s*\(', text, flags=re.M):
+            if not match.group(0).lstrip().startswith(('typedef', 'enum', '#')):
+                names.add(match.group(1))
+    return sorted(names)
+
+
+def test_header_declares_the_drop_in_symbol():
+    names = declared_functions()
+    assert 'tensor_apply' in names and 'he_apply' in names and len(names) >= 10
+
+
+def test_library_exports_every_declared_symbol():
+    from laqphysics_b200 import _lib
+    for name in declared_functions():
+        assert hasattr(_lib.LIB, name), name
+        assert name in _lib.SIGNATURES, f'{name} has no ctypes signature'
+
+
+def test_library_was_built_for_sm100a():
+    import subprocess
+    from laqphysics_b200 import _lib
+    out = subprocess.run(['cuobjdump', '--list-elf', str(_lib.LIBRARY)], capture_output=True, text=True)
+    if out.returncode != 0:
+        pytest.skip('cuobjdump unavailable')
+    assert 'sm_100a' in out.stdout
+
+
+def _create(h, **overrides):
+    from laqphysics_b200 import _lib
+    from laqphysics_b200.engine import _host_tables
+    t = _host_tables(h)
+    t.update(overrides)
+    p = lambda a: _lib.ptr(a) if a is not None else None
+    handle = ct.c_void_p()
+    status = _lib.LIB.he_create(ct.byref(handle), t.get('n', h.n), h.nc, len(t['tv']), p(t['ptr']), p(t['col']),
+                                p(t['tv']), p(t['diag']), p(t['d1']), p(t['d2']), len(t['vc']), p(t['vptr']),
+                                p(t['vc']), p(t['vl']), p(t['vcoef']), p(t['rad']), t['nlam'], len(t['dc']),
+                                p(t['dptr']), p(t['dc']), p(t['de']), p(t['dcoef']), p(t['ldiff']), p(t['r']), 0)
+    return status, _lib.LIB.he_last_error().decode()
+
+
+def test_create_rejects_out_of_range_kinetic_column():
+    from laqphysics_b200 import _lib
+    h = Tables(golden('apply_ecs'))
+    col = h.col.copy()
+    col[3] = h.n + 5
+    status, message = _create(h, col=col)
+    assert status == _lib.HE_ERR_SHAPE and 'kinetic' in message
+
+
+def test_create_rejects_multipole_outside_rad_table():
+    from laqphysics_b200 import _lib
+    h = Tables(golden('apply_ecs'))
+    vl = h.vl.copy()
+    vl[0] = 99
+    status, message = _create(h, vl=vl)
+    assert status == _lib.HE_ERR_SHAPE and 'multipole' in message
+
+
+def test_create_rejects_bad_dipole_electron_and_missing_diagonal():
+    from laqphysics_b200 import _lib
+    h = Tables(golden('apply_ecs'))
+    de = h.de.copy()
+    de[0] = 3
+    assert _create(h, de=de)[0] == _lib.HE_ERR_SHAPE
+    assert _create(h, diag=None)[0] == _lib.HE_ERR_ARG
+
+
+def test_apply_rejects_null_handle_and_bad_precision():
+    from laqphysics_b200 import _lib
+    f = np.zeros(3)
+    assert _lib.LIB.he_apply(None, None, None, _lib.ptr(f), 0, 0, None) == _lib.HE_ERR_ARG
+
+
+def test_native_tensor_apply_validates_field_shape():
+    from laqphysics_b200.native import tensor_apply
+    h = Tables(golden('apply_ecs'))
+    with pytest.raises(ValueError, match='three Cartesian'):
+        tensor_apply(h, np.zeros(h.size, complex), field=(0., 1.))

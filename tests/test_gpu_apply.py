@@ -1,0 +1,143 @@
+"""GPU parity of H·psi: the sm_100a kernels against the reference's own outputs
+(golden fixtures) and against the CPU oracle at sizes beyond the fixtures.
+
+Tolerances: complex128 uses the reference's own kernel-vs-Kronecker bound
+(tests/test_kernels.py:37: rtol 2e-13, atol 2e-12); complex64 is held to a relative
+L2 error of 2e-6 against the complex128 oracle.
+"""
+import json
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import Tables, golden
+from oracle import cpu
+
+pytestmark = pytest.mark.gpu
+DEVICE = 'cuda:0'
+C64_REL_L2 = 2e-6
+
+
+def engine(h, **kw):
+    from laqphysics_b200.engine import B200Hamiltonian
+    return B200Hamiltonian(h, DEVICE, **kw)
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.mark.parametrize('case', ['apply_ecs', 'apply_cut', 'apply_coupled'])
+@pytest.mark.parametrize('gauge', ['length', 'velocity'])
+def test_apply_matches_reference_goldens(case, gauge):
+    g = golden(case)
+    op = engine(Tables(g))
+    y = op.host(op.apply(op.state(g['x']), g['field'], gauge == 'velocity'))
+    np.testing.assert_allclose(y, g[f'kron_{gauge}'], rtol=2e-13, atol=2e-12)
+    np.testing.assert_allclose(y, g[f'torch_{gauge}'], rtol=2e-13, atol=2e-12)
+
+
+def _coupled(edges, order, angle, tail, lmax, L, cut=(2., 3.)):
+    from laqphysics_b200.coupled_angular import CoupledHelium
+    from laqphysics_b200.fedvr import make_grid
+    from laqphysics_b200.helium3d import Helium
+    return CoupledHelium(Helium(make_grid(edges, order, ecs_angle=angle, tail=tail), lmax, M=0, cutoff_radii=cut), L)
+
+
+def test_separable_diagonal_path_matches_reference_goldens():
+    g = golden('apply_coupled')
+    h = _coupled(**dict(zip(('edges', 'order', 'angle', 'tail'), json.loads(str(g['grid'])).values())), lmax=2, L=2,
+                 cut=(1., 2.))
+    assert hasattr(h, 'diag_parts')
+    op = engine(h)
+    for gauge in ('length', 'velocity'):
+        y = op.host(op.apply(op.state(g['x']), g['field'], gauge == 'velocity'))
+        np.testing.assert_allclose(y, g[f'kron_{gauge}'], rtol=2e-13, atol=2e-12)
+
+
+@pytest.mark.parametrize('velocity', [False, True])
+def test_apply_matches_oracle_on_larger_coupled_grid(velocity):
+    h = _coupled(np.linspace(0, 30, 16), 8, .3, 12, 3, 2)
+    rng = np.random.default_rng(7)
+    x = rng.normal(size=h.size) + 1j * rng.normal(size=h.size)
+    f = (0., 0., .07)
+    op = engine(h)
+    y = op.host(op.apply(op.state(x), f, velocity))
+    ref = cpu.tensor_apply(h, x, f, velocity)
+    assert rel_l2(y, ref) < 1e-13
+    np.testing.assert_allclose(y, ref, rtol=1e-12, atol=1e-10)
+
+
+def test_complex64_apply_within_stated_tolerance():
+    h = _coupled(np.linspace(0, 30, 16), 8, .3, 12, 3, 2)
+    rng = np.random.default_rng(8)
+    x = rng.normal(size=h.size) + 1j * rng.normal(size=h.size)
+    x /= np.linalg.norm(x)
+    op = engine(h)
+    ref = cpu.tensor_apply(h, x, (0, 0, .05), False)
+    y = op.apply(op.state(x).to(torch.complex64), (0, 0, .05), False, precision='complex64')
+    assert y.dtype == torch.complex64
+    assert rel_l2(op.host(y).astype(complex), ref) < C64_REL_L2
+
+
+def test_shifted_pade_operator():
+    g = golden('apply_cut')
+    h = Tables(g)
+    op = engine(h)
+    alpha = .05 / (3 + 1j * np.sqrt(3))
+    x = g['x']
+    y = op.host(op.apply_shifted(op.state(x), g['field'], alpha, -2.9, velocity=True))
+    ref = x + 1j * alpha * (cpu.tensor_apply(h, x, g['field'], True) + 2.9 * x)
+    np.testing.assert_allclose(y, ref, rtol=1e-13, atol=1e-13)
+
+
+def test_jacobi_diagonal_matches_reference_formula():
+    g = golden('apply_cut')
+    h = Tables(g)
+    op = engine(h)
+    n, nc = h.n, h.nc
+    td = np.array([h.tv[k] for i in range(n) for k in range(h.ptr[i], h.ptr[i + 1]) if h.col[k] == i])
+    d = h.diag.copy()
+    d += td[:, None, None] + td[None, :, None]
+    for a in range(nc):
+        for k in range(h.vptr[a], h.vptr[a + 1]):
+            if h.vc[k] == a:
+                d[:, :, a] += h.vcoef[k] * h.rad[:, :, h.vl[k]]
+    np.testing.assert_allclose(op.host(op.diagonal), d.ravel(order='F'), rtol=1e-14, atol=1e-13)
+
+
+def test_flux_matches_reference():
+    g = golden('apply_cut')
+    h = Tables(g)
+    h.surface_indices, h.surface_T, h.surface_P = g['surface_indices'], g['surface_T'], g['surface_P']
+    op = engine(h)
+    frame = op.flux(op.state(g['x']), g['field'])
+    np.testing.assert_allclose(frame, g['flux'], rtol=2e-12, atol=2e-12)
+    np.testing.assert_allclose(frame, g['flux_torch'], rtol=2e-12, atol=2e-12)
+
+
+def test_coupled_flux_matches_reference():
+    g = golden('apply_coupled')
+    args = json.loads(str(g['grid']))
+    h = _coupled(args['edges'], args['order'], args['ecs_angle'], args['tail'], 2, 2, cut=(1., 2.))
+    h.prepare_surface(5)
+    op = engine(h)
+    np.testing.assert_allclose(op.flux(op.state(g['x']), g['field']), g['flux'], rtol=2e-12, atol=2e-12)
+
+
+def test_host_pointer_tensor_apply_drop_in():
+    from laqphysics_b200.native import tensor_apply
+    g = golden('apply_ecs')
+    h = Tables(g)
+    for gauge in ('length', 'velocity'):
+        y = tensor_apply(h, g['x'], g['field'], gauge == 'velocity')
+        np.testing.assert_allclose(y, g[f'kron_{gauge}'], rtol=2e-13, atol=2e-12)
+
+
+def test_apply_rejects_wrong_dtype_and_size():
+    op = engine(Tables(golden('apply_ecs')))
+    with pytest.raises(ValueError):
+        op.apply(torch.zeros(op.size, dtype=torch.complex64, device=DEVICE), precision='complex128')
+    with pytest.raises(ValueError):
+        op.apply(torch.zeros(op.size + 1, dtype=torch.complex128, device=DEVICE))
