@@ -139,11 +139,15 @@ def cpu_oracle_rate(h, psi, field, budget_s):
     cpu.tensor_apply(h, psi, field, False, channels=(0, 1), tables=tables)
     per_channel = max(time.perf_counter() - start, 1e-6)
     count = int(min(h.nc, max(1, budget_s / per_channel)))
+    reps = max(1, int(budget_s / (per_channel * count)))
     start = time.perf_counter()
-    cpu.tensor_apply(h, psi, field, False, channels=(0, count), tables=tables)
+    for _ in range(reps):
+        cpu.tensor_apply(h, psi, field, False, channels=(0, count), tables=tables)
     elapsed = time.perf_counter() - start
-    gbs = 2 * h.size * 16 * (count / h.nc) / elapsed / 1e9
-    return gbs, cpu.threads(), f'output channels 0..{count - 1} of {h.nc} (one H.psi over {count / h.nc:.3f} of the state), {elapsed:.1f} s'
+    gbs = reps * 2 * h.size * 16 * (count / h.nc) / elapsed / 1e9
+    sample = (f'{reps} x H.psi over output channels 0..{count - 1} of {h.nc} '
+              f'({count / h.nc:.3f} of the state each), complex128, {elapsed:.1f} s')
+    return gbs, cpu.threads(), sample
 
 
 def run_reference(args, rank):
@@ -255,7 +259,7 @@ def main():
     launches0 = engine.apply_count
     with ClockSampler(gpu_identifier(torch, device)) as clocks:
         ms128 = timed(step128, args.steps)
-        launches = engine.apply_count - launches0
+        launches = (engine.apply_count - launches0) * engine.launches_per_apply
         ms64 = timed(step64, args.steps)
         e2e_steps = max(3, min(args.steps, 20))
         ms_e2e = timed(step_e2e, e2e_steps)
@@ -277,7 +281,9 @@ def main():
         'gpu_launches': launches,
         'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': hbm, 'unit': 'GB/s', 'frac': achieved / hbm,
                      'traffic': profile_traffic('hpsi_c128_microbench'), 'peak_kind': peak_kind,
-                     'kernel': 'hpsi_gather_kernel<double>',
+                     'kernel': ('contract_field + hpsi_radial_kernel + hpsi_mix_kernel (one apply)'
+                                if engine.tiled else 'hpsi_gather_kernel'),
+                     'plan': engine.plan_info,
                      'fp64_tflops': flops / (per128 * 1e-3) / 1e12, 'flops_per_apply': flops},
         'complex64': {'value': value64, 'unit': 'GB/s', 'ms_per_step': per64,
                       'frac': value64 / world / hbm, 'speedup_vs_complex128': per128 / per64},

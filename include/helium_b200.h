@@ -99,6 +99,41 @@ int he_diagonal(he_handle h, void *out, void *stream);
 int he_flux(he_handle h, const void *psi, void *frame, int ns, int lo, int width, const void *J,
             const void *JP, const double *field, void *stream);
 
+/* ------------------------------------------------------------------------------------
+ * Krylov workspace and Arnoldi exponential.
+ * Replaces exponential_action of python/propagate.py:6-39 and
+ * python/torch_backend.py:140-158 (CGS2, H[j+1,j] = ||v||, happy breakdown below 1e-13,
+ * checks at j >= 3 with (j+1) % 4 == 0 or j+1 == maxdim, c = expm(-i dt H_m)[:,0] beta,
+ * err = |dt h_{m+1,m} c_m|).  The small exponential is evaluated on the device
+ * (scaling and squaring, [13/13] Pade), so the host waits only at check points.
+ * A workspace holds maxdim+1 basis vectors of n complex128 elements (plus maxdim
+ * preconditioned directions when `flexible`), the Hessenberg matrix and scratch.
+ * ---------------------------------------------------------------------------------- */
+typedef struct he_krylov *he_krylov_handle;
+
+int he_krylov_create(he_krylov_handle *out, long long n, int maxdim, int flexible);
+int he_krylov_destroy(he_krylov_handle k);
+/* Device address of basis vector j (which = 0: Q_j, which = 1: Z_j of flexible GMRES). */
+int he_krylov_vector(he_krylov_handle k, int which, int j, void **ptr);
+
+/* Arnoldi for an operator applied by the caller:
+ *   he_krylov_start(x) -> beta (Q_0 = x / beta);
+ *   for j: caller writes H Q_j into vector j+1, he_krylov_orthogonalize(j),
+ *          he_expv_check(j, maxdim, dt, tol, sync) (normalises vector j+1 when not done);
+ *   he_krylov_combine(m, y): y = Q[:, :m] c.
+ * he_expv_check returns HE_ERR_NOCONV ("Arnoldi did not converge") when maxdim is
+ * reached without meeting tol; with sync = 0 it does not block. */
+int he_krylov_start(he_krylov_handle k, const void *x, double *beta, void *stream);
+int he_krylov_orthogonalize(he_krylov_handle k, int j, void *stream);
+int he_expv_check(he_krylov_handle k, int j, int maxdim, double dt, double tol, int sync, int *done, int *m,
+                  double *estimate, void *stream);
+int he_krylov_combine(he_krylov_handle k, int m, void *y, void *stream);
+
+/* Fused y = exp(-i dt H(field)) x with the device operator `op` (no host work between
+ * Krylov vectors).  x, y: n*n*nc complex128 device vectors, y != x. */
+int he_expv(he_krylov_handle k, he_handle op, const void *x, void *y, const double *field, int velocity,
+            double dt, double tol, int maxdim, int *dimension, double *estimate, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -33,6 +33,18 @@ SIGNATURES = {
     'he_apply_shifted': (I, [P, P, P, P, I, D, D, D, I, P]),
     'he_diagonal': (I, [P, P, P]),
     'he_flux': (I, [P, P, P, I, I, I, P, P, P, P]),
+    'he_krylov_create': (I, [ct.POINTER(P), ct.c_longlong, I, I]),
+    'he_krylov_destroy': (I, [P]),
+    'he_krylov_vector': (I, [P, I, I, ct.POINTER(P)]),
+    'he_krylov_start': (I, [P, P, ct.POINTER(D), P]),
+    'he_krylov_orthogonalize': (I, [P, I, P]),
+    'he_expv_check': (I, [P, I, I, D, D, I, ct.POINTER(I), ct.POINTER(I), ct.POINTER(D), P]),
+    'he_krylov_combine': (I, [P, I, P, P]),
+    'he_expv': (I, [P, P, P, P, P, I, D, D, I, ct.POINTER(I), ct.POINTER(D), P]),
+    'he_set_path': (I, [P, I]),
+    'he_plan_build': (P, [I, I, P, P, P, I, P, P, P, P, I, I, P, P, P, P]),
+    'he_plan_free': (None, [P]),
+    'he_plan_array': (ct.c_longlong, [P, I, P]),
 }
 
 for _name, (_res, _args) in SIGNATURES.items():

@@ -109,11 +109,63 @@ int build_tables(he_operator *h, he::DeviceTables<R> *t, const int *ptr, const i
     return HE_OK;
 }
 
+// Upload the tiled plan in precision R.
+template <typename R> int upload_plan(he_operator *h, he::TiledPlan<R> *pl, cplx<R> **coef)
+{
+    const he_plan_host &P = h->plan;
+    pl->n = h->n; pl->nc = h->nc; pl->ne = P.ne; pl->ntile = P.ntile;
+    pl->ng = P.ng; pl->nlam = P.nlam; pl->nwd = (int)P.dwsrc.size();
+    int s;
+    if ((s = upload(h, P.estart.data(), P.estart.size(), &pl->estart))) return s;
+    if ((s = upload(h, P.tstart.data(), P.tstart.size(), &pl->tstart))) return s;
+    if ((s = upload(h, P.eoff.data(), P.eoff.size(), &pl->eoff))) return s;
+    if ((s = upload(h, P.ereal.data(), P.ereal.size(), &pl->ereal))) return s;
+    if ((s = upload_c<R>(h, P.blocks.data(), P.blocks.size() / 2, &pl->blocks))) return s;
+    if ((s = upload_c<R>(h, P.bblocks.data(), P.bblocks.size() / 2, &pl->bblocks))) return s;
+    if ((s = upload(h, P.gch.data(), P.gch.size(), &pl->gch))) return s;
+    if ((s = upload(h, P.wptr.data(), P.wptr.size(), &pl->wptr))) return s;
+    const int dummy_i = 0;
+    const double dummy_d = 0.0;
+    if ((s = upload(h, P.wsrc.empty() ? &dummy_i : P.wsrc.data(), std::max<size_t>(1, P.wsrc.size()), &pl->wsrc))) return s;
+    if ((s = upload_r<R>(h, P.wcoef.empty() ? &dummy_d : P.wcoef.data(), std::max<size_t>(1, P.wcoef.size()), &pl->wcoef))) return s;
+    if ((s = upload(h, P.dwptr.data(), P.dwptr.size(), &pl->dwptr))) return s;
+    if ((s = upload(h, P.dwsrc.empty() ? &dummy_i : P.dwsrc.data(), std::max<size_t>(1, P.dwsrc.size()), &pl->dwsrc))) return s;
+    if ((s = upload(h, P.dwel.empty() ? &dummy_i : P.dwel.data(), std::max<size_t>(1, P.dwel.size()), &pl->dwel))) return s;
+    if ((s = upload(h, P.dwedge.empty() ? &dummy_i : P.dwedge.data(), std::max<size_t>(1, P.dwedge.size()), &pl->dwedge))) return s;
+    void *c = nullptr;
+    HE_CUDA_TRY(cudaMalloc(&c, std::max(1, h->nd) * sizeof(cplx<R>)));
+    h->allocations.push_back(c);
+    *coef = static_cast<cplx<R> *>(c);
+    return HE_OK;
+}
+
+// Velocity-gauge scratch (two n*n*nc vectors), allocated on first use.
+template <typename R> int velocity_scratch(he_operator *h, cplx<R> **w)
+{
+    if (w[0]) return HE_OK;
+    const size_t bytes = (size_t)h->n * h->n * h->nc * sizeof(cplx<R>);
+    for (int k = 0; k < 2; ++k) {
+        void *p = nullptr;
+        HE_CUDA_TRY(cudaMalloc(&p, bytes));
+        h->allocations.push_back(p);
+        w[k] = static_cast<cplx<R> *>(p);
+    }
+    return HE_OK;
+}
+
 }  // namespace
 
 he_operator::~he_operator()
 {
     for (void *p : allocations) cudaFree(p);
+}
+
+extern "C" int he_set_path(he_handle h, int tiled)
+{
+    if (!h) return he_fail(HE_ERR_ARG, "null handle", __FILE__, __LINE__);
+    if (tiled && !h->tiled) return he_fail(HE_ERR_UNSUPPORTED, "tables do not admit the tiled kernels", __FILE__, __LINE__);
+    h->path = tiled ? 1 : 0;
+    return HE_OK;
 }
 
 extern "C" int he_create(he_handle *out, int n, int nc, int nt, const int *ptr, const int *col, const double *tv,
@@ -165,6 +217,12 @@ extern "C" int he_create(he_handle *out, int n, int nc, int nt, const int *ptr, 
         s = upload_c<double>(h, tdiag.data(), (size_t)n, &td);
         h->tdiag = td;
     }
+    if (!s && he_build_plan(h->plan, n, nc, ptr, col, tv, nv, vptr, vc, vl, vcoef, nlam, nd, dptr, dc, de, r) &&
+        he::tiled_fits(nc, nlam, sizeof(double2))) {
+        s = upload_plan<double>(h, &h->p64, &h->coef64);
+        if (!s && h->has32) s = upload_plan<float>(h, &h->p32, &h->coef32);
+        h->tiled = !s;
+    }
     if (s) { delete h; g_status = s; return s; }
     *out = h;
     return HE_OK;
@@ -179,7 +237,9 @@ extern "C" int he_destroy(he_handle h)
 extern "C" int he_info(he_handle h, long long *values, int count)
 {
     if (!h || !values) return he_fail(HE_ERR_ARG, "null argument", __FILE__, __LINE__);
-    const long long all[] = {h->n, h->nc, h->nt, h->nv, h->nd, h->nlam, h->separable, h->has32, h->device};
+    const long long all[] = {h->n, h->nc, h->nt, h->nv, h->nd, h->nlam, h->separable, h->has32, h->device,
+                             h->tiled, h->path, h->plan.ne, h->plan.ntile, h->plan.ng,
+                             (long long)h->plan.wsrc.size(), (long long)h->plan.dwsrc.size()};
     for (int k = 0; k < count && k < (int)(sizeof(all) / sizeof(all[0])); ++k) values[k] = all[k];
     return HE_OK;
 }
@@ -194,14 +254,30 @@ int apply_common(he_handle h, const void *psi, void *out, const double *field, i
     if (psi == out) return he_fail(HE_ERR_ARG, "H·psi cannot run in place", __FILE__, __LINE__);
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
     int s;
+    const bool tiled = h->tiled && h->path == 1;
     if (precision == HE_C128) {
-        s = he::launch_hpsi<double>(h->t64, static_cast<const double2 *>(psi), static_cast<double2 *>(out), field,
-                                    velocity, mk<double>(beta_re, beta_im), mk<double>(gamma_re, gamma_im), st);
+        const double2 beta = mk<double>(beta_re, beta_im), gamma = mk<double>(gamma_re, gamma_im);
+        if (tiled) {
+            if (velocity && (s = velocity_scratch<double>(h, h->w64))) return g_status = s;
+            s = he::launch_hpsi_tiled<double>(h, h->t64, h->p64, h->coef64, h->w64[0], h->w64[1],
+                                              static_cast<const double2 *>(psi), static_cast<double2 *>(out), field,
+                                              velocity, beta, gamma, st);
+        } else {
+            s = he::launch_hpsi<double>(h->t64, static_cast<const double2 *>(psi), static_cast<double2 *>(out), field,
+                                        velocity, beta, gamma, st);
+        }
     } else if (precision == HE_C64) {
         if (!h->has32) return he_fail(HE_ERR_UNSUPPORTED, "handle built without complex64 tables", __FILE__, __LINE__);
-        s = he::launch_hpsi<float>(h->t32, static_cast<const float2 *>(psi), static_cast<float2 *>(out), field,
-                                   velocity, mk<float>((float)beta_re, (float)beta_im),
-                                   mk<float>((float)gamma_re, (float)gamma_im), st);
+        const float2 beta = mk<float>((float)beta_re, (float)beta_im), gamma = mk<float>((float)gamma_re, (float)gamma_im);
+        if (tiled) {
+            if (velocity && (s = velocity_scratch<float>(h, h->w32))) return g_status = s;
+            s = he::launch_hpsi_tiled<float>(h, h->t32, h->p32, h->coef32, h->w32[0], h->w32[1],
+                                             static_cast<const float2 *>(psi), static_cast<float2 *>(out), field,
+                                             velocity, beta, gamma, st);
+        } else {
+            s = he::launch_hpsi<float>(h->t32, static_cast<const float2 *>(psi), static_cast<float2 *>(out), field,
+                                       velocity, beta, gamma, st);
+        }
     } else {
         return he_fail(HE_ERR_ARG, "precision must be HE_C128 or HE_C64", __FILE__, __LINE__);
     }

@@ -1,0 +1,45 @@
+// Tiled H·psi (hpsi_tiled.cu): the radial-stencil kernel and the channel-mixing kernel,
+// plus the host-built plan they consume.
+#pragma once
+#include <vector>
+
+#include "common.cuh"
+
+namespace he {
+
+constexpr int MIX_POINTS = 128;     // points per channel-mixing CTA
+constexpr int MIX_GROUP = 4;        // output channels per thread (register block)
+constexpr int RAD_ELEMS = 4;        // elements per radial tile and axis
+constexpr int RAD_TMAX = 48;        // max owned nodes per radial tile and axis
+constexpr int RAD_CHUNK = 8;        // output rows per register chunk
+
+// Device view of the plan.
+template <typename R> struct TiledPlan {
+    int n, nc, ne, ntile;           // grid size, channels, elements, radial tiles per axis
+    const int *estart;              // ne+1 element starts (estart[ne] = n)
+    const int *tstart;              // ntile+1 element indices where radial tiles start
+    const int *eoff;                // ne+1 offsets of element blocks in `blocks`
+    const cplx<R> *blocks;          // per element: dense m x m block T[s+a, s+b], a,b < m
+    const cplx<R> *bblocks;         // same layout, B = T (r_b - r_a) (velocity-gauge commutator)
+    const int *ereal;               // 1 if the element block is real
+    // channel mixing
+    int ng, nlam, nwd;
+    const int *gch;                 // ng x MIX_GROUP output channels (-1 = padding)
+    const int *wptr;                // ng*nlam+1 wide Coulomb edge offsets, (g, lam) major
+    const int *wsrc;                // source channel per wide edge
+    const R *wcoef;                 // MIX_GROUP coefficients per wide edge (real)
+    const int *dwptr;               // ng+1 wide dipole edge offsets
+    const int *dwsrc;               // source channel per wide dipole edge
+    const int *dwel;                // electron (1 or 2)
+    const int *dwedge;              // MIX_GROUP original dipole edge indices (-1 = none)
+};
+
+}  // namespace he
+
+// Host-owned plan (built by he_create when the tables admit it).
+struct he_plan_host {
+    bool ok = false;
+    std::vector<int> estart, tstart, eoff, ereal, gch, wptr, wsrc, dwptr, dwsrc, dwel, dwedge;
+    std::vector<double> blocks, bblocks, wcoef;   // complex as interleaved doubles for blocks
+    int ne = 0, ntile = 0, ng = 0, nlam = 0, maxm = 0;
+};

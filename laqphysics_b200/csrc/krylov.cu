@@ -1,0 +1,573 @@
+// Krylov building blocks on the device: classical Gram-Schmidt applied twice (CGS2)
+// with deterministic block reductions, the small Hessenberg exponential
+// expm(-i dt H_m) in complex128 on one CTA, and the Arnoldi exponential action of
+// the reference's python/propagate.py:6-39 / python/torch_backend.py:140-158.
+//
+// Reductions: every pass writes one partial per (block, basis vector) into the
+// workspace's `partial` array; a single-CTA kernel then sums the partials in block
+// order, so results are bitwise reproducible run to run.
+#include <cmath>
+#include <cstring>
+
+#include "common.cuh"
+#include "hamiltonian.cuh"
+#include "krylov.cuh"
+#include "operator.cuh"
+
+namespace he {
+
+__device__ __forceinline__ double2 warp_sum(double2 v)
+{
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        v.x += __shfl_down_sync(0xffffffffu, v.x, off);
+        v.y += __shfl_down_sync(0xffffffffu, v.y, off);
+    }
+    return v;
+}
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    return v;
+}
+
+// Block-wide sum of KT complex accumulators; thread 0 of the block gets the result.
+template <int KT>
+__device__ __forceinline__ void block_sum(double2 (&acc)[KT], double2 *out)
+{
+    __shared__ double2 red[KRYLOV_THREADS / 32][KT];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < KT; ++k) {
+        const double2 s = warp_sum(acc[k]);
+        if (lane == 0) red[warp][k] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < KT) {
+        double2 s = mk<double>(0, 0);
+        for (int w = 0; w < KRYLOV_THREADS / 32; ++w) s = cadd<double>(s, red[w][threadIdx.x]);
+        out[threadIdx.x] = s;
+    }
+}
+
+// partial[b*ld + k0 + k] = sum over this block's elements of conj(Q_{k0+k}) v
+template <int KT>
+__global__ void __launch_bounds__(KRYLOV_THREADS)
+multidot_kernel(const double2 *__restrict__ Q, size_t n, int k0, int kc, const double2 *__restrict__ v,
+                double2 *__restrict__ partial, int ld, const KrylovStatus *st)
+{
+    if (st && st->done) return;
+    double2 acc[KT];
+#pragma unroll
+    for (int k = 0; k < KT; ++k) acc[k] = mk<double>(0, 0);
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        const double2 x = v[p];
+#pragma unroll
+        for (int k = 0; k < KT; ++k)
+            if (k < kc) acc[k] = cfma_conj<double>(Q[(size_t)(k0 + k) * n + p], x, acc[k]);
+    }
+    __shared__ double2 res[KT];
+    block_sum<KT>(acc, res);
+    __syncthreads();
+    if (threadIdx.x < kc) partial[(size_t)blockIdx.x * ld + k0 + threadIdx.x] = res[threadIdx.x];
+}
+
+// z[k] = sum_b partial[b*ld + k] for k < kc (fixed block order); optionally H[k] += z[k].
+__global__ void reduce_partials_kernel(const double2 *__restrict__ partial, int nb, int ld, int kc,
+                                       double2 *__restrict__ z, double2 *__restrict__ hcol, const KrylovStatus *st)
+{
+    if (st && st->done) return;
+    for (int k = threadIdx.x; k < kc; k += blockDim.x) {
+        double2 s = mk<double>(0, 0);
+        for (int b = 0; b < nb; ++b) s = cadd<double>(s, partial[(size_t)b * ld + k]);
+        z[k] = s;
+        if (hcol) hcol[k] = cadd<double>(hcol[k], s);
+    }
+}
+
+// v -= sum_k Q_k z_k ; optionally per-block |v|^2 partial sums.
+__global__ void __launch_bounds__(KRYLOV_THREADS)
+update_kernel(const double2 *__restrict__ Q, size_t n, int kc, const double2 *__restrict__ z, double2 *__restrict__ v,
+              double *__restrict__ norm_partial, const KrylovStatus *st)
+{
+    if (st && st->done) return;
+    __shared__ double2 zs[KRYLOV_MAXDIM + 1];
+    for (int k = threadIdx.x; k < kc; k += blockDim.x) zs[k] = z[k];
+    __syncthreads();
+    double nrm = 0;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        double2 x = v[p];
+        for (int k = 0; k < kc; ++k) {
+            const double2 q = Q[(size_t)k * n + p];
+            x = cfma<double>(mk<double>(-zs[k].x, -zs[k].y), q, x);
+        }
+        v[p] = x;
+        nrm += cabs2<double>(x);
+    }
+    if (norm_partial) {
+        __shared__ double red[KRYLOV_THREADS / 32];
+        const double s = warp_sum(nrm);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0;
+            for (int w = 0; w < KRYLOV_THREADS / 32; ++w) t += red[w];
+            norm_partial[blockIdx.x] = t;
+        }
+    }
+}
+
+// per-block |v|^2
+__global__ void __launch_bounds__(KRYLOV_THREADS)
+norm_kernel(const double2 *__restrict__ v, size_t n, double *__restrict__ norm_partial)
+{
+    double nrm = 0;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x)
+        nrm += cabs2<double>(v[p]);
+    __shared__ double red[KRYLOV_THREADS / 32];
+    const double s = warp_sum(nrm);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int w = 0; w < KRYLOV_THREADS / 32; ++w) t += red[w];
+        norm_partial[blockIdx.x] = t;
+    }
+}
+
+// h = sqrt(sum of partials) -> H[j+1, j], status.hnext, happy flag (h < 1e-13).
+__global__ void finish_norm_kernel(const double *__restrict__ norm_partial, int nb, double2 *hsub, KrylovStatus *st,
+                                   double happy_below)
+{
+    if (threadIdx.x != 0 || st->done) return;
+    double s = 0;
+    for (int b = 0; b < nb; ++b) s += norm_partial[b];
+    const double h = sqrt(s);
+    *hsub = mk<double>(h, 0);
+    st->hnext = h;
+    st->happy = h < happy_below;
+}
+
+// y = s * x with s = 1 / status.hnext (skipped once the solve is done)
+__global__ void __launch_bounds__(KRYLOV_THREADS)
+normalize_kernel(const double2 *x, double2 *y, size_t n, const KrylovStatus *st)
+{
+    if (st->done) return;
+    const double s = 1.0 / st->hnext;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x)
+        y[p] = cscale<double>(s, x[p]);
+}
+
+// start: beta = ||x||, Q_0 = x / beta (reads beta from the reduced norm)
+__global__ void start_kernel(const double *__restrict__ norm_partial, int nb, KrylovStatus *st)
+{
+    if (threadIdx.x != 0) return;
+    double s = 0;
+    for (int b = 0; b < nb; ++b) s += norm_partial[b];
+    memset(st, 0, sizeof(KrylovStatus));
+    st->beta = sqrt(s);
+    st->hnext = st->beta;
+    if (st->beta == 0) { st->done = 1; st->converged = 1; st->m = 0; }
+}
+
+// y = sum_{k < m} Q_k c_k with m taken from the status word (or from `mfix` >= 0).
+__global__ void __launch_bounds__(KRYLOV_THREADS)
+combine_kernel(const double2 *__restrict__ Q, size_t n, const double2 *__restrict__ c, double2 *__restrict__ y,
+               const KrylovStatus *st, int mfix, int accumulate)
+{
+    const int m = mfix >= 0 ? mfix : st->m;
+    __shared__ double2 cs[KRYLOV_MAXDIM];
+    for (int k = threadIdx.x; k < m; k += blockDim.x) cs[k] = c[k];
+    __syncthreads();
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        double2 acc = accumulate ? y[p] : mk<double>(0, 0);
+        for (int k = 0; k < m; ++k) acc = cfma<double>(cs[k], Q[(size_t)k * n + p], acc);
+        y[p] = acc;
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Small dense complex matrices on one CTA (column-major, leading dimension m).
+// ---------------------------------------------------------------------------------
+__device__ void mat_mul(const double2 *A, const double2 *B, double2 *C, int m)
+{
+    for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
+        const int i = idx % m, j = idx / m;
+        double2 s = mk<double>(0, 0);
+        for (int k = 0; k < m; ++k) s = cfma<double>(A[i + k * m], B[k + j * m], s);
+        C[idx] = s;
+    }
+    __syncthreads();
+}
+
+// C = a*A + b*B + c*Cm + d*I   (real coefficients)
+__device__ void mat_lin(double2 *out, double a, const double2 *A, double b, const double2 *B, double c,
+                        const double2 *Cm, double d, int m)
+{
+    for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
+        double2 s = cscale<double>(a, A[idx]);
+        if (B) s = rfma<double>(b, B[idx], s);
+        if (Cm) s = rfma<double>(c, Cm[idx], s);
+        if (idx % m == idx / m) s.x += d;
+        out[idx] = s;
+    }
+    __syncthreads();
+}
+
+// Solve A X = B in place (B overwritten by X), Gaussian elimination with partial pivoting.
+__device__ void lu_solve(double2 *A, double2 *B, int m, int nrhs)
+{
+    __shared__ int piv;
+    for (int k = 0; k < m; ++k) {
+        if (threadIdx.x == 0) {
+            int best = k;
+            double bv = cabs2<double>(A[k + k * m]);
+            for (int i = k + 1; i < m; ++i) {
+                const double v = cabs2<double>(A[i + k * m]);
+                if (v > bv) { bv = v; best = i; }
+            }
+            piv = best;
+        }
+        __syncthreads();
+        const int p = piv;
+        if (p != k) {
+            for (int j = threadIdx.x; j < m; j += blockDim.x) {
+                const double2 t = A[k + j * m]; A[k + j * m] = A[p + j * m]; A[p + j * m] = t;
+            }
+            for (int j = threadIdx.x; j < nrhs; j += blockDim.x) {
+                const double2 t = B[k + j * m]; B[k + j * m] = B[p + j * m]; B[p + j * m] = t;
+            }
+        }
+        __syncthreads();
+        const double2 d = A[k + k * m];
+        const double dd = cabs2<double>(d);
+        const double2 inv = mk<double>(d.x / dd, -d.y / dd);
+        // eliminate rows below k
+        for (int idx = threadIdx.x; idx < (m - k - 1) * (m - k + nrhs); idx += blockDim.x) {
+            const int i = k + 1 + idx % (m - k - 1);
+            const int jj = idx / (m - k - 1);
+            const double2 f = cmul<double>(A[i + k * m], inv);
+            if (jj < m - k - 1) {
+                const int j = k + 1 + jj;
+                A[i + j * m] = csub<double>(A[i + j * m], cmul<double>(f, A[k + j * m]));
+            } else {
+                const int j = jj - (m - k - 1);
+                B[i + j * m] = csub<double>(B[i + j * m], cmul<double>(f, B[k + j * m]));
+            }
+        }
+        __syncthreads();
+        for (int i = k + 1 + threadIdx.x; i < m; i += blockDim.x) A[i + k * m] = mk<double>(0, 0);
+        __syncthreads();
+    }
+    // back substitution, one right-hand side per thread group
+    for (int j = threadIdx.x; j < nrhs; j += blockDim.x) {
+        for (int i = m - 1; i >= 0; --i) {
+            double2 s = B[i + j * m];
+            for (int k = i + 1; k < m; ++k) s = csub<double>(s, cmul<double>(A[i + k * m], B[k + j * m]));
+            const double2 d = A[i + i * m];
+            const double dd = cabs2<double>(d);
+            B[i + j * m] = mk<double>((s.x * d.x + s.y * d.y) / dd, (s.y * d.x - s.x * d.y) / dd);
+        }
+    }
+    __syncthreads();
+}
+
+// expm(A) for a small complex matrix: scaling and squaring with the [13/13] Pade
+// approximant (N. J. Higham, SIAM J. Matrix Anal. Appl. 26 (2005) 1179-1193).
+// A is overwritten; the result is left in R.  work holds 6 m x m matrices.
+__device__ void expm_pade13(double2 *A, double2 *R, double2 *work, int m)
+{
+    const double b[14] = {64764752532480000., 32382376266240000., 7771770303897600., 1187353796428800.,
+                          129060195264000., 10559470521600., 670442572800., 33522128640., 1323241920.,
+                          40840800., 960960., 16380., 182., 1.};
+    const double theta13 = 5.371920351148152;
+    __shared__ int s_shared;
+    if (threadIdx.x == 0) {
+        double norm1 = 0;     // max column sum
+        for (int j = 0; j < m; ++j) {
+            double c = 0;
+            for (int i = 0; i < m; ++i) c += sqrt(cabs2<double>(A[i + j * m]));
+            norm1 = fmax(norm1, c);
+        }
+        int s = 0;
+        if (norm1 > theta13) s = (int)ceil(log2(norm1 / theta13));
+        s_shared = s;
+    }
+    __syncthreads();
+    const int s = s_shared;
+    const double scale = ldexp(1.0, -s);
+    for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) A[idx] = cscale<double>(scale, A[idx]);
+    __syncthreads();
+    double2 *A2 = work, *A4 = work + m * m, *A6 = work + 2 * m * m, *T = work + 3 * m * m, *U = work + 4 * m * m,
+            *V = work + 5 * m * m;
+    mat_mul(A, A, A2, m);
+    mat_mul(A2, A2, A4, m);
+    mat_mul(A4, A2, A6, m);
+    // U = A [A6 (b13 A6 + b11 A4 + b9 A2) + b7 A6 + b5 A4 + b3 A2 + b1 I]
+    mat_lin(T, b[13], A6, b[11], A4, b[9], A2, 0.0, m);
+    mat_mul(A6, T, U, m);
+    mat_lin(T, 1.0, U, b[7], A6, b[5], A4, b[1], m);
+    mat_lin(T, 1.0, T, b[3], A2, 0.0, nullptr, 0.0, m);
+    mat_mul(A, T, U, m);
+    // V = A6 (b12 A6 + b10 A4 + b8 A2) + b6 A6 + b4 A4 + b2 A2 + b0 I
+    mat_lin(T, b[12], A6, b[10], A4, b[8], A2, 0.0, m);
+    mat_mul(A6, T, V, m);
+    mat_lin(V, 1.0, V, b[6], A6, b[4], A4, b[0], m);
+    mat_lin(V, 1.0, V, b[2], A2, 0.0, nullptr, 0.0, m);
+    // (V - U) R = (V + U)
+    mat_lin(T, 1.0, V, -1.0, U, 0.0, nullptr, 0.0, m);
+    mat_lin(R, 1.0, V, 1.0, U, 0.0, nullptr, 0.0, m);
+    lu_solve(T, R, m, m);
+    for (int k = 0; k < s; ++k) {
+        mat_mul(R, R, T, m);
+        mat_lin(R, 1.0, T, 0.0, nullptr, 0.0, nullptr, 0.0, m);
+    }
+}
+
+// Arnoldi check at iteration j (python/propagate.py:28-38): on happy breakdown or at
+// j >= 3 with (j+1) % 4 == 0 or j+1 == maxdim, form c = expm(-i dt H_m)[:, 0] beta
+// and err = |dt h_{m+1,m} c_{m-1}|; accept if happy or err < tol.
+__global__ void __launch_bounds__(512)
+arnoldi_check_kernel(const double2 *__restrict__ H, int ld, int j, int maxdim, double dt, double tol,
+                     double2 *__restrict__ coef, double2 *__restrict__ work, KrylovStatus *st)
+{
+    if (st->done) return;
+    const int m = j + 1;
+    const bool happy = st->happy;
+    const bool check = happy || (j >= 3 && ((j + 1) % 4 == 0 || j + 1 == maxdim));
+    if (!check) return;
+    double2 *A = work, *R = work + m * m, *scratch = work + 2 * m * m;
+    for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
+        const int r = idx % m, c = idx / m;
+        const double2 h = H[r + c * ld];
+        A[idx] = mk<double>(dt * h.y, -dt * h.x);   // -i dt H
+    }
+    __syncthreads();
+    expm_pade13(A, R, scratch, m);
+    if (threadIdx.x == 0) {
+        const double beta = st->beta;
+        for (int k = 0; k < m; ++k) coef[k] = cscale<double>(beta, R[k]);
+        const double err = fabs(dt) * st->hnext * sqrt(cabs2<double>(coef[m - 1]));
+        st->estimate = err;
+        if (happy || err < tol) {
+            st->done = 1; st->converged = 1; st->m = m;
+        } else if (j + 1 == maxdim) {
+            st->done = 1; st->failed = 1; st->m = m;
+        }
+    }
+}
+
+}  // namespace he
+
+// =====================================================================================
+// Host side
+// =====================================================================================
+using namespace he;
+
+he_krylov::~he_krylov()
+{
+    cudaFree(Q); cudaFree(Z); cudaFree(H); cudaFree(partial); cudaFree(z); cudaFree(coef); cudaFree(work);
+    cudaFree(norm_partial); cudaFree(status);
+    if (host_status) cudaFreeHost(host_status);
+}
+
+extern "C" int he_krylov_create(he_krylov **out, long long n, int maxdim, int flexible)
+{
+    if (!out) return he_fail(HE_ERR_ARG, "null handle pointer", __FILE__, __LINE__);
+    *out = nullptr;
+    if (n < 1 || maxdim < 1 || maxdim > KRYLOV_MAXDIM)
+        return he_fail(HE_ERR_ARG, "Krylov dimension must be in [1, 64] and n >= 1", __FILE__, __LINE__);
+    he_krylov *k = new he_krylov();
+    k->n = (size_t)n; k->maxdim = maxdim; k->flexible = flexible;
+    cudaError_t e = cudaGetDevice(&k->device);
+    const size_t ld = maxdim + 1;
+    if (e == cudaSuccess) e = cudaMalloc(&k->Q, ld * k->n * sizeof(double2));
+    if (e == cudaSuccess && flexible) e = cudaMalloc(&k->Z, (size_t)maxdim * k->n * sizeof(double2));
+    if (e == cudaSuccess) e = cudaMalloc(&k->H, ld * maxdim * sizeof(double2));
+    if (e == cudaSuccess) e = cudaMalloc(&k->partial, (size_t)KRYLOV_BLOCKS * ld * sizeof(double2));
+    if (e == cudaSuccess) e = cudaMalloc(&k->z, ld * sizeof(double2));
+    if (e == cudaSuccess) e = cudaMalloc(&k->coef, ld * sizeof(double2));
+    if (e == cudaSuccess) e = cudaMalloc(&k->work, (size_t)8 * ld * ld * sizeof(double2));
+    if (e == cudaSuccess) e = cudaMalloc(&k->norm_partial, KRYLOV_BLOCKS * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&k->status, sizeof(KrylovStatus));
+    if (e == cudaSuccess) e = cudaMallocHost(&k->host_status, sizeof(KrylovStatus));
+    if (e != cudaSuccess) {
+        he_set_error(cudaGetErrorString(e), __FILE__, __LINE__);
+        delete k;
+        return HE_ERR_CUDA;
+    }
+    *out = k;
+    return HE_OK;
+}
+
+extern "C" int he_krylov_destroy(he_krylov *k)
+{
+    delete k;
+    return HE_OK;
+}
+
+extern "C" int he_krylov_vector(he_krylov *k, int which, int j, void **ptr)
+{
+    if (!k || !ptr) return he_fail(HE_ERR_ARG, "null argument", __FILE__, __LINE__);
+    if (which == 0 && j >= 0 && j <= k->maxdim) *ptr = k->Q + (size_t)j * k->n;
+    else if (which == 1 && k->Z && j >= 0 && j < k->maxdim) *ptr = k->Z + (size_t)j * k->n;
+    else return he_fail(HE_ERR_ARG, "basis index out of range", __FILE__, __LINE__);
+    return HE_OK;
+}
+
+namespace he {
+
+static const dim3 kGrid(KRYLOV_BLOCKS), kBlock(KRYLOV_THREADS);
+
+int krylov_multidot(he_krylov *k, int kc, const double2 *v, double2 *hcol, cudaStream_t s, const KrylovStatus *st,
+                    const double2 *basis)
+{
+    const int ld = k->maxdim + 1;
+    for (int k0 = 0; k0 < kc; k0 += KRYLOV_TILE) {
+        const int t = kc - k0 < KRYLOV_TILE ? kc - k0 : KRYLOV_TILE;
+        multidot_kernel<KRYLOV_TILE><<<kGrid, kBlock, 0, s>>>(basis, k->n, k0, t, v, k->partial, ld, st);
+    }
+    reduce_partials_kernel<<<1, 64, 0, s>>>(k->partial, KRYLOV_BLOCKS, ld, kc, k->z, hcol, st);
+    HE_CUDA_TRY(cudaGetLastError());
+    return HE_OK;
+}
+
+// CGS2 of v against basis[0..kc): twice (projection, update), H column += projections,
+// then h = ||v|| into *hsub and the status word.
+int krylov_cgs2(he_krylov *k, int kc, double2 *v, double2 *hcol, double2 *hsub, cudaStream_t s, double happy_below)
+{
+    int rc;
+    for (int rep = 0; rep < 2; ++rep) {
+        if ((rc = krylov_multidot(k, kc, v, hcol, s, k->status, k->Q))) return rc;
+        update_kernel<<<kGrid, kBlock, 0, s>>>(k->Q, k->n, kc, k->z, v, rep == 1 ? k->norm_partial : nullptr, k->status);
+    }
+    finish_norm_kernel<<<1, 32, 0, s>>>(k->norm_partial, KRYLOV_BLOCKS, hsub, k->status, happy_below);
+    HE_CUDA_TRY(cudaGetLastError());
+    return HE_OK;
+}
+
+int krylov_start(he_krylov *k, const double2 *x, cudaStream_t s)
+{
+    norm_kernel<<<kGrid, kBlock, 0, s>>>(x, k->n, k->norm_partial);
+    start_kernel<<<1, 32, 0, s>>>(k->norm_partial, KRYLOV_BLOCKS, k->status);
+    normalize_kernel<<<kGrid, kBlock, 0, s>>>(x, k->Q, k->n, k->status);
+    HE_CUDA_TRY(cudaMemsetAsync(k->H, 0, sizeof(double2) * (k->maxdim + 1) * k->maxdim, s));
+    HE_CUDA_TRY(cudaGetLastError());
+    return HE_OK;
+}
+
+int krylov_read_status(he_krylov *k, cudaStream_t s)
+{
+    HE_CUDA_TRY(cudaMemcpyAsync(k->host_status, k->status, sizeof(KrylovStatus), cudaMemcpyDeviceToHost, s));
+    HE_CUDA_TRY(cudaStreamSynchronize(s));
+    return HE_OK;
+}
+
+}  // namespace he
+
+// Arnoldi steps for an operator applied by the caller:
+//   start(x) -> beta; for j: caller writes H Q_j into vector j+1; orthogonalize(j);
+//   check(j) -> done?; when done: combine(y).
+extern "C" int he_krylov_start(he_krylov *k, const void *x, double *beta, void *stream)
+{
+    if (!k || !x) return he_fail(HE_ERR_ARG, "null argument", __FILE__, __LINE__);
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int rc = krylov_start(k, static_cast<const double2 *>(x), s);
+    if (!rc) rc = krylov_read_status(k, s);
+    if (!rc && beta) *beta = k->host_status->beta;
+    return rc;
+}
+
+extern "C" int he_krylov_orthogonalize(he_krylov *k, int j, void *stream)
+{
+    if (!k || j < 0 || j >= k->maxdim) return he_fail(HE_ERR_ARG, "bad Arnoldi index", __FILE__, __LINE__);
+    const int ld = k->maxdim + 1;
+    double2 *v = k->Q + (size_t)(j + 1) * k->n;
+    return krylov_cgs2(k, j + 1, v, k->H + (size_t)j * ld, k->H + (size_t)j * ld + j + 1,
+                       static_cast<cudaStream_t>(stream), 1e-13);
+}
+
+// Device-side check at iteration j, normalization of vector j+1 when not done.
+// sync != 0 reads the status back (done, m, estimate) and blocks the host.
+extern "C" int he_expv_check(he_krylov *k, int j, int maxdim, double dt, double tol, int sync, int *done, int *m,
+                             double *estimate, void *stream)
+{
+    if (!k || maxdim < 1 || maxdim > k->maxdim || j < 0 || j >= maxdim)
+        return he_fail(HE_ERR_ARG, "bad Arnoldi index", __FILE__, __LINE__);
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    arnoldi_check_kernel<<<1, 512, 0, s>>>(k->H, k->maxdim + 1, j, maxdim, dt, tol, k->coef, k->work, k->status);
+    if (j + 1 < maxdim)
+        normalize_kernel<<<kGrid, kBlock, 0, s>>>(k->Q + (size_t)(j + 1) * k->n, k->Q + (size_t)(j + 1) * k->n, k->n,
+                                                  k->status);
+    HE_CUDA_TRY(cudaGetLastError());
+    if (sync) {
+        int rc = krylov_read_status(k, s);
+        if (rc) return rc;
+        if (done) *done = k->host_status->done;
+        if (m) *m = k->host_status->m;
+        if (estimate) *estimate = k->host_status->estimate;
+        if (k->host_status->failed) return he_fail(HE_ERR_NOCONV, "Arnoldi did not converge", __FILE__, __LINE__);
+    }
+    return HE_OK;
+}
+
+extern "C" int he_krylov_combine(he_krylov *k, int m, void *y, void *stream)
+{
+    if (!k || !y || m > k->maxdim) return he_fail(HE_ERR_ARG, "bad combination", __FILE__, __LINE__);
+    combine_kernel<<<kGrid, kBlock, 0, static_cast<cudaStream_t>(stream)>>>(k->Q, k->n, k->coef,
+                                                                             static_cast<double2 *>(y), k->status, m, 0);
+    HE_CUDA_TRY(cudaGetLastError());
+    return HE_OK;
+}
+
+// Fused Arnoldi exponential action y = exp(-i dt H(field)) x with the device operator.
+// Host syncs only at the reference's check points (m = 4, 8, ..., maxdim).
+extern "C" int he_expv(he_krylov *k, he_handle op, const void *x, void *y, const double *field, int velocity,
+                       double dt, double tol, int maxdim, int *dimension, double *estimate, void *stream)
+{
+    if (!k || !op || !x || !y || !field) return he_fail(HE_ERR_ARG, "null argument", __FILE__, __LINE__);
+    if (maxdim < 1 || maxdim > k->maxdim) return he_fail(HE_ERR_ARG, "maxdim exceeds the workspace", __FILE__, __LINE__);
+    if ((size_t)op->n * op->n * op->nc != k->n) return he_fail(HE_ERR_SHAPE, "workspace size != operator size", __FILE__, __LINE__);
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int rc = krylov_start(k, static_cast<const double2 *>(x), s);
+    if (!rc) rc = krylov_read_status(k, s);
+    if (rc) return rc;
+    if (k->host_status->beta == 0) {
+        HE_CUDA_TRY(cudaMemcpyAsync(y, x, k->n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+        if (dimension) *dimension = 0;
+        if (estimate) *estimate = 0;
+        return HE_OK;
+    }
+    const int ld = k->maxdim + 1;
+    int done = 0, m = 0;
+    double err = 0;
+    for (int j = 0; j < maxdim && !done; ++j) {
+        double2 *qj = k->Q + (size_t)j * k->n, *v = k->Q + (size_t)(j + 1) * k->n;
+        rc = he::launch_hpsi<double>(op->t64, qj, v, field, velocity, mk<double>(0, 0), mk<double>(1, 0), s);
+        if (!rc) rc = krylov_cgs2(k, j + 1, v, k->H + (size_t)j * ld, k->H + (size_t)j * ld + j + 1, s, 1e-13);
+        if (rc) break;
+        const bool checkpoint = j >= 3 && ((j + 1) % 4 == 0 || j + 1 == maxdim);
+        arnoldi_check_kernel<<<1, 512, 0, s>>>(k->H, ld, j, maxdim, dt, tol, k->coef, k->work, k->status);
+        if (j + 1 < maxdim) normalize_kernel<<<kGrid, kBlock, 0, s>>>(v, v, k->n, k->status);
+        if (checkpoint || j + 1 == maxdim) {
+            if ((rc = krylov_read_status(k, s))) break;
+            done = k->host_status->done;
+            m = k->host_status->m;
+            err = k->host_status->estimate;
+        }
+    }
+    if (rc) return rc;
+    if (!done) {   // a happy breakdown recorded between check points
+        if ((rc = krylov_read_status(k, s))) return rc;
+        done = k->host_status->done; m = k->host_status->m; err = k->host_status->estimate;
+    }
+    if (estimate) *estimate = err;
+    if (dimension) *dimension = m;
+    if (k->host_status->failed || !k->host_status->converged)
+        return he_fail(HE_ERR_NOCONV, "Arnoldi did not converge", __FILE__, __LINE__);
+    combine_kernel<<<kGrid, kBlock, 0, s>>>(k->Q, k->n, k->coef, static_cast<double2 *>(y), k->status, m, 0);
+    HE_CUDA_TRY(cudaGetLastError());
+    return HE_OK;
+}

@@ -1,0 +1,45 @@
+// Krylov workspace shared by the Arnoldi exponential and GMRES (krylov.cu, gmres.cu).
+#pragma once
+#include "common.cuh"
+
+namespace he {
+
+// Device-resident status of one Krylov solve; kernels read `done` and return early
+// once the solve has finished, so a host loop (or a captured graph) may run ahead.
+struct KrylovStatus {
+    int done;        // 1 once converged, broken down or failed
+    int converged;   // 1 if the tolerance was met (or happy breakdown)
+    int happy;       // happy breakdown seen
+    int m;           // dimension of the accepted solution
+    int failed;      // 1 if maxdim was reached without convergence
+    int pad[3];
+    double beta;     // norm of the start vector
+    double estimate; // error estimate (Arnoldi) or residual estimate (GMRES)
+    double hnext;    // last subdiagonal h_{j+1,j}
+    double pad2;
+};
+
+constexpr int KRYLOV_BLOCKS = 296;    // 2 CTAs per SM on 148 SMs
+constexpr int KRYLOV_THREADS = 256;
+constexpr int KRYLOV_TILE = 8;        // basis vectors per register tile
+constexpr int KRYLOV_MAXDIM = 64;
+
+}  // namespace he
+
+struct he_krylov {
+    int device = 0;
+    size_t n = 0;                 // vector length (complex elements)
+    int maxdim = 0;
+    int flexible = 0;
+    double2 *Q = nullptr;         // (maxdim+1) vectors, column j at Q + j*n
+    double2 *Z = nullptr;         // flexible GMRES: preconditioned directions (maxdim vectors)
+    double2 *H = nullptr;         // (maxdim+1) x maxdim Hessenberg, column major, ld = maxdim+1
+    double2 *partial = nullptr;   // KRYLOV_BLOCKS x (maxdim+1) block partial sums (scratch)
+    double2 *z = nullptr;         // (maxdim+1) projections of the current CGS round
+    double2 *coef = nullptr;      // maxdim combination coefficients
+    double2 *work = nullptr;      // 8 * maxdim^2 complex: small dense scratch (expm / least squares)
+    double *norm_partial = nullptr;   // KRYLOV_BLOCKS
+    he::KrylovStatus *status = nullptr;      // device
+    he::KrylovStatus *host_status = nullptr; // pinned host mirror
+    ~he_krylov();
+};

@@ -3,17 +3,39 @@
 #include <vector>
 
 #include "common.cuh"
+#include "hpsi_tiled.cuh"
 
 struct he_operator {
     int device = 0;
     int n = 0, nc = 0, nt = 0, nv = 0, nd = 0, nlam = 0;
     bool separable = false;
     bool has32 = false;
+    bool tiled = false;                 // tiled kernels usable (plan built)
+    int path = 1;                       // 1: tiled when possible, 0: generic gather kernel
     he::DeviceTables<double> t64{};
     he::DeviceTables<float> t32{};
+    he::TiledPlan<double> p64{};
+    he::TiledPlan<float> p32{};
+    double2 *coef64 = nullptr;          // field-contracted dipole coefficients (nd)
+    float2 *coef32 = nullptr;
+    double2 *w64[2] = {nullptr, nullptr};   // velocity gauge B-stencil scratch (n*n*nc each)
+    float2 *w32[2] = {nullptr, nullptr};
     const double2 *tdiag = nullptr;     // diagonal of the kinetic CSR (n entries)
+    he_plan_host plan;
     std::vector<void *> allocations;    // every cudaMalloc made for this handle
     ~he_operator();
 };
 
 int he_fail(int status, const char *what, const char *file, int line);
+
+bool he_build_plan(he_plan_host &P, int n, int nc, const int *ptr, const int *col, const double *tv, int nv,
+                   const int *vptr, const int *vc, const int *vl, const double *vcoef, int nlam, int nd,
+                   const int *dptr, const int *dc, const int *de, const double *r);
+
+namespace he {
+template <typename R>
+int launch_hpsi_tiled(he_operator *h, const DeviceTables<R> &t, const TiledPlan<R> &pl, cplx<R> *coef, cplx<R> *w1,
+                      cplx<R> *w2, const cplx<R> *psi, cplx<R> *out, const double *field, int velocity,
+                      cplx<R> beta, cplx<R> gamma, cudaStream_t stream);
+bool tiled_fits(int nc, int nlam, size_t elem);
+}  // namespace he

@@ -95,8 +95,25 @@ class B200Hamiltonian:
         self.diagonal = torch.empty(self.size, dtype=torch.complex128, device=self.device)
         check(LIB.he_diagonal(self.op.handle, ct.c_void_p(self.diagonal.data_ptr()), _stream(self.device)), 'he_diagonal')
         self.apply_count = 0
+        info = (ct.c_longlong * 16)()
+        check(LIB.he_info(self.op.handle, info, 16), 'he_info')
+        self.tiled = bool(info[9])
+        self.plan_info = {'elements': int(info[11]), 'tiles_per_axis': int(info[12]), 'groups': int(info[13]),
+                          'wide_edges': int(info[14]), 'wide_dipole_edges': int(info[15])}
         if hasattr(h, 'surface_indices'):
             self._prepare_flux()
+
+    def use_tiled(self, flag=True):
+        """Select the tiled kernels (default when the tables admit them) or the generic one."""
+        check(LIB.he_set_path(self.op.handle, int(bool(flag))), 'he_set_path')
+        self.tiled = bool(flag)
+
+    @property
+    def launches_per_apply(self):
+        """Kernels one apply launches: field contraction, radial, mixing (tiled) or one."""
+        if not self.tiled:
+            return 1
+        return 3 if len(self.h.dc) else 2
 
     # --- state transfer -------------------------------------------------------------
     def state(self, x):

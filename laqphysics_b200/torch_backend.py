@@ -1,0 +1,173 @@
+"""Drop-in for the reference's python/torch_backend.py: ``TorchHamiltonian``,
+``exponential_action`` and ``step`` with the same signatures, messages and results,
+computed by this package's sm_100a kernels.
+
+* ``TorchHamiltonian`` is :class:`laqphysics_b200.engine.B200Hamiltonian`.
+* ``exponential_action(apply, x, dt, tol, maxdim)`` (python/torch_backend.py:140-158):
+  Arnoldi with CGS2, the small Hessenberg exponential and the error estimate all on
+  the device; ``apply`` may be any callable returning H·y.  The host waits only at the
+  reference's check points (m = 4, 8, ..., maxdim), not once per Krylov vector.
+  When ``apply`` is a :class:`FieldOperator` of this package the whole Krylov loop
+  runs inside the C-ABI (``he_expv``) with no Python in between.
+* ``step(apply_at, x, t, dt, tol, maxdim)`` (python/torch_backend.py:160-167): midpoint
+  Hamiltonian, recursive dt halving (depth <= 8) on 'Arnoldi did not converge'.
+"""
+import ctypes as ct
+
+import numpy as np
+import torch
+
+from ._lib import HE_ERR_NOCONV, LIB, HeliumError, check, ptr
+from .engine import B200Hamiltonian, _stream
+
+TorchHamiltonian = B200Hamiltonian
+
+_WORKSPACES = {}
+
+
+class KrylovWorkspace:
+    """Device Krylov basis (maxdim+1 vectors), Hessenberg matrix and reduction scratch."""
+
+    def __init__(self, n, maxdim, device, flexible=False):
+        self.n, self.maxdim, self.device = int(n), int(maxdim), torch.device(device)
+        handle = ct.c_void_p()
+        with torch.cuda.device(self.device):
+            check(LIB.he_krylov_create(ct.byref(handle), self.n, self.maxdim, int(flexible)), 'he_krylov_create')
+        self.handle = handle
+        self._views = {}
+
+    def vector(self, j, which=0):
+        """torch view of basis vector j (which=0: Q, which=1: Z of flexible GMRES)."""
+        key = (which, j)
+        if key not in self._views:
+            address = ct.c_void_p()
+            check(LIB.he_krylov_vector(self.handle, which, j, ct.byref(address)), 'he_krylov_vector')
+            self._views[key] = _device_view(address.value, self.n, self.device)
+        return self._views[key]
+
+    def __del__(self):
+        handle = getattr(self, 'handle', None)
+        if handle is not None and handle.value:
+            LIB.he_krylov_destroy(handle)
+            self.handle = None
+
+
+class _Owner:
+    """Keeps a raw device allocation visible to torch without taking ownership."""
+
+    def __init__(self, address, nbytes):
+        self.__cuda_array_interface__ = {'shape': (nbytes // 16,), 'typestr': '<c16', 'data': (address, False),
+                                         'version': 3, 'strides': None}
+
+
+def _device_view(address, n, device):
+    return torch.as_tensor(_Owner(address, n * 16), device=device)
+
+
+def workspace(n, maxdim, device, flexible=False):
+    """Cached workspace with at least ``maxdim`` Krylov vectors for vectors of length n."""
+    device = torch.device(device)
+    key = (device, int(n), bool(flexible))
+    ws = _WORKSPACES.get(key)
+    if ws is None or ws.maxdim < maxdim:
+        ws = KrylovWorkspace(n, max(maxdim, ws.maxdim if ws else 0), device, flexible)
+        _WORKSPACES[key] = ws
+    return ws
+
+
+class FieldOperator:
+    """y -> H(field) y of a B200Hamiltonian; also usable as a plain callable."""
+
+    def __init__(self, engine, field, velocity=True):
+        self.engine = engine
+        self.field = np.ascontiguousarray(field, dtype=np.float64)
+        self.velocity = bool(velocity)
+
+    def __call__(self, y):
+        return self.engine.apply(y, self.field, self.velocity)
+
+
+class FieldSchedule:
+    """(t, y) -> H(field(t)) y of a B200Hamiltonian; ``step`` recognises it and uses
+    the fused device Arnoldi."""
+
+    def __init__(self, engine, field_at, velocity=True):
+        self.engine = engine
+        self.field_at = field_at
+        self.velocity = bool(velocity)
+
+    def __call__(self, t, y):
+        return self.engine.apply(y, self.field_at(t), self.velocity)
+
+    def at(self, t):
+        return FieldOperator(self.engine, self.field_at(t), self.velocity)
+
+
+def _not_converged(maxdim, dt, err):
+    return RuntimeError(f'GPU Arnoldi did not converge: dim={maxdim}, dt={dt}, estimate={err:.3e}')
+
+
+@torch.no_grad()
+def exponential_action(apply, x, dt, tol=1e-10, maxdim=48):
+    """exp(-i dt H) x by Arnoldi (python/torch_backend.py:140-158)."""
+    if x.dtype != torch.complex128 or x.device.type != 'cuda':
+        raise ValueError('exponential_action needs a complex128 CUDA tensor')
+    x = x.contiguous()
+    ws = workspace(x.numel(), maxdim, x.device)
+    stream = _stream(x.device)
+    if isinstance(apply, FieldOperator):
+        return _fused(apply, ws, x, dt, tol, maxdim, stream)
+    beta = ct.c_double()
+    check(LIB.he_krylov_start(ws.handle, ct.c_void_p(x.data_ptr()), ct.byref(beta), stream), 'he_krylov_start')
+    if beta.value == 0:
+        return x.clone(), {'dimension': 0, 'residual_estimate': 0.}
+    done, m, err = ct.c_int(0), ct.c_int(0), ct.c_double(0.)
+    for j in range(maxdim):
+        v = apply(ws.vector(j))
+        ws.vector(j + 1).copy_(v)
+        check(LIB.he_krylov_orthogonalize(ws.handle, j, stream), 'he_krylov_orthogonalize')
+        sync = (j >= 3 and ((j + 1) % 4 == 0 or j + 1 == maxdim)) or j + 1 == maxdim
+        status = LIB.he_expv_check(ws.handle, j, maxdim, float(dt), float(tol), int(sync), ct.byref(done),
+                                   ct.byref(m), ct.byref(err), stream)
+        if status == HE_ERR_NOCONV:
+            raise _not_converged(maxdim, dt, err.value)
+        check(status, 'he_expv_check')
+        if sync and done.value:
+            y = torch.empty_like(x)
+            check(LIB.he_krylov_combine(ws.handle, m.value, ct.c_void_p(y.data_ptr()), stream), 'he_krylov_combine')
+            return y, {'dimension': m.value, 'residual_estimate': float(err.value)}
+    raise _not_converged(maxdim, dt, err.value)
+
+
+def _fused(op, ws, x, dt, tol, maxdim, stream):
+    y = torch.empty_like(x)
+    dim, err = ct.c_int(0), ct.c_double(0.)
+    status = LIB.he_expv(ws.handle, op.engine.op.handle, ct.c_void_p(x.data_ptr()), ct.c_void_p(y.data_ptr()),
+                         ptr(op.field), int(op.velocity), float(dt), float(tol), int(maxdim), ct.byref(dim),
+                         ct.byref(err), stream)
+    if status == HE_ERR_NOCONV:
+        raise _not_converged(maxdim, dt, err.value)
+    check(status, 'he_expv')
+    op.engine.apply_count += dim.value
+    return y, {'dimension': dim.value, 'residual_estimate': float(err.value)}
+
+
+def step(apply_at, x, t, dt, tol=1e-10, maxdim=48, depth=0):
+    """Midpoint exponential step with recursive halving (python/torch_backend.py:160-167)."""
+    try:
+        if isinstance(apply_at, FieldSchedule):
+            operator = apply_at.at(t + dt / 2)
+        else:
+            operator = lambda y: apply_at(t + dt / 2, y)
+        return exponential_action(operator, x, dt, tol, maxdim)
+    except RuntimeError as error:
+        if 'Arnoldi did not converge' not in str(error) or depth >= 8:
+            raise
+        y, a = step(apply_at, x, t, dt / 2, tol / 2, maxdim, depth + 1)
+        y, b = step(apply_at, y, t + dt / 2, dt / 2, tol / 2, maxdim, depth + 1)
+        return y, {'dimension': max(a['dimension'], b['dimension']),
+                   'residual_estimate': a['residual_estimate'] + b['residual_estimate'], 'subdivided': True}
+
+
+__all__ = ['TorchHamiltonian', 'B200Hamiltonian', 'exponential_action', 'step', 'FieldOperator', 'FieldSchedule',
+           'HeliumError']

@@ -69,6 +69,38 @@ def test_apply_matches_oracle_on_larger_coupled_grid(velocity):
     np.testing.assert_allclose(y, ref, rtol=1e-12, atol=1e-10)
 
 
+@pytest.mark.parametrize('velocity', [False, True])
+def test_tiled_and_generic_kernels_agree(velocity):
+    h = _coupled(np.linspace(0, 30, 16), 8, .3, 12, 3, 2)
+    op = engine(h)
+    assert op.tiled
+    rng = np.random.default_rng(17)
+    x = op.state(rng.normal(size=h.size) + 1j * rng.normal(size=h.size))
+    f = (0., 0., .2)
+    a = op.host(op.apply(x, f, velocity))
+    op.use_tiled(False)
+    b = op.host(op.apply(x, f, velocity))
+    op.use_tiled(True)
+    assert rel_l2(a, b) < 1e-14
+    alpha = .05 / (3 - 1j * np.sqrt(3))
+    c = op.host(op.apply_shifted(x, f, alpha, -2.9, velocity=velocity))
+    np.testing.assert_allclose(c, op.host(x) + 1j * alpha * (b + 2.9 * op.host(x)), rtol=1e-12, atol=1e-12)
+
+
+def test_microbenchmark_grid_apply_matches_oracle():
+    from laqphysics_b200.workloads import hpsi_microbench, seeded_state
+    h = hpsi_microbench()
+    op = engine(h)
+    assert op.tiled
+    x = seeded_state(h.size, 1234)
+    for velocity in (False, True):
+        y = op.host(op.apply(op.state(x), (0., 0., .02), velocity))
+        ref = cpu.tensor_apply(h, x, (0., 0., .02), velocity)
+        assert rel_l2(y, ref) < 1e-13
+        y64 = op.host(op.apply(op.state(x).to(torch.complex64), (0., 0., .02), velocity, precision='complex64'))
+        assert rel_l2(y64.astype(complex), ref) < C64_REL_L2
+
+
 def test_complex64_apply_within_stated_tolerance():
     h = _coupled(np.linspace(0, 30, 16), 8, .3, 12, 3, 2)
     rng = np.random.default_rng(8)

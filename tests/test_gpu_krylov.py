@@ -1,0 +1,106 @@
+"""GPU parity of the Arnoldi exponential (device CGS2, on-device expm, device checks)
+against the reference's own results (golden fixtures from python/propagate.py and
+python/torch_backend.py) and the numpy oracle.  Tolerance: the reference's own
+Torch-vs-Fortran Arnoldi bound (tests/test_torch_backend.py:18-20: 2e-11)."""
+import json
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import Tables, golden
+from oracle import arnoldi, cpu
+
+pytestmark = pytest.mark.gpu
+DEVICE = 'cuda:0'
+
+
+def engine(h):
+    from laqphysics_b200.engine import B200Hamiltonian
+    return B200Hamiltonian(h, DEVICE)
+
+
+@pytest.mark.parametrize('fused', [False, True])
+def test_arnoldi_matches_reference_on_helium(fused):
+    from laqphysics_b200.torch_backend import FieldOperator, exponential_action
+    g = golden('apply_cut')
+    op = engine(Tables(g))
+    f = g['field']
+    apply = FieldOperator(op, f, True) if fused else (lambda y: op.apply(y, f))
+    y, info = exponential_action(apply, op.state(g['x']), float(g['arnoldi_dt']), tol=float(g['arnoldi_tol']))
+    assert info['dimension'] == int(g['arnoldi_torch_dim'])
+    np.testing.assert_allclose(op.host(y), g['arnoldi_torch'], atol=2e-11, rtol=2e-11)
+    np.testing.assert_allclose(op.host(y), g['arnoldi_cpu'], atol=2e-11, rtol=2e-11)
+
+
+def test_arnoldi_dense_reference_case():
+    from laqphysics_b200.torch_backend import exponential_action
+    g = golden('arnoldi_dense')
+    H = torch.tensor(g['H'], device=DEVICE)
+    y, info = exponential_action(lambda z: H @ z, torch.tensor(g['x'], device=DEVICE), float(g['dt']),
+                                 tol=float(g['tol']), maxdim=60)
+    assert info['dimension'] == int(g['dimension'])
+    np.testing.assert_allclose(y.cpu().numpy(), g['y'], atol=1e-12, rtol=1e-12)
+    np.testing.assert_allclose(y.cpu().numpy(), g['exact'], atol=2e-11, rtol=2e-11)
+
+
+def test_arnoldi_reports_non_convergence_with_reference_message():
+    from laqphysics_b200.torch_backend import exponential_action
+    g = golden('arnoldi_dense')
+    H = torch.tensor(g['H'], device=DEVICE)
+    with pytest.raises(RuntimeError, match='Arnoldi did not converge'):
+        exponential_action(lambda z: H @ z, torch.tensor(g['x'], device=DEVICE), 1.0, tol=1e-10, maxdim=8)
+
+
+def test_step_subdivides_like_the_oracle():
+    from laqphysics_b200.torch_backend import step
+    g = golden('arnoldi_dense')
+    H = torch.tensor(g['H'], device=DEVICE)
+    y, info = step(lambda t, z: H @ z, torch.tensor(g['x'], device=DEVICE), 0., 1.0, tol=1e-10, maxdim=8)
+    ref, rinfo = arnoldi.step(lambda t, z: g['H'] @ z, g['x'], 0., 1.0, tol=1e-10, maxdim=8)
+    assert info.get('subdivided') and rinfo.get('subdivided')
+    np.testing.assert_allclose(y.cpu().numpy(), ref, atol=1e-11, rtol=1e-11)
+
+
+def _length_run_setup():
+    from laqphysics_b200.pulses import Pulse
+    from laqphysics_b200.workloads import coupled
+    g = golden('length_run')
+    grid = json.loads(str(g['grid']))
+    h = coupled(grid['edges'], grid['order'], int(g['lmax']), int(g['total_Lmax']), ecs_angle=grid['ecs_angle'],
+                tail=grid['tail'], cutoff_radii=tuple(g['cutoff']))
+    return g, h, Pulse(**json.loads(str(g['pulse'])))
+
+
+@pytest.mark.parametrize('fused', [False, True])
+def test_length_gauge_propagation_matches_reference(fused):
+    """Six midpoint Arnoldi steps in the length gauge (python/propagate.py:41-50 driven like
+    python/run3d.py:196-199) agree with the reference's complex128 run to 1e-10 rel L2."""
+    from laqphysics_b200.torch_backend import FieldSchedule, step
+    g, h, pulse = _length_run_setup()
+    op = engine(h)
+    field = lambda t: (0., 0., float(pulse.electric(t)))
+    apply_at = FieldSchedule(op, field, False) if fused else (lambda t, v: op.apply(v, field(t), False))
+    y = op.state(g['states'][0])
+    dt = float(g['dt'])
+    for i in range(len(g['dimensions'])):
+        y, info = step(apply_at, y, i * dt, dt, tol=float(g['tol']), maxdim=int(g['maxdim']))
+        assert info['dimension'] == int(g['dimensions'][i])
+        ref = g['states'][i + 1]
+        assert np.linalg.norm(op.host(y) - ref) / np.linalg.norm(ref) < 1e-10
+
+
+def test_fused_and_generic_arnoldi_agree_on_larger_grid():
+    from laqphysics_b200.torch_backend import FieldOperator, exponential_action
+    from laqphysics_b200.workloads import coupled, seeded_state
+    h = coupled(np.linspace(0, 30, 16), 8, 3, 2, ecs_angle=.3, tail=12, cutoff_radii=(20., 25.))
+    op = engine(h)
+    x = op.state(seeded_state(h.size, 21))
+    f = (0., 0., .03)
+    a, ia = exponential_action(FieldOperator(op, f, False), x, .05, tol=1e-10, maxdim=16)
+    b, ib = exponential_action(lambda y: op.apply(y, f, False), x, .05, tol=1e-10, maxdim=16)
+    c, ic = arnoldi.exponential_action(lambda v: cpu.tensor_apply(h, v, f, False), op.host(x), .05, tol=1e-10,
+                                       maxdim=16)
+    assert ia['dimension'] == ib['dimension'] == ic['dimension']
+    np.testing.assert_array_equal(op.host(a), op.host(b))
+    assert np.linalg.norm(op.host(a) - c) / np.linalg.norm(c) < 1e-12
