@@ -134,6 +134,58 @@ int he_krylov_combine(he_krylov_handle k, int m, void *y, void *stream);
 int he_expv(he_krylov_handle k, he_handle op, const void *x, void *y, const double *field, int velocity,
             double dt, double tol, int maxdim, int *dimension, double *estimate, void *stream);
 
+/* ------------------------------------------------------------------------------------
+ * GMRES / CF4 building blocks (python/implicit.py:45-109).  The GMRES driver keeps its
+ * Krylov basis in an he_krylov workspace (Q, and Z when flexible), orthogonalises with
+ * he_krylov_orthogonalize, reads the Hessenberg column it needs for the small least
+ * squares, and forms candidates and true residuals with these vector operations.
+ * ---------------------------------------------------------------------------------- */
+/* out = a x + b y (complex a, b); out may alias x or y. */
+int he_vec_axpby(long long n, double a_re, double a_im, const void *x, double b_re, double b_im, const void *y,
+                 void *out, void *stream);
+/* *norm = ||b - t|| (t = NULL: ||b||); r = b - t is stored when r != NULL.  Blocks. */
+int he_vec_residual_norm(long long n, const void *b, const void *t, void *r, double *norm, void *stream);
+/* y = x / (1 + i alpha (diag + shift)): the Jacobi preconditioner of python/implicit.py:80,85. */
+int he_vec_jacobi(long long n, const void *diag, double alpha_re, double alpha_im, double shift, const void *x,
+                  void *y, void *stream);
+/* Q_j (which = 0) or Z_j (which = 1) *= s. */
+int he_krylov_scale(he_krylov_handle k, int which, int j, double s, void *stream);
+/* Copy H[0:rows, j] (interleaved complex) to host memory `out`.  Blocks. */
+int he_krylov_hessenberg(he_krylov_handle k, int j, int rows, void *out, void *stream);
+/* H = 0 and a fresh status word (start of a GMRES cycle). */
+int he_krylov_reset(he_krylov_handle k, void *stream);
+/* y (+)= sum_{k<m} V_k c_k, V = Q (which = 0) or Z (which = 1), c: m host complex values. */
+int he_krylov_combine_coef(he_krylov_handle k, int which, int m, const void *coef, void *y, int accumulate,
+                           void *stream);
+
+/* ------------------------------------------------------------------------------------
+ * Separable ionic resolvent preconditioner.  Replaces SeparablePreconditioner
+ * (python/implicit.py:13-39): for channel c with one-electron momenta (l1[c], l2[c]),
+ * Y_c = S_{l1} [ (S_{l1}^-1 Psi_c S_{l2}^-T) / (1 + i alpha (e_{l1}(i) + e_{l2}(j) + shift)) ] S_{l2}^T.
+ * S, Sinv: nl column-major n x n complex128 matrices; evals: nl x n; the set-up
+ * eigendecompositions are the caller's.  precision HE_C64 runs the products in
+ * complex64 (the flexible-GMRES preconditioner of the reference) with complex128 in/out.
+ * ---------------------------------------------------------------------------------- */
+typedef struct he_separable *he_separable_handle;
+
+int he_separable_create(he_separable_handle *out, int n, int nc, int nl, const double *S, const double *Sinv,
+                        const double *evals, const int *l1, const int *l2, int precision);
+int he_separable_destroy(he_separable_handle h);
+int he_separable_apply(he_separable_handle h, const void *x, void *y, double alpha_re, double alpha_im,
+                       double shift, void *stream);
+
+/* ------------------------------------------------------------------------------------
+ * Operator set-up options and planner inspection (host only, no device work).
+ * he_set_path: 1 = tiled kernels (default when the tables admit them), 0 = generic.
+ * he_plan_build / he_plan_array / he_plan_free expose the tiled plan of a set of tables.
+ * ---------------------------------------------------------------------------------- */
+int he_set_path(he_handle h, int tiled);
+void *he_plan_build(int n, int nc, const int *ptr, const int *col, const double *tv, int nv, const int *vptr,
+                    const int *vc, const int *vl, const double *vcoef, int nlam, int nd, const int *dptr,
+                    const int *dc, const int *de, const double *r);
+long long he_plan_array(void *plan, int which, void *dst);
+void he_plan_free(void *plan);
+
 #ifdef __cplusplus
 }
 #endif

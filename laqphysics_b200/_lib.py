@@ -42,6 +42,16 @@ SIGNATURES = {
     'he_krylov_combine': (I, [P, I, P, P]),
     'he_expv': (I, [P, P, P, P, P, I, D, D, I, ct.POINTER(I), ct.POINTER(D), P]),
     'he_set_path': (I, [P, I]),
+    'he_vec_axpby': (I, [ct.c_longlong, D, D, P, D, D, P, P, P]),
+    'he_vec_residual_norm': (I, [ct.c_longlong, P, P, P, ct.POINTER(D), P]),
+    'he_vec_jacobi': (I, [ct.c_longlong, P, D, D, D, P, P, P]),
+    'he_krylov_scale': (I, [P, I, I, D, P]),
+    'he_krylov_hessenberg': (I, [P, I, I, P, P]),
+    'he_krylov_reset': (I, [P, P]),
+    'he_krylov_combine_coef': (I, [P, I, I, P, P, I, P]),
+    'he_separable_create': (I, [ct.POINTER(P), I, I, I, P, P, P, P, P, I]),
+    'he_separable_destroy': (I, [P]),
+    'he_separable_apply': (I, [P, P, P, D, D, D, P]),
     'he_plan_build': (P, [I, I, P, P, P, I, P, P, P, P, I, I, P, P, P, P]),
     'he_plan_free': (None, [P]),
     'he_plan_array': (ct.c_longlong, [P, I, P]),

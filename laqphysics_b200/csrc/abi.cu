@@ -114,7 +114,7 @@ template <typename R> int upload_plan(he_operator *h, he::TiledPlan<R> *pl, cplx
 {
     const he_plan_host &P = h->plan;
     pl->n = h->n; pl->nc = h->nc; pl->ne = P.ne; pl->ntile = P.ntile;
-    pl->ng = P.ng; pl->nlam = P.nlam; pl->nwd = (int)P.dwsrc.size();
+    pl->ng = P.ng; pl->nlam = P.nlam; pl->nwd = (int)P.dwsrc.size(); pl->nwide = (int)P.wsrc.size();
     int s;
     if ((s = upload(h, P.estart.data(), P.estart.size(), &pl->estart))) return s;
     if ((s = upload(h, P.tstart.data(), P.tstart.size(), &pl->tstart))) return s;
@@ -218,7 +218,7 @@ extern "C" int he_create(he_handle *out, int n, int nc, int nt, const int *ptr, 
         h->tdiag = td;
     }
     if (!s && he_build_plan(h->plan, n, nc, ptr, col, tv, nv, vptr, vc, vl, vcoef, nlam, nd, dptr, dc, de, r) &&
-        he::tiled_fits(nc, nlam, sizeof(double2))) {
+        he::tiled_fits(h->plan, nc, nd)) {
         s = upload_plan<double>(h, &h->p64, &h->coef64);
         if (!s && h->has32) s = upload_plan<float>(h, &h->p32, &h->coef32);
         h->tiled = !s;

@@ -1,5 +1,5 @@
 // Tiled two-electron H·psi for sm_100a (the production path; hamiltonian.cu keeps the
-// generic one-thread-per-output kernel for tables this plan cannot express).
+// generic one-thread-per-output kernel for tables the planner cannot express).
 //
 // H psi is split by the structure of the operator (python/torch_backend.py:109-131,
 // src/kernels.f90:132-171):
@@ -10,19 +10,16 @@
 //                       to two elements), the separable or tabulated diagonal and |A|^2;
 //                       in the velocity gauge also W_e = B_e psi with B = T (r_b - r_a),
 //                       the [T, r] commutator stencils of src/kernels.f90:153-168.
-//   hpsi_mix_kernel     per point, all channels of 128 points staged in shared memory:
+//   hpsi_mix_kernel     per point, all channels of NP points staged in shared memory:
 //                       Coulomb multipoles sum_lam rad_lam sum_c' V_lam[c,c'] psi_c' and the
 //                       dipole couplings, register-blocked over MIX_GROUP output channels
 //                       that share source channels ("wide edges"), then the epilogue
 //                       out = beta psi + gamma (H psi).
 //
-// Each kernel reads psi once from DRAM; the radial result travels through `out`.
+// psi is read once from DRAM by each kernel; the radial result travels through `out`.
+// Every table an inner loop touches (element blocks, wide edges, dipole edges) is
+// staged in shared memory first, so the loops issue no global loads.
 #include <algorithm>
-#include <complex>
-#include <cstring>
-#include <map>
-#include <numeric>
-#include <set>
 
 #include "common.cuh"
 #include "hpsi_tiled.cuh"
@@ -31,36 +28,154 @@
 namespace he {
 
 constexpr int RAD_THREADS = 256;
-constexpr int RAD_STRIDE = RAD_TMAX + 1;   // odd row stride (in complex elements): conflict-free columns
+constexpr int RAD_STRIDE = RAD_TMAX + 1;   // odd row stride (complex elements): conflict-free column reads
 
 template <typename R> __device__ __forceinline__ cplx<R> cmul_sel(bool real, cplx<R> a, cplx<R> x, cplx<R> acc)
 {
     return real ? rfma<R>(a.x, x, acc) : cfma<R>(a, x, acc);
 }
 
-// Element e: nodes [s, s + m - 1], m = estart[e+1] - s + 1 (last element: n - s).
-__device__ __forceinline__ int elem_size(const int *estart, int e, int ne, int n)
+// Per-axis description of a radial tile, built in shared memory by the CTA.
+struct AxisTile {
+    int ga, gb;                          // element range
+    int count;                           // gb - ga
+    int s[RAD_ELEMS], m[RAD_ELEMS], own[RAD_ELEMS], real[RAD_ELEMS];
+    int off[RAD_ELEMS];                  // offset of the element's T block in the staged blocks
+    int items[RAD_ELEMS + 1];            // prefix sums of work items (lines x chunks)
+    int prev, prev_m, prev_real, prev_off;   // previous element (bridge row), -1 if none
+};
+
+// Stage the element blocks of one axis: previous element's last row, then full blocks.
+// Returns the number of complex entries written for one matrix kind (T or B).
+template <typename R>
+__device__ void stage_axis(const TiledPlan<R> &pl, AxisTile &ax, int ga, int gb, int lines, cplx<R> *dst,
+                           cplx<R> *dstB, bool vel)
 {
-    return e + 1 < ne ? estart[e + 1] - estart[e] + 1 : n - estart[e];
+    const int n = pl.n, ne = pl.ne;
+    if (threadIdx.x == 0) {
+        ax.ga = ga; ax.gb = gb; ax.count = gb - ga;
+        int off = 0;
+        ax.prev = ga > 0 ? ga - 1 : -1;
+        if (ga > 0) {
+            const int e = ga - 1;
+            ax.prev_m = e + 1 < ne ? pl.estart[e + 1] - pl.estart[e] + 1 : n - pl.estart[e];
+            ax.prev_real = pl.ereal[e];
+            ax.prev_off = 0;
+            off = ax.prev_m;
+        }
+        ax.items[0] = 0;
+        for (int k = 0; k < ax.count; ++k) {
+            const int e = ga + k;
+            ax.s[k] = pl.estart[e];
+            ax.m[k] = e + 1 < ne ? pl.estart[e + 1] - pl.estart[e] + 1 : n - pl.estart[e];
+            ax.own[k] = (e + 1 < ne ? pl.estart[e + 1] : n) - pl.estart[e];
+            ax.real[k] = pl.ereal[e];
+            ax.off[k] = off;
+            off += ax.m[k] * ax.m[k];
+            ax.items[k + 1] = ax.items[k] + lines * ((ax.own[k] + RAD_CHUNK - 1) / RAD_CHUNK);
+        }
+    }
+    __syncthreads();
+    if (ax.prev >= 0) {
+        const int mp = ax.prev_m;
+        const size_t src = (size_t)pl.eoff[ax.prev] + (size_t)(mp - 1) * mp;
+        for (int b = threadIdx.x; b < mp; b += blockDim.x) {
+            dst[b] = pl.blocks[src + b];
+            if (vel) dstB[b] = pl.bblocks[src + b];
+        }
+    }
+    for (int k = 0; k < ax.count; ++k) {
+        const int mm = ax.m[k] * ax.m[k];
+        const size_t src = pl.eoff[ax.ga + k];
+        for (int q = threadIdx.x; q < mm; q += blockDim.x) {
+            dst[ax.off[k] + q] = pl.blocks[src + q];
+            if (vel) dstB[ax.off[k] + q] = pl.bblocks[src + q];
+        }
+    }
+}
+
+// One direction of the radial stencil on the staged tile.  ROWS = electron 1 (lines are
+// owned columns, element index runs along rows), else electron 2.
+template <typename R, bool VEL, bool ROWS>
+__device__ void radial_phase(const AxisTile &ax, const cplx<R> *BLK, const cplx<R> *BLKB, const cplx<R> *PS,
+                             cplx<R> *OS, int lines, int base, int r0, int c0, int n, const cplx<R> *pc,
+                             cplx<R> *wout, size_t nn, int c)
+{
+    const int nitems = ax.items[ax.count];
+    for (int item = threadIdx.x; item < nitems; item += blockDim.x) {
+        int k = 0;
+        while (k + 1 < ax.count && item >= ax.items[k + 1]) ++k;
+        const int rest = item - ax.items[k];
+        const int line = rest % lines, chunk = rest / lines;
+        const int s = ax.s[k], m = ax.m[k];
+        const int a0 = chunk * RAD_CHUNK, na = min(RAD_CHUNK, ax.own[k] - a0);
+        const cplx<R> *blk = BLK + ax.off[k], *bbl = BLKB + ax.off[k];
+        const bool real = ax.real[k];
+        cplx<R> acc[RAD_CHUNK], accb[RAD_CHUNK];
+#pragma unroll
+        for (int q = 0; q < RAD_CHUNK; ++q) { acc[q] = mk<R>(0, 0); accb[q] = mk<R>(0, 0); }
+        for (int b = 0; b < m; ++b) {
+            const int node = s - base + b;
+            const cplx<R> x = ROWS ? PS[node * RAD_STRIDE + line] : PS[line * RAD_STRIDE + node];
+#pragma unroll
+            for (int q = 0; q < RAD_CHUNK; ++q) {
+                if (q < na) {
+                    acc[q] = cmul_sel<R>(real, blk[(a0 + q) * m + b], x, acc[q]);
+                    if (VEL) accb[q] = cmul_sel<R>(real, bbl[(a0 + q) * m + b], x, accb[q]);
+                }
+            }
+        }
+        if (a0 == 0 && (k > 0 || ax.prev >= 0)) {   // bridge row s: the previous element's part
+            const cplx<R> *bp, *bq;
+            int mp, sp;
+            bool rp;
+            if (k > 0) {
+                mp = ax.m[k - 1]; sp = ax.s[k - 1]; rp = ax.real[k - 1];
+                bp = BLK + ax.off[k - 1] + (mp - 1) * mp; bq = BLKB + ax.off[k - 1] + (mp - 1) * mp;
+            } else {
+                mp = ax.prev_m; sp = s - (mp - 1); rp = ax.prev_real;
+                bp = BLK + ax.prev_off; bq = BLKB + ax.prev_off;
+            }
+            for (int b = 0; b < mp - 1; ++b) {
+                const int node = sp + b;   // global index along this axis
+                cplx<R> x;
+                if (node >= base) x = ROWS ? PS[(node - base) * RAD_STRIDE + line] : PS[line * RAD_STRIDE + node - base];
+                else x = ROWS ? pc[(size_t)node + (size_t)n * (c0 + line)] : pc[(size_t)(r0 + line) + (size_t)n * node];
+                acc[0] = cmul_sel<R>(rp, bp[b], x, acc[0]);
+                if (VEL) accb[0] = cmul_sel<R>(rp, bq[b], x, accb[0]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < RAD_CHUNK; ++q) {
+            if (q < na) {
+                const int node = s - base + a0 + q;
+                const int row = ROWS ? node : line, col = ROWS ? line : node;
+                if (ROWS) OS[row * RAD_STRIDE + col] = acc[q];
+                else OS[row * RAD_STRIDE + col] = cadd<R>(OS[row * RAD_STRIDE + col], acc[q]);
+                if (VEL) wout[(size_t)(r0 + row) + (size_t)n * (c0 + col) + nn * c] = accb[q];
+            }
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------------
 // Radial stencil kernel.  grid = (ntile * ntile, nc); one channel-tile per CTA.
-// Smem: PS[(rows+1) x RAD_STRIDE] staged psi (owned + right bridge), OS owned output,
-// W1S/W2S owned B-stencil results (velocity gauge only).
 // ---------------------------------------------------------------------------------
 template <typename R, bool VEL, bool SEP>
-__global__ void __launch_bounds__(RAD_THREADS)
+__global__ void __launch_bounds__(RAD_THREADS, 2)
 hpsi_radial_kernel(const DeviceTables<R> t, const TiledPlan<R> pl, const cplx<R> *__restrict__ psi,
-                   cplx<R> *__restrict__ out, cplx<R> *__restrict__ w1, cplx<R> *__restrict__ w2, R a2)
+                   cplx<R> *__restrict__ out, cplx<R> *__restrict__ w1, cplx<R> *__restrict__ w2, R a2, int blkmax)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cplx<R> *PS = reinterpret_cast<cplx<R> *>(smem_raw);
     cplx<R> *OS = PS + RAD_STRIDE * RAD_STRIDE;
-    cplx<R> *W1S = OS + RAD_TMAX * RAD_STRIDE;
-    cplx<R> *W2S = W1S + RAD_TMAX * RAD_STRIDE;
+    cplx<R> *B0 = OS + RAD_TMAX * RAD_STRIDE;        // electron-1 blocks (T), then B if VEL
+    cplx<R> *B0B = B0 + blkmax;
+    cplx<R> *B1 = B0 + (VEL ? 2 : 1) * blkmax;       // electron-2 blocks
+    cplx<R> *B1B = B1 + blkmax;
+    __shared__ AxisTile ax0, ax1;
 
-    const int n = pl.n, ne = pl.ne;
+    const int n = pl.n;
     const int ti = blockIdx.x % pl.ntile, tj = blockIdx.x / pl.ntile, c = blockIdx.y;
     const int ea = pl.tstart[ti], eb = pl.tstart[ti + 1];
     const int fa = pl.tstart[tj], fb = pl.tstart[tj + 1];
@@ -71,195 +186,99 @@ hpsi_radial_kernel(const DeviceTables<R> t, const TiledPlan<R> pl, const cplx<R>
     const size_t nn = (size_t)n * n;
     const cplx<R> *pc = psi + nn * c;
 
-    // stage psi rows [r0, r0+rs) x cols [c0, c0+cs): lanes along rows (contiguous i)
     for (int idx = threadIdx.x; idx < rs * cs; idx += blockDim.x) {
         const int a = idx % rs, b = idx / rs;
         PS[a * RAD_STRIDE + b] = pc[(size_t)(r0 + a) + (size_t)n * (c0 + b)];
     }
+    stage_axis<R>(pl, ax0, ea, eb, co, B0, B0B, VEL);
+    stage_axis<R>(pl, ax1, fa, fb, ro, B1, B1B, VEL);
+    __syncthreads();
+    radial_phase<R, VEL, true>(ax0, B0, B0B, PS, OS, co, r0, r0, c0, n, pc, w1, nn, c);
+    __syncthreads();
+    radial_phase<R, VEL, false>(ax1, B1, B1B, PS, OS, ro, c0, r0, c0, n, pc, w2, nn, c);
     __syncthreads();
 
-    // ---- phase 1: electron 1 (rows); item = (owned column, element, row chunk) -------
-    {
-        int nitems = 0;
-        for (int e = ea; e < eb; ++e) {
-            const int own = (e + 1 < ne ? pl.estart[e + 1] : n) - pl.estart[e];
-            nitems += co * ((own + RAD_CHUNK - 1) / RAD_CHUNK);
-        }
-        for (int item = threadIdx.x; item < nitems; item += blockDim.x) {
-            int rest = item, e = ea;
-            for (; e < eb; ++e) {
-                const int own = (e + 1 < ne ? pl.estart[e + 1] : n) - pl.estart[e];
-                const int cnt = co * ((own + RAD_CHUNK - 1) / RAD_CHUNK);
-                if (rest < cnt) break;
-                rest -= cnt;
-            }
-            const int col = rest % co, chunk = rest / co;
-            const int s = pl.estart[e], m = elem_size(pl.estart, e, ne, n);
-            const int own = (e + 1 < ne ? pl.estart[e + 1] : n) - s;
-            const int a0 = chunk * RAD_CHUNK, na = min(RAD_CHUNK, own - a0);
-            const cplx<R> *blk = pl.blocks + pl.eoff[e];
-            const cplx<R> *bbl = pl.bblocks + pl.eoff[e];
-            const bool real = pl.ereal[e];
-            cplx<R> acc[RAD_CHUNK], accb[RAD_CHUNK];
-#pragma unroll
-            for (int q = 0; q < RAD_CHUNK; ++q) { acc[q] = mk<R>(0, 0); accb[q] = mk<R>(0, 0); }
-            for (int b = 0; b < m; ++b) {
-                const cplx<R> x = PS[(s - r0 + b) * RAD_STRIDE + col];
-#pragma unroll
-                for (int q = 0; q < RAD_CHUNK; ++q) {
-                    if (q < na) {
-                        acc[q] = cmul_sel<R>(real, blk[(a0 + q) * m + b], x, acc[q]);
-                        if (VEL) accb[q] = cmul_sel<R>(real, bbl[(a0 + q) * m + b], x, accb[q]);
-                    }
-                }
-            }
-            if (a0 == 0 && e > 0) {   // left bridge row s: the previous element's part
-                const int sp = pl.estart[e - 1], mp = elem_size(pl.estart, e - 1, ne, n);
-                const cplx<R> *bp = pl.blocks + pl.eoff[e - 1] + (size_t)(mp - 1) * mp;
-                const cplx<R> *bq = pl.bblocks + pl.eoff[e - 1] + (size_t)(mp - 1) * mp;
-                const bool rp = pl.ereal[e - 1];
-                for (int b = 0; b < mp - 1; ++b) {
-                    const int row = sp + b;
-                    const cplx<R> x = row >= r0 ? PS[(row - r0) * RAD_STRIDE + col]
-                                                : pc[(size_t)row + (size_t)n * (c0 + col)];
-                    acc[0] = cmul_sel<R>(rp, bp[b], x, acc[0]);
-                    if (VEL) accb[0] = cmul_sel<R>(rp, bq[b], x, accb[0]);
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < RAD_CHUNK; ++q) {
-                if (q < na) {
-                    const int row = s - r0 + a0 + q;
-                    OS[row * RAD_STRIDE + col] = acc[q];
-                    if (VEL) W1S[row * RAD_STRIDE + col] = accb[q];
-                }
-            }
-        }
-    }
-    __syncthreads();
-
-    // ---- phase 2: electron 2 (columns); item = (owned row, element, column chunk) -----
-    {
-        int nitems = 0;
-        for (int f = fa; f < fb; ++f) {
-            const int own = (f + 1 < ne ? pl.estart[f + 1] : n) - pl.estart[f];
-            nitems += ro * ((own + RAD_CHUNK - 1) / RAD_CHUNK);
-        }
-        for (int item = threadIdx.x; item < nitems; item += blockDim.x) {
-            int rest = item, f = fa;
-            for (; f < fb; ++f) {
-                const int own = (f + 1 < ne ? pl.estart[f + 1] : n) - pl.estart[f];
-                const int cnt = ro * ((own + RAD_CHUNK - 1) / RAD_CHUNK);
-                if (rest < cnt) break;
-                rest -= cnt;
-            }
-            const int row = rest % ro, chunk = rest / ro;
-            const int s = pl.estart[f], m = elem_size(pl.estart, f, ne, n);
-            const int own = (f + 1 < ne ? pl.estart[f + 1] : n) - s;
-            const int a0 = chunk * RAD_CHUNK, na = min(RAD_CHUNK, own - a0);
-            const cplx<R> *blk = pl.blocks + pl.eoff[f];
-            const cplx<R> *bbl = pl.bblocks + pl.eoff[f];
-            const bool real = pl.ereal[f];
-            cplx<R> acc[RAD_CHUNK], accb[RAD_CHUNK];
-#pragma unroll
-            for (int q = 0; q < RAD_CHUNK; ++q) { acc[q] = mk<R>(0, 0); accb[q] = mk<R>(0, 0); }
-            for (int b = 0; b < m; ++b) {
-                const cplx<R> x = PS[row * RAD_STRIDE + (s - c0 + b)];
-#pragma unroll
-                for (int q = 0; q < RAD_CHUNK; ++q) {
-                    if (q < na) {
-                        acc[q] = cmul_sel<R>(real, blk[(a0 + q) * m + b], x, acc[q]);
-                        if (VEL) accb[q] = cmul_sel<R>(real, bbl[(a0 + q) * m + b], x, accb[q]);
-                    }
-                }
-            }
-            if (a0 == 0 && f > 0) {
-                const int sp = pl.estart[f - 1], mp = elem_size(pl.estart, f - 1, ne, n);
-                const cplx<R> *bp = pl.blocks + pl.eoff[f - 1] + (size_t)(mp - 1) * mp;
-                const cplx<R> *bq = pl.bblocks + pl.eoff[f - 1] + (size_t)(mp - 1) * mp;
-                const bool rp = pl.ereal[f - 1];
-                for (int b = 0; b < mp - 1; ++b) {
-                    const int colg = sp + b;
-                    const cplx<R> x = colg >= c0 ? PS[row * RAD_STRIDE + (colg - c0)]
-                                                 : pc[(size_t)(r0 + row) + (size_t)n * colg];
-                    acc[0] = cmul_sel<R>(rp, bp[b], x, acc[0]);
-                    if (VEL) accb[0] = cmul_sel<R>(rp, bq[b], x, accb[0]);
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < RAD_CHUNK; ++q) {
-                if (q < na) {
-                    const int col = s - c0 + a0 + q;
-                    OS[row * RAD_STRIDE + col] = cadd<R>(OS[row * RAD_STRIDE + col], acc[q]);
-                    if (VEL) W2S[row * RAD_STRIDE + col] = accb[q];
-                }
-            }
-        }
-    }
-    __syncthreads();
-
-    // ---- epilogue: diagonal (+|A|^2), write the radial part (and W) ------------------
     for (int idx = threadIdx.x; idx < ro * co; idx += blockDim.x) {
         const int a = idx % ro, b = idx / ro;
         const int i = r0 + a, j = c0 + b;
         const size_t p = (size_t)i + (size_t)n * j;
         const cplx<R> x = PS[a * RAD_STRIDE + b];
-        cplx<R> d = SEP ? cadd<R>(ldg<R>(t.d1 + i + (size_t)n * c), ldg<R>(t.d2 + j + (size_t)n * c))
-                        : ldg<R>(t.diag + p + nn * c);
+        const cplx<R> d = SEP ? cadd<R>(ldg<R>(t.d1 + i + (size_t)n * c), ldg<R>(t.d2 + j + (size_t)n * c))
+                              : ldg<R>(t.diag + p + nn * c);
         cplx<R> v = cfma<R>(d, x, OS[a * RAD_STRIDE + b]);
-        if (VEL) {
-            v = rfma<R>(a2, x, v);
-            w1[p + nn * c] = W1S[a * RAD_STRIDE + b];
-            w2[p + nn * c] = W2S[a * RAD_STRIDE + b];
-        }
+        if (VEL) v = rfma<R>(a2, x, v);
         out[p + nn * c] = v;
     }
 }
 
 // ---------------------------------------------------------------------------------
-// Field contraction of the dipole edges: coef_k = field . dcoef(:, k), zero below 1e-30
-// (the skip of src/kernels.f90:145).
+// Channel-mixing kernel.  CTA = NP consecutive flattened points p = i + n j.
+// Shared memory: PSI[c][NP], RAD[lam][NP], wide Coulomb edges (source offset, MIX_GROUP
+// coefficients), group x lam offsets, wide dipole edges and the field-contracted
+// dipole coefficients coef_k = field . dcoef(:, k) (zero below 1e-30, the skip of
+// src/kernels.f90:145).  A warp task is (32 points, one output group).
 // ---------------------------------------------------------------------------------
+template <typename R> struct MixSmem {
+    cplx<R> *psi, *rad, *coef;
+    R *wcoef, *ldiff;
+    int *wsrc, *wptr, *dsrc, *del, *dedge;
+};
+
 template <typename R>
-__global__ void contract_field_kernel(const cplx<R> *__restrict__ dcoef, int nd, R f0, R f1, R f2,
-                                      cplx<R> *__restrict__ coef)
+__device__ __forceinline__ MixSmem<R> mix_layout(unsigned char *raw, const TiledPlan<R> &pl, int nd, int np)
 {
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nd; k += gridDim.x * blockDim.x) {
-        cplx<R> v = cscale<R>(f0, dcoef[3 * k]);
-        v = rfma<R>(f1, dcoef[3 * k + 1], v);
-        v = rfma<R>(f2, dcoef[3 * k + 2], v);
-        if (sqrt(cabs2<R>(v)) < (R)1e-30) v = mk<R>(0, 0);
-        coef[k] = v;
-    }
+    MixSmem<R> s;
+    s.psi = reinterpret_cast<cplx<R> *>(raw);
+    s.rad = s.psi + (size_t)pl.nc * np;
+    s.coef = s.rad + (size_t)pl.nlam * np;
+    s.wcoef = reinterpret_cast<R *>(s.coef + max(nd, 1));
+    s.ldiff = s.wcoef + (size_t)pl.nwide * MIX_GROUP;
+    s.wsrc = reinterpret_cast<int *>(s.ldiff + max(nd, 1));
+    s.wptr = s.wsrc + pl.nwide;
+    s.dsrc = s.wptr + pl.ng * pl.nlam + 1;
+    s.del = s.dsrc + pl.nwd;
+    s.dedge = s.del + pl.nwd;
+    return s;
 }
 
-// ---------------------------------------------------------------------------------
-// Channel-mixing kernel.  CTA = NP consecutive flattened points p = i + n j, all
-// channels staged as PSI[c][NP]; multipoles staged as RAD[lam][NP].  A warp task is
-// (32 points, one output group); accumulators live in registers.
-// ---------------------------------------------------------------------------------
 template <typename R, bool VEL, int NP>
 __global__ void __launch_bounds__(256)
 hpsi_mix_kernel(const DeviceTables<R> t, const TiledPlan<R> pl, const cplx<R> *__restrict__ psi,
                 cplx<R> *__restrict__ out, const cplx<R> *__restrict__ w1, const cplx<R> *__restrict__ w2,
-                const cplx<R> *__restrict__ coef, cplx<R> beta, cplx<R> gamma)
+                R f0, R f1, R f2, cplx<R> beta, cplx<R> gamma)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cplx<R> *PSI = reinterpret_cast<cplx<R> *>(smem_raw);
-    cplx<R> *RAD = PSI + (size_t)pl.nc * NP;
-    const int n = pl.n, nc = pl.nc, nlam = pl.nlam;
+    const int n = pl.n, nc = pl.nc, nlam = pl.nlam, nd = t.nd;
+    const MixSmem<R> S = mix_layout<R>(smem_raw, pl, nd, NP);
     const size_t nn = (size_t)n * n;
     const size_t p0 = (size_t)blockIdx.x * NP;
     const int np = (int)min((size_t)NP, nn - p0);
 
     for (int idx = threadIdx.x; idx < nc * NP; idx += blockDim.x) {
         const int q = idx % NP, cc = idx / NP;
-        PSI[idx] = q < np ? psi[p0 + q + nn * cc] : mk<R>(0, 0);
+        S.psi[idx] = q < np ? psi[p0 + q + nn * cc] : mk<R>(0, 0);
     }
     for (int idx = threadIdx.x; idx < nlam * NP; idx += blockDim.x) {
         const int q = idx % NP, lam = idx / NP;
-        RAD[idx] = q < np ? ldg<R>(t.rad + p0 + q + nn * lam) : mk<R>(0, 0);
+        S.rad[idx] = q < np ? ldg<R>(t.rad + p0 + q + nn * lam) : mk<R>(0, 0);
     }
+    for (int k = threadIdx.x; k < nd; k += blockDim.x) {
+        const cplx<R> *dk = t.dcoef + 3 * (size_t)k;
+        cplx<R> v = cscale<R>(f0, dk[0]);
+        v = rfma<R>(f1, dk[1], v);
+        v = rfma<R>(f2, dk[2], v);
+        if (sqrt(cabs2<R>(v)) < (R)1e-30) v = mk<R>(0, 0);
+        S.coef[k] = v;
+        S.ldiff[k] = t.ldiff[k];
+    }
+    for (int k = threadIdx.x; k < pl.nwide * MIX_GROUP; k += blockDim.x) S.wcoef[k] = pl.wcoef[k];
+    for (int k = threadIdx.x; k < pl.nwide; k += blockDim.x) S.wsrc[k] = pl.wsrc[k] * NP;
+    for (int k = threadIdx.x; k <= pl.ng * nlam; k += blockDim.x) S.wptr[k] = pl.wptr[k];
+    for (int k = threadIdx.x; k < pl.nwd; k += blockDim.x) {
+        S.dsrc[k] = pl.dwsrc[k];
+        S.del[k] = pl.dwel[k];
+    }
+    for (int k = threadIdx.x; k < pl.nwd * MIX_GROUP; k += blockDim.x) S.dedge[k] = pl.dwedge[k];
     __syncthreads();
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
@@ -276,47 +295,49 @@ hpsi_mix_kernel(const DeviceTables<R> t, const TiledPlan<R> pl, const cplx<R> *_
             ch[d] = __ldg(pl.gch + g * MIX_GROUP + d);
             acc[d] = (valid && ch[d] >= 0) ? out[p + nn * ch[d]] : mk<R>(0, 0);
         }
-        // Coulomb multipoles, grouped by lambda
+        const int *wp = S.wptr + g * nlam;
         for (int lam = 0; lam < nlam; ++lam) {
-            const int k0 = __ldg(pl.wptr + g * nlam + lam), k1 = __ldg(pl.wptr + g * nlam + lam + 1);
+            const int k0 = wp[lam], k1 = wp[lam + 1];
             if (k0 == k1) continue;
             cplx<R> tsum[MIX_GROUP];
 #pragma unroll
             for (int d = 0; d < MIX_GROUP; ++d) tsum[d] = mk<R>(0, 0);
+#pragma unroll 2
             for (int k = k0; k < k1; ++k) {
-                const cplx<R> x = PSI[__ldg(pl.wsrc + k) * NP + q];
+                const cplx<R> x = S.psi[S.wsrc[k] + q];
+                const R *cf = S.wcoef + k * MIX_GROUP;
 #pragma unroll
-                for (int d = 0; d < MIX_GROUP; ++d) tsum[d] = rfma<R>(__ldg(pl.wcoef + k * MIX_GROUP + d), x, tsum[d]);
+                for (int d = 0; d < MIX_GROUP; ++d) tsum[d] = rfma<R>(cf[d], x, tsum[d]);
             }
-            const cplx<R> rl = RAD[lam * NP + q];
+            const cplx<R> rl = S.rad[lam * NP + q];
 #pragma unroll
             for (int d = 0; d < MIX_GROUP; ++d) acc[d] = cfma<R>(rl, tsum[d], acc[d]);
         }
-        // dipole couplings
         const int k0 = __ldg(pl.dwptr + g), k1 = __ldg(pl.dwptr + g + 1);
         if (k0 < k1 && valid) {
             const int i = (int)(p % n), j = (int)(p / n);
+            const cplx<R> r1 = ldg<R>(t.r + i), r2 = ldg<R>(t.r + j);
+            const cplx<R> h1 = ldg<R>(t.hinv + i), h2 = ldg<R>(t.hinv + j);
             for (int k = k0; k < k1; ++k) {
-                const int s = __ldg(pl.dwsrc + k);
-                const int el = __ldg(pl.dwel + k);
-                const int a = el == 1 ? i : j;
-                const cplx<R> x = PSI[s * NP + q];
+                const int s = S.dsrc[k];
+                const bool first = S.del[k] == 1;
+                const cplx<R> x = S.psi[s * NP + q];
                 if (!VEL) {
-                    const cplx<R> y = cmul<R>(ldg<R>(t.r + a), x);
+                    const cplx<R> y = cmul<R>(first ? r1 : r2, x);
 #pragma unroll
                     for (int d = 0; d < MIX_GROUP; ++d) {
-                        const int kk = __ldg(pl.dwedge + k * MIX_GROUP + d);
-                        if (kk >= 0) acc[d] = cfma<R>(ldg<R>(coef + kk), y, acc[d]);
+                        const int kk = S.dedge[k * MIX_GROUP + d];
+                        if (kk >= 0) acc[d] = cfma<R>(S.coef[kk], y, acc[d]);
                     }
                 } else {
-                    const cplx<R> w = (el == 1 ? w1 : w2)[p + nn * s];
-                    const cplx<R> hx = cmul<R>(ldg<R>(t.hinv + a), x);
+                    const cplx<R> w = (first ? w1 : w2)[p + nn * s];
+                    const cplx<R> hx = cmul<R>(first ? h1 : h2, x);
 #pragma unroll
                     for (int d = 0; d < MIX_GROUP; ++d) {
-                        const int kk = __ldg(pl.dwedge + k * MIX_GROUP + d);
+                        const int kk = S.dedge[k * MIX_GROUP + d];
                         if (kk >= 0) {
-                            const cplx<R> part = rfma<R>(__ldg(t.ldiff + kk), hx, w);
-                            const cplx<R> cf = ldg<R>(coef + kk);
+                            const cplx<R> part = rfma<R>(S.ldiff[kk], hx, w);
+                            const cplx<R> cf = S.coef[kk];
                             acc[d] = cfma<R>(mk<R>(-cf.y, cf.x), part, acc[d]);   // i coef part
                         }
                     }
@@ -326,19 +347,23 @@ hpsi_mix_kernel(const DeviceTables<R> t, const TiledPlan<R> pl, const cplx<R> *_
         if (valid) {
 #pragma unroll
             for (int d = 0; d < MIX_GROUP; ++d)
-                if (ch[d] >= 0) out[p + nn * ch[d]] = cfma<R>(gamma, acc[d], cmul<R>(beta, PSI[ch[d] * NP + q]));
+                if (ch[d] >= 0) out[p + nn * ch[d]] = cfma<R>(gamma, acc[d], cmul<R>(beta, S.psi[ch[d] * NP + q]));
         }
     }
 }
 
-template <typename R> static size_t radial_smem(bool vel)
+template <typename R> size_t radial_smem(bool vel, int blkmax)
 {
-    return sizeof(cplx<R>) * ((size_t)RAD_STRIDE * RAD_STRIDE + (vel ? 3 : 1) * (size_t)RAD_TMAX * RAD_STRIDE);
+    return sizeof(cplx<R>) * ((size_t)RAD_STRIDE * RAD_STRIDE + (size_t)RAD_TMAX * RAD_STRIDE +
+                              (vel ? 4 : 2) * (size_t)blkmax);
 }
 
-template <typename R> static size_t mix_smem(int nc, int nlam, int np)
+template <typename R> size_t mix_smem(const TiledPlan<R> &pl, int nd, int np)
 {
-    return sizeof(cplx<R>) * (size_t)(nc + nlam) * np;
+    const size_t c = sizeof(cplx<R>) * ((size_t)(pl.nc + pl.nlam) * np + std::max(nd, 1));
+    const size_t r = sizeof(R) * ((size_t)pl.nwide * MIX_GROUP + std::max(nd, 1));
+    const size_t i = sizeof(int) * ((size_t)pl.nwide + pl.ng * pl.nlam + 1 + pl.nwd * (2 + MIX_GROUP));
+    return c + r + i + 64;
 }
 
 template <typename R>
@@ -346,31 +371,33 @@ int launch_hpsi_tiled(he_operator *h, const DeviceTables<R> &t, const TiledPlan<
                       cplx<R> *w1, cplx<R> *w2, const cplx<R> *psi, cplx<R> *out, const double *field, int velocity,
                       cplx<R> beta, cplx<R> gamma, cudaStream_t stream)
 {
+    (void)coef;
     const R f0 = (R)field[0], f1 = (R)field[1], f2 = (R)field[2];
     const R a2 = (R)(field[0] * field[0] + field[1] * field[1] + field[2] * field[2]);
-    if (t.nd > 0) contract_field_kernel<R><<<1, 256, 0, stream>>>(t.dcoef, t.nd, f0, f1, f2, coef);
     const dim3 rgrid(pl.ntile * pl.ntile, pl.nc);
-    const size_t rs = radial_smem<R>(velocity);
+    const int blkmax = h->plan.blkmax;
+    const size_t rs = radial_smem<R>(velocity, blkmax);
 #define HE_RADIAL(V, S)                                                                                  \
     do {                                                                                                 \
         auto kern = hpsi_radial_kernel<R, V, S>;                                                         \
         HE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rs));   \
-        kern<<<rgrid, RAD_THREADS, rs, stream>>>(t, pl, psi, out, w1, w2, a2);                           \
+        kern<<<rgrid, RAD_THREADS, rs, stream>>>(t, pl, psi, out, w1, w2, a2, blkmax);                   \
     } while (0)
     if (velocity) { if (t.diag_separable) HE_RADIAL(true, true); else HE_RADIAL(true, false); }
     else { if (t.diag_separable) HE_RADIAL(false, true); else HE_RADIAL(false, false); }
 #undef HE_RADIAL
     HE_CUDA_TRY(cudaGetLastError());
     const size_t nn = (size_t)pl.n * pl.n;
-    const size_t limit = 200 * 1024;
+    const size_t limit = 110 * 1024;   // two CTAs per SM
+    const int np = (sizeof(R) == 4 && mix_smem<R>(pl, t.nd, 128) <= limit) ? 128
+                 : mix_smem<R>(pl, t.nd, 64) <= limit ? 64 : 32;
 #define HE_MIX(V, NP)                                                                                    \
     do {                                                                                                 \
         auto kern = hpsi_mix_kernel<R, V, NP>;                                                           \
-        const size_t ms = mix_smem<R>(pl.nc, pl.nlam, NP);                                               \
+        const size_t ms = mix_smem<R>(pl, t.nd, NP);                                                     \
         HE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ms));   \
-        kern<<<(unsigned)((nn + NP - 1) / NP), 256, ms, stream>>>(t, pl, psi, out, w1, w2, coef, beta, gamma); \
+        kern<<<(unsigned)((nn + NP - 1) / NP), 256, ms, stream>>>(t, pl, psi, out, w1, w2, f0, f1, f2, beta, gamma); \
     } while (0)
-    const int np = mix_smem<R>(pl.nc, pl.nlam, 128) <= limit ? 128 : mix_smem<R>(pl.nc, pl.nlam, 64) <= limit ? 64 : 32;
     if (velocity) {
         if (np == 128) HE_MIX(true, 128); else if (np == 64) HE_MIX(true, 64); else HE_MIX(true, 32);
     } else {
@@ -378,7 +405,6 @@ int launch_hpsi_tiled(he_operator *h, const DeviceTables<R> &t, const TiledPlan<
     }
 #undef HE_MIX
     HE_CUDA_TRY(cudaGetLastError());
-    (void)h;
     return HE_OK;
 }
 
@@ -389,223 +415,12 @@ template int launch_hpsi_tiled<float>(he_operator *, const DeviceTables<float> &
                                       float2 *, float2 *, const float2 *, float2 *, const double *, int, float2,
                                       float2, cudaStream_t);
 
-bool tiled_fits(int nc, int nlam, size_t elem)
+// The mixing kernel must fit two CTAs of 32 points per SM in complex128.
+bool tiled_fits(const he_plan_host &P, int nc, int nd)
 {
-    return elem * (size_t)(nc + nlam) * 32 <= 200 * 1024;
+    TiledPlan<double> pl{};
+    pl.nc = nc; pl.nlam = P.nlam; pl.ng = P.ng; pl.nwide = (int)P.wsrc.size(); pl.nwd = (int)P.dwsrc.size();
+    return mix_smem<double>(pl, nd, 32) <= 110 * 1024 && radial_smem<double>(true, P.blkmax) <= 110 * 1024;
 }
 
 }  // namespace he
-
-// =====================================================================================
-// Host planning
-// =====================================================================================
-namespace {
-
-struct UnionFind {
-    std::vector<int> p;
-    explicit UnionFind(int n) : p(n) { std::iota(p.begin(), p.end(), 0); }
-    int find(int x) { while (p[x] != x) x = p[x] = p[p[x]]; return x; }
-    void join(int a, int b) { p[find(a)] = find(b); }
-};
-
-}  // namespace
-
-// Build the tiled plan from the reference's tables.  Returns false (and the generic
-// kernel is used) when the kinetic matrix is not block banded by elements, an element
-// is too large for a shared-memory tile, or a Coulomb coefficient is not real.
-bool he_build_plan(he_plan_host &P, int n, int nc, const int *ptr, const int *col, const double *tv, int nv,
-                   const int *vptr, const int *vc, const int *vl, const double *vcoef, int nlam, int nd,
-                   const int *dptr, const int *dc, const int *de, const double *r)
-{
-    using he::MIX_GROUP;
-    P = he_plan_host();
-    // --- elements from the first column of each row ---------------------------------
-    std::vector<int> first(n), last(n);
-    std::set<int> starts;
-    for (int i = 0; i < n; ++i) {
-        if (ptr[i + 1] == ptr[i]) return false;
-        int lo = n, hi = -1;
-        for (int k = ptr[i]; k < ptr[i + 1]; ++k) { lo = std::min(lo, col[k]); hi = std::max(hi, col[k]); }
-        first[i] = lo; last[i] = hi;
-        starts.insert(lo);
-    }
-    if (!starts.count(0)) return false;
-    P.estart.assign(starts.begin(), starts.end());
-    const int ne = (int)P.estart.size();
-    P.estart.push_back(n);
-    P.ne = ne;
-    auto esize = [&](int e) { return e + 1 < ne ? P.estart[e + 1] - P.estart[e] + 1 : n - P.estart[e]; };
-    // every entry of row i (owned by element e) must lie in element e, or in e-1 for a bridge row
-    for (int e = 0; e < ne; ++e) {
-        const int s = P.estart[e], m = esize(e);
-        if (m > he::RAD_TMAX + 1 || m < 2) return false;
-        const int own_end = e + 1 < ne ? P.estart[e + 1] : n;
-        for (int i = s; i < own_end; ++i) {
-            const int lo_ok = (i == s && e > 0) ? P.estart[e - 1] : s;
-            if (first[i] < lo_ok || last[i] > s + m - 1) return false;
-        }
-    }
-    // --- dense element blocks of T and of B = T (r_b - r_a) ---------------------------
-    P.eoff.assign(ne + 1, 0);
-    for (int e = 0; e < ne; ++e) P.eoff[e + 1] = P.eoff[e] + esize(e) * esize(e);
-    P.blocks.assign(2 * (size_t)P.eoff[ne], 0.0);
-    P.bblocks.assign(2 * (size_t)P.eoff[ne], 0.0);
-    P.ereal.assign(ne, 1);
-    for (int e = 0; e < ne; ++e) {
-        const int s = P.estart[e], m = esize(e);
-        P.maxm = std::max(P.maxm, m);
-        for (int a = 0; a < m; ++a) {
-            const int i = s + a;
-            for (int k = ptr[i]; k < ptr[i + 1]; ++k) {
-                const int b = col[k] - s;
-                if (b < 0 || b >= m) continue;   // the previous element's part of a bridge row
-                const std::complex<double> T(tv[2 * k], tv[2 * k + 1]);
-                const std::complex<double> ra(r[2 * i], r[2 * i + 1]), rb(r[2 * col[k]], r[2 * col[k] + 1]);
-                const std::complex<double> B = T * (rb - ra);
-                const size_t o = 2 * ((size_t)P.eoff[e] + (size_t)a * m + b);
-                P.blocks[o] = T.real(); P.blocks[o + 1] = T.imag();
-                P.bblocks[o] = B.real(); P.bblocks[o + 1] = B.imag();
-                if (T.imag() != 0.0 || B.imag() != 0.0) P.ereal[e] = 0;
-            }
-        }
-    }
-    // --- radial tiles: up to RAD_ELEMS elements and RAD_TMAX owned nodes --------------
-    P.tstart.push_back(0);
-    for (int e = 0; e < ne;) {
-        int cnt = 0, own = 0, f = e;
-        while (f < ne && cnt < he::RAD_ELEMS) {
-            const int o = (f + 1 < ne ? P.estart[f + 1] : n) - P.estart[f];
-            if (own + o > he::RAD_TMAX) break;
-            own += o; ++cnt; ++f;
-        }
-        if (cnt == 0) return false;
-        e = f;
-        P.tstart.push_back(e);
-    }
-    P.ntile = (int)P.tstart.size() - 1;
-    // --- output groups: channels of one Coulomb component with shared sources ---------
-    for (int k = 0; k < nv; ++k)
-        if (vcoef[2 * k + 1] != 0.0) return false;
-    P.nlam = nlam;
-    UnionFind uf(nc);
-    std::vector<std::set<std::pair<int, int>>> src(nc);
-    for (int c = 0; c < nc; ++c)
-        for (int k = vptr[c]; k < vptr[c + 1]; ++k) { uf.join(c, vc[k]); src[c].insert({vc[k], vl[k]}); }
-    std::vector<int> assigned(nc, 0);
-    std::vector<std::vector<int>> groups;
-    for (int c = 0; c < nc; ++c) {
-        if (assigned[c]) continue;
-        std::vector<int> grp{c};
-        assigned[c] = 1;
-        while ((int)grp.size() < MIX_GROUP) {
-            int best = -1, score = -1;
-            for (int x = 0; x < nc; ++x) {
-                if (assigned[x] || uf.find(x) != uf.find(c)) continue;
-                int s = 0;
-                for (auto &e : src[x]) s += (int)src[c].count(e);
-                if (s > score) { score = s; best = x; }
-            }
-            if (best < 0) break;
-            grp.push_back(best);
-            assigned[best] = 1;
-        }
-        groups.push_back(grp);
-    }
-    P.ng = (int)groups.size();
-    P.gch.assign((size_t)P.ng * MIX_GROUP, -1);
-    P.wptr.assign((size_t)P.ng * nlam + 1, 0);
-    P.dwptr.assign(P.ng + 1, 0);
-    for (int g = 0; g < P.ng; ++g) {
-        const auto &grp = groups[g];
-        for (int d = 0; d < (int)grp.size(); ++d) P.gch[(size_t)g * MIX_GROUP + d] = grp[d];
-        for (int lam = 0; lam < nlam; ++lam) {
-            std::map<int, std::vector<double>> wide;
-            for (int d = 0; d < (int)grp.size(); ++d)
-                for (int k = vptr[grp[d]]; k < vptr[grp[d] + 1]; ++k)
-                    if (vl[k] == lam) {
-                        auto &w = wide[vc[k]];
-                        if (w.empty()) w.assign(MIX_GROUP, 0.0);
-                        w[d] += vcoef[2 * k];
-                    }
-            for (auto &kv : wide) {
-                P.wsrc.push_back(kv.first);
-                P.wcoef.insert(P.wcoef.end(), kv.second.begin(), kv.second.end());
-            }
-            P.wptr[(size_t)g * nlam + lam + 1] = (int)P.wsrc.size();
-        }
-        // dipole edges keyed by (source, electron); repeated keys of one channel open a new slot
-        std::vector<std::pair<std::pair<int, int>, std::vector<int>>> dw;
-        for (int d = 0; d < (int)grp.size(); ++d)
-            for (int k = dptr[grp[d]]; k < dptr[grp[d] + 1]; ++k) {
-                bool placed = false;
-                for (auto &slot : dw)
-                    if (slot.first == std::make_pair(dc[k], de[k]) && slot.second[d] < 0) {
-                        slot.second[d] = k; placed = true; break;
-                    }
-                if (!placed) {
-                    std::vector<int> v(MIX_GROUP, -1);
-                    v[d] = k;
-                    dw.push_back({{dc[k], de[k]}, v});
-                }
-            }
-        for (auto &slot : dw) {
-            P.dwsrc.push_back(slot.first.first);
-            P.dwel.push_back(slot.first.second);
-            P.dwedge.insert(P.dwedge.end(), slot.second.begin(), slot.second.end());
-        }
-        P.dwptr[g + 1] = (int)P.dwsrc.size();
-    }
-    (void)nd;
-    P.ok = true;
-    return true;
-}
-
-// ---------------------------------------------------------------------------------
-// Planner inspection (host only, no GPU needed): build the plan for a set of tables
-// and copy its arrays out, so the tile and group layout can be checked on the CPU.
-// ---------------------------------------------------------------------------------
-extern "C" void *he_plan_build(int n, int nc, const int *ptr, const int *col, const double *tv, int nv,
-                               const int *vptr, const int *vc, const int *vl, const double *vcoef, int nlam, int nd,
-                               const int *dptr, const int *dc, const int *de, const double *r)
-{
-    he_plan_host *P = new he_plan_host();
-    he_build_plan(*P, n, nc, ptr, col, tv, nv, vptr, vc, vl, vcoef, nlam, nd, dptr, dc, de, r);
-    return P;
-}
-
-extern "C" void he_plan_free(void *plan) { delete static_cast<he_plan_host *>(plan); }
-
-// which: 0 estart, 1 tstart, 2 eoff, 3 ereal, 4 gch, 5 wptr, 6 wsrc, 7 dwptr, 8 dwsrc, 9 dwel, 10 dwedge,
-//        20 blocks (interleaved complex), 21 bblocks, 22 wcoef, 30 scalars {ok, ne, ntile, ng, nlam, maxm}.
-// Returns the element count; copies when dst != NULL.
-extern "C" long long he_plan_array(void *plan, int which, void *dst)
-{
-    const he_plan_host &P = *static_cast<he_plan_host *>(plan);
-    const std::vector<int> *vi = nullptr;
-    const std::vector<double> *vd = nullptr;
-    switch (which) {
-    case 0: vi = &P.estart; break;
-    case 1: vi = &P.tstart; break;
-    case 2: vi = &P.eoff; break;
-    case 3: vi = &P.ereal; break;
-    case 4: vi = &P.gch; break;
-    case 5: vi = &P.wptr; break;
-    case 6: vi = &P.wsrc; break;
-    case 7: vi = &P.dwptr; break;
-    case 8: vi = &P.dwsrc; break;
-    case 9: vi = &P.dwel; break;
-    case 10: vi = &P.dwedge; break;
-    case 20: vd = &P.blocks; break;
-    case 21: vd = &P.bblocks; break;
-    case 22: vd = &P.wcoef; break;
-    case 30: {
-        const int s[6] = {P.ok, P.ne, P.ntile, P.ng, P.nlam, P.maxm};
-        if (dst) memcpy(dst, s, sizeof(s));
-        return 6;
-    }
-    default: return -1;
-    }
-    if (vi) { if (dst) memcpy(dst, vi->data(), vi->size() * sizeof(int)); return (long long)vi->size(); }
-    if (dst) memcpy(dst, vd->data(), vd->size() * sizeof(double));
-    return (long long)vd->size();
-}

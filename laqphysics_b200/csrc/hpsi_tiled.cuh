@@ -23,7 +23,7 @@ template <typename R> struct TiledPlan {
     const cplx<R> *bblocks;         // same layout, B = T (r_b - r_a) (velocity-gauge commutator)
     const int *ereal;               // 1 if the element block is real
     // channel mixing
-    int ng, nlam, nwd;
+    int ng, nlam, nwd, nwide;       // groups, multipoles, wide dipole edges, wide Coulomb edges
     const int *gch;                 // ng x MIX_GROUP output channels (-1 = padding)
     const int *wptr;                // ng*nlam+1 wide Coulomb edge offsets, (g, lam) major
     const int *wsrc;                // source channel per wide edge
@@ -42,4 +42,5 @@ struct he_plan_host {
     std::vector<int> estart, tstart, eoff, ereal, gch, wptr, wsrc, dwptr, dwsrc, dwel, dwedge;
     std::vector<double> blocks, bblocks, wcoef;   // complex as interleaved doubles for blocks
     int ne = 0, ntile = 0, ng = 0, nlam = 0, maxm = 0;
+    int blkmax = 0;   // max over tiles and axes of staged block entries (previous row + sum m^2)
 };

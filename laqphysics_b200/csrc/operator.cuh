@@ -37,5 +37,5 @@ template <typename R>
 int launch_hpsi_tiled(he_operator *h, const DeviceTables<R> &t, const TiledPlan<R> &pl, cplx<R> *coef, cplx<R> *w1,
                       cplx<R> *w2, const cplx<R> *psi, cplx<R> *out, const double *field, int velocity,
                       cplx<R> beta, cplx<R> gamma, cudaStream_t stream);
-bool tiled_fits(int nc, int nlam, size_t elem);
+bool tiled_fits(const he_plan_host &P, int nc, int nd);
 }  // namespace he

@@ -1,0 +1,194 @@
+// Complex128 vector primitives of the GMRES / CF4 drivers (python/implicit.py:45-109):
+// axpby, norms with deterministic two-stage reductions, residual norms, Jacobi
+// scaling, Hessenberg column transfer and basis combinations with host coefficients.
+#include <vector>
+
+#include "common.cuh"
+#include "krylov.cuh"
+#include "operator.cuh"
+
+namespace he {
+
+__global__ void __launch_bounds__(KRYLOV_THREADS)
+axpby_kernel(size_t n, double2 a, const double2 *x, double2 b, const double2 *y, double2 *out)
+{
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x)
+        out[p] = cfma<double>(a, x[p], cmul<double>(b, y[p]));
+}
+
+// r = b - t (written when r != nullptr) and per-block |b - t|^2 (t == nullptr: |b|^2)
+__global__ void __launch_bounds__(KRYLOV_THREADS)
+residual_kernel(size_t n, const double2 *b, const double2 *t, double2 *r, double *partial)
+{
+    double s = 0;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        const double2 v = t ? csub<double>(b[p], t[p]) : b[p];
+        if (r) r[p] = v;
+        s += cabs2<double>(v);
+    }
+    __shared__ double red[KRYLOV_THREADS / 32];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tt = 0;
+        for (int w = 0; w < KRYLOV_THREADS / 32; ++w) tt += red[w];
+        partial[blockIdx.x] = tt;
+    }
+}
+
+__global__ void sum_kernel(const double *partial, int nb, double *out)
+{
+    if (threadIdx.x != 0) return;
+    double s = 0;
+    for (int b = 0; b < nb; ++b) s += partial[b];
+    *out = s;
+}
+
+// y = x / (1 + i alpha d)   (Jacobi preconditioner of python/implicit.py:80,85)
+__global__ void __launch_bounds__(KRYLOV_THREADS)
+jacobi_kernel(size_t n, const double2 *d, double2 alpha, double shift, const double2 *x, double2 *y)
+{
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        const double2 dd = mk<double>(d[p].x + shift, d[p].y);
+        const double2 ia = mk<double>(-alpha.y, alpha.x);            // i alpha
+        const double2 den = cfma<double>(ia, dd, mk<double>(1, 0));  // 1 + i alpha d
+        const double q = cabs2<double>(den);
+        const double2 v = x[p];
+        y[p] = mk<double>((v.x * den.x + v.y * den.y) / q, (v.y * den.x - v.x * den.y) / q);
+    }
+}
+
+__global__ void __launch_bounds__(KRYLOV_THREADS)
+scale_kernel(size_t n, double s, double2 *x)
+{
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x)
+        x[p] = cscale<double>(s, x[p]);
+}
+
+__global__ void __launch_bounds__(KRYLOV_THREADS)
+combine_host_kernel(const double2 *__restrict__ V, size_t n, int m, const double2 *__restrict__ c, double2 *y,
+                    int accumulate)
+{
+    __shared__ double2 cs[KRYLOV_MAXDIM];
+    for (int k = threadIdx.x; k < m; k += blockDim.x) cs[k] = c[k];
+    __syncthreads();
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        double2 acc = accumulate ? y[p] : mk<double>(0, 0);
+        for (int k = 0; k < m; ++k) acc = cfma<double>(cs[k], V[(size_t)k * n + p], acc);
+        y[p] = acc;
+    }
+}
+
+}  // namespace he
+
+using namespace he;
+
+namespace {
+thread_local double *g_partial = nullptr;   // per-thread reduction scratch (KRYLOV_BLOCKS + 1 doubles)
+thread_local double *g_host = nullptr;
+thread_local int g_partial_device = -1;
+
+int reduction_scratch()
+{
+    int dev = 0;
+    HE_CUDA_TRY(cudaGetDevice(&dev));
+    if (g_partial && g_partial_device == dev) return HE_OK;
+    if (g_partial) cudaFree(g_partial);   // scratch of another device: replace it
+    g_partial = nullptr;
+    HE_CUDA_TRY(cudaMalloc(&g_partial, (KRYLOV_BLOCKS + 1) * sizeof(double)));
+    if (!g_host) HE_CUDA_TRY(cudaMallocHost(&g_host, sizeof(double)));
+    g_partial_device = dev;
+    return HE_OK;
+}
+}  // namespace
+
+extern "C" int he_vec_axpby(long long n, double a_re, double a_im, const void *x, double b_re, double b_im,
+                            const void *y, void *out, void *stream)
+{
+    if (n < 0 || !x || !y || !out) return he_fail(HE_ERR_ARG, "bad axpby argument", __FILE__, __LINE__);
+    axpby_kernel<<<KRYLOV_BLOCKS, KRYLOV_THREADS, 0, static_cast<cudaStream_t>(stream)>>>(
+        (size_t)n, mk<double>(a_re, a_im), static_cast<const double2 *>(x), mk<double>(b_re, b_im),
+        static_cast<const double2 *>(y), static_cast<double2 *>(out));
+    HE_CUDA_TRY(cudaGetLastError());
+    return HE_OK;
+}
+
+// ||b - t|| (t may be NULL: ||b||); r = b - t stored when r != NULL.  Blocks the host.
+extern "C" int he_vec_residual_norm(long long n, const void *b, const void *t, void *r, double *norm, void *stream)
+{
+    if (n < 0 || !b || !norm) return he_fail(HE_ERR_ARG, "bad residual argument", __FILE__, __LINE__);
+    int rc = reduction_scratch();
+    if (rc) return rc;
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    residual_kernel<<<KRYLOV_BLOCKS, KRYLOV_THREADS, 0, s>>>((size_t)n, static_cast<const double2 *>(b),
+                                                             static_cast<const double2 *>(t),
+                                                             static_cast<double2 *>(r), g_partial);
+    sum_kernel<<<1, 32, 0, s>>>(g_partial, KRYLOV_BLOCKS, g_partial + KRYLOV_BLOCKS);
+    HE_CUDA_TRY(cudaMemcpyAsync(g_host, g_partial + KRYLOV_BLOCKS, sizeof(double), cudaMemcpyDeviceToHost, s));
+    HE_CUDA_TRY(cudaStreamSynchronize(s));
+    *norm = sqrt(*g_host);
+    return HE_OK;
+}
+
+extern "C" int he_vec_jacobi(long long n, const void *diag, double alpha_re, double alpha_im, double shift,
+                             const void *x, void *y, void *stream)
+{
+    if (n < 0 || !diag || !x || !y) return he_fail(HE_ERR_ARG, "bad Jacobi argument", __FILE__, __LINE__);
+    jacobi_kernel<<<KRYLOV_BLOCKS, KRYLOV_THREADS, 0, static_cast<cudaStream_t>(stream)>>>(
+        (size_t)n, static_cast<const double2 *>(diag), mk<double>(alpha_re, alpha_im), shift,
+        static_cast<const double2 *>(x), static_cast<double2 *>(y));
+    HE_CUDA_TRY(cudaGetLastError());
+    return HE_OK;
+}
+
+extern "C" int he_krylov_vector(he_krylov *k, int which, int j, void **ptr);
+
+extern "C" int he_krylov_scale(he_krylov *k, int which, int j, double s, void *stream)
+{
+    void *p = nullptr;
+    int rc = he_krylov_vector(k, which, j, &p);
+    if (rc) return rc;
+    scale_kernel<<<KRYLOV_BLOCKS, KRYLOV_THREADS, 0, static_cast<cudaStream_t>(stream)>>>(k->n, s,
+                                                                                          static_cast<double2 *>(p));
+    HE_CUDA_TRY(cudaGetLastError());
+    return HE_OK;
+}
+
+// Copy H[0..rows) of column j (rows <= maxdim+1) to host memory (interleaved complex).  Blocks.
+extern "C" int he_krylov_hessenberg(he_krylov *k, int j, int rows, double *out, void *stream)
+{
+    if (!k || !out || j < 0 || j >= k->maxdim || rows < 1 || rows > k->maxdim + 1)
+        return he_fail(HE_ERR_ARG, "bad Hessenberg request", __FILE__, __LINE__);
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    HE_CUDA_TRY(cudaMemcpyAsync(out, k->H + (size_t)j * (k->maxdim + 1), rows * sizeof(double2),
+                                cudaMemcpyDeviceToHost, s));
+    HE_CUDA_TRY(cudaStreamSynchronize(s));
+    return HE_OK;
+}
+
+// Zero the Hessenberg matrix (start of a GMRES cycle).
+extern "C" int he_krylov_reset(he_krylov *k, void *stream)
+{
+    if (!k) return he_fail(HE_ERR_ARG, "null workspace", __FILE__, __LINE__);
+    HE_CUDA_TRY(cudaMemsetAsync(k->H, 0, sizeof(double2) * (k->maxdim + 1) * k->maxdim, static_cast<cudaStream_t>(stream)));
+    HE_CUDA_TRY(cudaMemsetAsync(k->status, 0, sizeof(KrylovStatus), static_cast<cudaStream_t>(stream)));
+    return HE_OK;
+}
+
+// y (+)= sum_{k<m} V_k c_k with V = Q (which = 0) or Z (which = 1) and host coefficients c.
+extern "C" int he_krylov_combine_coef(he_krylov *k, int which, int m, const double *coef, void *y, int accumulate,
+                                      void *stream)
+{
+    if (!k || !coef || !y || m < 0 || m > k->maxdim || (which == 1 && !k->Z))
+        return he_fail(HE_ERR_ARG, "bad combination", __FILE__, __LINE__);
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    HE_CUDA_TRY(cudaMemcpyAsync(k->coef, coef, m * sizeof(double2), cudaMemcpyHostToDevice, s));
+    combine_host_kernel<<<KRYLOV_BLOCKS, KRYLOV_THREADS, 0, s>>>(which ? k->Z : k->Q, k->n, m, k->coef,
+                                                                 static_cast<double2 *>(y), accumulate);
+    HE_CUDA_TRY(cudaGetLastError());
+    // the host coefficient buffer may be reused by the caller as soon as this returns
+    HE_CUDA_TRY(cudaStreamSynchronize(s));
+    return HE_OK;
+}

@@ -1,0 +1,114 @@
+"""GPU parity of the CF4-Pade step: device GMRES / FGMRES, separable preconditioner and
+Jacobi fallback against the reference's own results (golden fixtures from
+python/implicit.py).  Tolerances follow the reference's tests/test_implicit.py: the
+resolvent at 3e-10, CF4 steps (GMRES tolerance 1e-12) at rtol 1e-9 / atol 1e-10."""
+import json
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+DEVICE = 'cuda:0'
+
+
+def _cf4_operator(**kw):
+    from laqphysics_b200.engine import B200Hamiltonian
+    from laqphysics_b200.fedvr import make_grid
+    from laqphysics_b200.helium3d import Helium
+    g = golden('cf4')
+    h = Helium(make_grid(**json.loads(str(g['grid']))), int(g['lmax']), M=None)
+    return g, h, B200Hamiltonian(h, DEVICE, **kw)
+
+
+def test_separable_preconditioner_matches_reference():
+    from laqphysics_b200.implicit import SeparablePreconditioner
+    g, h, op = _cf4_operator()
+    pre = SeparablePreconditioner(op)
+    y = op.host(pre.apply(op.state(g['x_sep']), complex(g['alpha']), float(g['shift'])))
+    np.testing.assert_allclose(y, g['y_sep'], rtol=1e-11, atol=1e-11)
+
+
+def test_separable_preconditioner_inverts_the_ionic_sum():
+    from laqphysics_b200.implicit import SeparablePreconditioner
+    g, h, op = _cf4_operator()
+    pre = SeparablePreconditioner(op)
+    x = g['x_sep']
+    alpha, shift = complex(g['alpha']), float(g['shift'])
+    y = op.host(pre.apply(op.state(x), alpha, shift)).reshape(h.shape, order='F')
+    out = np.empty_like(y)
+    T = h.grid.kinetic.toarray()
+    r = h.r
+    for c, ((l, _), (ll, _)) in enumerate(h.ch):
+        h1 = T + np.diag(-2 * h.cut / r + l * (l + 1) / (2 * r * r))
+        h2 = T + np.diag(-2 * h.cut / r + ll * (ll + 1) / (2 * r * r))
+        out[:, :, c] = y[:, :, c] + 1j * alpha * (h1 @ y[:, :, c] + y[:, :, c] @ h2.T + shift * y[:, :, c])
+    np.testing.assert_allclose(out.ravel(order='F'), x, atol=3e-10, rtol=3e-10)
+
+
+@pytest.mark.parametrize('precision', ['complex128', 'complex64'])
+def test_cf4_step_matches_reference(precision):
+    from laqphysics_b200.implicit import SeparablePreconditioner, cf4_step
+    g, h, op = _cf4_operator()
+    op.separable = SeparablePreconditioner(op, precision)
+    A = lambda t: np.array([.02 * np.cos(t), .01 * np.sin(t), .03])
+    y, info = cf4_step(op, op.state(g['x']), A, 0, float(g['dt']), float(g['e_ref']), tol=float(g['tol']))
+    assert y.dtype == torch.complex128 and info['linear_residual'] <= 1e-12
+    ref = g['y128'] if precision == 'complex128' else g['y64']
+    np.testing.assert_allclose(op.host(y), ref, rtol=1e-9, atol=1e-10)
+    np.testing.assert_allclose(op.host(y), g['y128'], rtol=1e-9, atol=1e-10)
+
+
+def test_cf4_with_jacobi_fallback_preconditioner():
+    from laqphysics_b200.implicit import cf4_step
+    g, h, op = _cf4_operator()
+    assert not hasattr(op, 'separable')
+    A = lambda t: np.array([.02 * np.cos(t), .01 * np.sin(t), .03])
+    y, info = cf4_step(op, op.state(g['x']), A, 0, float(g['dt']), float(g['e_ref']), tol=float(g['tol']))
+    np.testing.assert_allclose(op.host(y), g['y128'], rtol=1e-9, atol=1e-10)
+
+
+def test_coupled_cf4_sequence_matches_reference():
+    from laqphysics_b200.engine import B200Hamiltonian
+    from laqphysics_b200.implicit import SeparablePreconditioner, cf4_step
+    from laqphysics_b200.pulses import Pulse
+    from laqphysics_b200.workloads import coupled
+    g = golden('cf4')
+    grid = json.loads(str(g['grid']))
+    h = coupled(grid['edges'], grid['order'], int(g['coupled_lmax']), int(g['coupled_L']), ecs_angle=grid['ecs_angle'],
+                tail=grid['tail'], cutoff_radii=tuple(g['coupled_cut']))
+    op = B200Hamiltonian(h, DEVICE)
+    op.separable = SeparablePreconditioner(op)
+    p = Pulse(**json.loads(str(g['coupled_pulse'])))
+    Az = lambda t: np.array([0., 0., float(p.vector(t))])
+    states = g['coupled_states']
+    y = op.state(states[0])
+    dt = float(g['coupled_dt'])
+    for i in range(len(states) - 1):
+        y, _ = cf4_step(op, y, Az, i * dt, dt, float(g['coupled_e_ref']), tol=float(g['coupled_tol']))
+        ref = states[i + 1]
+        assert np.linalg.norm(op.host(y) - ref) / np.linalg.norm(ref) < 1e-9
+
+
+def test_flexible_gmres_reference_case():
+    from laqphysics_b200.implicit import gmres
+    g = golden('gmres')
+    A = torch.tensor(g['A'], device=DEVICE)
+    b = torch.tensor(g['b'], device=DEVICE)
+    pre = torch.tensor(1 / np.diag(g['A']), dtype=torch.complex64, device=DEVICE)
+    x, info = gmres(lambda y: A @ y, b, lambda y: (pre * y.to(torch.complex64)).to(torch.complex128), tol=1e-12,
+                    restart=16, flexible=True)
+    assert info['relative_residual'] < 1e-12
+    np.testing.assert_allclose(x.cpu().numpy(), g['x'], rtol=1e-10, atol=1e-11)
+    np.testing.assert_allclose(x.cpu().numpy(), g['solve'], rtol=1e-10, atol=1e-11)
+
+
+def test_gmres_non_convergence_message():
+    from laqphysics_b200.implicit import gmres
+    g = golden('gmres')
+    A = torch.tensor(g['A'], device=DEVICE)
+    b = torch.tensor(g['b'], device=DEVICE)
+    with pytest.raises(RuntimeError, match='GMRES did not converge'):
+        gmres(lambda y: A @ y, b, lambda y: y.clone(), tol=1e-14, restart=2, max_restarts=2)

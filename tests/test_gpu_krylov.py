@@ -97,9 +97,9 @@ def test_fused_and_generic_arnoldi_agree_on_larger_grid():
     op = engine(h)
     x = op.state(seeded_state(h.size, 21))
     f = (0., 0., .03)
-    a, ia = exponential_action(FieldOperator(op, f, False), x, .05, tol=1e-10, maxdim=16)
-    b, ib = exponential_action(lambda y: op.apply(y, f, False), x, .05, tol=1e-10, maxdim=16)
-    c, ic = arnoldi.exponential_action(lambda v: cpu.tensor_apply(h, v, f, False), op.host(x), .05, tol=1e-10,
+    a, ia = exponential_action(FieldOperator(op, f, False), x, .005, tol=1e-10, maxdim=16)
+    b, ib = exponential_action(lambda y: op.apply(y, f, False), x, .005, tol=1e-10, maxdim=16)
+    c, ic = arnoldi.exponential_action(lambda v: cpu.tensor_apply(h, v, f, False), op.host(x), .005, tol=1e-10,
                                        maxdim=16)
     assert ia['dimension'] == ib['dimension'] == ic['dimension']
     np.testing.assert_array_equal(op.host(a), op.host(b))

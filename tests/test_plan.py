@@ -33,7 +33,7 @@ def build_plan(h):
             return out
         scalars = get(30, np.int32)
         plan = {'ok': bool(scalars[0]), 'ne': int(scalars[1]), 'ntile': int(scalars[2]), 'ng': int(scalars[3]),
-                'nlam': int(scalars[4]), 'maxm': int(scalars[5])}
+                'nlam': int(scalars[4]), 'maxm': int(scalars[5]), 'blkmax': int(scalars[6])}
         if plan['ok']:
             for which, name in enumerate(['estart', 'tstart', 'eoff', 'ereal', 'gch', 'wptr', 'wsrc', 'dwptr',
                                           'dwsrc', 'dwel', 'dwedge']):
@@ -69,6 +69,9 @@ def emulate(h, x, field, velocity, P, beta=0, gamma=1):
             r0, r1, c0, c1 = es[ea], es[eb], es[fa], es[fb]
             rs, cs, ro, co = min(r1 + 1, n) - r0, min(c1 + 1, n) - c0, r1 - r0, c1 - c0
             assert 0 < rs <= RAD_STRIDE and 0 < cs <= RAD_STRIDE and ro <= RAD_TMAX and co <= RAD_TMAX
+            for ga, gb in ((ea, eb), (fa, fb)):   # staged element blocks of one axis fit the buffer
+                staged = (size(ga - 1) if ga > 0 else 0) + sum(size(e) ** 2 for e in range(ga, gb))
+                assert staged <= P['blkmax'] and gb - ga <= 4
             for c in range(nc):
                 PS = psi[r0:r0 + rs, c0:c0 + cs, c]
                 OS = np.zeros((ro, co), complex)
