@@ -175,6 +175,28 @@ int he_separable_apply(he_separable_handle h, const void *x, void *y, double alp
                        double shift, void *stream);
 
 /* ------------------------------------------------------------------------------------
+ * Online tSURFF (complex128).
+ * he_surface_contract replaces SurfaceContractor.__call__ (python/surface_contract.py:41-56):
+ *   q[j, o, s] = sum_{entries e of label j with eouter[e] = o} ecoef[e]
+ *                sum_r conj(chi[(einner[e] n + r) nunique + column[j]]) frame[r fr + s fs + ecol[e] fc]
+ * (entry lists per label, eptr[nlab+1], built from the reference's contraction set-up;
+ * chi: (na n) x nunique row-major; frame strides in elements; q: (nlab, nouter, ns)
+ * row-major).  he_volkov_add replaces VolkovAccumulator.add
+ * (python/streaming_surface.py:54-64): current = i sqrt(2) (radial @ harmonics) phase,
+ * radial[j,e,l] = sum_s q[j,l,s] tests[l,e,s], phase = exp(i (E_e t + k_e u_a.int_a + int_a2/2)),
+ * amplitude += d (previous + current) / 2 unless `first`, previous = current.
+ * All arrays are device arrays except int_a (3 host doubles).
+ * ---------------------------------------------------------------------------------- */
+int he_surface_contract(long long n, int nunique, int nlab, int nouter, int ns, const void *chi, const void *frame,
+                        long long fr, long long fs, long long fc, const int *eptr, const int *ecol,
+                        const int *einner, const double *ecoef, const int *eouter, const int *column, void *q,
+                        void *stream);
+int he_volkov_add(int nlab, int nouter, int ns, int ne, int nang, const void *q, const void *tests,
+                  const void *harmonics, const double *energy, const double *k, const double *unit, double time,
+                  const double *int_a, double int_a2, double d, int first, void *amplitude, void *previous,
+                  void *stream);
+
+/* ------------------------------------------------------------------------------------
  * Operator set-up options and planner inspection (host only, no device work).
  * he_set_path: 1 = tiled kernels (default when the tables admit them), 0 = generic.
  * he_plan_build / he_plan_array / he_plan_free expose the tiled plan of a set of tables.

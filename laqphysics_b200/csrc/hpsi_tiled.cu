@@ -10,15 +10,17 @@
 //                       to two elements), the separable or tabulated diagonal and |A|^2;
 //                       in the velocity gauge also W_e = B_e psi with B = T (r_b - r_a),
 //                       the [T, r] commutator stencils of src/kernels.f90:153-168.
-//   hpsi_mix_kernel     per point, all channels of NP points staged in shared memory:
+//                       A warp works on one element and 32 lines; each lane keeps the
+//                       element's inputs and all its output rows in registers.
+//   hpsi_mix_kernel     per point, all channels of MIX_NP points staged in shared memory:
 //                       Coulomb multipoles sum_lam rad_lam sum_c' V_lam[c,c'] psi_c' and the
 //                       dipole couplings, register-blocked over MIX_GROUP output channels
-//                       that share source channels ("wide edges"), then the epilogue
-//                       out = beta psi + gamma (H psi).
+//                       that share source channels ("wide edges") and two points per lane,
+//                       then the epilogue out = beta psi + gamma (H psi).
 //
 // psi is read once from DRAM by each kernel; the radial result travels through `out`.
-// Every table an inner loop touches (element blocks, wide edges, dipole edges) is
-// staged in shared memory first, so the loops issue no global loads.
+// Every table an inner loop touches (element blocks, wide edges, dipole coefficients)
+// is staged in shared memory first, so the loops issue no global loads.
 #include <algorithm>
 
 #include "common.cuh"
@@ -29,24 +31,20 @@ namespace he {
 
 constexpr int RAD_THREADS = 256;
 constexpr int RAD_STRIDE = RAD_TMAX + 1;   // odd row stride (complex elements): conflict-free column reads
-
-template <typename R> __device__ __forceinline__ cplx<R> cmul_sel(bool real, cplx<R> a, cplx<R> x, cplx<R> acc)
-{
-    return real ? rfma<R>(a.x, x, acc) : cfma<R>(a, x, acc);
-}
+constexpr int EMAX = 12;                   // elements up to EMAX nodes run the fully unrolled register path
+constexpr int MIX_NP = 64;                 // points per mixing CTA (two per lane)
+constexpr int MIX_THREADS = 128;
 
 // Per-axis description of a radial tile, built in shared memory by the CTA.
 struct AxisTile {
-    int ga, gb;                          // element range
-    int count;                           // gb - ga
-    int s[RAD_ELEMS], m[RAD_ELEMS], own[RAD_ELEMS], real[RAD_ELEMS];
-    int off[RAD_ELEMS];                  // offset of the element's T block in the staged blocks
-    int items[RAD_ELEMS + 1];            // prefix sums of work items (lines x chunks)
+    int ga, gb, count;                   // element range, gb - ga
+    int lines, linechunks;               // lines of the other axis, ceil(lines / 32)
+    int s[RAD_ELEMS], m[RAD_ELEMS], own[RAD_ELEMS], real[RAD_ELEMS], chunks[RAD_ELEMS];
+    int off[RAD_ELEMS];                  // offset of the element's block in the staged blocks
+    int tasks[RAD_ELEMS + 1];            // prefix sums of warp tasks (row chunks x line chunks)
     int prev, prev_m, prev_real, prev_off;   // previous element (bridge row), -1 if none
 };
 
-// Stage the element blocks of one axis: previous element's last row, then full blocks.
-// Returns the number of complex entries written for one matrix kind (T or B).
 template <typename R>
 __device__ void stage_axis(const TiledPlan<R> &pl, AxisTile &ax, int ga, int gb, int lines, cplx<R> *dst,
                            cplx<R> *dstB, bool vel)
@@ -54,8 +52,10 @@ __device__ void stage_axis(const TiledPlan<R> &pl, AxisTile &ax, int ga, int gb,
     const int n = pl.n, ne = pl.ne;
     if (threadIdx.x == 0) {
         ax.ga = ga; ax.gb = gb; ax.count = gb - ga;
+        ax.lines = lines; ax.linechunks = (lines + 31) / 32;
         int off = 0;
         ax.prev = ga > 0 ? ga - 1 : -1;
+        ax.prev_off = 0; ax.prev_m = 0; ax.prev_real = 1;
         if (ga > 0) {
             const int e = ga - 1;
             ax.prev_m = e + 1 < ne ? pl.estart[e + 1] - pl.estart[e] + 1 : n - pl.estart[e];
@@ -63,16 +63,17 @@ __device__ void stage_axis(const TiledPlan<R> &pl, AxisTile &ax, int ga, int gb,
             ax.prev_off = 0;
             off = ax.prev_m;
         }
-        ax.items[0] = 0;
+        ax.tasks[0] = 0;
         for (int k = 0; k < ax.count; ++k) {
             const int e = ga + k;
             ax.s[k] = pl.estart[e];
             ax.m[k] = e + 1 < ne ? pl.estart[e + 1] - pl.estart[e] + 1 : n - pl.estart[e];
             ax.own[k] = (e + 1 < ne ? pl.estart[e + 1] : n) - pl.estart[e];
             ax.real[k] = pl.ereal[e];
+            ax.chunks[k] = ax.m[k] <= EMAX ? 1 : (ax.own[k] + EMAX - 1) / EMAX;
             ax.off[k] = off;
             off += ax.m[k] * ax.m[k];
-            ax.items[k + 1] = ax.items[k] + lines * ((ax.own[k] + RAD_CHUNK - 1) / RAD_CHUNK);
+            ax.tasks[k + 1] = ax.tasks[k] + ax.chunks[k] * ax.linechunks;
         }
     }
     __syncthreads();
@@ -94,65 +95,117 @@ __device__ void stage_axis(const TiledPlan<R> &pl, AxisTile &ax, int ga, int gb,
     }
 }
 
-// One direction of the radial stencil on the staged tile.  ROWS = electron 1 (lines are
-// owned columns, element index runs along rows), else electron 2.
-template <typename R, bool VEL, bool ROWS>
-__device__ void radial_phase(const AxisTile &ax, const cplx<R> *BLK, const cplx<R> *BLKB, const cplx<R> *PS,
-                             cplx<R> *OS, int lines, int base, int r0, int c0, int n, const cplx<R> *pc,
-                             cplx<R> *wout, size_t nn, int c)
+// acc[a] = sum_b blk[a m + b] x[b] for a < na, b < m <= EMAX (m, na warp uniform).
+template <typename R, bool REAL>
+__device__ __forceinline__ void small_rows(const cplx<R> *blk, int m, int na, const cplx<R> (&x)[EMAX],
+                                           cplx<R> (&acc)[EMAX])
 {
-    const int nitems = ax.items[ax.count];
-    for (int item = threadIdx.x; item < nitems; item += blockDim.x) {
-        int k = 0;
-        while (k + 1 < ax.count && item >= ax.items[k + 1]) ++k;
-        const int rest = item - ax.items[k];
-        const int line = rest % lines, chunk = rest / lines;
-        const int s = ax.s[k], m = ax.m[k];
-        const int a0 = chunk * RAD_CHUNK, na = min(RAD_CHUNK, ax.own[k] - a0);
-        const cplx<R> *blk = BLK + ax.off[k], *bbl = BLKB + ax.off[k];
+#pragma unroll
+    for (int a = 0; a < EMAX; ++a) {
+        if (a < na) {
+            const cplx<R> *row = blk + a * m;
+            cplx<R> s = mk<R>(0, 0);
+#pragma unroll
+            for (int b = 0; b < EMAX; ++b)
+                if (b < m) s = REAL ? rfma<R>(row[b].x, x[b], s) : cfma<R>(row[b], x[b], s);
+            acc[a] = s;
+        }
+    }
+}
+
+// Rows [a0, a0 + na) of element k applied to one line, with the previous element's part
+// of the bridge row added when a0 == 0.  `blocks` is the staged T (or B) block set,
+// `prevrow` the previous element's last row of the same kind.
+template <typename R, bool ROWS>
+__device__ __forceinline__ void element_line(const AxisTile &ax, int k, const cplx<R> *blocks, const cplx<R> *prevrow,
+                                             const cplx<R> *PS, int base, int r0, int c0, int n, const cplx<R> *pc,
+                                             int line, int a0, int na, cplx<R> (&acc)[EMAX])
+{
+    const int s = ax.s[k], m = ax.m[k];
+    const cplx<R> *blk = blocks + ax.off[k];
+    const cplx<R> *xs = ROWS ? PS + (s - base) * RAD_STRIDE + line : PS + line * RAD_STRIDE + (s - base);
+    const int xstride = ROWS ? RAD_STRIDE : 1;
+#pragma unroll
+    for (int q = 0; q < EMAX; ++q) acc[q] = mk<R>(0, 0);
+    if (m <= EMAX) {
+        cplx<R> x[EMAX];
+#pragma unroll
+        for (int b = 0; b < EMAX; ++b) x[b] = b < m ? xs[b * xstride] : mk<R>(0, 0);
+        if (ax.real[k]) small_rows<R, true>(blk, m, na, x, acc);
+        else small_rows<R, false>(blk, m, na, x, acc);
+    } else {   // large element (the exterior-scaled tail): stream over its nodes
         const bool real = ax.real[k];
-        cplx<R> acc[RAD_CHUNK], accb[RAD_CHUNK];
-#pragma unroll
-        for (int q = 0; q < RAD_CHUNK; ++q) { acc[q] = mk<R>(0, 0); accb[q] = mk<R>(0, 0); }
         for (int b = 0; b < m; ++b) {
-            const int node = s - base + b;
-            const cplx<R> x = ROWS ? PS[node * RAD_STRIDE + line] : PS[line * RAD_STRIDE + node];
+            const cplx<R> x = xs[b * xstride];
 #pragma unroll
-            for (int q = 0; q < RAD_CHUNK; ++q) {
+            for (int q = 0; q < EMAX; ++q) {
                 if (q < na) {
-                    acc[q] = cmul_sel<R>(real, blk[(a0 + q) * m + b], x, acc[q]);
-                    if (VEL) accb[q] = cmul_sel<R>(real, bbl[(a0 + q) * m + b], x, accb[q]);
+                    const cplx<R> tv = blk[(a0 + q) * m + b];
+                    acc[q] = real ? rfma<R>(tv.x, x, acc[q]) : cfma<R>(tv, x, acc[q]);
                 }
             }
         }
-        if (a0 == 0 && (k > 0 || ax.prev >= 0)) {   // bridge row s: the previous element's part
-            const cplx<R> *bp, *bq;
-            int mp, sp;
-            bool rp;
-            if (k > 0) {
-                mp = ax.m[k - 1]; sp = ax.s[k - 1]; rp = ax.real[k - 1];
-                bp = BLK + ax.off[k - 1] + (mp - 1) * mp; bq = BLKB + ax.off[k - 1] + (mp - 1) * mp;
-            } else {
-                mp = ax.prev_m; sp = s - (mp - 1); rp = ax.prev_real;
-                bp = BLK + ax.prev_off; bq = BLKB + ax.prev_off;
-            }
-            for (int b = 0; b < mp - 1; ++b) {
-                const int node = sp + b;   // global index along this axis
-                cplx<R> x;
-                if (node >= base) x = ROWS ? PS[(node - base) * RAD_STRIDE + line] : PS[line * RAD_STRIDE + node - base];
-                else x = ROWS ? pc[(size_t)node + (size_t)n * (c0 + line)] : pc[(size_t)(r0 + line) + (size_t)n * node];
-                acc[0] = cmul_sel<R>(rp, bp[b], x, acc[0]);
-                if (VEL) accb[0] = cmul_sel<R>(rp, bq[b], x, accb[0]);
-            }
+    }
+    if (a0 == 0 && (k > 0 || ax.prev >= 0)) {   // bridge row s: the previous element's part
+        const cplx<R> *bp;
+        int mp, sp;
+        bool rp;
+        if (k > 0) {
+            mp = ax.m[k - 1]; sp = ax.s[k - 1]; rp = ax.real[k - 1];
+            bp = blocks + ax.off[k - 1] + (mp - 1) * mp;
+        } else {
+            mp = ax.prev_m; sp = s - (mp - 1); rp = ax.prev_real;
+            bp = prevrow;
         }
+        for (int b = 0; b < mp - 1; ++b) {
+            const int node = sp + b;   // global index along this axis
+            cplx<R> x;
+            if (node >= base) x = ROWS ? PS[(node - base) * RAD_STRIDE + line] : PS[line * RAD_STRIDE + node - base];
+            else x = ROWS ? pc[(size_t)node + (size_t)n * (c0 + line)] : pc[(size_t)(r0 + line) + (size_t)n * node];
+            acc[0] = rp ? rfma<R>(bp[b].x, x, acc[0]) : cfma<R>(bp[b], x, acc[0]);
+        }
+    }
+}
+
+// One direction of the radial stencil on the staged tile.  ROWS = electron 1 (lines are
+// owned columns, the element index runs along rows), else electron 2.  The kinetic
+// result goes to OS; in the velocity gauge a second pass applies B and writes W.
+template <typename R, bool VEL, bool ROWS>
+__device__ void radial_phase(const AxisTile &ax, const cplx<R> *BLK, const cplx<R> *BLKB, const cplx<R> *PS,
+                             cplx<R> *OS, int base, int r0, int c0, int n, const cplx<R> *pc, cplx<R> *wout,
+                             size_t nn, int c)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int ntasks = ax.tasks[ax.count];
+    for (int task = warp; task < ntasks; task += nwarps) {
+        int k = 0;
+        while (k + 1 < ax.count && task >= ax.tasks[k + 1]) ++k;
+        const int rest = task - ax.tasks[k];
+        const int lc = rest % ax.linechunks, chunk = rest / ax.linechunks;
+        const int line = lc * 32 + lane;
+        if (line >= ax.lines) continue;
+        const int s = ax.s[k];
+        const int a0 = chunk * EMAX, na = min(EMAX, ax.own[k] - a0);
+        cplx<R> acc[EMAX];
+        element_line<R, ROWS>(ax, k, BLK, BLK + ax.prev_off, PS, base, r0, c0, n, pc, line, a0, na, acc);
 #pragma unroll
-        for (int q = 0; q < RAD_CHUNK; ++q) {
+        for (int q = 0; q < EMAX; ++q) {
             if (q < na) {
                 const int node = s - base + a0 + q;
                 const int row = ROWS ? node : line, col = ROWS ? line : node;
                 if (ROWS) OS[row * RAD_STRIDE + col] = acc[q];
                 else OS[row * RAD_STRIDE + col] = cadd<R>(OS[row * RAD_STRIDE + col], acc[q]);
-                if (VEL) wout[(size_t)(r0 + row) + (size_t)n * (c0 + col) + nn * c] = accb[q];
+            }
+        }
+        if (VEL) {
+            element_line<R, ROWS>(ax, k, BLKB, BLKB + ax.prev_off, PS, base, r0, c0, n, pc, line, a0, na, acc);
+#pragma unroll
+            for (int q = 0; q < EMAX; ++q) {
+                if (q < na) {
+                    const int node = s - base + a0 + q;
+                    const int row = ROWS ? node : line, col = ROWS ? line : node;
+                    wout[(size_t)(r0 + row) + (size_t)n * (c0 + col) + nn * c] = acc[q];
+                }
             }
         }
     }
@@ -193,9 +246,9 @@ hpsi_radial_kernel(const DeviceTables<R> t, const TiledPlan<R> pl, const cplx<R>
     stage_axis<R>(pl, ax0, ea, eb, co, B0, B0B, VEL);
     stage_axis<R>(pl, ax1, fa, fb, ro, B1, B1B, VEL);
     __syncthreads();
-    radial_phase<R, VEL, true>(ax0, B0, B0B, PS, OS, co, r0, r0, c0, n, pc, w1, nn, c);
+    radial_phase<R, VEL, true>(ax0, B0, B0B, PS, OS, r0, r0, c0, n, pc, w1, nn, c);
     __syncthreads();
-    radial_phase<R, VEL, false>(ax1, B1, B1B, PS, OS, ro, c0, r0, c0, n, pc, w2, nn, c);
+    radial_phase<R, VEL, false>(ax1, B1, B1B, PS, OS, c0, r0, c0, n, pc, w2, nn, c);
     __syncthreads();
 
     for (int idx = threadIdx.x; idx < ro * co; idx += blockDim.x) {
@@ -212,142 +265,161 @@ hpsi_radial_kernel(const DeviceTables<R> t, const TiledPlan<R> pl, const cplx<R>
 }
 
 // ---------------------------------------------------------------------------------
-// Channel-mixing kernel.  CTA = NP consecutive flattened points p = i + n j.
-// Shared memory: PSI[c][NP], RAD[lam][NP], wide Coulomb edges (source offset, MIX_GROUP
-// coefficients), group x lam offsets, wide dipole edges and the field-contracted
-// dipole coefficients coef_k = field . dcoef(:, k) (zero below 1e-30, the skip of
-// src/kernels.f90:145).  A warp task is (32 points, one output group).
+// Channel-mixing kernel.  CTA = MIX_NP consecutive flattened points p = i + n j.
+// Shared memory: PSI[c][MIX_NP], RAD[lam][MIX_NP], wide Coulomb edges (source offset,
+// MIX_GROUP coefficients), group x lam offsets, wide dipole edges with their
+// field-contracted coefficients per group slot:
+//   length gauge   DA = coef_k                (acc += DA r_a psi_s)
+//   velocity gauge DA = i coef_k ldiff_k, DB = i coef_k   (acc += DA psi_s/(2 r_a) + DB W_a[s])
+// with coef_k = field . dcoef(:, k), zero below 1e-30 (the skip of src/kernels.f90:145).
+// A warp task is one output group over all MIX_NP points (two per lane).
 // ---------------------------------------------------------------------------------
 template <typename R> struct MixSmem {
-    cplx<R> *psi, *rad, *coef;
-    R *wcoef, *ldiff;
-    int *wsrc, *wptr, *dsrc, *del, *dedge;
+    cplx<R> *psi, *rad, *da, *db;
+    R *wcoef;
+    int *wsrc, *wptr, *dsrc, *del;
 };
 
 template <typename R>
-__device__ __forceinline__ MixSmem<R> mix_layout(unsigned char *raw, const TiledPlan<R> &pl, int nd, int np)
+__device__ __forceinline__ MixSmem<R> mix_layout(unsigned char *raw, const TiledPlan<R> &pl)
 {
     MixSmem<R> s;
     s.psi = reinterpret_cast<cplx<R> *>(raw);
-    s.rad = s.psi + (size_t)pl.nc * np;
-    s.coef = s.rad + (size_t)pl.nlam * np;
-    s.wcoef = reinterpret_cast<R *>(s.coef + max(nd, 1));
-    s.ldiff = s.wcoef + (size_t)pl.nwide * MIX_GROUP;
-    s.wsrc = reinterpret_cast<int *>(s.ldiff + max(nd, 1));
+    s.rad = s.psi + (size_t)pl.nc * MIX_NP;
+    s.da = s.rad + (size_t)pl.nlam * MIX_NP;
+    s.db = s.da + (size_t)max(pl.nwd, 1) * MIX_GROUP;
+    s.wcoef = reinterpret_cast<R *>(s.db + (size_t)max(pl.nwd, 1) * MIX_GROUP);
+    s.wsrc = reinterpret_cast<int *>(s.wcoef + (size_t)pl.nwide * MIX_GROUP);
     s.wptr = s.wsrc + pl.nwide;
     s.dsrc = s.wptr + pl.ng * pl.nlam + 1;
     s.del = s.dsrc + pl.nwd;
-    s.dedge = s.del + pl.nwd;
     return s;
 }
 
-template <typename R, bool VEL, int NP>
-__global__ void __launch_bounds__(256)
+template <typename R, bool VEL>
+__global__ void __launch_bounds__(MIX_THREADS)
 hpsi_mix_kernel(const DeviceTables<R> t, const TiledPlan<R> pl, const cplx<R> *__restrict__ psi,
                 cplx<R> *__restrict__ out, const cplx<R> *__restrict__ w1, const cplx<R> *__restrict__ w2,
                 R f0, R f1, R f2, cplx<R> beta, cplx<R> gamma)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int n = pl.n, nc = pl.nc, nlam = pl.nlam, nd = t.nd;
-    const MixSmem<R> S = mix_layout<R>(smem_raw, pl, nd, NP);
+    const int n = pl.n, nc = pl.nc, nlam = pl.nlam;
+    const MixSmem<R> S = mix_layout<R>(smem_raw, pl);
     const size_t nn = (size_t)n * n;
-    const size_t p0 = (size_t)blockIdx.x * NP;
-    const int np = (int)min((size_t)NP, nn - p0);
+    const size_t p0 = (size_t)blockIdx.x * MIX_NP;
+    const int np = (int)min((size_t)MIX_NP, nn - p0);
 
-    for (int idx = threadIdx.x; idx < nc * NP; idx += blockDim.x) {
-        const int q = idx % NP, cc = idx / NP;
+    for (int idx = threadIdx.x; idx < nc * MIX_NP; idx += blockDim.x) {
+        const int q = idx % MIX_NP, cc = idx / MIX_NP;
         S.psi[idx] = q < np ? psi[p0 + q + nn * cc] : mk<R>(0, 0);
     }
-    for (int idx = threadIdx.x; idx < nlam * NP; idx += blockDim.x) {
-        const int q = idx % NP, lam = idx / NP;
+    for (int idx = threadIdx.x; idx < nlam * MIX_NP; idx += blockDim.x) {
+        const int q = idx % MIX_NP, lam = idx / MIX_NP;
         S.rad[idx] = q < np ? ldg<R>(t.rad + p0 + q + nn * lam) : mk<R>(0, 0);
     }
-    for (int k = threadIdx.x; k < nd; k += blockDim.x) {
-        const cplx<R> *dk = t.dcoef + 3 * (size_t)k;
-        cplx<R> v = cscale<R>(f0, dk[0]);
-        v = rfma<R>(f1, dk[1], v);
-        v = rfma<R>(f2, dk[2], v);
-        if (sqrt(cabs2<R>(v)) < (R)1e-30) v = mk<R>(0, 0);
-        S.coef[k] = v;
-        S.ldiff[k] = t.ldiff[k];
+    for (int idx = threadIdx.x; idx < pl.nwd * MIX_GROUP; idx += blockDim.x) {
+        const int kk = pl.dwedge[idx];
+        cplx<R> a = mk<R>(0, 0), b = mk<R>(0, 0);
+        if (kk >= 0) {
+            const cplx<R> *dk = t.dcoef + 3 * (size_t)kk;
+            cplx<R> v = cscale<R>(f0, dk[0]);
+            v = rfma<R>(f1, dk[1], v);
+            v = rfma<R>(f2, dk[2], v);
+            if (sqrt(cabs2<R>(v)) < (R)1e-30) v = mk<R>(0, 0);
+            if (VEL) {
+                b = mk<R>(-v.y, v.x);                 // i coef
+                a = cscale<R>(t.ldiff[kk], b);        // i coef ldiff
+            } else {
+                a = v;
+            }
+        }
+        S.da[idx] = a;
+        S.db[idx] = b;
     }
     for (int k = threadIdx.x; k < pl.nwide * MIX_GROUP; k += blockDim.x) S.wcoef[k] = pl.wcoef[k];
-    for (int k = threadIdx.x; k < pl.nwide; k += blockDim.x) S.wsrc[k] = pl.wsrc[k] * NP;
+    for (int k = threadIdx.x; k < pl.nwide; k += blockDim.x) S.wsrc[k] = pl.wsrc[k] * MIX_NP;
     for (int k = threadIdx.x; k <= pl.ng * nlam; k += blockDim.x) S.wptr[k] = pl.wptr[k];
     for (int k = threadIdx.x; k < pl.nwd; k += blockDim.x) {
-        S.dsrc[k] = pl.dwsrc[k];
+        S.dsrc[k] = pl.dwsrc[k] * MIX_NP;
         S.del[k] = pl.dwel[k];
     }
-    for (int k = threadIdx.x; k < pl.nwd * MIX_GROUP; k += blockDim.x) S.dedge[k] = pl.dwedge[k];
     __syncthreads();
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    constexpr int QUARTERS = NP / 32;
-    for (int task = warp; task < pl.ng * QUARTERS; task += nwarps) {
-        const int g = task / QUARTERS, quarter = task % QUARTERS;
-        const int q = quarter * 32 + lane;
-        const bool valid = q < np;
-        const size_t p = p0 + q;
+    const bool v0 = lane < np, v1 = lane + 32 < np;
+    const size_t pa = p0 + lane, pb = p0 + lane + 32;
+    for (int g = warp; g < pl.ng; g += nwarps) {
         int ch[MIX_GROUP];
-        cplx<R> acc[MIX_GROUP];
+        cplx<R> a0[MIX_GROUP], a1[MIX_GROUP];
 #pragma unroll
         for (int d = 0; d < MIX_GROUP; ++d) {
             ch[d] = __ldg(pl.gch + g * MIX_GROUP + d);
-            acc[d] = (valid && ch[d] >= 0) ? out[p + nn * ch[d]] : mk<R>(0, 0);
+            a0[d] = (v0 && ch[d] >= 0) ? out[pa + nn * ch[d]] : mk<R>(0, 0);
+            a1[d] = (v1 && ch[d] >= 0) ? out[pb + nn * ch[d]] : mk<R>(0, 0);
         }
         const int *wp = S.wptr + g * nlam;
         for (int lam = 0; lam < nlam; ++lam) {
             const int k0 = wp[lam], k1 = wp[lam + 1];
             if (k0 == k1) continue;
-            cplx<R> tsum[MIX_GROUP];
+            cplx<R> t0[MIX_GROUP], t1[MIX_GROUP];
 #pragma unroll
-            for (int d = 0; d < MIX_GROUP; ++d) tsum[d] = mk<R>(0, 0);
+            for (int d = 0; d < MIX_GROUP; ++d) { t0[d] = mk<R>(0, 0); t1[d] = mk<R>(0, 0); }
 #pragma unroll 2
             for (int k = k0; k < k1; ++k) {
-                const cplx<R> x = S.psi[S.wsrc[k] + q];
+                const int off = S.wsrc[k];
+                const cplx<R> x0 = S.psi[off + lane], x1 = S.psi[off + lane + 32];
                 const R *cf = S.wcoef + k * MIX_GROUP;
 #pragma unroll
-                for (int d = 0; d < MIX_GROUP; ++d) tsum[d] = rfma<R>(cf[d], x, tsum[d]);
+                for (int d = 0; d < MIX_GROUP; ++d) {
+                    const R w = cf[d];
+                    t0[d] = rfma<R>(w, x0, t0[d]);
+                    t1[d] = rfma<R>(w, x1, t1[d]);
+                }
             }
-            const cplx<R> rl = S.rad[lam * NP + q];
+            const cplx<R> r0 = S.rad[lam * MIX_NP + lane], r1 = S.rad[lam * MIX_NP + lane + 32];
 #pragma unroll
-            for (int d = 0; d < MIX_GROUP; ++d) acc[d] = cfma<R>(rl, tsum[d], acc[d]);
+            for (int d = 0; d < MIX_GROUP; ++d) {
+                a0[d] = cfma<R>(r0, t0[d], a0[d]);
+                a1[d] = cfma<R>(r1, t1[d], a1[d]);
+            }
         }
         const int k0 = __ldg(pl.dwptr + g), k1 = __ldg(pl.dwptr + g + 1);
-        if (k0 < k1 && valid) {
-            const int i = (int)(p % n), j = (int)(p / n);
-            const cplx<R> r1 = ldg<R>(t.r + i), r2 = ldg<R>(t.r + j);
-            const cplx<R> h1 = ldg<R>(t.hinv + i), h2 = ldg<R>(t.hinv + j);
+        if (k0 < k1) {
+            const int ia = (int)(pa % n), ja = (int)(pa / n), ib = (int)(pb % n), jb = (int)(pb / n);
+            // per point and electron: r (length) or 1/(2r) (velocity)
+            const cplx<R> *rt = VEL ? t.hinv : t.r;
+            const cplx<R> ra1 = v0 ? ldg<R>(rt + ia) : mk<R>(0, 0), ra2 = v0 ? ldg<R>(rt + ja) : mk<R>(0, 0);
+            const cplx<R> rb1 = v1 ? ldg<R>(rt + ib) : mk<R>(0, 0), rb2 = v1 ? ldg<R>(rt + jb) : mk<R>(0, 0);
             for (int k = k0; k < k1; ++k) {
-                const int s = S.dsrc[k];
+                const int off = S.dsrc[k];
                 const bool first = S.del[k] == 1;
-                const cplx<R> x = S.psi[s * NP + q];
-                if (!VEL) {
-                    const cplx<R> y = cmul<R>(first ? r1 : r2, x);
+                const cplx<R> y0 = cmul<R>(first ? ra1 : ra2, S.psi[off + lane]);
+                const cplx<R> y1 = cmul<R>(first ? rb1 : rb2, S.psi[off + lane + 32]);
+                const cplx<R> *da = S.da + k * MIX_GROUP;
+#pragma unroll
+                for (int d = 0; d < MIX_GROUP; ++d) {
+                    a0[d] = cfma<R>(da[d], y0, a0[d]);
+                    a1[d] = cfma<R>(da[d], y1, a1[d]);
+                }
+                if (VEL) {
+                    const int s = off / MIX_NP;
+                    const cplx<R> *wsrc = first ? w1 : w2;
+                    const cplx<R> wa = v0 ? wsrc[pa + nn * s] : mk<R>(0, 0);
+                    const cplx<R> wb = v1 ? wsrc[pb + nn * s] : mk<R>(0, 0);
+                    const cplx<R> *db = S.db + k * MIX_GROUP;
 #pragma unroll
                     for (int d = 0; d < MIX_GROUP; ++d) {
-                        const int kk = S.dedge[k * MIX_GROUP + d];
-                        if (kk >= 0) acc[d] = cfma<R>(S.coef[kk], y, acc[d]);
-                    }
-                } else {
-                    const cplx<R> w = (first ? w1 : w2)[p + nn * s];
-                    const cplx<R> hx = cmul<R>(first ? h1 : h2, x);
-#pragma unroll
-                    for (int d = 0; d < MIX_GROUP; ++d) {
-                        const int kk = S.dedge[k * MIX_GROUP + d];
-                        if (kk >= 0) {
-                            const cplx<R> part = rfma<R>(S.ldiff[kk], hx, w);
-                            const cplx<R> cf = S.coef[kk];
-                            acc[d] = cfma<R>(mk<R>(-cf.y, cf.x), part, acc[d]);   // i coef part
-                        }
+                        a0[d] = cfma<R>(db[d], wa, a0[d]);
+                        a1[d] = cfma<R>(db[d], wb, a1[d]);
                     }
                 }
             }
         }
-        if (valid) {
 #pragma unroll
-            for (int d = 0; d < MIX_GROUP; ++d)
-                if (ch[d] >= 0) out[p + nn * ch[d]] = cfma<R>(gamma, acc[d], cmul<R>(beta, S.psi[ch[d] * NP + q]));
+        for (int d = 0; d < MIX_GROUP; ++d) {
+            if (ch[d] < 0) continue;
+            if (v0) out[pa + nn * ch[d]] = cfma<R>(gamma, a0[d], cmul<R>(beta, S.psi[ch[d] * MIX_NP + lane]));
+            if (v1) out[pb + nn * ch[d]] = cfma<R>(gamma, a1[d], cmul<R>(beta, S.psi[ch[d] * MIX_NP + lane + 32]));
         }
     }
 }
@@ -358,11 +430,11 @@ template <typename R> size_t radial_smem(bool vel, int blkmax)
                               (vel ? 4 : 2) * (size_t)blkmax);
 }
 
-template <typename R> size_t mix_smem(const TiledPlan<R> &pl, int nd, int np)
+template <typename R> size_t mix_smem(int nc, int nlam, int ng, int nwide, int nwd)
 {
-    const size_t c = sizeof(cplx<R>) * ((size_t)(pl.nc + pl.nlam) * np + std::max(nd, 1));
-    const size_t r = sizeof(R) * ((size_t)pl.nwide * MIX_GROUP + std::max(nd, 1));
-    const size_t i = sizeof(int) * ((size_t)pl.nwide + pl.ng * pl.nlam + 1 + pl.nwd * (2 + MIX_GROUP));
+    const size_t c = sizeof(cplx<R>) * ((size_t)(nc + nlam) * MIX_NP + 2 * (size_t)std::max(nwd, 1) * MIX_GROUP);
+    const size_t r = sizeof(R) * (size_t)nwide * MIX_GROUP;
+    const size_t i = sizeof(int) * ((size_t)nwide + (size_t)ng * nlam + 1 + 2 * (size_t)nwd);
     return c + r + i + 64;
 }
 
@@ -388,22 +460,15 @@ int launch_hpsi_tiled(he_operator *h, const DeviceTables<R> &t, const TiledPlan<
 #undef HE_RADIAL
     HE_CUDA_TRY(cudaGetLastError());
     const size_t nn = (size_t)pl.n * pl.n;
-    const size_t limit = 110 * 1024;   // two CTAs per SM
-    const int np = (sizeof(R) == 4 && mix_smem<R>(pl, t.nd, 128) <= limit) ? 128
-                 : mix_smem<R>(pl, t.nd, 64) <= limit ? 64 : 32;
-#define HE_MIX(V, NP)                                                                                    \
-    do {                                                                                                 \
-        auto kern = hpsi_mix_kernel<R, V, NP>;                                                           \
-        const size_t ms = mix_smem<R>(pl, t.nd, NP);                                                     \
-        HE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ms));   \
-        kern<<<(unsigned)((nn + NP - 1) / NP), 256, ms, stream>>>(t, pl, psi, out, w1, w2, f0, f1, f2, beta, gamma); \
-    } while (0)
+    const size_t ms = mix_smem<R>(pl.nc, pl.nlam, pl.ng, pl.nwide, pl.nwd);
+    const unsigned blocks = (unsigned)((nn + MIX_NP - 1) / MIX_NP);
     if (velocity) {
-        if (np == 128) HE_MIX(true, 128); else if (np == 64) HE_MIX(true, 64); else HE_MIX(true, 32);
+        HE_CUDA_TRY(cudaFuncSetAttribute(hpsi_mix_kernel<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ms));
+        hpsi_mix_kernel<R, true><<<blocks, MIX_THREADS, ms, stream>>>(t, pl, psi, out, w1, w2, f0, f1, f2, beta, gamma);
     } else {
-        if (np == 128) HE_MIX(false, 128); else if (np == 64) HE_MIX(false, 64); else HE_MIX(false, 32);
+        HE_CUDA_TRY(cudaFuncSetAttribute(hpsi_mix_kernel<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ms));
+        hpsi_mix_kernel<R, false><<<blocks, MIX_THREADS, ms, stream>>>(t, pl, psi, out, w1, w2, f0, f1, f2, beta, gamma);
     }
-#undef HE_MIX
     HE_CUDA_TRY(cudaGetLastError());
     return HE_OK;
 }
@@ -415,12 +480,12 @@ template int launch_hpsi_tiled<float>(he_operator *, const DeviceTables<float> &
                                       float2 *, float2 *, const float2 *, float2 *, const double *, int, float2,
                                       float2, cudaStream_t);
 
-// The mixing kernel must fit two CTAs of 32 points per SM in complex128.
+// Both kernels must fit two CTAs per SM in complex128.
 bool tiled_fits(const he_plan_host &P, int nc, int nd)
 {
-    TiledPlan<double> pl{};
-    pl.nc = nc; pl.nlam = P.nlam; pl.ng = P.ng; pl.nwide = (int)P.wsrc.size(); pl.nwd = (int)P.dwsrc.size();
-    return mix_smem<double>(pl, nd, 32) <= 110 * 1024 && radial_smem<double>(true, P.blkmax) <= 110 * 1024;
+    (void)nd;
+    return mix_smem<double>(nc, P.nlam, P.ng, (int)P.wsrc.size(), (int)P.dwsrc.size()) <= 110 * 1024 &&
+           radial_smem<double>(true, P.blkmax) <= 110 * 1024;
 }
 
 }  // namespace he

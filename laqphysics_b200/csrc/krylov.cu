@@ -545,7 +545,7 @@ extern "C" int he_expv(he_krylov *k, he_handle op, const void *x, void *y, const
     double err = 0;
     for (int j = 0; j < maxdim && !done; ++j) {
         double2 *qj = k->Q + (size_t)j * k->n, *v = k->Q + (size_t)(j + 1) * k->n;
-        rc = he::launch_hpsi<double>(op->t64, qj, v, field, velocity, mk<double>(0, 0), mk<double>(1, 0), s);
+        rc = he_apply(op, qj, v, field, velocity, HE_C128, stream);   // same kernels as every other apply
         if (!rc) rc = krylov_cgs2(k, j + 1, v, k->H + (size_t)j * ld, k->H + (size_t)j * ld + j + 1, s, 1e-13);
         if (rc) break;
         const bool checkpoint = j >= 3 && ((j + 1) % 4 == 0 || j + 1 == maxdim);

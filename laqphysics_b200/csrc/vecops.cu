@@ -157,7 +157,7 @@ extern "C" int he_krylov_scale(he_krylov *k, int which, int j, double s, void *s
 }
 
 // Copy H[0..rows) of column j (rows <= maxdim+1) to host memory (interleaved complex).  Blocks.
-extern "C" int he_krylov_hessenberg(he_krylov *k, int j, int rows, double *out, void *stream)
+extern "C" int he_krylov_hessenberg(he_krylov *k, int j, int rows, void *out, void *stream)
 {
     if (!k || !out || j < 0 || j >= k->maxdim || rows < 1 || rows > k->maxdim + 1)
         return he_fail(HE_ERR_ARG, "bad Hessenberg request", __FILE__, __LINE__);
@@ -178,7 +178,7 @@ extern "C" int he_krylov_reset(he_krylov *k, void *stream)
 }
 
 // y (+)= sum_{k<m} V_k c_k with V = Q (which = 0) or Z (which = 1) and host coefficients c.
-extern "C" int he_krylov_combine_coef(he_krylov *k, int which, int m, const double *coef, void *y, int accumulate,
+extern "C" int he_krylov_combine_coef(he_krylov *k, int which, int m, const void *coef, void *y, int accumulate,
                                       void *stream)
 {
     if (!k || !coef || !y || m < 0 || m > k->maxdim || (which == 1 && !k->Z))

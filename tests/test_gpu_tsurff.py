@@ -1,0 +1,101 @@
+"""GPU parity of online tSURFF: the device ionic contraction and the FP64 Volkov
+trapezoid accumulator against the reference's OnlineSurface run (golden fixture
+'volkov': python/streaming_surface.py:39-64 + python/surface_contract.py:41-56 on the
+reference test configuration tests/test_streaming_surface.py:10-20, linear coupled
+variant).  Tolerance: the reference's own GPU-vs-numpy accumulator bound, 3e-12
+(tests/test_streaming_surface.py:132)."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+DEVICE = 'cuda:0'
+
+CONFIG = {'radial': {'edges': [0, 1, 2, 4, 6, 8], 'order': 3, 'tail': 6, 'ecs_angle': .3},
+          'lmax': 1, 'M': 0, 'total_Lmax': 2, 'cutoff_radii': [1, 2], 'surface': 5.,
+          'pulses': [{'pulse': {'omega': 5., 'cycles': 2, 'field': .15}, 'polarization': 'z'}],
+          'ionic_channels': [[1, 0, 0], [2, 0, 0], [2, 1, 0]],
+          'spectrum_energy': [.2, 1.2, 7], 'spectrum': {'theta_points': 4, 'phi_points': 1}}
+
+
+def _setup():
+    from laqphysics_b200.pulses import Pulse
+    from laqphysics_b200.surface3d import Ionic
+    from laqphysics_b200.surface_contract import SurfaceContractor
+    from laqphysics_b200.workloads import coupled
+    rc = CONFIG['radial']
+    h = coupled(rc['edges'], rc['order'], CONFIG['lmax'], CONFIG['total_Lmax'], ecs_angle=rc['ecs_angle'],
+                tail=rc['tail'], cutoff_radii=tuple(CONFIG['cutoff_radii']))
+    base = h.uncoupled
+    base.prepare_surface(CONFIG['surface'])
+    h.prepare_surface(CONFIG['surface'])
+    labels = [tuple(x) for x in CONFIG['ionic_channels']]
+    unique = list(dict.fromkeys((n, l, abs(m)) for n, l, m in labels))
+    columns = [unique.index((n, l, abs(m))) for n, l, m in labels]
+    ion = Ionic(base, {m for n, l, m in unique})
+    contractor = SurfaceContractor(base, ion, labels, unique, columns, True, h.transform, DEVICE)
+    pulse = Pulse(**CONFIG['pulses'][0]['pulse'])
+    avec = lambda t: np.array([0., 0., float(pulse.vector(t))])
+    return h, base, ion, contractor, avec
+
+
+def test_contraction_matches_reference():
+    g = golden('volkov')
+    h, base, ion, contractor, avec = _setup()
+    assert ion.na == int(g['nion']) and contractor.outerstates == [tuple(x) for x in g['outerstates']]
+    for i in range(len(g['times'])):
+        q = contractor(g['chi'][i], g['frames'][i])
+        np.testing.assert_allclose(q, g['q'][i], rtol=1e-12, atol=1e-13)
+
+
+def test_volkov_accumulation_matches_reference():
+    from laqphysics_b200.streaming_surface import VolkovAccumulator
+    g = golden('volkov')
+    h, base, ion, contractor, avec = _setup()
+    np.testing.assert_allclose(np.array([avec(t) for t in g['times']]), g['avec'], atol=1e-15)
+    acc = VolkovAccumulator(contractor, CONFIG, avec, device=DEVICE)
+    np.testing.assert_allclose(acc.tests, g['tests'], rtol=1e-13, atol=1e-15)
+    np.testing.assert_allclose(acc.harmonics, g['harmonics'], rtol=1e-13, atol=1e-15)
+    for i, t in enumerate(g['times']):
+        acc.add(i, t, g['q'][i])
+    np.testing.assert_allclose(acc.amplitude.cpu().numpy(), g['amplitude'], rtol=3e-12, atol=3e-12)
+
+
+def test_accumulator_checkpoint_restore_continues_identically():
+    from laqphysics_b200.streaming_surface import VolkovAccumulator
+    g = golden('volkov')
+    h, base, ion, contractor, avec = _setup()
+    acc = VolkovAccumulator(contractor, CONFIG, avec, device=DEVICE)
+    for i in range(8):
+        acc.add(i, g['times'][i], g['q'][i])
+    saved = {k: np.array(v, copy=True) for k, v in acc.payload().items()}
+    resumed = VolkovAccumulator(contractor, CONFIG, avec, device=DEVICE)
+    resumed.restore(saved)
+    for i in range(8, len(g['times'])):
+        resumed.add(i, g['times'][i], g['q'][i])
+    np.testing.assert_allclose(resumed.amplitude.cpu().numpy(), g['amplitude'], rtol=3e-12, atol=3e-12)
+    with pytest.raises(ValueError, match='nonsequential'):
+        resumed.add(3, 0., g['q'][0])
+
+
+def test_fused_surface_sample_from_device_state():
+    """flux frame of a device state -> contraction -> accumulation, no host copies,
+    equals the host flux + reference-order contraction."""
+    from laqphysics_b200.engine import B200Hamiltonian
+    from laqphysics_b200.streaming_surface import SurfaceSampler, VolkovAccumulator
+    from laqphysics_b200.workloads import seeded_state
+    g = golden('volkov')
+    h, base, ion, contractor, avec = _setup()
+    op = B200Hamiltonian(h, DEVICE)
+    sampler = SurfaceSampler(op, contractor, VolkovAccumulator(contractor, CONFIG, avec, device=DEVICE))
+    ref_acc = VolkovAccumulator(contractor, CONFIG, avec, device=DEVICE)
+    for i, t in enumerate(g['times'][:5]):
+        x = seeded_state(h.size, 100 + i)
+        q = sampler.record(i, t, op.state(x), avec(t), g['chi'][i])
+        q_ref = contractor(g['chi'][i], h.flux(x, avec(t)))
+        np.testing.assert_allclose(q.cpu().numpy(), q_ref, rtol=1e-11, atol=1e-13)
+        ref_acc.add(i, t, q_ref)
+    np.testing.assert_allclose(sampler.accumulator.amplitude.cpu().numpy(), ref_acc.amplitude.cpu().numpy(),
+                               rtol=1e-11, atol=1e-13)
