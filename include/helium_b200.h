@@ -197,6 +197,20 @@ int he_volkov_add(int nlab, int nouter, int ns, int ne, int nang, const void *q,
                   void *stream);
 
 /* ------------------------------------------------------------------------------------
+ * Batched norms with no device allocation.  No counterpart in the reference: it serves
+ * callers that cannot let a call allocate device memory (a process whose device memory
+ * belongs to a pool allocator, a latency-critical loop that must not stall on the
+ * allocator, a host runtime that forbids allocations outside its own allocator).
+ * norms[v] = ||x + v*ld|| for v < count, count <= 64 (larger counts are rejected with
+ * HE_ERR_ARG); x: complex128 device vectors of n elements; norms: host memory.  The
+ * scratch is a fixed file-scope device array (152,064 bytes, held by every GPU that loads
+ * the library until exit), shared by all calls: calls that overlap on the GPU race.  The
+ * first call on a device looks up that array's address and should come before any
+ * stream capture on the device.  Blocks the host until the norms are ready.
+ * ---------------------------------------------------------------------------------- */
+int he_vec_norms_noalloc(long long n, int count, const void *x, long long ld, double *norms, void *stream);
+
+/* ------------------------------------------------------------------------------------
  * Operator set-up options and planner inspection (host only, no device work).
  * he_set_path: 1 = tiled kernels (default when the tables admit them), 0 = generic.
  * he_plan_build / he_plan_array / he_plan_free expose the tiled plan of a set of tables.
