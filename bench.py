@@ -39,6 +39,7 @@ def parse():
     p.add_argument('--warmup', type=int, default=5)
     p.add_argument('--impl', choices=['b200', 'reference'], default='b200')
     p.add_argument('--no-cpu-baseline', action='store_true')
+    p.add_argument('--no-arnoldi', action='store_true', help='skip the Arnoldi steps/s leg')
     p.add_argument('--profile', choices=['c128', 'c64'], default=None,
                    help='run only W+K applications of one precision (for ncu captures); prints no JSON')
     return p.parse_args()
@@ -148,6 +149,55 @@ def cpu_oracle_rate(h, psi, field, budget_s):
     sample = (f'{reps} x H.psi over output channels 0..{count - 1} of {h.nc} '
               f'({count / h.nc:.3f} of the state each), complex128, {elapsed:.1f} s')
     return gbs, cpu.threads(), sample
+
+
+def arnoldi_leg(torch, device, steps, cpu_steps):
+    """Plain FP64 Arnoldi propagation (the reference's propagate.step driven as in
+    run3d.py:196-199, length gauge, field E(t) along z): 15 elements x order 8 + 12-point
+    ECS tail (n=132), coupled l<=3 L<=2 (nc=17), ground-state start, maxdim 12, dt 0.02,
+    sin^2 pulse omega 1.6, 10 cycles, F0 0.01.  Returns steps/s on the device and of the
+    oracle on the host, plus Krylov dimensions."""
+    from laqphysics_b200 import workloads
+    from laqphysics_b200.engine import B200Hamiltonian
+    from laqphysics_b200.torch_backend import FieldSchedule, step
+    h, hreal = workloads.arnoldi_small(), workloads.arnoldi_small_real()
+    E0, g, _ = hreal.ground(tol=1e-9)
+    ratio = np.sqrt(h.grid.weights / hreal.grid.weights)
+    psi0 = (g.reshape(h.shape, order='F') * ratio[:, None, None] * ratio[None, :, None]).ravel(order='F')
+    engine = B200Hamiltonian(h, device)
+    pulse = workloads.length_pulse()
+    field = lambda t: (0., 0., float(pulse.electric(t)))
+    apply_at = FieldSchedule(engine, field, velocity=False)
+    dt, tol, maxdim = .02, 1e-10, 12
+    state = engine.state(psi0)
+    for i in range(3):
+        state, _ = step(apply_at, state, i * dt, dt, tol, maxdim)
+    torch.cuda.synchronize(device)
+    dims = []
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    t0 = time.perf_counter()
+    for i in range(3, 3 + steps):
+        state, info = step(apply_at, state, i * dt, dt, tol, maxdim)
+        dims.append(info['dimension'])
+    stop.record()
+    torch.cuda.synchronize(device)
+    ms = start.elapsed_time(stop)
+    out = {'workload': 'Arnoldi FP64 length gauge: n=132 nc=17 (N=296,208), maxdim 12, dt 0.02, ground-state start',
+           'steps': steps, 'steps_per_s': steps / (ms * 1e-3), 'ms_per_step': ms / steps,
+           'mean_dimension': float(np.mean(dims)), 'ground_energy': E0}
+    if cpu_steps:
+        from oracle import arnoldi, cpu
+        x = psi0.copy()
+        tables = cpu.host_tables(h)
+        t0 = time.perf_counter()
+        for i in range(cpu_steps):
+            x, _ = arnoldi.step(lambda t, y: cpu.tensor_apply(h, y, field(t), False, tables=tables), x, i * dt, dt,
+                                tol, maxdim)
+        el = time.perf_counter() - t0
+        out['cpu_baseline'] = {'steps_per_s': cpu_steps / el, 'cores': cpu.threads(), 'kind': 'port',
+                               'sample': f'{cpu_steps} Arnoldi steps (oracle numpy Arnoldi + C tensor_apply)'}
+    return out
 
 
 def run_reference(args, rank):
@@ -292,6 +342,9 @@ def main():
                 'path': 'pinned host psi -> H2D -> B200Hamiltonian.apply -> D2H pinned host'},
         'clocks': clocks.summary(),
     }
+    if not args.no_arnoldi:
+        line['arnoldi'] = arnoldi_leg(torch, device, steps=max(10, min(args.steps, 100)),
+                                      cpu_steps=0 if (args.no_cpu_baseline or world > 1 or rank) else 3)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         os.environ.setdefault('OMP_NUM_THREADS', str(os.cpu_count()))
         gbs, cores, sample = cpu_oracle_rate(h, workloads.seeded_state(N, 1234), field, 15.0)

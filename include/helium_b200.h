@@ -133,6 +133,11 @@ int he_krylov_combine(he_krylov_handle k, int m, void *y, void *stream);
  * Krylov vectors).  x, y: n*n*nc complex128 device vectors, y != x. */
 int he_expv(he_krylov_handle k, he_handle op, const void *x, void *y, const double *field, int velocity,
             double dt, double tol, int maxdim, int *dimension, double *estimate, void *stream);
+/* Mixed precision: as he_expv, but each H·psi runs in complex64 with FP32 accumulation
+ * (the operator needs complex64 tables); the basis, CGS2, the Hessenberg exponential
+ * and the error estimate stay complex128. */
+int he_expv_mixed(he_krylov_handle k, he_handle op, const void *x, void *y, const double *field, int velocity,
+                  double dt, double tol, int maxdim, int *dimension, double *estimate, void *stream);
 
 /* ------------------------------------------------------------------------------------
  * GMRES / CF4 building blocks (python/implicit.py:45-109).  The GMRES driver keeps its

@@ -41,6 +41,7 @@ SIGNATURES = {
     'he_expv_check': (I, [P, I, I, D, D, I, ct.POINTER(I), ct.POINTER(I), ct.POINTER(D), P]),
     'he_krylov_combine': (I, [P, I, P, P]),
     'he_expv': (I, [P, P, P, P, P, I, D, D, I, ct.POINTER(I), ct.POINTER(D), P]),
+    'he_expv_mixed': (I, [P, P, P, P, P, I, D, D, I, ct.POINTER(I), ct.POINTER(D), P]),
     'he_set_path': (I, [P, I]),
     'he_vec_axpby': (I, [ct.c_longlong, D, D, P, D, D, P, P, P]),
     'he_vec_residual_norm': (I, [ct.c_longlong, P, P, P, ct.POINTER(D), P]),

@@ -41,7 +41,7 @@ struct AxisTile {
     int lines, linechunks;               // lines of the other axis, ceil(lines / 32)
     int s[RAD_ELEMS], m[RAD_ELEMS], own[RAD_ELEMS], real[RAD_ELEMS], chunks[RAD_ELEMS];
     int off[RAD_ELEMS];                  // offset of the element's block in the staged blocks
-    int tasks[RAD_ELEMS + 1];            // prefix sums of warp tasks (row chunks x line chunks)
+    int tasks[RAD_ELEMS + 1];            // prefix sums of per-lane items (row chunks x lines)
     int prev, prev_m, prev_real, prev_off;   // previous element (bridge row), -1 if none
 };
 
@@ -73,7 +73,7 @@ __device__ void stage_axis(const TiledPlan<R> &pl, AxisTile &ax, int ga, int gb,
             ax.chunks[k] = ax.m[k] <= EMAX ? 1 : (ax.own[k] + EMAX - 1) / EMAX;
             ax.off[k] = off;
             off += ax.m[k] * ax.m[k];
-            ax.tasks[k + 1] = ax.tasks[k] + ax.chunks[k] * ax.linechunks;
+            ax.tasks[k + 1] = ax.tasks[k] + ax.chunks[k] * ax.lines;   // per-lane items
         }
     }
     __syncthreads();
@@ -95,11 +95,48 @@ __device__ void stage_axis(const TiledPlan<R> &pl, AxisTile &ax, int ga, int gb,
     }
 }
 
-// acc[a] = sum_b blk[a m + b] x[b] for a < na, b < m <= EMAX (m, na warp uniform).
-template <typename R, bool REAL>
-__device__ __forceinline__ void small_rows(const cplx<R> *blk, int m, int na, const cplx<R> (&x)[EMAX],
+// ---------------------------------------------------------------------------------
+// Asynchronous global -> shared copies (cp.async, zero fill when src_bytes == 0).
+// ---------------------------------------------------------------------------------
+template <int BYTES> __device__ __forceinline__ void cp_async(void *smem, const void *gmem, int src_bytes)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    if (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(gmem), "r"(src_bytes) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(s), "l"(gmem), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// acc[a] = sum_b blk[a M + b] x[b], a < na, for an element of exactly M nodes.
+template <typename R, bool REAL, int M>
+__device__ __forceinline__ void rows_fixed(const cplx<R> *blk, int na, const cplx<R> *xs, int xstride,
                                            cplx<R> (&acc)[EMAX])
 {
+    cplx<R> x[M];
+#pragma unroll
+    for (int b = 0; b < M; ++b) x[b] = xs[b * xstride];
+#pragma unroll
+    for (int a = 0; a < M; ++a) {
+        if (a < na) {
+            const cplx<R> *row = blk + a * M;
+            cplx<R> s = mk<R>(0, 0);
+#pragma unroll
+            for (int b = 0; b < M; ++b) s = REAL ? rfma<R>(row[b].x, x[b], s) : cfma<R>(row[b], x[b], s);
+            acc[a] = s;
+        }
+    }
+}
+
+// Same for any m <= EMAX (predicated; used for element sizes without a fixed variant).
+template <typename R, bool REAL>
+__device__ __forceinline__ void rows_any(const cplx<R> *blk, int m, int na, const cplx<R> *xs, int xstride,
+                                         cplx<R> (&acc)[EMAX])
+{
+    cplx<R> x[EMAX];
+#pragma unroll
+    for (int b = 0; b < EMAX; ++b) x[b] = b < m ? xs[b * xstride] : mk<R>(0, 0);
 #pragma unroll
     for (int a = 0; a < EMAX; ++a) {
         if (a < na) {
@@ -110,6 +147,19 @@ __device__ __forceinline__ void small_rows(const cplx<R> *blk, int m, int na, co
                 if (b < m) s = REAL ? rfma<R>(row[b].x, x[b], s) : cfma<R>(row[b], x[b], s);
             acc[a] = s;
         }
+    }
+}
+
+template <typename R, bool REAL>
+__device__ __forceinline__ void rows_small(const cplx<R> *blk, int m, int na, const cplx<R> *xs, int xstride,
+                                           cplx<R> (&acc)[EMAX])
+{
+    switch (m) {   // m is warp uniform: the common FE orders get exact unrolls
+    case 8: rows_fixed<R, REAL, 8>(blk, na, xs, xstride, acc); break;
+    case 9: rows_fixed<R, REAL, 9>(blk, na, xs, xstride, acc); break;
+    case 10: rows_fixed<R, REAL, 10>(blk, na, xs, xstride, acc); break;
+    case 11: rows_fixed<R, REAL, 11>(blk, na, xs, xstride, acc); break;
+    default: rows_any<R, REAL>(blk, m, na, xs, xstride, acc); break;
     }
 }
 
@@ -128,11 +178,8 @@ __device__ __forceinline__ void element_line(const AxisTile &ax, int k, const cp
 #pragma unroll
     for (int q = 0; q < EMAX; ++q) acc[q] = mk<R>(0, 0);
     if (m <= EMAX) {
-        cplx<R> x[EMAX];
-#pragma unroll
-        for (int b = 0; b < EMAX; ++b) x[b] = b < m ? xs[b * xstride] : mk<R>(0, 0);
-        if (ax.real[k]) small_rows<R, true>(blk, m, na, x, acc);
-        else small_rows<R, false>(blk, m, na, x, acc);
+        if (ax.real[k]) rows_small<R, true>(blk, m, na, xs, xstride, acc);
+        else rows_small<R, false>(blk, m, na, xs, xstride, acc);
     } else {   // large element (the exterior-scaled tail): stream over its nodes
         const bool real = ax.real[k];
         for (int b = 0; b < m; ++b) {
@@ -175,15 +222,14 @@ __device__ void radial_phase(const AxisTile &ax, const cplx<R> *BLK, const cplx<
                              cplx<R> *OS, int base, int r0, int c0, int n, const cplx<R> *pc, cplx<R> *wout,
                              size_t nn, int c)
 {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const int ntasks = ax.tasks[ax.count];
-    for (int task = warp; task < ntasks; task += nwarps) {
+    // Items are (element k, row chunk, line), line fastest, flattened over the tile so that
+    // every lane of every warp has one; neighbouring lanes share the element's block.
+    const int nitems = ax.tasks[ax.count];
+    for (int item = threadIdx.x; item < nitems; item += blockDim.x) {
         int k = 0;
-        while (k + 1 < ax.count && task >= ax.tasks[k + 1]) ++k;
-        const int rest = task - ax.tasks[k];
-        const int lc = rest % ax.linechunks, chunk = rest / ax.linechunks;
-        const int line = lc * 32 + lane;
-        if (line >= ax.lines) continue;
+        while (k + 1 < ax.count && item >= ax.tasks[k + 1]) ++k;
+        const int rest = item - ax.tasks[k];
+        const int line = rest % ax.lines, chunk = rest / ax.lines;
         const int s = ax.s[k];
         const int a0 = chunk * EMAX, na = min(EMAX, ax.own[k] - a0);
         cplx<R> acc[EMAX];
@@ -212,16 +258,31 @@ __device__ void radial_phase(const AxisTile &ax, const cplx<R> *BLK, const cplx<
 }
 
 // ---------------------------------------------------------------------------------
-// Radial stencil kernel.  grid = (ntile * ntile, nc); one channel-tile per CTA.
+// Radial stencil kernel.  grid = (ntile * ntile, ceil(nc / RAD_CH)); a CTA owns one tile
+// and RAD_CH channels.  The staged psi of channel c+1 streams in (cp.async, second
+// buffer) while channel c is computed.
 // ---------------------------------------------------------------------------------
+constexpr int RAD_CH = 4;
+
+template <typename R>
+__device__ __forceinline__ void radial_prefetch(const cplx<R> *pc, cplx<R> *dst, int r0, int c0, int rs, int cs, int n)
+{
+    for (int idx = threadIdx.x; idx < rs * cs; idx += blockDim.x) {
+        const int a = idx % rs, b = idx / rs;
+        cp_async<sizeof(cplx<R>)>(dst + a * RAD_STRIDE + b, pc + (size_t)(r0 + a) + (size_t)n * (c0 + b),
+                                  (int)sizeof(cplx<R>));
+    }
+    cp_async_commit();
+}
+
 template <typename R, bool VEL, bool SEP>
 __global__ void __launch_bounds__(RAD_THREADS, 2)
 hpsi_radial_kernel(const DeviceTables<R> t, const TiledPlan<R> pl, const cplx<R> *__restrict__ psi,
                    cplx<R> *__restrict__ out, cplx<R> *__restrict__ w1, cplx<R> *__restrict__ w2, R a2, int blkmax)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cplx<R> *PS = reinterpret_cast<cplx<R> *>(smem_raw);
-    cplx<R> *OS = PS + RAD_STRIDE * RAD_STRIDE;
+    cplx<R> *PSB = reinterpret_cast<cplx<R> *>(smem_raw);          // two staged psi buffers
+    cplx<R> *OS = PSB + 2 * RAD_STRIDE * RAD_STRIDE;
     cplx<R> *B0 = OS + RAD_TMAX * RAD_STRIDE;        // electron-1 blocks (T), then B if VEL
     cplx<R> *B0B = B0 + blkmax;
     cplx<R> *B1 = B0 + (VEL ? 2 : 1) * blkmax;       // electron-2 blocks
@@ -229,7 +290,8 @@ hpsi_radial_kernel(const DeviceTables<R> t, const TiledPlan<R> pl, const cplx<R>
     __shared__ AxisTile ax0, ax1;
 
     const int n = pl.n;
-    const int ti = blockIdx.x % pl.ntile, tj = blockIdx.x / pl.ntile, c = blockIdx.y;
+    const int ti = blockIdx.x % pl.ntile, tj = blockIdx.x / pl.ntile;
+    const int cbeg = blockIdx.y * RAD_CH, cend = min(pl.nc, cbeg + RAD_CH);
     const int ea = pl.tstart[ti], eb = pl.tstart[ti + 1];
     const int fa = pl.tstart[tj], fb = pl.tstart[tj + 1];
     const int r0 = pl.estart[ea], r1 = pl.estart[eb];          // owned rows [r0, r1)
@@ -237,45 +299,53 @@ hpsi_radial_kernel(const DeviceTables<R> t, const TiledPlan<R> pl, const cplx<R>
     const int rs = min(r1 + 1, n) - r0, cs = min(c1 + 1, n) - c0;   // staged extents (+ right bridge)
     const int ro = r1 - r0, co = c1 - c0;
     const size_t nn = (size_t)n * n;
-    const cplx<R> *pc = psi + nn * c;
 
-    for (int idx = threadIdx.x; idx < rs * cs; idx += blockDim.x) {
-        const int a = idx % rs, b = idx / rs;
-        PS[a * RAD_STRIDE + b] = pc[(size_t)(r0 + a) + (size_t)n * (c0 + b)];
-    }
+    radial_prefetch<R>(psi + nn * cbeg, PSB, r0, c0, rs, cs, n);
     stage_axis<R>(pl, ax0, ea, eb, co, B0, B0B, VEL);
     stage_axis<R>(pl, ax1, fa, fb, ro, B1, B1B, VEL);
-    __syncthreads();
-    radial_phase<R, VEL, true>(ax0, B0, B0B, PS, OS, r0, r0, c0, n, pc, w1, nn, c);
-    __syncthreads();
-    radial_phase<R, VEL, false>(ax1, B1, B1B, PS, OS, c0, r0, c0, n, pc, w2, nn, c);
-    __syncthreads();
-
-    for (int idx = threadIdx.x; idx < ro * co; idx += blockDim.x) {
-        const int a = idx % ro, b = idx / ro;
-        const int i = r0 + a, j = c0 + b;
-        const size_t p = (size_t)i + (size_t)n * j;
-        const cplx<R> x = PS[a * RAD_STRIDE + b];
-        const cplx<R> d = SEP ? cadd<R>(ldg<R>(t.d1 + i + (size_t)n * c), ldg<R>(t.d2 + j + (size_t)n * c))
-                              : ldg<R>(t.diag + p + nn * c);
-        cplx<R> v = cfma<R>(d, x, OS[a * RAD_STRIDE + b]);
-        if (VEL) v = rfma<R>(a2, x, v);
-        out[p + nn * c] = v;
+    for (int c = cbeg; c < cend; ++c) {
+        const int buf = (c - cbeg) & 1;
+        cplx<R> *PS = PSB + buf * RAD_STRIDE * RAD_STRIDE;
+        if (c + 1 < cend) {
+            radial_prefetch<R>(psi + nn * (c + 1), PSB + (buf ^ 1) * RAD_STRIDE * RAD_STRIDE, r0, c0, rs, cs, n);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const cplx<R> *pc = psi + nn * c;
+        radial_phase<R, VEL, true>(ax0, B0, B0B, PS, OS, r0, r0, c0, n, pc, w1, nn, c);
+        __syncthreads();
+        radial_phase<R, VEL, false>(ax1, B1, B1B, PS, OS, c0, r0, c0, n, pc, w2, nn, c);
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < ro * co; idx += blockDim.x) {
+            const int a = idx % ro, b = idx / ro;
+            const int i = r0 + a, j = c0 + b;
+            const size_t p = (size_t)i + (size_t)n * j;
+            const cplx<R> x = PS[a * RAD_STRIDE + b];
+            const cplx<R> d = SEP ? cadd<R>(ldg<R>(t.d1 + i + (size_t)n * c), ldg<R>(t.d2 + j + (size_t)n * c))
+                                  : ldg<R>(t.diag + p + nn * c);
+            cplx<R> v = cfma<R>(d, x, OS[a * RAD_STRIDE + b]);
+            if (VEL) v = rfma<R>(a2, x, v);
+            out[p + nn * c] = v;
+        }
+        __syncthreads();   // PS[buf] and OS are reused by the next channels
     }
 }
 
 // ---------------------------------------------------------------------------------
-// Channel-mixing kernel.  CTA = MIX_NP consecutive flattened points p = i + n j.
-// Shared memory: PSI[c][MIX_NP], RAD[lam][MIX_NP], wide Coulomb edges (source offset,
-// MIX_GROUP coefficients), group x lam offsets, wide dipole edges with their
-// field-contracted coefficients per group slot:
+// Channel-mixing kernel.  Persistent over tiles of MIX_NP consecutive flattened points
+// p = i + n j; one warp per output group; the group tables are staged once per CTA and
+// the psi/rad tile of the next point block streams in (cp.async) while the current one
+// is computed.
+// Shared memory: tables, then two stages of PSI[c][MIX_NP] + RAD[lam][MIX_NP].  Wide
+// dipole coefficients per group slot are field contracted at staging:
 //   length gauge   DA = coef_k                (acc += DA r_a psi_s)
 //   velocity gauge DA = i coef_k ldiff_k, DB = i coef_k   (acc += DA psi_s/(2 r_a) + DB W_a[s])
 // with coef_k = field . dcoef(:, k), zero below 1e-30 (the skip of src/kernels.f90:145).
-// A warp task is one output group over all MIX_NP points (two per lane).
 // ---------------------------------------------------------------------------------
 template <typename R> struct MixSmem {
-    cplx<R> *psi, *rad, *da, *db;
+    cplx<R> *da, *db, *stage;
     R *wcoef;
     int *wsrc, *wptr, *dsrc, *del;
 };
@@ -284,11 +354,10 @@ template <typename R>
 __device__ __forceinline__ MixSmem<R> mix_layout(unsigned char *raw, const TiledPlan<R> &pl)
 {
     MixSmem<R> s;
-    s.psi = reinterpret_cast<cplx<R> *>(raw);
-    s.rad = s.psi + (size_t)pl.nc * MIX_NP;
-    s.da = s.rad + (size_t)pl.nlam * MIX_NP;
+    s.da = reinterpret_cast<cplx<R> *>(raw);
     s.db = s.da + (size_t)max(pl.nwd, 1) * MIX_GROUP;
-    s.wcoef = reinterpret_cast<R *>(s.db + (size_t)max(pl.nwd, 1) * MIX_GROUP);
+    s.stage = s.db + (size_t)max(pl.nwd, 1) * MIX_GROUP;
+    s.wcoef = reinterpret_cast<R *>(s.stage + 2 * (size_t)(pl.nc + pl.nlam) * MIX_NP);
     s.wsrc = reinterpret_cast<int *>(s.wcoef + (size_t)pl.nwide * MIX_GROUP);
     s.wptr = s.wsrc + pl.nwide;
     s.dsrc = s.wptr + pl.ng * pl.nlam + 1;
@@ -296,8 +365,23 @@ __device__ __forceinline__ MixSmem<R> mix_layout(unsigned char *raw, const Tiled
     return s;
 }
 
+template <typename R>
+__device__ __forceinline__ void mix_prefetch(const cplx<R> *psi, const cplx<R> *rad, size_t nn, int nc, int nlam,
+                                             size_t p0, cplx<R> *dst)
+{
+    const int rows = nc + nlam;
+    for (int idx = threadIdx.x; idx < rows * MIX_NP; idx += blockDim.x) {
+        const int q = idx % MIX_NP, row = idx / MIX_NP;
+        const size_t p = p0 + q;
+        const bool ok = p < nn;
+        const cplx<R> *src = row < nc ? psi + (ok ? p : 0) + nn * row : rad + (ok ? p : 0) + nn * (row - nc);
+        cp_async<sizeof(cplx<R>)>(dst + idx, src, ok ? (int)sizeof(cplx<R>) : 0);
+    }
+    cp_async_commit();
+}
+
 template <typename R, bool VEL>
-__global__ void __launch_bounds__(MIX_THREADS)
+__global__ void __launch_bounds__(512, 1)
 hpsi_mix_kernel(const DeviceTables<R> t, const TiledPlan<R> pl, const cplx<R> *__restrict__ psi,
                 cplx<R> *__restrict__ out, const cplx<R> *__restrict__ w1, const cplx<R> *__restrict__ w2,
                 R f0, R f1, R f2, cplx<R> beta, cplx<R> gamma)
@@ -306,17 +390,11 @@ hpsi_mix_kernel(const DeviceTables<R> t, const TiledPlan<R> pl, const cplx<R> *_
     const int n = pl.n, nc = pl.nc, nlam = pl.nlam;
     const MixSmem<R> S = mix_layout<R>(smem_raw, pl);
     const size_t nn = (size_t)n * n;
-    const size_t p0 = (size_t)blockIdx.x * MIX_NP;
-    const int np = (int)min((size_t)MIX_NP, nn - p0);
+    const size_t ntiles = (nn + MIX_NP - 1) / MIX_NP;
+    const int stage_elems = (nc + nlam) * MIX_NP;
 
-    for (int idx = threadIdx.x; idx < nc * MIX_NP; idx += blockDim.x) {
-        const int q = idx % MIX_NP, cc = idx / MIX_NP;
-        S.psi[idx] = q < np ? psi[p0 + q + nn * cc] : mk<R>(0, 0);
-    }
-    for (int idx = threadIdx.x; idx < nlam * MIX_NP; idx += blockDim.x) {
-        const int q = idx % MIX_NP, lam = idx / MIX_NP;
-        S.rad[idx] = q < np ? ldg<R>(t.rad + p0 + q + nn * lam) : mk<R>(0, 0);
-    }
+    size_t tile = blockIdx.x;
+    if (tile < ntiles) mix_prefetch<R>(psi, t.rad, nn, nc, nlam, tile * MIX_NP, S.stage);
     for (int idx = threadIdx.x; idx < pl.nwd * MIX_GROUP; idx += blockDim.x) {
         const int kk = pl.dwedge[idx];
         cplx<R> a = mk<R>(0, 0), b = mk<R>(0, 0);
@@ -343,96 +421,112 @@ hpsi_mix_kernel(const DeviceTables<R> t, const TiledPlan<R> pl, const cplx<R> *_
         S.dsrc[k] = pl.dwsrc[k] * MIX_NP;
         S.del[k] = pl.dwel[k];
     }
-    __syncthreads();
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const bool v0 = lane < np, v1 = lane + 32 < np;
-    const size_t pa = p0 + lane, pb = p0 + lane + 32;
-    for (int g = warp; g < pl.ng; g += nwarps) {
-        int ch[MIX_GROUP];
-        cplx<R> a0[MIX_GROUP], a1[MIX_GROUP];
-#pragma unroll
-        for (int d = 0; d < MIX_GROUP; ++d) {
-            ch[d] = __ldg(pl.gch + g * MIX_GROUP + d);
-            a0[d] = (v0 && ch[d] >= 0) ? out[pa + nn * ch[d]] : mk<R>(0, 0);
-            a1[d] = (v1 && ch[d] >= 0) ? out[pb + nn * ch[d]] : mk<R>(0, 0);
+    for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
+        const int buf = it & 1;
+        const cplx<R> *PSI = S.stage + buf * stage_elems;
+        const cplx<R> *RAD = PSI + (size_t)nc * MIX_NP;
+        const size_t next = tile + gridDim.x;
+        if (next < ntiles) {
+            mix_prefetch<R>(psi, t.rad, nn, nc, nlam, next * MIX_NP, S.stage + (buf ^ 1) * stage_elems);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
         }
-        const int *wp = S.wptr + g * nlam;
-        for (int lam = 0; lam < nlam; ++lam) {
-            const int k0 = wp[lam], k1 = wp[lam + 1];
-            if (k0 == k1) continue;
-            cplx<R> t0[MIX_GROUP], t1[MIX_GROUP];
+        __syncthreads();
+        const size_t p0 = tile * MIX_NP;
+        const int np = (int)min((size_t)MIX_NP, nn - p0);
+        const bool v0 = lane < np, v1 = lane + 32 < np;
+        const size_t pa = p0 + lane, pb = p0 + lane + 32;
+        for (int g = warp; g < pl.ng; g += nwarps) {
+            int ch[MIX_GROUP];
+            cplx<R> o0[MIX_GROUP], o1[MIX_GROUP], a0[MIX_GROUP], a1[MIX_GROUP];
 #pragma unroll
-            for (int d = 0; d < MIX_GROUP; ++d) { t0[d] = mk<R>(0, 0); t1[d] = mk<R>(0, 0); }
+            for (int d = 0; d < MIX_GROUP; ++d) {   // radial part: loads issued now, used at the end
+                ch[d] = __ldg(pl.gch + g * MIX_GROUP + d);
+                o0[d] = (v0 && ch[d] >= 0) ? out[pa + nn * ch[d]] : mk<R>(0, 0);
+                o1[d] = (v1 && ch[d] >= 0) ? out[pb + nn * ch[d]] : mk<R>(0, 0);
+                a0[d] = mk<R>(0, 0);
+                a1[d] = mk<R>(0, 0);
+            }
+            const int *wp = S.wptr + g * nlam;
+            for (int lam = 0; lam < nlam; ++lam) {
+                const int k0 = wp[lam], k1 = wp[lam + 1];
+                if (k0 == k1) continue;
+                cplx<R> t0[MIX_GROUP], t1[MIX_GROUP];
+#pragma unroll
+                for (int d = 0; d < MIX_GROUP; ++d) { t0[d] = mk<R>(0, 0); t1[d] = mk<R>(0, 0); }
 #pragma unroll 2
-            for (int k = k0; k < k1; ++k) {
-                const int off = S.wsrc[k];
-                const cplx<R> x0 = S.psi[off + lane], x1 = S.psi[off + lane + 32];
-                const R *cf = S.wcoef + k * MIX_GROUP;
-#pragma unroll
-                for (int d = 0; d < MIX_GROUP; ++d) {
-                    const R w = cf[d];
-                    t0[d] = rfma<R>(w, x0, t0[d]);
-                    t1[d] = rfma<R>(w, x1, t1[d]);
-                }
-            }
-            const cplx<R> r0 = S.rad[lam * MIX_NP + lane], r1 = S.rad[lam * MIX_NP + lane + 32];
-#pragma unroll
-            for (int d = 0; d < MIX_GROUP; ++d) {
-                a0[d] = cfma<R>(r0, t0[d], a0[d]);
-                a1[d] = cfma<R>(r1, t1[d], a1[d]);
-            }
-        }
-        const int k0 = __ldg(pl.dwptr + g), k1 = __ldg(pl.dwptr + g + 1);
-        if (k0 < k1) {
-            const int ia = (int)(pa % n), ja = (int)(pa / n), ib = (int)(pb % n), jb = (int)(pb / n);
-            // per point and electron: r (length) or 1/(2r) (velocity)
-            const cplx<R> *rt = VEL ? t.hinv : t.r;
-            const cplx<R> ra1 = v0 ? ldg<R>(rt + ia) : mk<R>(0, 0), ra2 = v0 ? ldg<R>(rt + ja) : mk<R>(0, 0);
-            const cplx<R> rb1 = v1 ? ldg<R>(rt + ib) : mk<R>(0, 0), rb2 = v1 ? ldg<R>(rt + jb) : mk<R>(0, 0);
-            for (int k = k0; k < k1; ++k) {
-                const int off = S.dsrc[k];
-                const bool first = S.del[k] == 1;
-                const cplx<R> y0 = cmul<R>(first ? ra1 : ra2, S.psi[off + lane]);
-                const cplx<R> y1 = cmul<R>(first ? rb1 : rb2, S.psi[off + lane + 32]);
-                const cplx<R> *da = S.da + k * MIX_GROUP;
-#pragma unroll
-                for (int d = 0; d < MIX_GROUP; ++d) {
-                    a0[d] = cfma<R>(da[d], y0, a0[d]);
-                    a1[d] = cfma<R>(da[d], y1, a1[d]);
-                }
-                if (VEL) {
-                    const int s = off / MIX_NP;
-                    const cplx<R> *wsrc = first ? w1 : w2;
-                    const cplx<R> wa = v0 ? wsrc[pa + nn * s] : mk<R>(0, 0);
-                    const cplx<R> wb = v1 ? wsrc[pb + nn * s] : mk<R>(0, 0);
-                    const cplx<R> *db = S.db + k * MIX_GROUP;
+                for (int k = k0; k < k1; ++k) {
+                    const int off = S.wsrc[k];
+                    const cplx<R> x0 = PSI[off + lane], x1 = PSI[off + lane + 32];
+                    const R *cf = S.wcoef + k * MIX_GROUP;
 #pragma unroll
                     for (int d = 0; d < MIX_GROUP; ++d) {
-                        a0[d] = cfma<R>(db[d], wa, a0[d]);
-                        a1[d] = cfma<R>(db[d], wb, a1[d]);
+                        const R w = cf[d];
+                        t0[d] = rfma<R>(w, x0, t0[d]);
+                        t1[d] = rfma<R>(w, x1, t1[d]);
+                    }
+                }
+                const cplx<R> r0 = RAD[lam * MIX_NP + lane], r1 = RAD[lam * MIX_NP + lane + 32];
+#pragma unroll
+                for (int d = 0; d < MIX_GROUP; ++d) {
+                    a0[d] = cfma<R>(r0, t0[d], a0[d]);
+                    a1[d] = cfma<R>(r1, t1[d], a1[d]);
+                }
+            }
+            const int k0 = __ldg(pl.dwptr + g), k1 = __ldg(pl.dwptr + g + 1);
+            if (k0 < k1) {
+                const int ia = (int)(pa % n), ja = (int)(pa / n), ib = (int)(pb % n), jb = (int)(pb / n);
+                const cplx<R> *rt = VEL ? t.hinv : t.r;   // r (length) or 1/(2r) (velocity)
+                const cplx<R> ra1 = v0 ? ldg<R>(rt + ia) : mk<R>(0, 0), ra2 = v0 ? ldg<R>(rt + ja) : mk<R>(0, 0);
+                const cplx<R> rb1 = v1 ? ldg<R>(rt + ib) : mk<R>(0, 0), rb2 = v1 ? ldg<R>(rt + jb) : mk<R>(0, 0);
+                for (int k = k0; k < k1; ++k) {
+                    const int off = S.dsrc[k];
+                    const bool first = S.del[k] == 1;
+                    const cplx<R> y0 = cmul<R>(first ? ra1 : ra2, PSI[off + lane]);
+                    const cplx<R> y1 = cmul<R>(first ? rb1 : rb2, PSI[off + lane + 32]);
+                    const cplx<R> *da = S.da + k * MIX_GROUP;
+#pragma unroll
+                    for (int d = 0; d < MIX_GROUP; ++d) {
+                        a0[d] = cfma<R>(da[d], y0, a0[d]);
+                        a1[d] = cfma<R>(da[d], y1, a1[d]);
+                    }
+                    if (VEL) {
+                        const int s = off / MIX_NP;
+                        const cplx<R> *wsrc = first ? w1 : w2;
+                        const cplx<R> wa = v0 ? wsrc[pa + nn * s] : mk<R>(0, 0);
+                        const cplx<R> wb = v1 ? wsrc[pb + nn * s] : mk<R>(0, 0);
+                        const cplx<R> *db = S.db + k * MIX_GROUP;
+#pragma unroll
+                        for (int d = 0; d < MIX_GROUP; ++d) {
+                            a0[d] = cfma<R>(db[d], wa, a0[d]);
+                            a1[d] = cfma<R>(db[d], wb, a1[d]);
+                        }
                     }
                 }
             }
-        }
 #pragma unroll
-        for (int d = 0; d < MIX_GROUP; ++d) {
-            if (ch[d] < 0) continue;
-            if (v0) out[pa + nn * ch[d]] = cfma<R>(gamma, a0[d], cmul<R>(beta, S.psi[ch[d] * MIX_NP + lane]));
-            if (v1) out[pb + nn * ch[d]] = cfma<R>(gamma, a1[d], cmul<R>(beta, S.psi[ch[d] * MIX_NP + lane + 32]));
+            for (int d = 0; d < MIX_GROUP; ++d) {
+                if (ch[d] < 0) continue;
+                if (v0) out[pa + nn * ch[d]] = cfma<R>(gamma, cadd<R>(a0[d], o0[d]), cmul<R>(beta, PSI[ch[d] * MIX_NP + lane]));
+                if (v1) out[pb + nn * ch[d]] = cfma<R>(gamma, cadd<R>(a1[d], o1[d]), cmul<R>(beta, PSI[ch[d] * MIX_NP + lane + 32]));
+            }
         }
+        __syncthreads();   // the stage buffer is refilled two tiles later
     }
 }
 
 template <typename R> size_t radial_smem(bool vel, int blkmax)
 {
-    return sizeof(cplx<R>) * ((size_t)RAD_STRIDE * RAD_STRIDE + (size_t)RAD_TMAX * RAD_STRIDE +
+    return sizeof(cplx<R>) * (2 * (size_t)RAD_STRIDE * RAD_STRIDE + (size_t)RAD_TMAX * RAD_STRIDE +
                               (vel ? 4 : 2) * (size_t)blkmax);
 }
 
 template <typename R> size_t mix_smem(int nc, int nlam, int ng, int nwide, int nwd)
 {
-    const size_t c = sizeof(cplx<R>) * ((size_t)(nc + nlam) * MIX_NP + 2 * (size_t)std::max(nwd, 1) * MIX_GROUP);
+    const size_t c = sizeof(cplx<R>) * (2 * (size_t)(nc + nlam) * MIX_NP + 2 * (size_t)std::max(nwd, 1) * MIX_GROUP);
     const size_t r = sizeof(R) * (size_t)nwide * MIX_GROUP;
     const size_t i = sizeof(int) * ((size_t)nwide + (size_t)ng * nlam + 1 + 2 * (size_t)nwd);
     return c + r + i + 64;
@@ -446,7 +540,7 @@ int launch_hpsi_tiled(he_operator *h, const DeviceTables<R> &t, const TiledPlan<
     (void)coef;
     const R f0 = (R)field[0], f1 = (R)field[1], f2 = (R)field[2];
     const R a2 = (R)(field[0] * field[0] + field[1] * field[1] + field[2] * field[2]);
-    const dim3 rgrid(pl.ntile * pl.ntile, pl.nc);
+    const dim3 rgrid(pl.ntile * pl.ntile, (pl.nc + RAD_CH - 1) / RAD_CH);
     const int blkmax = h->plan.blkmax;
     const size_t rs = radial_smem<R>(velocity, blkmax);
 #define HE_RADIAL(V, S)                                                                                  \
@@ -461,13 +555,16 @@ int launch_hpsi_tiled(he_operator *h, const DeviceTables<R> &t, const TiledPlan<
     HE_CUDA_TRY(cudaGetLastError());
     const size_t nn = (size_t)pl.n * pl.n;
     const size_t ms = mix_smem<R>(pl.nc, pl.nlam, pl.ng, pl.nwide, pl.nwd);
-    const unsigned blocks = (unsigned)((nn + MIX_NP - 1) / MIX_NP);
+    const size_t ntiles = (nn + MIX_NP - 1) / MIX_NP;
+    const int per_sm = std::max<int>(1, (int)((227 * 1024) / (ms + 1024)));
+    const unsigned blocks = (unsigned)std::min<size_t>(ntiles, (size_t)148 * per_sm);
+    const int threads = 32 * std::min(16, std::max(1, pl.ng));
     if (velocity) {
         HE_CUDA_TRY(cudaFuncSetAttribute(hpsi_mix_kernel<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ms));
-        hpsi_mix_kernel<R, true><<<blocks, MIX_THREADS, ms, stream>>>(t, pl, psi, out, w1, w2, f0, f1, f2, beta, gamma);
+        hpsi_mix_kernel<R, true><<<blocks, threads, ms, stream>>>(t, pl, psi, out, w1, w2, f0, f1, f2, beta, gamma);
     } else {
         HE_CUDA_TRY(cudaFuncSetAttribute(hpsi_mix_kernel<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ms));
-        hpsi_mix_kernel<R, false><<<blocks, MIX_THREADS, ms, stream>>>(t, pl, psi, out, w1, w2, f0, f1, f2, beta, gamma);
+        hpsi_mix_kernel<R, false><<<blocks, threads, ms, stream>>>(t, pl, psi, out, w1, w2, f0, f1, f2, beta, gamma);
     }
     HE_CUDA_TRY(cudaGetLastError());
     return HE_OK;
@@ -480,12 +577,12 @@ template int launch_hpsi_tiled<float>(he_operator *, const DeviceTables<float> &
                                       float2 *, float2 *, const float2 *, float2 *, const double *, int, float2,
                                       float2, cudaStream_t);
 
-// Both kernels must fit two CTAs per SM in complex128.
+// Both kernels must fit in shared memory (one CTA per SM) in complex128.
 bool tiled_fits(const he_plan_host &P, int nc, int nd)
 {
     (void)nd;
-    return mix_smem<double>(nc, P.nlam, P.ng, (int)P.wsrc.size(), (int)P.dwsrc.size()) <= 110 * 1024 &&
-           radial_smem<double>(true, P.blkmax) <= 110 * 1024;
+    return mix_smem<double>(nc, P.nlam, P.ng, (int)P.wsrc.size(), (int)P.dwsrc.size()) <= 200 * 1024 &&
+           radial_smem<double>(true, P.blkmax) <= 200 * 1024;
 }
 
 }  // namespace he

@@ -369,7 +369,7 @@ using namespace he;
 he_krylov::~he_krylov()
 {
     cudaFree(Q); cudaFree(Z); cudaFree(H); cudaFree(partial); cudaFree(z); cudaFree(coef); cudaFree(work);
-    cudaFree(norm_partial); cudaFree(status);
+    cudaFree(norm_partial); cudaFree(status); cudaFree(s32[0]); cudaFree(s32[1]);
     if (host_status) cudaFreeHost(host_status);
 }
 
@@ -524,10 +524,27 @@ extern "C" int he_krylov_combine(he_krylov *k, int m, void *y, void *stream)
 
 // Fused Arnoldi exponential action y = exp(-i dt H(field)) x with the device operator.
 // Host syncs only at the reference's check points (m = 4, 8, ..., maxdim).
-extern "C" int he_expv(he_krylov *k, he_handle op, const void *x, void *y, const double *field, int velocity,
-                       double dt, double tol, int maxdim, int *dimension, double *estimate, void *stream)
+namespace {
+__global__ void krylov_to_c64(size_t n, const double2 *x, float2 *y)
+{
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x)
+        y[p] = make_float2((float)x[p].x, (float)x[p].y);
+}
+__global__ void krylov_to_c128(size_t n, const float2 *x, double2 *y)
+{
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x)
+        y[p] = make_double2((double)x[p].x, (double)x[p].y);
+}
+
+// y = exp(-i dt H) x.  precision HE_C64: H·psi in complex64 (the basis, CGS2, the
+// Hessenberg exponential and the error estimate stay complex128).
+int expv_impl(he_krylov *k, he_handle op, const void *x, void *y, const double *field, int velocity, double dt,
+              double tol, int maxdim, int *dimension, double *estimate, void *stream, int precision)
 {
     if (!k || !op || !x || !y || !field) return he_fail(HE_ERR_ARG, "null argument", __FILE__, __LINE__);
+    if (precision == HE_C64 && !k->s32[0]) {
+        for (int q = 0; q < 2; ++q) HE_CUDA_TRY(cudaMalloc(&k->s32[q], k->n * sizeof(float2)));
+    }
     if (maxdim < 1 || maxdim > k->maxdim) return he_fail(HE_ERR_ARG, "maxdim exceeds the workspace", __FILE__, __LINE__);
     if ((size_t)op->n * op->n * op->nc != k->n) return he_fail(HE_ERR_SHAPE, "workspace size != operator size", __FILE__, __LINE__);
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -545,7 +562,13 @@ extern "C" int he_expv(he_krylov *k, he_handle op, const void *x, void *y, const
     double err = 0;
     for (int j = 0; j < maxdim && !done; ++j) {
         double2 *qj = k->Q + (size_t)j * k->n, *v = k->Q + (size_t)(j + 1) * k->n;
-        rc = he_apply(op, qj, v, field, velocity, HE_C128, stream);   // same kernels as every other apply
+        if (precision == HE_C64) {
+            krylov_to_c64<<<kGrid, kBlock, 0, s>>>(k->n, qj, k->s32[0]);
+            rc = he_apply(op, k->s32[0], k->s32[1], field, velocity, HE_C64, stream);
+            krylov_to_c128<<<kGrid, kBlock, 0, s>>>(k->n, k->s32[1], v);
+        } else {
+            rc = he_apply(op, qj, v, field, velocity, HE_C128, stream);   // same kernels as every other apply
+        }
         if (!rc) rc = krylov_cgs2(k, j + 1, v, k->H + (size_t)j * ld, k->H + (size_t)j * ld + j + 1, s, 1e-13);
         if (rc) break;
         const bool checkpoint = j >= 3 && ((j + 1) % 4 == 0 || j + 1 == maxdim);
@@ -570,4 +593,17 @@ extern "C" int he_expv(he_krylov *k, he_handle op, const void *x, void *y, const
     combine_kernel<<<kGrid, kBlock, 0, s>>>(k->Q, k->n, k->coef, static_cast<double2 *>(y), k->status, m, 0);
     HE_CUDA_TRY(cudaGetLastError());
     return HE_OK;
+}
+}  // namespace
+
+extern "C" int he_expv(he_krylov *k, he_handle op, const void *x, void *y, const double *field, int velocity,
+                       double dt, double tol, int maxdim, int *dimension, double *estimate, void *stream)
+{
+    return expv_impl(k, op, x, y, field, velocity, dt, tol, maxdim, dimension, estimate, stream, HE_C128);
+}
+
+extern "C" int he_expv_mixed(he_krylov *k, he_handle op, const void *x, void *y, const double *field, int velocity,
+                             double dt, double tol, int maxdim, int *dimension, double *estimate, void *stream)
+{
+    return expv_impl(k, op, x, y, field, velocity, dt, tol, maxdim, dimension, estimate, stream, HE_C64);
 }

@@ -39,6 +39,7 @@ struct he_krylov {
     double2 *coef = nullptr;      // maxdim combination coefficients
     double2 *work = nullptr;      // 8 * maxdim^2 complex: small dense scratch (expm / least squares)
     double *norm_partial = nullptr;   // KRYLOV_BLOCKS
+    float2 *s32[2] = {nullptr, nullptr};   // complex64 operand/result of mixed-precision applies
     he::KrylovStatus *status = nullptr;      // device
     he::KrylovStatus *host_status = nullptr; // pinned host mirror
     ~he_krylov();

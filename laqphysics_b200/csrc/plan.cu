@@ -106,34 +106,28 @@ bool he_build_plan(he_plan_host &P, int n, int nc, const int *ptr, const int *co
         for (int e = P.tstart[k]; e < P.tstart[k + 1]; ++e) entries += esize(e) * esize(e);
         P.blkmax = std::max(P.blkmax, entries);
     }
-    // --- output groups: channels of one Coulomb component with shared sources ---------
+    // --- output groups ------------------------------------------------------------------
+    // Channels that share Coulomb sources: the connected components of the Coulomb edges
+    // (total-L blocks in the coupled basis), split by connectivity through even multipoles
+    // (the l1-parity classes: even lambda keeps the parity of l1, odd lambda flips it, so
+    // a class sees one parity of sources per lambda).  Each class is cut into groups of
+    // MIX_GROUP channels in index order.
     for (int k = 0; k < nv; ++k)
         if (vcoef[2 * k + 1] != 0.0) return false;
     P.nlam = nlam;
-    UnionFind uf(nc);
-    std::vector<std::set<std::pair<int, int>>> src(nc);
+    UnionFind component(nc), even(nc);
     for (int c = 0; c < nc; ++c)
-        for (int k = vptr[c]; k < vptr[c + 1]; ++k) { uf.join(c, vc[k]); src[c].insert({vc[k], vl[k]}); }
-    std::vector<int> assigned(nc, 0);
-    std::vector<std::vector<int>> groups;
-    for (int c = 0; c < nc; ++c) {
-        if (assigned[c]) continue;
-        std::vector<int> grp{c};
-        assigned[c] = 1;
-        while ((int)grp.size() < MIX_GROUP) {
-            int best = -1, score = -1;
-            for (int x = 0; x < nc; ++x) {
-                if (assigned[x] || uf.find(x) != uf.find(c)) continue;
-                int s = 0;
-                for (auto &e : src[x]) s += (int)src[c].count(e);
-                if (s > score) { score = s; best = x; }
-            }
-            if (best < 0) break;
-            grp.push_back(best);
-            assigned[best] = 1;
+        for (int k = vptr[c]; k < vptr[c + 1]; ++k) {
+            component.join(c, vc[k]);
+            if (vl[k] % 2 == 0) even.join(c, vc[k]);
         }
-        groups.push_back(grp);
-    }
+    std::map<std::pair<int, int>, std::vector<int>> classes;
+    for (int c = 0; c < nc; ++c) classes[{component.find(c), even.find(c)}].push_back(c);
+    std::vector<std::vector<int>> groups;
+    for (auto &kv : classes)
+        for (size_t i = 0; i < kv.second.size(); i += MIX_GROUP)
+            groups.emplace_back(kv.second.begin() + i,
+                                kv.second.begin() + std::min(kv.second.size(), i + (size_t)MIX_GROUP));
     P.ng = (int)groups.size();
     P.gch.assign((size_t)P.ng * MIX_GROUP, -1);
     P.wptr.assign((size_t)P.ng * nlam + 1, 0);

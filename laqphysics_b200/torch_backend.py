@@ -76,14 +76,22 @@ def workspace(n, maxdim, device, flexible=False):
 
 
 class FieldOperator:
-    """y -> H(field) y of a B200Hamiltonian; also usable as a plain callable."""
+    """y -> H(field) y of a B200Hamiltonian; also usable as a plain callable.
+    precision='mixed' runs H·psi in complex64 inside the fused Arnoldi (the Krylov basis,
+    CGS2, the Hessenberg exponential and the error estimate stay complex128)."""
 
-    def __init__(self, engine, field, velocity=True):
+    def __init__(self, engine, field, velocity=True, precision='complex128'):
+        if precision not in ('complex128', 'mixed'):
+            raise ValueError("precision must be 'complex128' or 'mixed'")
         self.engine = engine
         self.field = np.ascontiguousarray(field, dtype=np.float64)
         self.velocity = bool(velocity)
+        self.precision = precision
 
     def __call__(self, y):
+        if self.precision == 'mixed':
+            return self.engine.apply(y.to(torch.complex64), self.field, self.velocity,
+                                     precision='complex64').to(torch.complex128)
         return self.engine.apply(y, self.field, self.velocity)
 
 
@@ -91,16 +99,17 @@ class FieldSchedule:
     """(t, y) -> H(field(t)) y of a B200Hamiltonian; ``step`` recognises it and uses
     the fused device Arnoldi."""
 
-    def __init__(self, engine, field_at, velocity=True):
+    def __init__(self, engine, field_at, velocity=True, precision='complex128'):
         self.engine = engine
         self.field_at = field_at
         self.velocity = bool(velocity)
+        self.precision = precision
 
     def __call__(self, t, y):
-        return self.engine.apply(y, self.field_at(t), self.velocity)
+        return self.at(t)(y)
 
     def at(self, t):
-        return FieldOperator(self.engine, self.field_at(t), self.velocity)
+        return FieldOperator(self.engine, self.field_at(t), self.velocity, self.precision)
 
 
 def _not_converged(maxdim, dt, err):
@@ -142,7 +151,8 @@ def exponential_action(apply, x, dt, tol=1e-10, maxdim=48):
 def _fused(op, ws, x, dt, tol, maxdim, stream):
     y = torch.empty_like(x)
     dim, err = ct.c_int(0), ct.c_double(0.)
-    status = LIB.he_expv(ws.handle, op.engine.op.handle, ct.c_void_p(x.data_ptr()), ct.c_void_p(y.data_ptr()),
+    fn = LIB.he_expv_mixed if op.precision == 'mixed' else LIB.he_expv
+    status = fn(ws.handle, op.engine.op.handle, ct.c_void_p(x.data_ptr()), ct.c_void_p(y.data_ptr()),
                          ptr(op.field), int(op.velocity), float(dt), float(tol), int(maxdim), ct.byref(dim),
                          ct.byref(err), stream)
     if status == HE_ERR_NOCONV:

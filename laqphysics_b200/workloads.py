@@ -34,9 +34,10 @@ def arnoldi_small(tail=12):
     return coupled(np.linspace(0, 25, 16), 8, 3, 2, ecs_angle=.3, tail=tail, cutoff_radii=(18., 22.))
 
 
-def arnoldi_small_real():
-    """Real (unscaled) twin of :func:`arnoldi_small` for the ground-state solve."""
-    return coupled(np.linspace(0, 25, 16), 8, 3, 2, cutoff_radii=(18., 22.))
+def arnoldi_small_real(tail=12):
+    """Real (unscaled, theta = 0) twin of :func:`arnoldi_small`, same nodes count, for the
+    ground-state solve (python/run3d.py:24-25 builds both grids from one config)."""
+    return coupled(np.linspace(0, 25, 16), 8, 3, 2, ecs_angle=0., tail=tail, cutoff_radii=(18., 22.))
 
 
 def length_pulse():

@@ -179,8 +179,9 @@ def test_microbenchmark_plan_shape():
     h = hpsi_microbench()
     P = build_plan(h)
     assert P['ok'] and P['ne'] == 61 and P['maxm'] == 21
-    # register blocking: 13 groups of <= 4 output channels read 592 sources instead of 1071
-    assert P['ng'] <= 16 and len(P['wsrc']) <= 640
+    # register blocking: 14 groups of <= 4 output channels (total-L block x l1-parity
+    # classes) read 521 sources per point instead of 1071 edges
+    assert P['ng'] == 14 and len(P['wsrc']) == 521
     est, ts = P['estart'], P['tstart']
     owned = [(est[ts[k + 1]] if ts[k + 1] < P['ne'] else h.n) - est[ts[k]] for k in range(P['ntile'])]
     assert max(owned) <= RAD_TMAX and sum(owned) == h.n
