@@ -40,7 +40,7 @@ def parse():
     p.add_argument('--impl', choices=['b200', 'reference'], default='b200')
     p.add_argument('--no-cpu-baseline', action='store_true')
     p.add_argument('--no-arnoldi', action='store_true', help='skip the Arnoldi steps/s leg')
-    p.add_argument('--profile', choices=['c128', 'c64'], default=None,
+    p.add_argument('--profile', choices=['c128', 'c64', 'arnoldi'], default=None,
                    help='run only W+K applications of one precision (for ncu captures); prints no JSON')
     return p.parse_args()
 
@@ -257,6 +257,9 @@ def main():
         if world > 1:
             dist.barrier()
 
+    if args.profile == 'arnoldi':   # W + K Arnoldi steps on the small grid, for launch lists
+        arnoldi_leg(torch, device, steps=args.steps, cpu_steps=0)
+        return 0
     h = workloads.hpsi_microbench()
     engine = B200Hamiltonian(h, device)
     field = (0., 0., .02)
