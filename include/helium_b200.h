@@ -24,7 +24,8 @@ enum {
     HE_ERR_SHAPE = 2,      /* table inconsistent with its sizes (index out of range ...)  */
     HE_ERR_CUDA = 3,       /* CUDA runtime error; see he_last_error()                     */
     HE_ERR_NOCONV = 4,     /* Arnoldi or GMRES did not converge within its limits         */
-    HE_ERR_UNSUPPORTED = 5 /* requested combination not built (e.g. no complex64 tables)  */
+    HE_ERR_UNSUPPORTED = 5,/* requested combination not built (e.g. no complex64 tables)  */
+    HE_ERR_DEVICE = 6      /* a bounded device-side wait ran out (data not delivered)     */
 };
 
 enum { HE_C128 = 0, HE_C64 = 1 };   /* arithmetic of an apply: complex128 or complex64 */
@@ -217,10 +218,15 @@ int he_vec_norms_noalloc(long long n, int count, const void *x, long long ld, do
 
 /* ------------------------------------------------------------------------------------
  * Operator set-up options and planner inspection (host only, no device work).
- * he_set_path: 1 = tiled kernels (default when the tables admit them), 0 = generic.
+ * he_set_path: 1 = tiled kernels (default when the tables admit them; the radial part
+ *   runs on the TMA-staged kinetic kernel when psi is 16-byte aligned), 2 = tiled kernels
+ *   with the shared-memory radial kernel (no TMA), 0 = generic gather kernel.
+ * he_device_status: waits for the handle's device work and reports HE_ERR_DEVICE once
+ *   (then clears it) when a bounded device-side wait of a kernel ran out.
  * he_plan_build / he_plan_array / he_plan_free expose the tiled plan of a set of tables.
  * ---------------------------------------------------------------------------------- */
 int he_set_path(he_handle h, int tiled);
+int he_device_status(he_handle h);
 void *he_plan_build(int n, int nc, const int *ptr, const int *col, const double *tv, int nv, const int *vptr,
                     const int *vc, const int *vl, const double *vcoef, int nlam, int nd, const int *dptr,
                     const int *dc, const int *de, const double *r);

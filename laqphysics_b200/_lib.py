@@ -13,7 +13,7 @@ if not LIBRARY.exists():
     raise ImportError(f'{LIBRARY} is missing: build it with `python -m laqphysics_b200.build`')
 LIB = ct.CDLL(str(LIBRARY))
 
-HE_OK, HE_ERR_ARG, HE_ERR_SHAPE, HE_ERR_CUDA, HE_ERR_NOCONV, HE_ERR_UNSUPPORTED = range(6)
+HE_OK, HE_ERR_ARG, HE_ERR_SHAPE, HE_ERR_CUDA, HE_ERR_NOCONV, HE_ERR_UNSUPPORTED, HE_ERR_DEVICE = range(7)
 HE_C128, HE_C64 = 0, 1
 
 P = ct.c_void_p
@@ -43,6 +43,7 @@ SIGNATURES = {
     'he_expv': (I, [P, P, P, P, P, I, D, D, I, ct.POINTER(I), ct.POINTER(D), P]),
     'he_expv_mixed': (I, [P, P, P, P, P, I, D, D, I, ct.POINTER(I), ct.POINTER(D), P]),
     'he_set_path': (I, [P, I]),
+    'he_device_status': (I, [P]),
     'he_vec_axpby': (I, [ct.c_longlong, D, D, P, D, D, P, P, P]),
     'he_vec_residual_norm': (I, [ct.c_longlong, P, P, P, ct.POINTER(D), P]),
     'he_vec_jacobi': (I, [ct.c_longlong, P, D, D, D, P, P, P]),

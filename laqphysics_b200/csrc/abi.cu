@@ -136,6 +136,37 @@ template <typename R> int upload_plan(he_operator *h, he::TiledPlan<R> *pl, cplx
     HE_CUDA_TRY(cudaMalloc(&c, std::max(1, h->nd) * sizeof(cplx<R>)));
     h->allocations.push_back(c);
     *coef = static_cast<cplx<R> *>(c);
+    // kinetic kernel: shares the element tables of the tiled plan
+    he::KineticPlan<R> *kp;
+    if constexpr (sizeof(R) == 8) kp = &h->k64; else kp = &h->k32;
+    *kp = he::KineticPlan<R>{};
+    if (!P.kin_ok) return HE_OK;
+    if (!h->kerr) {
+        void *e = nullptr;
+        HE_CUDA_TRY(cudaMalloc(&e, sizeof(int)));
+        h->allocations.push_back(e);
+        HE_CUDA_TRY(cudaMemset(e, 0, sizeof(int)));
+        h->kerr = static_cast<int *>(e);
+    }
+    he::KineticPlan<R> k{};
+    k.n = h->n; k.nc = h->nc; k.ne = P.ne; k.ntr = P.ntr; k.nct = P.nct;
+    k.box_r = sizeof(R) == 8 ? P.kbox_r64 : P.kbox_r32;
+    k.box_c = P.kbox_c;
+    const size_t box = (size_t)k.box_r * k.box_c * sizeof(cplx<R>);
+    k.stage_bytes = (int)((box + he::KIN_STAGE_ALIGN - 1) / he::KIN_STAGE_ALIGN * he::KIN_STAGE_ALIGN);
+    k.estart = pl->estart; k.ereal = pl->ereal; k.eoff = pl->eoff;
+    if ((s = upload(h, P.nodeelem.data(), P.nodeelem.size(), &k.nodeelem))) return s;
+    if ((s = upload_r<R>(h, P.tre.data(), P.tre.size(), &k.tre))) return s;
+    if ((s = upload_r<R>(h, P.tim.data(), P.tim.size(), &k.tim))) return s;
+    if ((s = upload_r<R>(h, P.bre.data(), P.bre.size(), &k.bre))) return s;
+    if ((s = upload_r<R>(h, P.bim.data(), P.bim.size(), &k.bim))) return s;
+    if ((s = upload(h, P.krow.data(), P.krow.size(), &k.krow))) return s;
+    if ((s = upload(h, P.krbase.data(), P.krbase.size(), &k.krbase))) return s;
+    if ((s = upload(h, P.krcplx.data(), P.krcplx.size(), &k.krcplx))) return s;
+    if ((s = upload(h, P.kslot.data(), P.kslot.size(), &k.kslot))) return s;
+    if ((s = upload(h, P.kcbase.data(), P.kcbase.size(), &k.kcbase))) return s;
+    k.err = h->kerr;
+    *kp = k;
     return HE_OK;
 }
 
@@ -163,9 +194,23 @@ he_operator::~he_operator()
 extern "C" int he_set_path(he_handle h, int tiled)
 {
     if (!h) return he_fail(HE_ERR_ARG, "null handle", __FILE__, __LINE__);
+    if (tiled < 0 || tiled > 2) return he_fail(HE_ERR_ARG, "path must be 0, 1 or 2", __FILE__, __LINE__);
     if (tiled && !h->tiled) return he_fail(HE_ERR_UNSUPPORTED, "tables do not admit the tiled kernels", __FILE__, __LINE__);
-    h->path = tiled ? 1 : 0;
+    h->path = tiled;
     return HE_OK;
+}
+
+extern "C" int he_device_status(he_handle h)
+{
+    if (!h) return he_fail(HE_ERR_ARG, "null handle", __FILE__, __LINE__);
+    if (!h->kerr) return HE_OK;
+    int v = 0;
+    HE_CUDA_TRY(cudaDeviceSynchronize());
+    HE_CUDA_TRY(cudaMemcpy(&v, h->kerr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (!v) return HE_OK;
+    HE_CUDA_TRY(cudaMemset(h->kerr, 0, sizeof(int)));
+    return he_fail(HE_ERR_DEVICE, "a staged tile of the kinetic kernel did not arrive within its wait limit",
+                   __FILE__, __LINE__);
 }
 
 extern "C" int he_create(he_handle *out, int n, int nc, int nt, const int *ptr, const int *col, const double *tv,
@@ -254,7 +299,7 @@ int apply_common(he_handle h, const void *psi, void *out, const double *field, i
     if (psi == out) return he_fail(HE_ERR_ARG, "H·psi cannot run in place", __FILE__, __LINE__);
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
     int s;
-    const bool tiled = h->tiled && h->path == 1;
+    const bool tiled = h->tiled && h->path >= 1;
     if (precision == HE_C128) {
         const double2 beta = mk<double>(beta_re, beta_im), gamma = mk<double>(gamma_re, gamma_im);
         if (tiled) {

@@ -42,6 +42,34 @@ template <typename R> __host__ __device__ __forceinline__ R cabs2(cplx<R> a) { r
 template <typename R> __device__ __forceinline__ cplx<R> ldg(const cplx<R>* p) { return __ldg(p); }
 
 // ---------------------------------------------------------------------------------
+// Sum of nb per-block partials p[b * stride] by one warp in a fixed order: lane l adds
+// b = l, l + 32, ... in sequence, then a butterfly over the lanes.  Every lane returns
+// the same value and the order never depends on timing, so results are reproducible.
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ double warp_fixed_sum(const double* p, int nb, size_t stride)
+{
+    const int lane = threadIdx.x & 31;
+    double s = 0;
+    for (int b = lane; b < nb; b += 32) s += p[(size_t)b * stride];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    return s;
+}
+
+__device__ __forceinline__ double2 warp_fixed_sum(const double2* p, int nb, size_t stride)
+{
+    const int lane = threadIdx.x & 31;
+    double2 s = mk<double>(0, 0);
+    for (int b = lane; b < nb; b += 32) s = cadd<double>(s, p[(size_t)b * stride]);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        s.x += __shfl_xor_sync(0xffffffffu, s.x, off);
+        s.y += __shfl_xor_sync(0xffffffffu, s.y, off);
+    }
+    return s;
+}
+
+// ---------------------------------------------------------------------------------
 // Device-resident operator tables.  Indices are zero based, psi(i,j,c) has i fastest
 // (the reference's Fortran order, src/kernels.f90:125).
 // ---------------------------------------------------------------------------------

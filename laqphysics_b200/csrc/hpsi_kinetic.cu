@@ -1,0 +1,325 @@
+// Kinetic energy of both electrons, the diagonal and |A|^2 of H·psi on TMA-staged tiles
+// (src/kernels.f90:132-143 and :170; in the velocity gauge also the commutator stencils
+// W_e = B_e psi, B = T (r_b - r_a), of :153-168, which the channel-mixing kernel consumes).
+//
+// Work is a list of (row tile, column tile, channel) items, split evenly over a
+// persistent grid of two CTAs per SM.  For each item one TMA copy (cp.async.bulk.tensor,
+// 3-D map over psi(re/im, r1, r2·channel)) brings the staged box into shared memory;
+// the copy of the next item is in flight while the current one is computed (two stages,
+// one mbarrier each, one __syncthreads per item).
+//
+// Thread (row lane, slot) owns up to KIN_NA outputs psi(i, s_f + a0 + q): lanes run along
+// r1, so every global store is coalesced and both directions accumulate in registers:
+//   along r2   acc[q] += sum_b T_f[a0+q][b] psi(i, s_f + b)       (slot-uniform T, broadcast)
+//   along r1   acc[q] += sum_b T_e[a_i][b] psi(s_e + b, s_f+a0+q) (per-lane T row)
+// plus the bridge rows/columns, whose previous-element nodes are part of the staged box.
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "common.cuh"
+#include "hpsi_kinetic.cuh"
+#include "operator.cuh"
+
+namespace he {
+
+constexpr int KIN_WAIT_LIMIT = 1 << 21;          // try_wait rounds before a stage counts as lost
+constexpr unsigned KIN_WAIT_HINT_NS = 2000;      // suspend hint of one try_wait round
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(KIN_WAIT_HINT_NS)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity)
+{
+    for (int k = 0; k < KIN_WAIT_LIMIT; ++k)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// Tiled TMA load of one box (no multicast) completing on `bar`.
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
+template <typename R> __device__ __forceinline__ int elem_size(const KineticPlan<R> &kp, int e)
+{
+    return (e + 1 < kp.ne ? kp.estart[e + 1] + 1 : kp.n) - kp.estart[e];
+}
+
+// Along r2 for one slot: acc[q] += sum_b X_f[a0+q][b] S(s_f + b, i), plus for the bridge
+// column s_f (a0 == 0) the previous element's last row.  X = T or B (transposed planes).
+template <typename R>
+__device__ __forceinline__ void along_r2(const KineticPlan<R> &kp, const R *__restrict__ xre, const R *__restrict__ xim,
+                                         const cplx<R> *S, int box_r, int il, int y0, int f, int a0, int na,
+                                         cplx<R> (&acc)[KIN_NA])
+{
+    const int sf = kp.estart[f], mf = elem_size(kp, f), off = kp.eoff[f];
+    const cplx<R> *col = S + (size_t)(sf - y0) * box_r + il;
+    if (kp.ereal[f]) {
+        for (int b = 0; b < mf; ++b) {
+            const cplx<R> x = col[(size_t)b * box_r];
+            const R *tr = xre + off + b * mf + a0;
+#pragma unroll
+            for (int q = 0; q < KIN_NA; ++q)
+                if (q < na) acc[q] = rfma<R>(__ldg(tr + q), x, acc[q]);
+        }
+    } else {
+        for (int b = 0; b < mf; ++b) {
+            const cplx<R> x = col[(size_t)b * box_r];
+            const R *tr = xre + off + b * mf + a0, *ti = xim + off + b * mf + a0;
+#pragma unroll
+            for (int q = 0; q < KIN_NA; ++q)
+                if (q < na) acc[q] = cfma<R>(mk<R>(__ldg(tr + q), __ldg(ti + q)), x, acc[q]);
+        }
+    }
+    if (a0 == 0 && f > 0) {
+        const int fp = f - 1, sp = kp.estart[fp], mp = sf - sp + 1, offp = kp.eoff[fp];
+        const cplx<R> *colp = S + (size_t)(sp - y0) * box_r + il;
+        const bool real = kp.ereal[fp];
+        cplx<R> s = acc[0];
+        for (int b = 0; b < mp - 1; ++b) {
+            const size_t k = (size_t)offp + (size_t)b * mp + (mp - 1);
+            const cplx<R> x = colp[(size_t)b * box_r];
+            s = real ? rfma<R>(__ldg(xre + k), x, s) : cfma<R>(mk<R>(__ldg(xre + k), __ldg(xim + k)), x, s);
+        }
+        acc[0] = s;
+    }
+}
+
+// Along r1 for row i (node a_i of element e): acc[q] += sum_b X_e[a_i][b] S(cq0 + q, s_e + b),
+// plus the previous element's last row when i is a bridge row.
+template <typename R>
+__device__ __forceinline__ void along_r1(const KineticPlan<R> &kp, const R *__restrict__ xre, const R *__restrict__ xim,
+                                         const cplx<R> *S, int box_r, int i, int x0, int cq0, int y0, int na,
+                                         cplx<R> (&acc)[KIN_NA])
+{
+    const int e = kp.nodeelem[i], se = kp.estart[e], me = elem_size(kp, e), ai = i - se, off = kp.eoff[e];
+    const cplx<R> *rows = S + (size_t)(cq0 - y0) * box_r + (se - x0);
+    if (kp.ereal[e]) {
+        for (int b = 0; b < me; ++b) {
+            const R tr = __ldg(xre + off + b * me + ai);
+#pragma unroll
+            for (int q = 0; q < KIN_NA; ++q)
+                if (q < na) acc[q] = rfma<R>(tr, rows[(size_t)q * box_r + b], acc[q]);
+        }
+    } else {
+        for (int b = 0; b < me; ++b) {
+            const cplx<R> tv = mk<R>(__ldg(xre + off + b * me + ai), __ldg(xim + off + b * me + ai));
+#pragma unroll
+            for (int q = 0; q < KIN_NA; ++q)
+                if (q < na) acc[q] = cfma<R>(tv, rows[(size_t)q * box_r + b], acc[q]);
+        }
+    }
+    if (ai == 0 && e > 0) {
+        const int ep = e - 1, sp = kp.estart[ep], mp = se - sp + 1, offp = kp.eoff[ep];
+        const cplx<R> *rp = S + (size_t)(cq0 - y0) * box_r + (sp - x0);
+        const bool real = kp.ereal[ep];
+        for (int b = 0; b < mp - 1; ++b) {
+            const size_t k = (size_t)offp + (size_t)b * mp + (mp - 1);
+            const cplx<R> tv = mk<R>(__ldg(xre + k), real ? (R)0 : __ldg(xim + k));
+#pragma unroll
+            for (int q = 0; q < KIN_NA; ++q)
+                if (q < na) acc[q] = real ? rfma<R>(tv.x, rp[(size_t)q * box_r + b], acc[q])
+                                          : cfma<R>(tv, rp[(size_t)q * box_r + b], acc[q]);
+        }
+    }
+}
+
+template <typename R, bool VEL, bool SEP>
+__global__ void __launch_bounds__(KIN_THREADS, 2)
+hpsi_kinetic_kernel(const __grid_constant__ CUtensorMap tmap, const DeviceTables<R> t, const KineticPlan<R> kp,
+                    cplx<R> *__restrict__ out, cplx<R> *__restrict__ w1, cplx<R> *__restrict__ w2, R a2)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    // staged boxes start on a 1024-byte boundary (the launch adds the slack)
+    unsigned char *smem = smem_raw + ((KIN_STAGE_ALIGN - (smem_u32(smem_raw) & (KIN_STAGE_ALIGN - 1))) & (KIN_STAGE_ALIGN - 1));
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * (size_t)kp.stage_bytes);
+    constexpr int ALIGN = 16 / (int)sizeof(cplx<R>);   // nodes per 16 bytes (TMA start alignment)
+    const int n = kp.n, nc = kp.nc, box_r = kp.box_r;
+    const size_t nn = (size_t)n * n;
+    const long long items = (long long)kp.ntr * kp.nct * nc;
+    const long long per = (items + gridDim.x - 1) / gridDim.x;
+    const long long first = (long long)blockIdx.x * per;
+    const long long last = first + per < items ? first + per : items;
+    if (first >= last) return;
+    const unsigned box_bytes = (unsigned)((size_t)box_r * kp.box_c * sizeof(cplx<R>));
+
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        mbar_init(bar + 1, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    auto issue = [&](long long it, int stage) {
+        const long long tile = it / nc;
+        const int c = (int)(it % nc), tr = (int)(tile / kp.nct), tc = (int)(tile % kp.nct);
+        const int x0 = kp.krbase[tr] / ALIGN * ALIGN;
+        mbar_expect_tx(bar + stage, box_bytes);
+        tma_load_3d(smem + (size_t)stage * kp.stage_bytes, &tmap, 2 * x0, kp.kcbase[tc], c, bar + stage);
+    };
+    if (threadIdx.x == 0) issue(first, 0);
+
+    const int slot = threadIdx.x / KIN_ROWS, lane_row = threadIdx.x % KIN_ROWS;
+    for (long long it = first; it < last; ++it) {
+        const int k = (int)(it - first), stage = k & 1;
+        const bool ok = mbar_wait_bounded(bar + stage, (unsigned)((k >> 1) & 1));
+        if (__syncthreads_or(!ok)) {
+            // a stage that never arrived: record it, wait (bounded) for the copy in flight, leave
+            if (threadIdx.x == 0) {
+                atomicExch(kp.err, 1);
+                mbar_wait_bounded(bar + stage, (unsigned)((k >> 1) & 1));
+            }
+            return;
+        }
+        if (threadIdx.x == 0 && it + 1 < last) issue(it + 1, stage ^ 1);
+
+        const long long tile = it / nc;
+        const int c = (int)(it % nc), tr = (int)(tile / kp.nct), tc = (int)(tile % kp.nct);
+        const int ea = kp.krow[tr], eb = kp.krow[tr + 1];
+        const int r0 = kp.estart[ea], r1 = eb < kp.ne ? kp.estart[eb] : n;
+        const int i = r0 + lane_row;
+        const int *sl = kp.kslot + (tc * KIN_SLOTS + slot) * 3;
+        const int f = sl[0], a0 = sl[1], na = sl[2];
+        if (i >= r1 || na == 0) continue;
+        const cplx<R> *S = reinterpret_cast<const cplx<R> *>(smem + (size_t)stage * kp.stage_bytes);
+        const int x0 = kp.krbase[tr] / ALIGN * ALIGN, y0 = kp.kcbase[tc];
+        const int il = i - x0, cq0 = kp.estart[f] + a0;
+        cplx<R> acc[KIN_NA];
+        if (VEL) {
+#pragma unroll
+            for (int q = 0; q < KIN_NA; ++q) acc[q] = mk<R>(0, 0);
+            along_r2<R>(kp, kp.bre, kp.bim, S, box_r, il, y0, f, a0, na, acc);
+#pragma unroll
+            for (int q = 0; q < KIN_NA; ++q)
+                if (q < na) w2[(size_t)i + (size_t)n * (cq0 + q) + nn * c] = acc[q];
+#pragma unroll
+            for (int q = 0; q < KIN_NA; ++q) acc[q] = mk<R>(0, 0);
+            along_r1<R>(kp, kp.bre, kp.bim, S, box_r, i, x0, cq0, y0, na, acc);
+#pragma unroll
+            for (int q = 0; q < KIN_NA; ++q)
+                if (q < na) w1[(size_t)i + (size_t)n * (cq0 + q) + nn * c] = acc[q];
+        }
+#pragma unroll
+        for (int q = 0; q < KIN_NA; ++q) acc[q] = mk<R>(0, 0);
+        along_r2<R>(kp, kp.tre, kp.tim, S, box_r, il, y0, f, a0, na, acc);
+        along_r1<R>(kp, kp.tre, kp.tim, S, box_r, i, x0, cq0, y0, na, acc);
+#pragma unroll
+        for (int q = 0; q < KIN_NA; ++q) {
+            if (q < na) {
+                const int j = cq0 + q;
+                const cplx<R> x = S[(size_t)(j - y0) * box_r + il];
+                const size_t p = (size_t)i + (size_t)n * j + nn * c;
+                const cplx<R> d = SEP ? cadd<R>(ldg<R>(t.d1 + i + (size_t)n * c), ldg<R>(t.d2 + j + (size_t)n * c))
+                                      : ldg<R>(t.diag + p);
+                cplx<R> v = cfma<R>(d, x, acc[q]);
+                if (VEL) v = rfma<R>(a2, x, v);
+                out[p] = v;
+            }
+        }
+    }
+}
+
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+int sm_count(int device)
+{
+    static int counts[64] = {0};
+    if (device < 0 || device >= 64) return 148;
+    if (!counts[device]) {
+        int v = 0;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || v <= 0) v = 148;
+        counts[device] = v;
+    }
+    return counts[device];
+}
+
+}  // namespace
+
+// True when the kinetic kernel can stage `psi` with TMA: 16-byte aligned base and rows
+// (the r1 extent in bytes) a multiple of 16 bytes.
+template <typename R> bool kinetic_usable(const KineticPlan<R> &kp, const void *psi)
+{
+    return kp.ntr > 0 && (reinterpret_cast<uintptr_t>(psi) & 15) == 0 && ((size_t)kp.n * sizeof(cplx<R>)) % 16 == 0 &&
+           tensor_map_encoder() != nullptr;
+}
+
+template <typename R>
+int launch_kinetic(he_operator *h, const DeviceTables<R> &t, const KineticPlan<R> &kp, const cplx<R> *psi,
+                   cplx<R> *out, cplx<R> *w1, cplx<R> *w2, R a2, int velocity, cudaStream_t stream)
+{
+    CUtensorMap map;
+    const cuuint64_t dims[3] = {2 * (cuuint64_t)kp.n, (cuuint64_t)kp.n, (cuuint64_t)kp.nc};
+    const cuuint64_t strides[2] = {2 * (cuuint64_t)kp.n * sizeof(R), 2 * (cuuint64_t)kp.n * kp.n * sizeof(R)};
+    const cuuint32_t box[3] = {2 * (cuuint32_t)kp.box_r, (cuuint32_t)kp.box_c, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    const CUresult r = tensor_map_encoder()(&map, sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                                            3, const_cast<cplx<R> *>(psi), dims, strides, box, es,
+                                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return he_fail(HE_ERR_CUDA, "cuTensorMapEncodeTiled failed", __FILE__, __LINE__);
+    const size_t smem = 2 * (size_t)kp.stage_bytes + 16 + KIN_STAGE_ALIGN;
+    const long long items = (long long)kp.ntr * kp.nct * kp.nc;
+    const unsigned grid = (unsigned)std::min<long long>(items, 2LL * sm_count(h->device));
+#define HE_KINETIC(V, S)                                                                                   \
+    do {                                                                                                   \
+        auto kern = hpsi_kinetic_kernel<R, V, S>;                                                          \
+        HE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));   \
+        kern<<<grid, KIN_THREADS, smem, stream>>>(map, t, kp, out, w1, w2, a2);                            \
+    } while (0)
+    if (velocity) { if (t.diag_separable) HE_KINETIC(true, true); else HE_KINETIC(true, false); }
+    else { if (t.diag_separable) HE_KINETIC(false, true); else HE_KINETIC(false, false); }
+#undef HE_KINETIC
+    HE_CUDA_TRY(cudaGetLastError());
+    return HE_OK;
+}
+
+template bool kinetic_usable<double>(const KineticPlan<double> &, const void *);
+template bool kinetic_usable<float>(const KineticPlan<float> &, const void *);
+template int launch_kinetic<double>(he_operator *, const DeviceTables<double> &, const KineticPlan<double> &,
+                                    const double2 *, double2 *, double2 *, double2 *, double, int, cudaStream_t);
+template int launch_kinetic<float>(he_operator *, const DeviceTables<float> &, const KineticPlan<float> &,
+                                   const float2 *, float2 *, float2 *, float2 *, float, int, cudaStream_t);
+
+}  // namespace he

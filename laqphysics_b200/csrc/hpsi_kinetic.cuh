@@ -1,0 +1,31 @@
+// Kinetic-energy kernel of H·psi with TMA-staged tiles (hpsi_kinetic.cu).
+//
+// One CTA works through (row tile, column tile, channel) items.  A row tile is a run of
+// whole elements along r1 with at most KIN_ROWS owned nodes; a column tile is up to
+// KIN_SLOTS "slots" along r2, a slot being at most KIN_NA owned nodes of one element.
+// The staged box holds the tile plus the nodes its bridge rows and columns reach into
+// (the previous element), so both kinetic directions read shared memory only.
+#pragma once
+#include <cuda.h>
+
+#include "common.cuh"
+
+namespace he {
+
+constexpr int KIN_ROWS = 64;                     // owned rows per tile (thread lanes along r1)
+constexpr int KIN_SLOTS = 4;                     // column slots per tile
+constexpr int KIN_NA = 10;                       // owned columns per slot (outputs per thread)
+constexpr int KIN_THREADS = KIN_ROWS * KIN_SLOTS;
+constexpr int KIN_STAGE_ALIGN = 1024;            // byte alignment of each staged box
+
+template <typename R> struct KineticPlan {
+    int n, nc, ne, ntr, nct, box_r, box_c;
+    int stage_bytes;                             // box bytes, rounded up to KIN_STAGE_ALIGN
+    const int *estart, *nodeelem, *ereal, *eoff;
+    const R *tre, *tim, *bre, *bim;              // transposed element blocks (planes)
+    const int *krow, *krbase, *krcplx;           // row tiles
+    const int *kslot, *kcbase;                   // column tiles
+    int *err;                                    // device error word (bounded waits that ran out)
+};
+
+}  // namespace he

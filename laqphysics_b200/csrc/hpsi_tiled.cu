@@ -540,19 +540,25 @@ int launch_hpsi_tiled(he_operator *h, const DeviceTables<R> &t, const TiledPlan<
     (void)coef;
     const R f0 = (R)field[0], f1 = (R)field[1], f2 = (R)field[2];
     const R a2 = (R)(field[0] * field[0] + field[1] * field[1] + field[2] * field[2]);
-    const dim3 rgrid(pl.ntile * pl.ntile, (pl.nc + RAD_CH - 1) / RAD_CH);
-    const int blkmax = h->plan.blkmax;
-    const size_t rs = radial_smem<R>(velocity, blkmax);
+    const KineticPlan<R> &kp = kinetic_plan<R>(h);
+    if (h->path == 1 && kinetic_usable<R>(kp, psi)) {
+        const int s = launch_kinetic<R>(h, t, kp, psi, out, w1, w2, a2, velocity, stream);
+        if (s) return s;
+    } else {
+        const dim3 rgrid(pl.ntile * pl.ntile, (pl.nc + RAD_CH - 1) / RAD_CH);
+        const int blkmax = h->plan.blkmax;
+        const size_t rs = radial_smem<R>(velocity, blkmax);
 #define HE_RADIAL(V, S)                                                                                  \
     do {                                                                                                 \
         auto kern = hpsi_radial_kernel<R, V, S>;                                                         \
         HE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rs));   \
         kern<<<rgrid, RAD_THREADS, rs, stream>>>(t, pl, psi, out, w1, w2, a2, blkmax);                   \
     } while (0)
-    if (velocity) { if (t.diag_separable) HE_RADIAL(true, true); else HE_RADIAL(true, false); }
-    else { if (t.diag_separable) HE_RADIAL(false, true); else HE_RADIAL(false, false); }
+        if (velocity) { if (t.diag_separable) HE_RADIAL(true, true); else HE_RADIAL(true, false); }
+        else { if (t.diag_separable) HE_RADIAL(false, true); else HE_RADIAL(false, false); }
 #undef HE_RADIAL
-    HE_CUDA_TRY(cudaGetLastError());
+        HE_CUDA_TRY(cudaGetLastError());
+    }
     const size_t nn = (size_t)pl.n * pl.n;
     const size_t ms = mix_smem<R>(pl.nc, pl.nlam, pl.ng, pl.nwide, pl.nwd);
     const size_t ntiles = (nn + MIX_NP - 1) / MIX_NP;

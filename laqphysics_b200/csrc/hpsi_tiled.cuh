@@ -43,4 +43,11 @@ struct he_plan_host {
     std::vector<double> blocks, bblocks, wcoef;   // complex as interleaved doubles for blocks
     int ne = 0, ntile = 0, ng = 0, nlam = 0, maxm = 0;
     int blkmax = 0;   // max over tiles and axes of staged block entries (previous row + sum m^2)
+    // kinetic kernel (TMA-staged tiles, hpsi_kinetic.cu)
+    bool kin_ok = false;
+    std::vector<int> nodeelem;              // n: element owning each node (a bridge node belongs to the later element)
+    std::vector<int> krow, krbase, krcplx;  // row tiles: ntr+1 element starts, first staged row, any complex block
+    std::vector<int> kslot, kcbase;         // column tiles: nct x KIN_SLOTS x (element, a0, na), first staged column
+    std::vector<double> tre, tim, bre, bim; // transposed element blocks: [eoff[e] + b m + a] = X[a][b]
+    int ntr = 0, nct = 0, kbox_r64 = 0, kbox_r32 = 0, kbox_c = 0;
 };

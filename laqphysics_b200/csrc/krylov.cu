@@ -4,8 +4,9 @@
 // the reference's python/propagate.py:6-39 / python/torch_backend.py:140-158.
 //
 // Reductions: every pass writes one partial per (block, basis vector) into the
-// workspace's `partial` array; a single-CTA kernel then sums the partials in block
-// order, so results are bitwise reproducible run to run.
+// workspace's `partial` array; a single-CTA kernel then sums them, one warp per value
+// in a fixed order, so results are bitwise reproducible run to run.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -74,16 +75,19 @@ multidot_kernel(const double2 *__restrict__ Q, size_t n, int k0, int kc, const d
     if (threadIdx.x < kc) partial[(size_t)blockIdx.x * ld + k0 + threadIdx.x] = res[threadIdx.x];
 }
 
-// z[k] = sum_b partial[b*ld + k] for k < kc (fixed block order); optionally H[k] += z[k].
+// z[k] = sum_b partial[b*ld + k] for k < kc (fixed order, one warp per k); optionally
+// H[k] += z[k].
 __global__ void reduce_partials_kernel(const double2 *__restrict__ partial, int nb, int ld, int kc,
                                        double2 *__restrict__ z, double2 *__restrict__ hcol, const KrylovStatus *st)
 {
     if (st && st->done) return;
-    for (int k = threadIdx.x; k < kc; k += blockDim.x) {
-        double2 s = mk<double>(0, 0);
-        for (int b = 0; b < nb; ++b) s = cadd<double>(s, partial[(size_t)b * ld + k]);
-        z[k] = s;
-        if (hcol) hcol[k] = cadd<double>(hcol[k], s);
+    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (int k = warp; k < kc; k += nwarps) {
+        const double2 s = warp_fixed_sum(partial + k, nb, (size_t)ld);
+        if ((threadIdx.x & 31) == 0) {
+            z[k] = s;
+            if (hcol) hcol[k] = cadd<double>(hcol[k], s);
+        }
     }
 }
 
@@ -141,9 +145,9 @@ norm_kernel(const double2 *__restrict__ v, size_t n, double *__restrict__ norm_p
 __global__ void finish_norm_kernel(const double *__restrict__ norm_partial, int nb, double2 *hsub, KrylovStatus *st,
                                    double happy_below)
 {
-    if (threadIdx.x != 0 || st->done) return;
-    double s = 0;
-    for (int b = 0; b < nb; ++b) s += norm_partial[b];
+    if (st->done) return;
+    const double s = warp_fixed_sum(norm_partial, nb, 1);
+    if (threadIdx.x != 0) return;
     const double h = sqrt(s);
     *hsub = mk<double>(h, 0);
     st->hnext = h;
@@ -163,9 +167,8 @@ normalize_kernel(const double2 *x, double2 *y, size_t n, const KrylovStatus *st)
 // start: beta = ||x||, Q_0 = x / beta (reads beta from the reduced norm)
 __global__ void start_kernel(const double *__restrict__ norm_partial, int nb, KrylovStatus *st)
 {
+    const double s = warp_fixed_sum(norm_partial, nb, 1);
     if (threadIdx.x != 0) return;
-    double s = 0;
-    for (int b = 0; b < nb; ++b) s += norm_partial[b];
     memset(st, 0, sizeof(KrylovStatus));
     st->beta = sqrt(s);
     st->hnext = st->beta;
@@ -429,7 +432,7 @@ int krylov_multidot(he_krylov *k, int kc, const double2 *v, double2 *hcol, cudaS
         const int t = kc - k0 < KRYLOV_TILE ? kc - k0 : KRYLOV_TILE;
         multidot_kernel<KRYLOV_TILE><<<kGrid, kBlock, 0, s>>>(basis, k->n, k0, t, v, k->partial, ld, st);
     }
-    reduce_partials_kernel<<<1, 64, 0, s>>>(k->partial, KRYLOV_BLOCKS, ld, kc, k->z, hcol, st);
+    reduce_partials_kernel<<<1, 32 * std::max(1, std::min(kc, 16)), 0, s>>>(k->partial, KRYLOV_BLOCKS, ld, kc, k->z, hcol, st);
     HE_CUDA_TRY(cudaGetLastError());
     return HE_OK;
 }

@@ -3,6 +3,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "hpsi_kinetic.cuh"
 #include "hpsi_tiled.cuh"
 
 struct he_operator {
@@ -16,6 +17,9 @@ struct he_operator {
     he::DeviceTables<float> t32{};
     he::TiledPlan<double> p64{};
     he::TiledPlan<float> p32{};
+    he::KineticPlan<double> k64{};      // kinetic-kernel plan (ntr == 0: not usable)
+    he::KineticPlan<float> k32{};
+    int *kerr = nullptr;                // device error word of the kinetic kernel
     double2 *coef64 = nullptr;          // field-contracted dipole coefficients (nd)
     float2 *coef32 = nullptr;
     double2 *w64[2] = {nullptr, nullptr};   // velocity gauge B-stencil scratch (n*n*nc each)
@@ -38,4 +42,11 @@ int launch_hpsi_tiled(he_operator *h, const DeviceTables<R> &t, const TiledPlan<
                       cplx<R> *w2, const cplx<R> *psi, cplx<R> *out, const double *field, int velocity,
                       cplx<R> beta, cplx<R> gamma, cudaStream_t stream);
 bool tiled_fits(const he_plan_host &P, int nc, int nd);
+template <typename R> bool kinetic_usable(const KineticPlan<R> &kp, const void *psi);
+template <typename R>
+int launch_kinetic(he_operator *h, const DeviceTables<R> &t, const KineticPlan<R> &kp, const cplx<R> *psi,
+                   cplx<R> *out, cplx<R> *w1, cplx<R> *w2, R a2, int velocity, cudaStream_t stream);
+template <typename R> inline const KineticPlan<R> &kinetic_plan(const he_operator *h);
+template <> inline const KineticPlan<double> &kinetic_plan<double>(const he_operator *h) { return h->k64; }
+template <> inline const KineticPlan<float> &kinetic_plan<float>(const he_operator *h) { return h->k32; }
 }  // namespace he

@@ -9,6 +9,7 @@
 #include <set>
 
 #include "common.cuh"
+#include "hpsi_kinetic.cuh"
 #include "hpsi_tiled.cuh"
 #include "operator.cuh"
 
@@ -24,6 +25,83 @@ struct UnionFind {
     int find(int x) { while (p[x] != x) x = p[x] = p[p[x]]; return x; }
     void join(int a, int b) { p[find(a)] = find(b); }
 };
+
+// Tiles of the kinetic kernel (hpsi_kinetic.cu): row tiles of whole elements with at most
+// KIN_ROWS owned nodes, column tiles of KIN_SLOTS slots (<= KIN_NA owned nodes of one
+// element each), the first staged node of every tile (the previous element's first node
+// when its bridge row is owned) and the staged box extents.  Leaves kin_ok false when an
+// element does not fit or the box exceeds the TMA / shared-memory limits.
+void build_kinetic(he_plan_host &P, int n)
+{
+    using namespace he;
+    const int ne = P.ne;
+    auto esize = [&](int e) { return e + 1 < ne ? P.estart[e + 1] - P.estart[e] + 1 : n - P.estart[e]; };
+    auto own = [&](int e) { return (e + 1 < ne ? P.estart[e + 1] : n) - P.estart[e]; };
+    P.kin_ok = false;
+    P.nodeelem.assign(n, 0);
+    for (int e = 0; e < ne; ++e)
+        for (int i = P.estart[e]; i < P.estart[e] + own(e); ++i) P.nodeelem[i] = e;
+    const size_t total = P.eoff[ne];
+    P.tre.assign(total, 0.0); P.tim.assign(total, 0.0); P.bre.assign(total, 0.0); P.bim.assign(total, 0.0);
+    for (int e = 0; e < ne; ++e) {
+        const int m = esize(e);
+        for (int a = 0; a < m; ++a)
+            for (int b = 0; b < m; ++b) {
+                const size_t src = 2 * ((size_t)P.eoff[e] + (size_t)a * m + b), dst = (size_t)P.eoff[e] + (size_t)b * m + a;
+                P.tre[dst] = P.blocks[src]; P.tim[dst] = P.blocks[src + 1];
+                P.bre[dst] = P.bblocks[src]; P.bim[dst] = P.bblocks[src + 1];
+            }
+    }
+    // row tiles
+    P.krow.assign(1, 0); P.krbase.clear(); P.krcplx.clear();
+    P.kbox_r64 = P.kbox_r32 = P.kbox_c = 0;
+    for (int e = 0; e < ne;) {
+        int o = 0, f = e;
+        while (f < ne && o + own(f) <= KIN_ROWS) { o += own(f); ++f; }
+        if (f == e) return;
+        P.krow.push_back(f);
+        e = f;
+    }
+    P.ntr = (int)P.krow.size() - 1;
+    for (int t = 0; t < P.ntr; ++t) {
+        const int ea = P.krow[t], eb = P.krow[t + 1];
+        const int rb = ea > 0 ? P.estart[ea - 1] : P.estart[ea];
+        const int last = eb < ne ? P.estart[eb] : n - 1;
+        P.krbase.push_back(rb);
+        P.kbox_r64 = std::max(P.kbox_r64, last - rb + 1);
+        P.kbox_r32 = std::max(P.kbox_r32, last - (rb & ~1) + 1);
+        int cplx = 0;
+        for (int e = std::max(ea - 1, 0); e < eb; ++e) cplx |= !P.ereal[e];
+        P.krcplx.push_back(cplx);
+    }
+    P.kbox_r32 += P.kbox_r32 & 1;   // complex64 rows: 8-byte nodes, the box starts and spans 16-byte multiples
+    // column slots, packed KIN_SLOTS per tile
+    std::vector<int> slots;
+    for (int f = 0; f < ne; ++f)
+        for (int a0 = 0; a0 < own(f); a0 += KIN_NA) {
+            slots.push_back(f); slots.push_back(a0); slots.push_back(std::min(KIN_NA, own(f) - a0));
+        }
+    const int nslots = (int)slots.size() / 3;
+    P.kslot.clear(); P.kcbase.clear();
+    for (int s0 = 0; s0 < nslots; s0 += KIN_SLOTS) {
+        int first = n, last = 0;
+        for (int k = 0; k < KIN_SLOTS; ++k) {
+            if (s0 + k < nslots) {
+                const int f = slots[3 * (s0 + k)], a0 = slots[3 * (s0 + k) + 1];
+                first = std::min(first, (a0 == 0 && f > 0) ? P.estart[f - 1] : P.estart[f]);
+                last = std::max(last, std::min(n - 1, P.estart[f] + esize(f) - 1));
+                for (int q = 0; q < 3; ++q) P.kslot.push_back(slots[3 * (s0 + k) + q]);
+            } else {
+                P.kslot.push_back(0); P.kslot.push_back(0); P.kslot.push_back(0);
+            }
+        }
+        P.kcbase.push_back(first);
+        P.kbox_c = std::max(P.kbox_c, last - first + 1);
+    }
+    P.nct = (int)P.kcbase.size();
+    const size_t stage = ((size_t)P.kbox_r64 * P.kbox_c * 16 + KIN_STAGE_ALIGN - 1) / KIN_STAGE_ALIGN * KIN_STAGE_ALIGN;
+    P.kin_ok = 2 * P.kbox_r64 <= 256 && 2 * P.kbox_r32 <= 256 && P.kbox_c <= 256 && 2 * stage + 64 <= 200 * 1024;
+}
 
 }  // namespace
 
@@ -173,6 +251,7 @@ bool he_build_plan(he_plan_host &P, int n, int nc, const int *ptr, const int *co
         P.dwptr[g + 1] = (int)P.dwsrc.size();
     }
     (void)nd;
+    build_kinetic(P, n);
     P.ok = true;
     return true;
 }
@@ -193,7 +272,10 @@ extern "C" void *he_plan_build(int n, int nc, const int *ptr, const int *col, co
 extern "C" void he_plan_free(void *plan) { delete static_cast<he_plan_host *>(plan); }
 
 // which: 0 estart, 1 tstart, 2 eoff, 3 ereal, 4 gch, 5 wptr, 6 wsrc, 7 dwptr, 8 dwsrc, 9 dwel, 10 dwedge,
-//        20 blocks (interleaved complex), 21 bblocks, 22 wcoef, 30 scalars {ok, ne, ntile, ng, nlam, maxm}.
+//        11 nodeelem, 12 krow, 13 krbase, 14 krcplx, 15 kslot, 16 kcbase,
+//        20 blocks (interleaved complex), 21 bblocks, 22 wcoef, 23 tre, 24 tim, 25 bre, 26 bim,
+//        30 scalars {ok, ne, ntile, ng, nlam, maxm, blkmax},
+//        31 kinetic scalars {kin_ok, ntr, nct, box_r (complex128), box_r (complex64), box_c}.
 // Returns the element count; copies when dst != NULL.
 extern "C" long long he_plan_array(void *plan, int which, void *dst)
 {
@@ -215,6 +297,21 @@ extern "C" long long he_plan_array(void *plan, int which, void *dst)
     case 20: vd = &P.blocks; break;
     case 21: vd = &P.bblocks; break;
     case 22: vd = &P.wcoef; break;
+    case 11: vi = &P.nodeelem; break;
+    case 12: vi = &P.krow; break;
+    case 13: vi = &P.krbase; break;
+    case 14: vi = &P.krcplx; break;
+    case 15: vi = &P.kslot; break;
+    case 16: vi = &P.kcbase; break;
+    case 23: vd = &P.tre; break;
+    case 24: vd = &P.tim; break;
+    case 25: vd = &P.bre; break;
+    case 26: vd = &P.bim; break;
+    case 31: {
+        const int s[6] = {P.kin_ok, P.ntr, P.nct, P.kbox_r64, P.kbox_r32, P.kbox_c};
+        if (dst) memcpy(dst, s, sizeof(s));
+        return 6;
+    }
     case 30: {
         const int s[7] = {P.ok, P.ne, P.ntile, P.ng, P.nlam, P.maxm, P.blkmax};
         if (dst) memcpy(dst, s, sizeof(s));

@@ -40,10 +40,8 @@ residual_kernel(size_t n, const double2 *b, const double2 *t, double2 *r, double
 
 __global__ void sum_kernel(const double *partial, int nb, double *out)
 {
-    if (threadIdx.x != 0) return;
-    double s = 0;
-    for (int b = 0; b < nb; ++b) s += partial[b];
-    *out = s;
+    const double s = warp_fixed_sum(partial, nb, 1);
+    if (threadIdx.x == 0) *out = s;
 }
 
 // y = x / (1 + i alpha d)   (Jacobi preconditioner of python/implicit.py:80,85)

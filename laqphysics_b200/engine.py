@@ -105,15 +105,23 @@ class B200Hamiltonian:
 
     def use_tiled(self, flag=True):
         """Select the tiled kernels (default when the tables admit them) or the generic one."""
-        check(LIB.he_set_path(self.op.handle, int(bool(flag))), 'he_set_path')
-        self.tiled = bool(flag)
+        self.set_path(1 if flag else 0)
+
+    def set_path(self, path):
+        """0: generic gather kernel; 1: tiled kernels with the TMA-staged kinetic kernel
+        (default); 2: tiled kernels with the shared-memory radial kernel."""
+        check(LIB.he_set_path(self.op.handle, int(path)), 'he_set_path')
+        self.tiled = path != 0
+        self.path = int(path)
 
     @property
     def launches_per_apply(self):
-        """Kernels one apply launches: field contraction, radial, mixing (tiled) or one."""
-        if not self.tiled:
-            return 1
-        return 3 if len(self.h.dc) else 2
+        """Kernels one apply launches: radial (kinetic) and channel mixing, or one generic."""
+        return 2 if self.tiled else 1
+
+    def device_status(self):
+        """Wait for the device and raise if a bounded device-side wait ran out."""
+        check(LIB.he_device_status(self.op.handle), 'device status')
 
     # --- state transfer -------------------------------------------------------------
     def state(self, x):
@@ -124,6 +132,7 @@ class B200Hamiltonian:
 
     def synchronize(self):
         torch.cuda.synchronize(self.device)
+        self.device_status()
 
     def _check(self, x, dtype):
         if x.device != self.device or x.dtype != dtype or not x.is_contiguous() or x.numel() != self.size:

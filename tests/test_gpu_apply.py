@@ -87,6 +87,29 @@ def test_tiled_and_generic_kernels_agree(velocity):
     np.testing.assert_allclose(c, op.host(x) + 1j * alpha * (b + 2.9 * op.host(x)), rtol=1e-12, atol=1e-12)
 
 
+@pytest.mark.parametrize('velocity', [False, True])
+def test_kinetic_tma_and_shared_memory_radial_kernels_agree(velocity):
+    """Path 1 (TMA-staged kinetic kernel) against path 2 (shared-memory radial kernel)
+    and path 0 (generic kernel) in both precisions, on a grid whose exterior tail is
+    split over column slots."""
+    h = _coupled(np.linspace(0, 24, 7), 6, .3, 24, 2, 1, cut=(12., 15.))
+    op = engine(h)
+    rng = np.random.default_rng(23)
+    x = op.state(rng.normal(size=h.size) + 1j * rng.normal(size=h.size))
+    f = (0., 0., .15)
+    results = {}
+    for path in (1, 2, 0):
+        op.set_path(path)
+        results[path] = (op.host(op.apply(x, f, velocity)),
+                         op.host(op.apply(x.to(torch.complex64), f, velocity, precision='complex64')))
+    op.set_path(1)
+    op.synchronize()
+    ref = cpu.tensor_apply(h, op.host(x), f, velocity)
+    for path, (y, y64) in results.items():
+        assert rel_l2(y, ref) < 1e-13, path
+        assert rel_l2(y64.astype(complex), ref) < C64_REL_L2, path
+
+
 def test_microbenchmark_grid_apply_matches_oracle():
     from laqphysics_b200.workloads import hpsi_microbench, seeded_state
     h = hpsi_microbench()
