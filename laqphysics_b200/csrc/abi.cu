@@ -154,7 +154,8 @@ template <typename R> int upload_plan(he_operator *h, he::TiledPlan<R> *pl, cplx
     k.box_c = P.kbox_c;
     const size_t box = (size_t)k.box_r * k.box_c * sizeof(cplx<R>);
     k.stage_bytes = (int)((box + he::KIN_STAGE_ALIGN - 1) / he::KIN_STAGE_ALIGN * he::KIN_STAGE_ALIGN);
-    k.estart = pl->estart; k.ereal = pl->ereal; k.eoff = pl->eoff;
+    k.estart = pl->estart; k.ereal = pl->ereal;
+    if ((s = upload(h, P.koff.data(), P.koff.size(), &k.koff))) return s;
     if ((s = upload(h, P.nodeelem.data(), P.nodeelem.size(), &k.nodeelem))) return s;
     if ((s = upload_r<R>(h, P.tre.data(), P.tre.size(), &k.tre))) return s;
     if ((s = upload_r<R>(h, P.tim.data(), P.tim.size(), &k.tim))) return s;

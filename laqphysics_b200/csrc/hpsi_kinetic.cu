@@ -74,81 +74,148 @@ template <typename R> __device__ __forceinline__ int elem_size(const KineticPlan
     return (e + 1 < kp.ne ? kp.estart[e + 1] + 1 : kp.n) - kp.estart[e];
 }
 
-// Along r2 for one slot: acc[q] += sum_b X_f[a0+q][b] S(s_f + b, i), plus for the bridge
-// column s_f (a0 == 0) the previous element's last row.  X = T or B (transposed planes).
-template <typename R>
-__device__ __forceinline__ void along_r2(const KineticPlan<R> &kp, const R *__restrict__ xre, const R *__restrict__ xim,
-                                         const cplx<R> *S, int box_r, int il, int y0, int f, int a0, int na,
-                                         cplx<R> (&acc)[KIN_NA])
+template <typename R> struct pair_t;
+template <> struct pair_t<double> { using type = double2; };
+template <> struct pair_t<float> { using type = float2; };
+template <typename R> __device__ __forceinline__ typename pair_t<R>::type ldg_pair(const R *p)
 {
-    const int sf = kp.estart[f], mf = elem_size(kp, f), off = kp.eoff[f];
-    const cplx<R> *col = S + (size_t)(sf - y0) * box_r + il;
-    if (kp.ereal[f]) {
-        for (int b = 0; b < mf; ++b) {
-            const cplx<R> x = col[(size_t)b * box_r];
-            const R *tr = xre + off + b * mf + a0;
+    return __ldg(reinterpret_cast<const typename pair_t<R>::type *>(p));
+}
+
+// acc[q] += X[a0+q][b] x for q < na; k = index of X^T[b][a0] in the padded planes (even,
+// so each pair of coefficients is one vector load; the loads are uniform over the warp).
+template <typename R, bool REAL>
+__device__ __forceinline__ void r2_tap(const R *__restrict__ xre, const R *__restrict__ xim, int k, cplx<R> x, int na,
+                                       cplx<R> (&acc)[KIN_NA])
+{
 #pragma unroll
-            for (int q = 0; q < KIN_NA; ++q)
-                if (q < na) acc[q] = rfma<R>(__ldg(tr + q), x, acc[q]);
-        }
-    } else {
-        for (int b = 0; b < mf; ++b) {
-            const cplx<R> x = col[(size_t)b * box_r];
-            const R *tr = xre + off + b * mf + a0, *ti = xim + off + b * mf + a0;
-#pragma unroll
-            for (int q = 0; q < KIN_NA; ++q)
-                if (q < na) acc[q] = cfma<R>(mk<R>(__ldg(tr + q), __ldg(ti + q)), x, acc[q]);
+    for (int q = 0; q < KIN_NA; q += 2) {
+        if (q < na) {
+            const auto tr = ldg_pair<R>(xre + k + q);
+            if (REAL) {
+                acc[q] = rfma<R>(tr.x, x, acc[q]);
+                if (q + 1 < na) acc[q + 1] = rfma<R>(tr.y, x, acc[q + 1]);
+            } else {
+                const auto ti = ldg_pair<R>(xim + k + q);
+                acc[q] = cfma<R>(mk<R>(tr.x, ti.x), x, acc[q]);
+                if (q + 1 < na) acc[q + 1] = cfma<R>(mk<R>(tr.y, ti.y), x, acc[q + 1]);
+            }
         }
     }
-    if (a0 == 0 && f > 0) {
-        const int fp = f - 1, sp = kp.estart[fp], mp = sf - sp + 1, offp = kp.eoff[fp];
-        const cplx<R> *colp = S + (size_t)(sp - y0) * box_r + il;
-        const bool real = kp.ereal[fp];
+}
+
+// Along r2 over the nodes of element f (size M at compile time, or m when M == 0):
+// acc[q] += sum_b X_f[a0+q][b] S(s_f + b, i); `col` points at S(s_f, i).
+template <typename R, bool REAL, int M>
+__device__ __forceinline__ void r2_element(const R *xre, const R *xim, int koff, int m, int a0, int na,
+                                           const cplx<R> *col, int pitch, cplx<R> (&acc)[KIN_NA])
+{
+    if constexpr (M > 0) {
+        constexpr int MP = M + (M & 1);
+#pragma unroll
+        for (int b = 0; b < M; ++b) r2_tap<R, REAL>(xre, xim, koff + b * MP + a0, col[b * pitch], na, acc);
+    } else {
+        const int mp = m + (m & 1);
+        for (int b = 0; b < m; ++b) r2_tap<R, REAL>(xre, xim, koff + b * mp + a0, col[b * pitch], na, acc);
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ void along_r2(const KineticPlan<R> &kp, const R *__restrict__ xre, const R *__restrict__ xim,
+                                         const cplx<R> *S, int pitch, int il, int y0, int f, int a0, int na,
+                                         cplx<R> (&acc)[KIN_NA])
+{
+    const int sf = kp.estart[f], mf = elem_size(kp, f), koff = kp.koff[f];
+    const cplx<R> *col = S + (sf - y0) * pitch + il;
+    const bool real = kp.ereal[f];
+    switch (real ? mf : -mf) {   // slot-uniform: the common FE sizes get exact unrolls
+    case 9: r2_element<R, true, 9>(xre, xim, koff, mf, a0, na, col, pitch, acc); break;
+    case 10: r2_element<R, true, 10>(xre, xim, koff, mf, a0, na, col, pitch, acc); break;
+    case -9: r2_element<R, false, 9>(xre, xim, koff, mf, a0, na, col, pitch, acc); break;
+    case -10: r2_element<R, false, 10>(xre, xim, koff, mf, a0, na, col, pitch, acc); break;
+    default:
+        if (real) r2_element<R, true, 0>(xre, xim, koff, mf, a0, na, col, pitch, acc);
+        else r2_element<R, false, 0>(xre, xim, koff, mf, a0, na, col, pitch, acc);
+    }
+    if (a0 == 0 && f > 0) {   // bridge column s_f: the previous element's last row
+        const int fp = f - 1, sp = kp.estart[fp], mp = sf - sp + 1, mpp = mp + (mp & 1), kf = kp.koff[fp];
+        const cplx<R> *colp = S + (sp - y0) * pitch + il;
+        const bool rp = kp.ereal[fp];
         cplx<R> s = acc[0];
         for (int b = 0; b < mp - 1; ++b) {
-            const size_t k = (size_t)offp + (size_t)b * mp + (mp - 1);
-            const cplx<R> x = colp[(size_t)b * box_r];
-            s = real ? rfma<R>(__ldg(xre + k), x, s) : cfma<R>(mk<R>(__ldg(xre + k), __ldg(xim + k)), x, s);
+            const int k = kf + b * mpp + (mp - 1);
+            const cplx<R> x = colp[b * pitch];
+            s = rp ? rfma<R>(__ldg(xre + k), x, s) : cfma<R>(mk<R>(__ldg(xre + k), __ldg(xim + k)), x, s);
         }
         acc[0] = s;
     }
 }
 
-// Along r1 for row i (node a_i of element e): acc[q] += sum_b X_e[a_i][b] S(cq0 + q, s_e + b),
-// plus the previous element's last row when i is a bridge row.
-template <typename R>
-__device__ __forceinline__ void along_r1(const KineticPlan<R> &kp, const R *__restrict__ xre, const R *__restrict__ xim,
-                                         const cplx<R> *S, int box_r, int i, int x0, int cq0, int y0, int na,
-                                         cplx<R> (&acc)[KIN_NA])
+// Along r1 for row i = s_e + a_i over element e's own nodes: acc[q] += sum_b X_e[a_i][b]
+// S(cq0 + q, s_e + b); `rows` points at S(cq0, s_e).  The coefficient row sits in registers.
+template <typename R, bool REAL, int M>
+__device__ __forceinline__ void r1_row(const R *__restrict__ xre, const R *__restrict__ xim, int koff, int m, int ai,
+                                       int na, const cplx<R> *rows, int pitch, cplx<R> (&acc)[KIN_NA])
 {
-    const int e = kp.nodeelem[i], se = kp.estart[e], me = elem_size(kp, e), ai = i - se, off = kp.eoff[e];
-    const cplx<R> *rows = S + (size_t)(cq0 - y0) * box_r + (se - x0);
-    if (kp.ereal[e]) {
-        for (int b = 0; b < me; ++b) {
-            const R tr = __ldg(xre + off + b * me + ai);
+    if constexpr (M > 0) {
+        constexpr int MP = M + (M & 1);
+        R tr[M], ti[M];
 #pragma unroll
-            for (int q = 0; q < KIN_NA; ++q)
-                if (q < na) acc[q] = rfma<R>(tr, rows[(size_t)q * box_r + b], acc[q]);
+        for (int b = 0; b < M; ++b) {
+            tr[b] = __ldg(xre + koff + b * MP + ai);
+            ti[b] = REAL ? (R)0 : __ldg(xim + koff + b * MP + ai);
+        }
+#pragma unroll
+        for (int q = 0; q < KIN_NA; ++q) {
+            if (q < na) {
+                const cplx<R> *rq = rows + q * pitch;
+                cplx<R> s = acc[q];
+#pragma unroll
+                for (int b = 0; b < M; ++b) s = REAL ? rfma<R>(tr[b], rq[b], s) : cfma<R>(mk<R>(tr[b], ti[b]), rq[b], s);
+                acc[q] = s;
+            }
         }
     } else {
-        for (int b = 0; b < me; ++b) {
-            const cplx<R> tv = mk<R>(__ldg(xre + off + b * me + ai), __ldg(xim + off + b * me + ai));
+        const int mp = m + (m & 1);
+        for (int b = 0; b < m; ++b) {
+            const R tr = __ldg(xre + koff + b * mp + ai), ti = REAL ? (R)0 : __ldg(xim + koff + b * mp + ai);
 #pragma unroll
             for (int q = 0; q < KIN_NA; ++q)
-                if (q < na) acc[q] = cfma<R>(tv, rows[(size_t)q * box_r + b], acc[q]);
+                if (q < na) acc[q] = REAL ? rfma<R>(tr, rows[q * pitch + b], acc[q])
+                                          : cfma<R>(mk<R>(tr, ti), rows[q * pitch + b], acc[q]);
         }
     }
-    if (ai == 0 && e > 0) {
-        const int ep = e - 1, sp = kp.estart[ep], mp = se - sp + 1, offp = kp.eoff[ep];
-        const cplx<R> *rp = S + (size_t)(cq0 - y0) * box_r + (sp - x0);
-        const bool real = kp.ereal[ep];
+}
+
+// Along r1 for row i.  The bridge-row part (i = s_e: the previous element's last row) is
+// added here only when `bridge` is set (the velocity-gauge W1 pass); the kinetic pass
+// takes it from the per-item bridge partials instead.
+template <typename R>
+__device__ __forceinline__ void along_r1(const KineticPlan<R> &kp, const R *__restrict__ xre, const R *__restrict__ xim,
+                                         const cplx<R> *S, int pitch, int i, int x0, int cq0, int y0, int na, bool bridge,
+                                         cplx<R> (&acc)[KIN_NA])
+{
+    const int e = kp.nodeelem[i], se = kp.estart[e], me = elem_size(kp, e), ai = i - se, koff = kp.koff[e];
+    const cplx<R> *rows = S + (cq0 - y0) * pitch + (se - x0);
+    const bool real = kp.ereal[e];
+    switch (real ? me : -me) {
+    case 9: r1_row<R, true, 9>(xre, xim, koff, me, ai, na, rows, pitch, acc); break;
+    case 10: r1_row<R, true, 10>(xre, xim, koff, me, ai, na, rows, pitch, acc); break;
+    default:
+        if (real) r1_row<R, true, 0>(xre, xim, koff, me, ai, na, rows, pitch, acc);
+        else r1_row<R, false, 0>(xre, xim, koff, me, ai, na, rows, pitch, acc);
+    }
+    if (bridge && ai == 0 && e > 0) {
+        const int ep = e - 1, sp = kp.estart[ep], mp = se - sp + 1, mpp = mp + (mp & 1), kf = kp.koff[ep];
+        const cplx<R> *rp = S + (cq0 - y0) * pitch + (sp - x0);
+        const bool real_p = kp.ereal[ep];
         for (int b = 0; b < mp - 1; ++b) {
-            const size_t k = (size_t)offp + (size_t)b * mp + (mp - 1);
-            const cplx<R> tv = mk<R>(__ldg(xre + k), real ? (R)0 : __ldg(xim + k));
+            const int k = kf + b * mpp + (mp - 1);
+            const cplx<R> tv = mk<R>(__ldg(xre + k), real_p ? (R)0 : __ldg(xim + k));
 #pragma unroll
             for (int q = 0; q < KIN_NA; ++q)
-                if (q < na) acc[q] = real ? rfma<R>(tv.x, rp[(size_t)q * box_r + b], acc[q])
-                                          : cfma<R>(tv, rp[(size_t)q * box_r + b], acc[q]);
+                if (q < na) acc[q] = real_p ? rfma<R>(tv.x, rp[q * pitch + b], acc[q])
+                                            : cfma<R>(tv, rp[q * pitch + b], acc[q]);
         }
     }
 }
@@ -158,19 +225,20 @@ __global__ void __launch_bounds__(KIN_THREADS, 2)
 hpsi_kinetic_kernel(const __grid_constant__ CUtensorMap tmap, const DeviceTables<R> t, const KineticPlan<R> kp,
                     cplx<R> *__restrict__ out, cplx<R> *__restrict__ w1, cplx<R> *__restrict__ w2, R a2)
 {
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
-    // staged boxes start on a 1024-byte boundary (the launch adds the slack)
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    // staged boxes start on a KIN_STAGE_ALIGN boundary (the launch adds the slack)
     unsigned char *smem = smem_raw + ((KIN_STAGE_ALIGN - (smem_u32(smem_raw) & (KIN_STAGE_ALIGN - 1))) & (KIN_STAGE_ALIGN - 1));
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * (size_t)kp.stage_bytes);
+    cplx<R> *BR = reinterpret_cast<cplx<R> *>(smem + 2 * (size_t)kp.stage_bytes);      // bridge-row partials
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + 2 * (size_t)kp.stage_bytes + KIN_BRIDGE_BYTES);
     constexpr int ALIGN = 16 / (int)sizeof(cplx<R>);   // nodes per 16 bytes (TMA start alignment)
-    const int n = kp.n, nc = kp.nc, box_r = kp.box_r;
+    const int n = kp.n, nc = kp.nc, pitch = kp.box_r;
     const size_t nn = (size_t)n * n;
     const long long items = (long long)kp.ntr * kp.nct * nc;
     const long long per = (items + gridDim.x - 1) / gridDim.x;
     const long long first = (long long)blockIdx.x * per;
     const long long last = first + per < items ? first + per : items;
     if (first >= last) return;
-    const unsigned box_bytes = (unsigned)((size_t)box_r * kp.box_c * sizeof(cplx<R>));
+    const unsigned box_bytes = (unsigned)((size_t)pitch * kp.box_c * sizeof(cplx<R>));
 
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
@@ -205,37 +273,65 @@ hpsi_kinetic_kernel(const __grid_constant__ CUtensorMap tmap, const DeviceTables
         const int c = (int)(it % nc), tr = (int)(tile / kp.nct), tc = (int)(tile % kp.nct);
         const int ea = kp.krow[tr], eb = kp.krow[tr + 1];
         const int r0 = kp.estart[ea], r1 = eb < kp.ne ? kp.estart[eb] : n;
-        const int i = r0 + lane_row;
-        const int *sl = kp.kslot + (tc * KIN_SLOTS + slot) * 3;
-        const int f = sl[0], a0 = sl[1], na = sl[2];
-        if (i >= r1 || na == 0) continue;
         const cplx<R> *S = reinterpret_cast<const cplx<R> *>(smem + (size_t)stage * kp.stage_bytes);
         const int x0 = kp.krbase[tr] / ALIGN * ALIGN, y0 = kp.kcbase[tc];
+        const int *slots = kp.kslot + tc * KIN_SLOTS * 3;
+        const int c0 = kp.estart[slots[0]] + slots[1];   // first owned column of the tile
+
+        // bridge-row partials: for every bridge row s_e (e >= max(ea, 1)) of the row tile and
+        // every owned column, the previous element's last row applied along r1
+        const int e_br = ea > 0 ? ea : 1, nbr = eb - e_br;
+        const int ncol = slots[2] + slots[5] + slots[8] + slots[11];
+        for (int idx = threadIdx.x; idx < nbr * ncol; idx += KIN_THREADS) {
+            const int kb = idx / ncol, jj = idx - kb * ncol;
+            const int e = e_br + kb, ep = e - 1, sp = kp.estart[ep], mp = kp.estart[e] - sp + 1;
+            const int mpp = mp + (mp & 1), kf = kp.koff[ep];
+            const cplx<R> *src = S + (c0 + jj - y0) * pitch + (sp - x0);
+            const bool rp = kp.ereal[ep];
+            cplx<R> s = mk<R>(0, 0);
+            for (int b = 0; b < mp - 1; ++b) {
+                const int kk = kf + b * mpp + (mp - 1);
+                s = rp ? rfma<R>(__ldg(kp.tre + kk), src[b], s) : cfma<R>(mk<R>(__ldg(kp.tre + kk), __ldg(kp.tim + kk)), src[b], s);
+            }
+            BR[kb * KIN_BRCOLS + jj] = s;
+        }
+        __syncthreads();
+
+        const int i = r0 + lane_row;
+        const int f = slots[3 * slot], a0 = slots[3 * slot + 1], na = slots[3 * slot + 2];
+        if (i >= r1 || na == 0) continue;
         const int il = i - x0, cq0 = kp.estart[f] + a0;
         cplx<R> acc[KIN_NA];
         if (VEL) {
 #pragma unroll
             for (int q = 0; q < KIN_NA; ++q) acc[q] = mk<R>(0, 0);
-            along_r2<R>(kp, kp.bre, kp.bim, S, box_r, il, y0, f, a0, na, acc);
+            along_r2<R>(kp, kp.bre, kp.bim, S, pitch, il, y0, f, a0, na, acc);
 #pragma unroll
             for (int q = 0; q < KIN_NA; ++q)
                 if (q < na) w2[(size_t)i + (size_t)n * (cq0 + q) + nn * c] = acc[q];
 #pragma unroll
             for (int q = 0; q < KIN_NA; ++q) acc[q] = mk<R>(0, 0);
-            along_r1<R>(kp, kp.bre, kp.bim, S, box_r, i, x0, cq0, y0, na, acc);
+            along_r1<R>(kp, kp.bre, kp.bim, S, pitch, i, x0, cq0, y0, na, true, acc);
 #pragma unroll
             for (int q = 0; q < KIN_NA; ++q)
                 if (q < na) w1[(size_t)i + (size_t)n * (cq0 + q) + nn * c] = acc[q];
         }
 #pragma unroll
         for (int q = 0; q < KIN_NA; ++q) acc[q] = mk<R>(0, 0);
-        along_r2<R>(kp, kp.tre, kp.tim, S, box_r, il, y0, f, a0, na, acc);
-        along_r1<R>(kp, kp.tre, kp.tim, S, box_r, i, x0, cq0, y0, na, acc);
+        along_r2<R>(kp, kp.tre, kp.tim, S, pitch, il, y0, f, a0, na, acc);
+        along_r1<R>(kp, kp.tre, kp.tim, S, pitch, i, x0, cq0, y0, na, false, acc);
+        const int e = kp.nodeelem[i];
+        if (i == kp.estart[e] && e > 0) {   // bridge row: add its partials
+            const cplx<R> *br = BR + (e - e_br) * KIN_BRCOLS + (cq0 - c0);
+#pragma unroll
+            for (int q = 0; q < KIN_NA; ++q)
+                if (q < na) acc[q] = cadd<R>(acc[q], br[q]);
+        }
 #pragma unroll
         for (int q = 0; q < KIN_NA; ++q) {
             if (q < na) {
                 const int j = cq0 + q;
-                const cplx<R> x = S[(size_t)(j - y0) * box_r + il];
+                const cplx<R> x = S[(j - y0) * pitch + il];
                 const size_t p = (size_t)i + (size_t)n * j + nn * c;
                 const cplx<R> d = SEP ? cadd<R>(ldg<R>(t.d1 + i + (size_t)n * c), ldg<R>(t.d2 + j + (size_t)n * c))
                                       : ldg<R>(t.diag + p);
@@ -299,7 +395,7 @@ int launch_kinetic(he_operator *h, const DeviceTables<R> &t, const KineticPlan<R
                                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return he_fail(HE_ERR_CUDA, "cuTensorMapEncodeTiled failed", __FILE__, __LINE__);
-    const size_t smem = 2 * (size_t)kp.stage_bytes + 16 + KIN_STAGE_ALIGN;
+    const size_t smem = 2 * (size_t)kp.stage_bytes + KIN_BRIDGE_BYTES + 16 + KIN_STAGE_ALIGN;
     const long long items = (long long)kp.ntr * kp.nct * kp.nc;
     const unsigned grid = (unsigned)std::min<long long>(items, 2LL * sm_count(h->device));
 #define HE_KINETIC(V, S)                                                                                   \

@@ -15,14 +15,17 @@ namespace he {
 constexpr int KIN_ROWS = 64;                     // owned rows per tile (thread lanes along r1)
 constexpr int KIN_SLOTS = 4;                     // column slots per tile
 constexpr int KIN_NA = 10;                       // owned columns per slot (outputs per thread)
+constexpr int KIN_RELEMS = 8;                    // elements per row tile (bridge rows per tile)
 constexpr int KIN_THREADS = KIN_ROWS * KIN_SLOTS;
-constexpr int KIN_STAGE_ALIGN = 1024;            // byte alignment of each staged box
+constexpr int KIN_STAGE_ALIGN = 128;             // byte alignment of each staged box
+constexpr int KIN_BRCOLS = KIN_SLOTS * KIN_NA;   // owned columns of a column tile, at most
+constexpr int KIN_BRIDGE_BYTES = KIN_RELEMS * KIN_BRCOLS * 16;   // bridge-row partials (complex128)
 
 template <typename R> struct KineticPlan {
     int n, nc, ne, ntr, nct, box_r, box_c;
     int stage_bytes;                             // box bytes, rounded up to KIN_STAGE_ALIGN
-    const int *estart, *nodeelem, *ereal, *eoff;
-    const R *tre, *tim, *bre, *bim;              // transposed element blocks (planes)
+    const int *estart, *nodeelem, *ereal, *koff;
+    const R *tre, *tim, *bre, *bim;              // transposed element blocks (planes, even row stride)
     const int *krow, *krbase, *krcplx;           // row tiles
     const int *kslot, *kcbase;                   // column tiles
     int *err;                                    // device error word (bounded waits that ran out)

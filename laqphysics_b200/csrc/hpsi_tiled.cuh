@@ -48,6 +48,7 @@ struct he_plan_host {
     std::vector<int> nodeelem;              // n: element owning each node (a bridge node belongs to the later element)
     std::vector<int> krow, krbase, krcplx;  // row tiles: ntr+1 element starts, first staged row, any complex block
     std::vector<int> kslot, kcbase;         // column tiles: nct x KIN_SLOTS x (element, a0, na), first staged column
-    std::vector<double> tre, tim, bre, bim; // transposed element blocks: [eoff[e] + b m + a] = X[a][b]
+    std::vector<int> koff;                  // ne+1 offsets of the transposed blocks
+    std::vector<double> tre, tim, bre, bim; // transposed element blocks: [koff[e] + b mp + a] = X[a][b], mp = m + (m & 1)
     int ntr = 0, nct = 0, kbox_r64 = 0, kbox_r32 = 0, kbox_c = 0;
 };

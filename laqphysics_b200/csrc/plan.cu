@@ -26,8 +26,8 @@ struct UnionFind {
     void join(int a, int b) { p[find(a)] = find(b); }
 };
 
-// Tiles of the kinetic kernel (hpsi_kinetic.cu): row tiles of whole elements with at most
-// KIN_ROWS owned nodes, column tiles of KIN_SLOTS slots (<= KIN_NA owned nodes of one
+// Tiles of the kinetic kernel (hpsi_kinetic.cu): row tiles of at most KIN_RELEMS whole
+// elements and KIN_ROWS owned nodes, column tiles of KIN_SLOTS slots (<= KIN_NA owned nodes of one
 // element each), the first staged node of every tile (the previous element's first node
 // when its bridge row is owned) and the staged box extents.  Leaves kin_ok false when an
 // element does not fit or the box exceeds the TMA / shared-memory limits.
@@ -41,13 +41,18 @@ void build_kinetic(he_plan_host &P, int n)
     P.nodeelem.assign(n, 0);
     for (int e = 0; e < ne; ++e)
         for (int i = P.estart[e]; i < P.estart[e] + own(e); ++i) P.nodeelem[i] = e;
-    const size_t total = P.eoff[ne];
+    // transposed planes, rows padded to an even length so that pairs of outputs load as
+    // one 16-byte (complex128 plan) or 8-byte (complex64 plan) vector; two entries of
+    // padding at the end keep the last pair load inside the array
+    P.koff.assign(ne + 1, 0);
+    for (int e = 0; e < ne; ++e) P.koff[e + 1] = P.koff[e] + esize(e) * (esize(e) + (esize(e) & 1));
+    const size_t total = (size_t)P.koff[ne] + 2;
     P.tre.assign(total, 0.0); P.tim.assign(total, 0.0); P.bre.assign(total, 0.0); P.bim.assign(total, 0.0);
     for (int e = 0; e < ne; ++e) {
-        const int m = esize(e);
+        const int m = esize(e), mp = m + (m & 1);
         for (int a = 0; a < m; ++a)
             for (int b = 0; b < m; ++b) {
-                const size_t src = 2 * ((size_t)P.eoff[e] + (size_t)a * m + b), dst = (size_t)P.eoff[e] + (size_t)b * m + a;
+                const size_t src = 2 * ((size_t)P.eoff[e] + (size_t)a * m + b), dst = (size_t)P.koff[e] + (size_t)b * mp + a;
                 P.tre[dst] = P.blocks[src]; P.tim[dst] = P.blocks[src + 1];
                 P.bre[dst] = P.bblocks[src]; P.bim[dst] = P.bblocks[src + 1];
             }
@@ -57,7 +62,7 @@ void build_kinetic(he_plan_host &P, int n)
     P.kbox_r64 = P.kbox_r32 = P.kbox_c = 0;
     for (int e = 0; e < ne;) {
         int o = 0, f = e;
-        while (f < ne && o + own(f) <= KIN_ROWS) { o += own(f); ++f; }
+        while (f < ne && f - e < KIN_RELEMS && o + own(f) <= KIN_ROWS) { o += own(f); ++f; }
         if (f == e) return;
         P.krow.push_back(f);
         e = f;
@@ -100,7 +105,8 @@ void build_kinetic(he_plan_host &P, int n)
     }
     P.nct = (int)P.kcbase.size();
     const size_t stage = ((size_t)P.kbox_r64 * P.kbox_c * 16 + KIN_STAGE_ALIGN - 1) / KIN_STAGE_ALIGN * KIN_STAGE_ALIGN;
-    P.kin_ok = 2 * P.kbox_r64 <= 256 && 2 * P.kbox_r32 <= 256 && P.kbox_c <= 256 && 2 * stage + 64 <= 200 * 1024;
+    P.kin_ok = 2 * P.kbox_r64 <= 256 && 2 * P.kbox_r32 <= 256 && P.kbox_c <= 256 &&
+               2 * stage + KIN_BRIDGE_BYTES + 64 <= 200 * 1024;
 }
 
 }  // namespace
@@ -272,7 +278,7 @@ extern "C" void *he_plan_build(int n, int nc, const int *ptr, const int *col, co
 extern "C" void he_plan_free(void *plan) { delete static_cast<he_plan_host *>(plan); }
 
 // which: 0 estart, 1 tstart, 2 eoff, 3 ereal, 4 gch, 5 wptr, 6 wsrc, 7 dwptr, 8 dwsrc, 9 dwel, 10 dwedge,
-//        11 nodeelem, 12 krow, 13 krbase, 14 krcplx, 15 kslot, 16 kcbase,
+//        11 nodeelem, 12 krow, 13 krbase, 14 krcplx, 15 kslot, 16 kcbase, 17 koff,
 //        20 blocks (interleaved complex), 21 bblocks, 22 wcoef, 23 tre, 24 tim, 25 bre, 26 bim,
 //        30 scalars {ok, ne, ntile, ng, nlam, maxm, blkmax},
 //        31 kinetic scalars {kin_ok, ntr, nct, box_r (complex128), box_r (complex64), box_c}.
@@ -303,6 +309,7 @@ extern "C" long long he_plan_array(void *plan, int which, void *dst)
     case 14: vi = &P.krcplx; break;
     case 15: vi = &P.kslot; break;
     case 16: vi = &P.kcbase; break;
+    case 17: vi = &P.koff; break;
     case 23: vd = &P.tre; break;
     case 24: vd = &P.tim; break;
     case 25: vd = &P.bre; break;

@@ -13,7 +13,7 @@ import pytest
 
 from conftest import Tables, golden
 
-KIN_ROWS, KIN_SLOTS, KIN_NA = 64, 4, 10
+KIN_ROWS, KIN_SLOTS, KIN_NA, KIN_RELEMS = 64, 4, 10, 8
 
 
 def kinetic_plan(h):
@@ -34,7 +34,7 @@ def kinetic_plan(h):
         K = {'ok': bool(s[0]), 'ntr': int(s[1]), 'nct': int(s[2]), 'box_r64': int(s[3]), 'box_r32': int(s[4]),
              'box_c': int(s[5])}
         for which, name in ((0, 'estart'), (2, 'eoff'), (3, 'ereal'), (11, 'nodeelem'), (12, 'krow'),
-                            (13, 'krbase'), (14, 'krcplx'), (15, 'kslot'), (16, 'kcbase')):
+                            (13, 'krbase'), (14, 'krcplx'), (15, 'kslot'), (16, 'kcbase'), (17, 'koff')):
             K[name] = get(which, np.int32)
         for which, name in ((23, 'tre'), (24, 'tim'), (25, 'bre'), (26, 'bim')):
             K[name] = get(which, np.float64)
@@ -59,10 +59,15 @@ def emulate_kinetic(h, x, K, velocity, a2=0.0, align=1):
     W = [np.full((n, n, nc), np.nan, complex), np.full((n, n, nc), np.nan, complex)]
     planes = {'T': (K['tre'], K['tim']), 'B': (K['bre'], K['bim'])}
 
-    def coef(which, e, a, b):          # X_e[a][b] from the transposed planes
+    koff = K['koff']
+
+    def coef(which, e, a, b, pair=False):   # X_e[a][b] from the padded transposed planes
         re, im = planes[which]
         m = msize(e)
-        k = eoff[e] + b * m + a
+        k = koff[e] + b * (m + (m & 1)) + a
+        assert 0 <= a < m and 0 <= b < m and k < koff[e + 1]
+        if pair:                             # the kernel loads (k, k+1) as one vector
+            assert k % 2 == 0 and k + 1 < len(re)
         return re[k] + 1j * im[k]
 
     covered = np.zeros((n, n), int)
@@ -71,6 +76,7 @@ def emulate_kinetic(h, x, K, velocity, a2=0.0, align=1):
         r0, r1 = es[ea], (es[eb] if eb < ne else n)
         x0 = K['krbase'][tr] // align * align
         assert (x0 * 16 // align) % 16 == 0 and x0 >= 0
+        assert eb - ea <= KIN_RELEMS
         for tc in range(K['nct']):
             y0 = K['kcbase'][tc]
             valid = np.zeros((box_c, box_r), bool)   # S[col][row] holds a real node
@@ -83,6 +89,8 @@ def emulate_kinetic(h, x, K, velocity, a2=0.0, align=1):
                 assert 0 <= cc < box_c and 0 <= rr < box_r and valid[cc, rr], (col, row, y0, x0)
                 return psi[row, col, c]
 
+            c0 = es[K['kslot'][tc, 0, 0]] + K['kslot'][tc, 0, 1]
+            assert K['kslot'][tc, :, 2].sum() <= KIN_SLOTS * KIN_NA
             for slot in range(KIN_SLOTS):
                 f, a0, na = K['kslot'][tc, slot]
                 if na == 0:
@@ -98,10 +106,11 @@ def emulate_kinetic(h, x, K, velocity, a2=0.0, align=1):
                     for c in range(nc):
                         def r2(which):
                             acc = np.zeros(na, complex)
+                            assert a0 % 2 == 0
                             for b in range(mf):
                                 xv = S(c, sf + b, i)
                                 for q in range(na):
-                                    acc[q] += coef(which, f, a0 + q, b) * xv
+                                    acc[q] += coef(which, f, a0 + q, b, pair=q % 2 == 0) * xv
                             if a0 == 0 and f > 0:
                                 fp = f - 1
                                 sp, mp = es[fp], sf - es[fp] + 1
@@ -119,7 +128,8 @@ def emulate_kinetic(h, x, K, velocity, a2=0.0, align=1):
                                 t = coef(which, e, ai, b)
                                 for q in range(na):
                                     acc[q] += t * S(c, cq0 + q, se + b)
-                            if ai == 0 and e > 0:
+                            if ai == 0 and e > 0:   # kernel: bridge partials (kinetic) or in-lane (W1)
+                                assert 0 <= e - max(ea, 1) < KIN_RELEMS and 0 <= cq0 - c0 and cq0 - c0 + na <= KIN_SLOTS * KIN_NA
                                 ep = e - 1
                                 sp, mp = es[ep], se - es[ep] + 1
                                 for b in range(mp - 1):
@@ -202,5 +212,6 @@ def test_microbenchmark_kinetic_tiles():
     assert max(owned) <= KIN_ROWS and sum(owned) == h.n
     assert K['kslot'][:, :, 2].sum() == h.n
     # two staged boxes per CTA and two CTAs per SM fit the 228 KB of an SM
-    stage = -(-K['box_r64'] * K['box_c'] * 16 // 1024) * 1024
-    assert 2 * (2 * stage + 16 + 1024 + 1024) <= 228 * 1024, (K['box_r64'], K['box_c'])
+    stage = -(-K['box_r64'] * K['box_c'] * 16 // 128) * 128
+    bridge = KIN_RELEMS * KIN_SLOTS * KIN_NA * 16
+    assert 2 * (2 * stage + bridge + 16 + 128 + 1024) <= 228 * 1024, (K['box_r64'], K['box_c'])
