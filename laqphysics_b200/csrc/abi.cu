@@ -109,6 +109,34 @@ int build_tables(he_operator *h, he::DeviceTables<R> *t, const int *ptr, const i
     return HE_OK;
 }
 
+// Kinetic (TMA-staged, FP32/FP64 FMA) plan; shares the element tables of the tiled plan.
+template <typename R> int upload_kinetic(he_operator *h, const he::TiledPlan<R> *pl, he::KineticPlan<R> *kp)
+{
+    const he_plan_host &P = h->plan;
+    int s;
+    he::KineticPlan<R> k{};
+    k.n = h->n; k.nc = h->nc; k.ne = P.ne; k.ntr = P.ntr; k.nct = P.nct;
+    k.box_r = sizeof(R) == 8 ? P.kbox_r64 : P.kbox_r32;
+    k.box_c = P.kbox_c;
+    const size_t box = (size_t)k.box_r * k.box_c * sizeof(cplx<R>);
+    k.stage_bytes = (int)((box + he::KIN_STAGE_ALIGN - 1) / he::KIN_STAGE_ALIGN * he::KIN_STAGE_ALIGN);
+    k.estart = pl->estart; k.ereal = pl->ereal;
+    if ((s = upload(h, P.koff.data(), P.koff.size(), &k.koff))) return s;
+    if ((s = upload(h, P.nodeelem.data(), P.nodeelem.size(), &k.nodeelem))) return s;
+    if ((s = upload_r<R>(h, P.tre.data(), P.tre.size(), &k.tre))) return s;
+    if ((s = upload_r<R>(h, P.tim.data(), P.tim.size(), &k.tim))) return s;
+    if ((s = upload_r<R>(h, P.bre.data(), P.bre.size(), &k.bre))) return s;
+    if ((s = upload_r<R>(h, P.bim.data(), P.bim.size(), &k.bim))) return s;
+    if ((s = upload(h, P.krow.data(), P.krow.size(), &k.krow))) return s;
+    if ((s = upload(h, P.krbase.data(), P.krbase.size(), &k.krbase))) return s;
+    if ((s = upload(h, P.krcplx.data(), P.krcplx.size(), &k.krcplx))) return s;
+    if ((s = upload(h, P.kslot.data(), P.kslot.size(), &k.kslot))) return s;
+    if ((s = upload(h, P.kcbase.data(), P.kcbase.size(), &k.kcbase))) return s;
+    k.err = h->kerr;
+    *kp = k;
+    return HE_OK;
+}
+
 // Upload the tiled plan in precision R.
 template <typename R> int upload_plan(he_operator *h, he::TiledPlan<R> *pl, cplx<R> **coef)
 {
@@ -140,7 +168,6 @@ template <typename R> int upload_plan(he_operator *h, he::TiledPlan<R> *pl, cplx
     he::KineticPlan<R> *kp;
     if constexpr (sizeof(R) == 8) kp = &h->k64; else kp = &h->k32;
     *kp = he::KineticPlan<R>{};
-    if (!P.kin_ok) return HE_OK;
     if (!h->kerr) {
         void *e = nullptr;
         HE_CUDA_TRY(cudaMalloc(&e, sizeof(int)));
@@ -148,26 +175,26 @@ template <typename R> int upload_plan(he_operator *h, he::TiledPlan<R> *pl, cplx
         HE_CUDA_TRY(cudaMemset(e, 0, sizeof(int)));
         h->kerr = static_cast<int *>(e);
     }
-    he::KineticPlan<R> k{};
-    k.n = h->n; k.nc = h->nc; k.ne = P.ne; k.ntr = P.ntr; k.nct = P.nct;
-    k.box_r = sizeof(R) == 8 ? P.kbox_r64 : P.kbox_r32;
-    k.box_c = P.kbox_c;
-    const size_t box = (size_t)k.box_r * k.box_c * sizeof(cplx<R>);
-    k.stage_bytes = (int)((box + he::KIN_STAGE_ALIGN - 1) / he::KIN_STAGE_ALIGN * he::KIN_STAGE_ALIGN);
-    k.estart = pl->estart; k.ereal = pl->ereal;
-    if ((s = upload(h, P.koff.data(), P.koff.size(), &k.koff))) return s;
-    if ((s = upload(h, P.nodeelem.data(), P.nodeelem.size(), &k.nodeelem))) return s;
-    if ((s = upload_r<R>(h, P.tre.data(), P.tre.size(), &k.tre))) return s;
-    if ((s = upload_r<R>(h, P.tim.data(), P.tim.size(), &k.tim))) return s;
-    if ((s = upload_r<R>(h, P.bre.data(), P.bre.size(), &k.bre))) return s;
-    if ((s = upload_r<R>(h, P.bim.data(), P.bim.size(), &k.bim))) return s;
-    if ((s = upload(h, P.krow.data(), P.krow.size(), &k.krow))) return s;
-    if ((s = upload(h, P.krbase.data(), P.krbase.size(), &k.krbase))) return s;
-    if ((s = upload(h, P.krcplx.data(), P.krcplx.size(), &k.krcplx))) return s;
-    if ((s = upload(h, P.kslot.data(), P.kslot.size(), &k.kslot))) return s;
-    if ((s = upload(h, P.kcbase.data(), P.kcbase.size(), &k.kcbase))) return s;
-    k.err = h->kerr;
-    *kp = k;
+    if (P.kin_ok && (s = upload_kinetic<R>(h, pl, kp))) return s;
+    if constexpr (sizeof(R) == 8) {   // banded FP64 tensor-core kinetic plan
+        h->b64 = he::BandPlan<double>{};
+        if (P.band_ok) {
+            he::BandPlan<double> b{};
+            b.n = h->n; b.nc = h->nc; b.ngroup = P.ngroup; b.ntr = P.bntr; b.nct = P.bnct;
+            b.box_r = P.bbox_r64; b.box_c = P.bbox_c;
+            const size_t bytes = (size_t)b.box_r * b.box_c * sizeof(double2);
+            b.stage_bytes = (int)((bytes + he::KIN_STAGE_ALIGN - 1) / he::KIN_STAGE_ALIGN * he::KIN_STAGE_ALIGN);
+            if ((s = upload(h, P.glo.data(), P.glo.size(), &b.glo))) return s;
+            if ((s = upload(h, P.gks.data(), P.gks.size(), &b.gks))) return s;
+            if ((s = upload(h, P.greal.data(), P.greal.size(), &b.greal))) return s;
+            if ((s = upload(h, P.brbase.data(), P.brbase.size(), &b.brbase))) return s;
+            if ((s = upload(h, P.bcbase.data(), P.bcbase.size(), &b.bcbase))) return s;
+            if ((s = upload_c<double>(h, P.gfrag.data(), P.gfrag.size() / 2, &b.frag))) return s;
+            if ((s = upload_c<double>(h, P.gfragb.data(), P.gfragb.size() / 2, &b.fragb))) return s;
+            b.err = h->kerr;
+            h->b64 = b;
+        }
+    }
     return HE_OK;
 }
 
@@ -195,7 +222,7 @@ he_operator::~he_operator()
 extern "C" int he_set_path(he_handle h, int tiled)
 {
     if (!h) return he_fail(HE_ERR_ARG, "null handle", __FILE__, __LINE__);
-    if (tiled < 0 || tiled > 2) return he_fail(HE_ERR_ARG, "path must be 0, 1 or 2", __FILE__, __LINE__);
+    if (tiled < 0 || tiled > 3) return he_fail(HE_ERR_ARG, "path must be 0, 1, 2 or 3", __FILE__, __LINE__);
     if (tiled && !h->tiled) return he_fail(HE_ERR_UNSUPPORTED, "tables do not admit the tiled kernels", __FILE__, __LINE__);
     h->path = tiled;
     return HE_OK;

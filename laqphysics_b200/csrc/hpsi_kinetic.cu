@@ -343,6 +343,186 @@ hpsi_kinetic_kernel(const __grid_constant__ CUtensorMap tmap, const DeviceTables
     }
 }
 
+// ---------------------------------------------------------------------------------
+// Banded kinetic kernel on the FP64 tensor cores (complex128).
+//
+// Output fragments C[j][i] (8 columns j x 8 rows i of one channel) collect both electrons:
+//   electron 1:  C[j][i] += sum_r S[r][j] T[i][r]     A = S^T (shared), B = row-group fragments
+//   electron 2:  C[j][i] += sum_r T[j][r] S[i][r]     A = column-group fragments, B = S (shared)
+// over the 4-node k-steps of each group's window; complex products take two (real T) or
+// four (complex T) mma.sync m8n8k4 f64 per k-step.  A CTA of 8 warps owns a 64 x 32
+// tile: warp w keeps the fragments of row group w in registers and all four column
+// groups' fragments come from shared memory (staged when the column tile changes).
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
+{
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+        : "+d"(d0), "+d"(d1)
+        : "d"(a), "d"(b));
+}
+
+// acc += A B for complex operands; B_real / A_real select the two-product form.
+__device__ __forceinline__ void cmma_ab(double (&cr)[2], double (&ci)[2], double2 a, double2 b, bool b_real)
+{
+    dmma(cr[0], cr[1], a.x, b.x);
+    dmma(ci[0], ci[1], a.y, b.x);
+    if (!b_real) {
+        dmma(cr[0], cr[1], -a.y, b.y);
+        dmma(ci[0], ci[1], a.x, b.y);
+    }
+}
+
+__device__ __forceinline__ void cmma_ba(double (&cr)[2], double (&ci)[2], double2 a, double2 b, bool a_real)
+{
+    dmma(cr[0], cr[1], a.x, b.x);
+    dmma(ci[0], ci[1], a.x, b.y);
+    if (!a_real) {
+        dmma(cr[0], cr[1], -a.y, b.y);
+        dmma(ci[0], ci[1], a.y, b.x);
+    }
+}
+
+// Electron 1 over the window of this warp's row group: block q covers columns j0 + (0..7).
+__device__ __forceinline__ void band_r1(const double2 *S, int P, int x0, int y0, int j0, int glo, int gks, bool real,
+                                        const double2 (&rf)[BAND_KS], int lr, int lk, double (&cr)[2], double (&ci)[2])
+{
+    const double2 *a = S + (j0 + lr - y0) * P + (glo + lk - x0);
+#pragma unroll
+    for (int s = 0; s < BAND_KS; ++s)
+        if (s < gks) cmma_ab(cr, ci, a[4 * s], rf[s], real);
+}
+
+// Electron 2 over the window of column group gc, fragments `cf` (k-step major, 32 lanes).
+__device__ __forceinline__ void band_r2(const double2 *S, int P, int x0, int y0, int i0, int glo, int gks, bool real,
+                                        const double2 *cf, int lane, int lr, int lk, double (&cr)[2], double (&ci)[2])
+{
+    const double2 *b = S + (glo + lk - y0) * P + (i0 + lr - x0);
+#pragma unroll
+    for (int s = 0; s < BAND_KS; ++s)
+        if (s < gks) cmma_ba(cr, ci, cf[s * 32 + lane], b[4 * s * P], real);
+}
+
+template <bool VEL, bool SEP>
+__global__ void __launch_bounds__(BAND_THREADS, 1)
+hpsi_band_kernel(const __grid_constant__ CUtensorMap tmap, const DeviceTables<double> t, const BandPlan<double> bp,
+                 double2 *__restrict__ out, double2 *__restrict__ w1, double2 *__restrict__ w2, double a2)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char *smem = smem_raw + ((KIN_STAGE_ALIGN - (smem_u32(smem_raw) & (KIN_STAGE_ALIGN - 1))) & (KIN_STAGE_ALIGN - 1));
+    double2 *CF = reinterpret_cast<double2 *>(smem + 2 * (size_t)bp.stage_bytes);   // [BAND_CG][BAND_KS][32]
+    uint64_t *bar = reinterpret_cast<uint64_t *>(CF + BAND_CG * BAND_KS * 32);
+    const int n = bp.n, nc = bp.nc, P = bp.box_r, G = bp.ngroup;
+    const size_t nn = (size_t)n * n;
+    const long long items = (long long)bp.ntr * bp.nct * nc;
+    const long long per = (items + gridDim.x - 1) / gridDim.x;
+    const long long first = (long long)blockIdx.x * per;
+    const long long last = first + per < items ? first + per : items;
+    if (first >= last) return;
+    const unsigned box_bytes = (unsigned)((size_t)P * bp.box_c * sizeof(double2));
+
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        mbar_init(bar + 1, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    auto issue = [&](long long it, int stage) {
+        const long long tile = it / nc;
+        const int c = (int)(it % nc), tr = (int)(tile / bp.nct), tc = (int)(tile % bp.nct);
+        mbar_expect_tx(bar + stage, box_bytes);
+        tma_load_3d(smem + (size_t)stage * bp.stage_bytes, &tmap, 2 * bp.brbase[tr], bp.bcbase[tc], c, bar + stage);
+    };
+    if (threadIdx.x == 0) issue(first, 0);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, lr = lane >> 2, lk = lane & 3;
+    int cur_tr = -1, cur_tc = -1;
+    double2 rf[BAND_KS];
+    int glo_r = 0, gks_r = 0;
+    bool real_r = true;
+    for (long long it = first; it < last; ++it) {
+        const int k = (int)(it - first), stage = k & 1;
+        const bool ok = mbar_wait_bounded(bar + stage, (unsigned)((k >> 1) & 1));
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) {
+                atomicExch(bp.err, 1);
+                mbar_wait_bounded(bar + stage, (unsigned)((k >> 1) & 1));
+            }
+            return;
+        }
+        if (threadIdx.x == 0 && it + 1 < last) issue(it + 1, stage ^ 1);
+        const long long tile = it / nc;
+        const int c = (int)(it % nc), tr = (int)(tile / bp.nct), tc = (int)(tile % bp.nct);
+        if (tc != cur_tc) {   // CTA-uniform: stage the column groups' fragments
+            for (int idx = threadIdx.x; idx < BAND_CG * BAND_KS * 32; idx += BAND_THREADS) {
+                const int g = tc * BAND_CG + idx / (BAND_KS * 32);
+                CF[idx] = g < G ? bp.frag[(size_t)g * BAND_KS * 32 + idx % (BAND_KS * 32)] : make_double2(0, 0);
+            }
+            cur_tc = tc;
+            __syncthreads();
+        }
+        const int gr = tr * BAND_WARPS + warp;
+        if (tr != cur_tr) {   // this warp's row-group fragments
+            cur_tr = tr;
+            if (gr < G) {
+#pragma unroll
+                for (int s = 0; s < BAND_KS; ++s) rf[s] = bp.frag[((size_t)gr * BAND_KS + s) * 32 + lane];
+                glo_r = bp.glo[gr]; gks_r = bp.gks[gr]; real_r = bp.greal[gr] & 1;
+            }
+        }
+        if (gr >= G) continue;
+        const double2 *S = reinterpret_cast<const double2 *>(smem + (size_t)stage * bp.stage_bytes);
+        const int x0 = bp.brbase[tr], y0 = bp.bcbase[tc], i0 = gr * BAND_G;
+        if (VEL) {   // commutator stencils W1 (electron 1), W2 (electron 2) with the B fragments
+            double2 bf[BAND_KS];
+#pragma unroll
+            for (int s = 0; s < BAND_KS; ++s) bf[s] = bp.fragb[((size_t)gr * BAND_KS + s) * 32 + lane];
+            const bool breal_r = (bp.greal[gr] & 2) != 0;
+#pragma unroll
+            for (int q = 0; q < BAND_CG; ++q) {
+                const int gc = tc * BAND_CG + q, j0 = gc * BAND_G;
+                if (gc >= G) break;
+                double cr[2] = {0, 0}, ci[2] = {0, 0};
+                band_r1(S, P, x0, y0, j0, glo_r, gks_r, breal_r, bf, lr, lk, cr, ci);
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const int i = i0 + 2 * lk + u, j = j0 + lr;
+                    if (i < n && j < n) w1[(size_t)i + (size_t)n * j + nn * c] = make_double2(cr[u], ci[u]);
+                }
+                double dr[2] = {0, 0}, di[2] = {0, 0};
+                band_r2(S, P, x0, y0, i0, bp.glo[gc], bp.gks[gc], (bp.greal[gc] & 2) != 0,
+                        bp.fragb + (size_t)gc * BAND_KS * 32, lane, lr, lk, dr, di);
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const int i = i0 + 2 * lk + u, j = j0 + lr;
+                    if (i < n && j < n) w2[(size_t)i + (size_t)n * j + nn * c] = make_double2(dr[u], di[u]);
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < BAND_CG; ++q) {
+            const int gc = tc * BAND_CG + q, j0 = gc * BAND_G;
+            if (gc >= G) break;
+            double cr[2] = {0, 0}, ci[2] = {0, 0};
+            band_r1(S, P, x0, y0, j0, glo_r, gks_r, real_r, rf, lr, lk, cr, ci);
+            band_r2(S, P, x0, y0, i0, bp.glo[gc], bp.gks[gc], (bp.greal[gc] & 1) != 0, CF + q * BAND_KS * 32, lane,
+                    lr, lk, cr, ci);
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const int i = i0 + 2 * lk + u, j = j0 + lr;
+                if (i < n && j < n) {
+                    const double2 x = S[(j - y0) * P + (i - x0)];
+                    const size_t p = (size_t)i + (size_t)n * j + nn * c;
+                    const double2 d = SEP ? cadd<double>(__ldg(t.d1 + i + (size_t)n * c), __ldg(t.d2 + j + (size_t)n * c))
+                                          : __ldg(t.diag + p);
+                    double2 v = cfma<double>(d, x, make_double2(cr[u], ci[u]));
+                    if (VEL) v = rfma<double>(a2, x, v);
+                    out[p] = v;
+                }
+            }
+        }
+    }
+}
+
 namespace {
 
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
@@ -407,6 +587,39 @@ int launch_kinetic(he_operator *h, const DeviceTables<R> &t, const KineticPlan<R
     if (velocity) { if (t.diag_separable) HE_KINETIC(true, true); else HE_KINETIC(true, false); }
     else { if (t.diag_separable) HE_KINETIC(false, true); else HE_KINETIC(false, false); }
 #undef HE_KINETIC
+    HE_CUDA_TRY(cudaGetLastError());
+    return HE_OK;
+}
+
+bool band_usable(const BandPlan<double> &bp, const void *psi)
+{
+    return bp.ntr > 0 && (reinterpret_cast<uintptr_t>(psi) & 15) == 0 && tensor_map_encoder() != nullptr;
+}
+
+int launch_band(he_operator *h, const DeviceTables<double> &t, const BandPlan<double> &bp, const double2 *psi,
+                double2 *out, double2 *w1, double2 *w2, double a2, int velocity, cudaStream_t stream)
+{
+    CUtensorMap map;
+    const cuuint64_t dims[3] = {2 * (cuuint64_t)bp.n, (cuuint64_t)bp.n, (cuuint64_t)bp.nc};
+    const cuuint64_t strides[2] = {2 * (cuuint64_t)bp.n * sizeof(double), 2 * (cuuint64_t)bp.n * bp.n * sizeof(double)};
+    const cuuint32_t box[3] = {2 * (cuuint32_t)bp.box_r, (cuuint32_t)bp.box_c, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    const CUresult r = tensor_map_encoder()(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double2 *>(psi), dims,
+                                            strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return he_fail(HE_ERR_CUDA, "cuTensorMapEncodeTiled failed", __FILE__, __LINE__);
+    const size_t smem = 2 * (size_t)bp.stage_bytes + (size_t)BAND_CG * BAND_KS * 32 * sizeof(double2) + 16 + KIN_STAGE_ALIGN;
+    const long long items = (long long)bp.ntr * bp.nct * bp.nc;
+    const unsigned grid = (unsigned)std::min<long long>(items, (long long)sm_count(h->device));
+#define HE_BAND(V, S)                                                                                      \
+    do {                                                                                                   \
+        auto kern = hpsi_band_kernel<V, S>;                                                                \
+        HE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));   \
+        kern<<<grid, BAND_THREADS, smem, stream>>>(map, t, bp, out, w1, w2, a2);                           \
+    } while (0)
+    if (velocity) { if (t.diag_separable) HE_BAND(true, true); else HE_BAND(true, false); }
+    else { if (t.diag_separable) HE_BAND(false, true); else HE_BAND(false, false); }
+#undef HE_BAND
     HE_CUDA_TRY(cudaGetLastError());
     return HE_OK;
 }

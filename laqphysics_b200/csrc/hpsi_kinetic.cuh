@@ -21,6 +21,28 @@ constexpr int KIN_STAGE_ALIGN = 128;             // byte alignment of each stage
 constexpr int KIN_BRCOLS = KIN_SLOTS * KIN_NA;   // owned columns of a column tile, at most
 constexpr int KIN_BRIDGE_BYTES = KIN_RELEMS * KIN_BRCOLS * 16;   // bridge-row partials (complex128)
 
+// Banded formulation on the FP64 tensor cores (mma.sync m8n8k4 f64).  Rows of the
+// kinetic matrix are taken in groups of 8; group g couples to the window of nodes
+// [glo[g], glo[g] + 4 gks[g]) and its fragment table holds, for k-step s and lane l,
+// T[8g + l/4][glo[g] + 4s + l%4] -- the A operand of one direction and the B operand of
+// the other, so both electrons accumulate into the same 8x8 output fragments.
+constexpr int BAND_G = 8;                        // rows per group (mma M = N = 8)
+constexpr int BAND_KS = 8;                       // k-steps per window, at most (window <= 32 nodes)
+constexpr int BAND_TR = 64;                      // rows per tile: 8 warps x one row group
+constexpr int BAND_TC = 32;                      // columns per tile: 4 column groups
+constexpr int BAND_WARPS = BAND_TR / BAND_G;
+constexpr int BAND_THREADS = 32 * BAND_WARPS;
+constexpr int BAND_CG = BAND_TC / BAND_G;
+
+template <typename R> struct BandPlan {
+    int n, nc, ngroup, ntr, nct, box_r, box_c;
+    int stage_bytes;
+    const int *glo, *gks, *greal;                // per group
+    const int *brbase, *bcbase;                  // per tile
+    const cplx<R> *frag, *fragb;                 // [group][BAND_KS][32]
+    int *err;
+};
+
 template <typename R> struct KineticPlan {
     int n, nc, ne, ntr, nct, box_r, box_c;
     int stage_bytes;                             // box bytes, rounded up to KIN_STAGE_ALIGN

@@ -541,7 +541,14 @@ int launch_hpsi_tiled(he_operator *h, const DeviceTables<R> &t, const TiledPlan<
     const R f0 = (R)field[0], f1 = (R)field[1], f2 = (R)field[2];
     const R a2 = (R)(field[0] * field[0] + field[1] * field[1] + field[2] * field[2]);
     const KineticPlan<R> &kp = kinetic_plan<R>(h);
-    if (h->path == 1 && kinetic_usable<R>(kp, psi)) {
+    bool band = false;
+    if constexpr (sizeof(R) == 8) band = h->path == 1 && band_usable(h->b64, psi);
+    if (band) {
+        if constexpr (sizeof(R) == 8) {
+            const int s = launch_band(h, t, h->b64, psi, out, w1, w2, a2, velocity, stream);
+            if (s) return s;
+        }
+    } else if ((h->path == 1 || h->path == 3) && kinetic_usable<R>(kp, psi)) {
         const int s = launch_kinetic<R>(h, t, kp, psi, out, w1, w2, a2, velocity, stream);
         if (s) return s;
     } else {

@@ -43,6 +43,12 @@ struct he_plan_host {
     std::vector<double> blocks, bblocks, wcoef;   // complex as interleaved doubles for blocks
     int ne = 0, ntile = 0, ng = 0, nlam = 0, maxm = 0;
     int blkmax = 0;   // max over tiles and axes of staged block entries (previous row + sum m^2)
+    // banded kinetic kernel (FP64 tensor cores, hpsi_kinetic.cu)
+    bool band_ok = false;
+    int ngroup = 0, bks = 0, bntr = 0, bnct = 0, bbox_r64 = 0, bbox_r32 = 0, bbox_c = 0;
+    std::vector<int> glo, gks, greal;       // per 8-row group: window start, k-steps, T and B real
+    std::vector<int> brbase, bcbase;        // per row / column tile: first staged row / column
+    std::vector<double> gfrag, gfragb;      // [group][k-step][lane] complex T / B fragments
     // kinetic kernel (TMA-staged tiles, hpsi_kinetic.cu)
     bool kin_ok = false;
     std::vector<int> nodeelem;              // n: element owning each node (a bridge node belongs to the later element)

@@ -19,6 +19,7 @@ struct he_operator {
     he::TiledPlan<float> p32{};
     he::KineticPlan<double> k64{};      // kinetic-kernel plan (ntr == 0: not usable)
     he::KineticPlan<float> k32{};
+    he::BandPlan<double> b64{};         // banded FP64 tensor-core kinetic plan (ntr == 0: not usable)
     int *kerr = nullptr;                // device error word of the kinetic kernel
     double2 *coef64 = nullptr;          // field-contracted dipole coefficients (nd)
     float2 *coef32 = nullptr;
@@ -46,6 +47,9 @@ template <typename R> bool kinetic_usable(const KineticPlan<R> &kp, const void *
 template <typename R>
 int launch_kinetic(he_operator *h, const DeviceTables<R> &t, const KineticPlan<R> &kp, const cplx<R> *psi,
                    cplx<R> *out, cplx<R> *w1, cplx<R> *w2, R a2, int velocity, cudaStream_t stream);
+bool band_usable(const BandPlan<double> &bp, const void *psi);
+int launch_band(he_operator *h, const DeviceTables<double> &t, const BandPlan<double> &bp, const double2 *psi,
+                double2 *out, double2 *w1, double2 *w2, double a2, int velocity, cudaStream_t stream);
 template <typename R> inline const KineticPlan<R> &kinetic_plan(const he_operator *h);
 template <> inline const KineticPlan<double> &kinetic_plan<double>(const he_operator *h) { return h->k64; }
 template <> inline const KineticPlan<float> &kinetic_plan<float>(const he_operator *h) { return h->k32; }

@@ -109,6 +109,78 @@ void build_kinetic(he_plan_host &P, int n)
                2 * stage + KIN_BRIDGE_BYTES + 64 <= 200 * 1024;
 }
 
+// Banded kinetic kernel (hpsi_kinetic.cu): the window and FP64-mma fragments of every
+// 8-row group, straight from the CSR (any banded kinetic matrix; no element structure is
+// needed), and the staged box of every 64 x 32 tile.  Leaves band_ok false when a window
+// exceeds BAND_KS k-steps or the box exceeds the TMA / shared-memory limits.
+void build_band(he_plan_host &P, int n, const int *ptr, const int *col, const double *tv, const double *r)
+{
+    using namespace he;
+    P.band_ok = false;
+    const int G = (n + BAND_G - 1) / BAND_G;
+    P.ngroup = G;
+    P.glo.assign(G, 0); P.gks.assign(G, 0); P.greal.assign(G, 3);
+    P.gfrag.assign((size_t)G * BAND_KS * 32 * 2, 0.0);
+    P.gfragb.assign((size_t)G * BAND_KS * 32 * 2, 0.0);
+    for (int g = 0; g < G; ++g) {
+        int lo = n, hi = -1;
+        for (int i = BAND_G * g; i < std::min(n, BAND_G * (g + 1)); ++i)
+            for (int k = ptr[i]; k < ptr[i + 1]; ++k) { lo = std::min(lo, col[k]); hi = std::max(hi, col[k]); }
+        if (hi < 0) { lo = std::min(BAND_G * g, n - 1); hi = lo; }
+        const int ks = (hi - lo + 4) / 4;
+        if (ks > BAND_KS) return;
+        P.glo[g] = lo; P.gks[g] = ks;
+        for (int i = BAND_G * g; i < std::min(n, BAND_G * (g + 1)); ++i)
+            for (int k = ptr[i]; k < ptr[i + 1]; ++k) {
+                const int c = col[k], step = (c - lo) / 4, lane = (i - BAND_G * g) * 4 + (c - lo) % 4;
+                const size_t idx = 2 * (((size_t)g * BAND_KS + step) * 32 + lane);
+                const std::complex<double> T(tv[2 * k], tv[2 * k + 1]);
+                const std::complex<double> B = T * (std::complex<double>(r[2 * c], r[2 * c + 1]) -
+                                                    std::complex<double>(r[2 * i], r[2 * i + 1]));
+                P.gfrag[idx] += T.real(); P.gfrag[idx + 1] += T.imag();
+                P.gfragb[idx] += B.real(); P.gfragb[idx + 1] += B.imag();
+            }
+    }
+    for (int g = 0; g < G; ++g)
+        for (size_t q = 0; q < (size_t)BAND_KS * 32; ++q) {
+            const size_t idx = 2 * ((size_t)g * BAND_KS * 32 + q);
+            if (P.gfrag[idx + 1] != 0.0) P.greal[g] &= ~1;
+            if (P.gfragb[idx + 1] != 0.0) P.greal[g] &= ~2;
+        }
+    // tiles: the staged box spans the windows of the tile's groups and the tile itself
+    auto span = [&](int first_group, int groups, int extent, int start, int &lo, int &hi) {
+        lo = start; hi = start + extent - 1;
+        for (int g = first_group; g < std::min(G, first_group + groups); ++g) {
+            lo = std::min(lo, P.glo[g]);
+            hi = std::max(hi, P.glo[g] + 4 * P.gks[g] - 1);
+        }
+    };
+    P.bntr = (n + BAND_TR - 1) / BAND_TR;
+    P.bnct = (n + BAND_TC - 1) / BAND_TC;
+    P.brbase.clear(); P.bcbase.clear();
+    P.bbox_r64 = P.bbox_r32 = P.bbox_c = 0;
+    for (int t = 0; t < P.bntr; ++t) {
+        int lo, hi;
+        span(t * BAND_WARPS, BAND_WARPS, BAND_TR, t * BAND_TR, lo, hi);
+        P.brbase.push_back(lo);
+        P.bbox_r64 = std::max(P.bbox_r64, hi - lo + 1);
+        P.bbox_r32 = std::max(P.bbox_r32, hi - (lo & ~1) + 1);
+    }
+    for (int t = 0; t < P.bnct; ++t) {
+        int lo, hi;
+        span(t * BAND_CG, BAND_CG, BAND_TC, t * BAND_TC, lo, hi);
+        P.bcbase.push_back(lo);
+        P.bbox_c = std::max(P.bbox_c, hi - lo + 1);
+    }
+    // row pitch = 4 (mod 8) in nodes: the operand loads of one 8-lane phase hit distinct banks
+    auto pad = [](int v) { return v + ((12 - v % 8) % 8); };
+    P.bbox_r64 = pad(P.bbox_r64);
+    P.bbox_r32 = pad(P.bbox_r32);
+    const size_t stage = ((size_t)P.bbox_r64 * P.bbox_c * 16 + KIN_STAGE_ALIGN - 1) / KIN_STAGE_ALIGN * KIN_STAGE_ALIGN;
+    const size_t cfrag = (size_t)BAND_CG * BAND_KS * 32 * 16;
+    P.band_ok = 2 * P.bbox_r64 <= 256 && P.bbox_c <= 256 && 2 * stage + cfrag + 64 + KIN_STAGE_ALIGN <= 220 * 1024;
+}
+
 }  // namespace
 
 // Build the tiled plan from the reference's tables.  Returns false (and the generic
@@ -258,6 +330,7 @@ bool he_build_plan(he_plan_host &P, int n, int nc, const int *ptr, const int *co
     }
     (void)nd;
     build_kinetic(P, n);
+    build_band(P, n, ptr, col, tv, r);
     P.ok = true;
     return true;
 }
@@ -278,7 +351,9 @@ extern "C" void *he_plan_build(int n, int nc, const int *ptr, const int *col, co
 extern "C" void he_plan_free(void *plan) { delete static_cast<he_plan_host *>(plan); }
 
 // which: 0 estart, 1 tstart, 2 eoff, 3 ereal, 4 gch, 5 wptr, 6 wsrc, 7 dwptr, 8 dwsrc, 9 dwel, 10 dwedge,
-//        11 nodeelem, 12 krow, 13 krbase, 14 krcplx, 15 kslot, 16 kcbase, 17 koff,
+//        11 nodeelem, 12 krow, 13 krbase, 14 krcplx, 15 kslot, 16 kcbase, 17 koff, 18 glo, 19 gks,
+//        27 gfrag, 28 gfragb (complex [group][k-step][lane]), 29 greal (bit 0 T, bit 1 B real),
+//        32 brbase, 33 bcbase, 34 band scalars {band_ok, ngroup, ntr, nct, box_r64, box_r32, box_c},
 //        20 blocks (interleaved complex), 21 bblocks, 22 wcoef, 23 tre, 24 tim, 25 bre, 26 bim,
 //        30 scalars {ok, ne, ntile, ng, nlam, maxm, blkmax},
 //        31 kinetic scalars {kin_ok, ntr, nct, box_r (complex128), box_r (complex64), box_c}.
@@ -314,6 +389,18 @@ extern "C" long long he_plan_array(void *plan, int which, void *dst)
     case 24: vd = &P.tim; break;
     case 25: vd = &P.bre; break;
     case 26: vd = &P.bim; break;
+    case 18: vi = &P.glo; break;
+    case 19: vi = &P.gks; break;
+    case 27: vd = &P.gfrag; break;
+    case 28: vd = &P.gfragb; break;
+    case 29: vi = &P.greal; break;
+    case 32: vi = &P.brbase; break;
+    case 33: vi = &P.bcbase; break;
+    case 34: {
+        const int s[7] = {P.band_ok, P.ngroup, P.bntr, P.bnct, P.bbox_r64, P.bbox_r32, P.bbox_c};
+        if (dst) memcpy(dst, s, sizeof(s));
+        return 7;
+    }
     case 31: {
         const int s[6] = {P.kin_ok, P.ntr, P.nct, P.kbox_r64, P.kbox_r32, P.kbox_c};
         if (dst) memcpy(dst, s, sizeof(s));

@@ -89,16 +89,18 @@ def test_tiled_and_generic_kernels_agree(velocity):
 
 @pytest.mark.parametrize('velocity', [False, True])
 def test_kinetic_tma_and_shared_memory_radial_kernels_agree(velocity):
-    """Path 1 (TMA-staged kinetic kernel) against path 2 (shared-memory radial kernel)
-    and path 0 (generic kernel) in both precisions, on a grid whose exterior tail is
-    split over column slots."""
+    """Path 1 (banded FP64 tensor-core kinetic kernel for complex128, TMA-staged FMA
+    kinetic kernel for complex64), path 3 (TMA-staged FMA kinetic kernel), path 2
+    (shared-memory radial kernel) and path 0 (generic kernel) in both precisions, on a
+    grid whose exterior tail is split over column slots and whose last row group is
+    ragged."""
     h = _coupled(np.linspace(0, 24, 7), 6, .3, 24, 2, 1, cut=(12., 15.))
     op = engine(h)
     rng = np.random.default_rng(23)
     x = op.state(rng.normal(size=h.size) + 1j * rng.normal(size=h.size))
     f = (0., 0., .15)
     results = {}
-    for path in (1, 2, 0):
+    for path in (1, 3, 2, 0):
         op.set_path(path)
         results[path] = (op.host(op.apply(x, f, velocity)),
                          op.host(op.apply(x.to(torch.complex64), f, velocity, precision='complex64')))

@@ -215,3 +215,154 @@ def test_microbenchmark_kinetic_tiles():
     stage = -(-K['box_r64'] * K['box_c'] * 16 // 128) * 128
     bridge = KIN_RELEMS * KIN_SLOTS * KIN_NA * 16
     assert 2 * (2 * stage + bridge + 16 + 128 + 1024) <= 228 * 1024, (K['box_r64'], K['box_c'])
+
+
+# --------------------------------------------------------------------------------------
+# Banded FP64 tensor-core kernel (hpsi_band_kernel)
+# --------------------------------------------------------------------------------------
+BAND_G, BAND_KS, BAND_TR, BAND_TC = 8, 8, 64, 32
+
+
+def band_plan(h):
+    from laqphysics_b200 import _lib
+    from laqphysics_b200.engine import _host_tables
+    t = _host_tables(h)
+    p = _lib.ptr
+    handle = _lib.LIB.he_plan_build(h.n, h.nc, p(t['ptr']), p(t['col']), p(t['tv']), len(t['vc']), p(t['vptr']),
+                                    p(t['vc']), p(t['vl']), p(t['vcoef']), t['nlam'], len(t['dc']), p(t['dptr']),
+                                    p(t['dc']), p(t['de']), p(t['r']))
+    try:
+        def get(which, dtype):
+            count = _lib.LIB.he_plan_array(handle, which, None)
+            out = np.zeros(count, dtype)
+            _lib.LIB.he_plan_array(handle, which, ct.c_void_p(out.ctypes.data))
+            return out
+        s = get(34, np.int32)
+        B = dict(zip(('ok', 'ngroup', 'ntr', 'nct', 'box_r', 'box_r32', 'box_c'), (int(v) for v in s)))
+        for which, name in ((18, 'glo'), (19, 'gks'), (29, 'greal'), (32, 'brbase'), (33, 'bcbase')):
+            B[name] = get(which, np.int32)
+        for which, name in ((27, 'frag'), (28, 'fragb')):
+            B[name] = get(which, np.float64).view(np.complex128).reshape(-1, BAND_KS, 32)
+        return B
+    finally:
+        _lib.LIB.he_plan_free(handle)
+
+
+def emulate_band(h, x, B, velocity, a2=0.0, channels=None):
+    """hpsi_band_kernel item by item: mma fragments formed lane by lane from the staged box
+    (every index asserted inside it), C[j][i] accumulated as 8x4 @ 4x8 products."""
+    n, nc = h.n, h.nc
+    G, P, BC = B['ngroup'], B['box_r'], B['box_c']
+    assert P % 8 == 4 and 2 * P <= 256 and BC <= 256
+    psi = np.asarray(x).reshape((n, n, nc), order='F')
+    diag = np.asarray(h.diag).reshape((n, n, nc), order='F')
+    chans = range(nc) if channels is None else channels
+    out = {c: np.full((n, n), np.nan, complex) for c in chans}
+    W = [{c: np.full((n, n), np.nan, complex) for c in chans} for _ in range(2)]
+    lanes = np.arange(32)
+    lr, lk = lanes >> 2, lanes & 3
+    for tr in range(B['ntr']):
+        x0 = B['brbase'][tr]
+        for tc in range(B['nct']):
+            y0 = B['bcbase'][tc]
+            for c in chans:
+                box = np.zeros((P, BC), complex)        # box[row - x0, col - y0], zero fill past the grid
+                rr, cc = np.arange(P) + x0, np.arange(BC) + y0
+                box[np.ix_(rr < n, cc < n)] = psi[np.ix_(rr[rr < n], cc[cc < n], [c])][:, :, 0]
+
+                def S(rows, cols):
+                    rows, cols = np.asarray(rows), np.asarray(cols)
+                    assert (rows >= x0).all() and (rows < x0 + P).all() and (cols >= y0).all() and (cols < y0 + BC).all()
+                    return box[rows - x0, cols - y0]
+
+                for w in range(BAND_TR // BAND_G):
+                    gr = tr * (BAND_TR // BAND_G) + w
+                    if gr >= G:
+                        continue
+                    i0 = gr * BAND_G
+                    for q in range(BAND_TC // BAND_G):
+                        gc = tc * (BAND_TC // BAND_G) + q
+                        if gc >= G:
+                            break
+                        j0 = gc * BAND_G
+
+                        def r1(frag):
+                            C = np.zeros((8, 8), complex)
+                            for s in range(B['gks'][gr]):
+                                a = np.zeros((8, 4), complex)
+                                b = np.zeros((4, 8), complex)
+                                a[lr, lk] = S(B['glo'][gr] + 4 * s + lk, j0 + lr)   # A[m][k] = S[r][j0+m]
+                                b[lk, lr] = frag[gr, s, lanes]                        # B[k][n] = T[i0+n][r]
+                                C += a @ b
+                            return C
+
+                        def r2(frag):
+                            C = np.zeros((8, 8), complex)
+                            for s in range(B['gks'][gc]):
+                                a = np.zeros((8, 4), complex)
+                                b = np.zeros((4, 8), complex)
+                                a[lr, lk] = frag[gc, s, lanes]                        # A[m][k] = T[j0+m][r']
+                                b[lk, lr] = S(i0 + lr, B['glo'][gc] + 4 * s + lk)    # B[k][n] = S[i0+n][r']
+                                C += a @ b
+                            return C
+
+                        def put(dst, C):
+                            for m in range(8):
+                                for nn_ in range(8):
+                                    i, j = i0 + nn_, j0 + m
+                                    if i < n and j < n:
+                                        dst[i, j] = C[m, nn_]
+
+                        if velocity:
+                            put(W[0][c], r1(B['fragb']))
+                            put(W[1][c], r2(B['fragb']))
+                        C = r1(B['frag']) + r2(B['frag'])
+                        for m in range(8):
+                            for nn_ in range(8):
+                                i, j = i0 + nn_, j0 + m
+                                if i < n and j < n:
+                                    xv = S(i, j)
+                                    out[c][i, j] = C[m, nn_] + diag[i, j, c] * xv + (a2 * xv if velocity else 0)
+    return out, W
+
+
+@pytest.mark.parametrize('case', ['apply_ecs', 'apply_cut', 'apply_coupled'])
+def test_band_plan_reproduces_the_stencils(case):
+    g = golden(case)
+    h = Tables(g)
+    B = band_plan(h)
+    assert B['ok']
+    x = np.asarray(g['x'])
+    chans = sorted({0, h.nc - 1})
+    out, W = emulate_band(h, x, B, True, a2=0.3, channels=chans)
+    ref, Wref = reference_kinetic(h, x, True, a2=0.3)
+    for c in chans:
+        np.testing.assert_allclose(out[c], ref[:, :, c], rtol=1e-12, atol=1e-11)
+        np.testing.assert_allclose(W[0][c], Wref[0][:, :, c], rtol=1e-12, atol=1e-11)
+        np.testing.assert_allclose(W[1][c], Wref[1][:, :, c], rtol=1e-12, atol=1e-11)
+
+
+def test_band_plan_with_tail_and_ragged_group():
+    from laqphysics_b200.workloads import coupled, seeded_state
+    # n = 6*6 + 24 + 1 - 1 is not a multiple of 8: the last row group is ragged
+    h = coupled(np.linspace(0, 24, 7), 6, 1, 1, ecs_angle=.3, tail=24, cutoff_radii=(12., 15.))
+    B = band_plan(h)
+    assert B['ok'] and h.n % 8 != 0
+    x = seeded_state(h.size, 9)
+    out, W = emulate_band(h, x, B, True, a2=0.05, channels=[0, h.nc - 1])
+    ref, Wref = reference_kinetic(h, x, True, a2=0.05)
+    for c in (0, h.nc - 1):
+        np.testing.assert_allclose(out[c], ref[:, :, c], rtol=1e-12, atol=1e-11)
+        np.testing.assert_allclose(W[0][c], Wref[0][:, :, c], rtol=1e-12, atol=1e-11)
+        np.testing.assert_allclose(W[1][c], Wref[1][:, :, c], rtol=1e-12, atol=1e-11)
+
+
+def test_microbenchmark_band_tiles():
+    from laqphysics_b200.workloads import hpsi_microbench
+    h = hpsi_microbench()
+    B = band_plan(h)
+    assert B['ok'] and B['ngroup'] == 70 and B['ntr'] == 9 and B['nct'] == 18
+    assert B['gks'].max() <= BAND_KS
+    stage = -(-B['box_r'] * B['box_c'] * 16 // 128) * 128
+    smem = 2 * stage + 4 * BAND_KS * 32 * 16 + 16 + 128
+    assert smem + 1024 <= 228 * 1024, (B['box_r'], B['box_c'], smem)
