@@ -334,8 +334,7 @@ def main():
         'gpu_launches': launches,
         'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': hbm, 'unit': 'GB/s', 'frac': achieved / hbm,
                      'traffic': profile_traffic('hpsi_c128_microbench'), 'peak_kind': peak_kind,
-                     'kernel': ('contract_field + hpsi_radial_kernel + hpsi_mix_kernel (one apply)'
-                                if engine.tiled else 'hpsi_gather_kernel'),
+                     'kernel': ' + '.join(engine.kernels()) + ' (one apply)',
                      'plan': engine.plan_info,
                      'fp64_tflops': flops / (per128 * 1e-3) / 1e12, 'flops_per_apply': flops},
         'complex64': {'value': value64, 'unit': 'GB/s', 'ms_per_step': per64,

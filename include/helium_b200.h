@@ -227,6 +227,22 @@ int he_vec_norms_noalloc(long long n, int count, const void *x, long long ld, do
  * ---------------------------------------------------------------------------------- */
 int he_set_path(he_handle h, int tiled);
 int he_device_status(he_handle h);
+
+/* ------------------------------------------------------------------------------------
+ * Channel mixing: he_set_mix(h, 1) (default) uses the kernel generated for the handle's
+ * coupling structure (every Coulomb and dipole edge unrolled, NVRTC-compiled for sm_100a
+ * on the first tiled apply and cached by source); 0 uses the table-driven kernel.
+ * he_mix_status: 0 not compiled yet, 1 generated kernel in use, -1 it failed to compile
+ * (the table-driven kernel runs instead; he_last_error has the log).
+ * he_plan_mix_source / he_plan_mix_program / he_nvrtc_check: the generated source and the
+ * mixing program (JSON) of a planner handle, and an NVRTC compile check for sm_100a
+ * (host only).
+ * ---------------------------------------------------------------------------------- */
+int he_set_mix(he_handle h, int generated);
+int he_mix_status(he_handle h);
+long long he_plan_mix_source(void *plan, int dipole_real, char *buf, long long cap);
+long long he_plan_mix_program(void *plan, char *buf, long long cap);
+int he_nvrtc_check(const char *src, char *log, long long cap);
 void *he_plan_build(int n, int nc, const int *ptr, const int *col, const double *tv, int nv, const int *vptr,
                     const int *vc, const int *vl, const double *vcoef, int nlam, int nd, const int *dptr,
                     const int *dc, const int *de, const double *r);

@@ -44,6 +44,11 @@ SIGNATURES = {
     'he_expv_mixed': (I, [P, P, P, P, P, I, D, D, I, ct.POINTER(I), ct.POINTER(D), P]),
     'he_set_path': (I, [P, I]),
     'he_device_status': (I, [P]),
+    'he_set_mix': (I, [P, I]),
+    'he_mix_status': (I, [P]),
+    'he_plan_mix_source': (ct.c_longlong, [P, I, ct.c_char_p, ct.c_longlong]),
+    'he_nvrtc_check': (I, [ct.c_char_p, ct.c_char_p, ct.c_longlong]),
+    'he_plan_mix_program': (ct.c_longlong, [P, ct.c_char_p, ct.c_longlong]),
     'he_vec_axpby': (I, [ct.c_longlong, D, D, P, D, D, P, P, P]),
     'he_vec_residual_norm': (I, [ct.c_longlong, P, P, P, ct.POINTER(D), P]),
     'he_vec_jacobi': (I, [ct.c_longlong, P, D, D, D, P, P, P]),

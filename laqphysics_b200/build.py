@@ -49,7 +49,7 @@ def build(force=False, verbose=False):
         return LIBRARY
     LIBDIR.mkdir(exist_ok=True)
     tmp = LIBRARY.with_suffix('.so.tmp')
-    cmd = [nvcc(), *ARCH, *FLAGS, f'-I{INCLUDE}', *map(str, sources()), '-o', str(tmp), '-lcublas']
+    cmd = [nvcc(), *ARCH, *FLAGS, f'-I{INCLUDE}', *map(str, sources()), '-o', str(tmp), '-lcublas', '-lnvrtc']
     if verbose:
         cmd.insert(1, '-Xptxas=-v')
     result = subprocess.run(cmd, capture_output=True, text=True)

@@ -228,6 +228,25 @@ extern "C" int he_set_path(he_handle h, int tiled)
     return HE_OK;
 }
 
+extern "C" int he_set_mix(he_handle h, int generated)
+{
+    if (!h) return he_fail(HE_ERR_ARG, "null handle", __FILE__, __LINE__);
+    if (generated != 0 && generated != 1) return he_fail(HE_ERR_ARG, "mix mode must be 0 or 1", __FILE__, __LINE__);
+    h->mixpath = generated;
+    return HE_OK;
+}
+
+extern "C" int he_mix_status(he_handle h)
+{
+    if (!h) return he_fail(HE_ERR_ARG, "null handle", __FILE__, __LINE__);
+    int any = 0;
+    for (int v = 0; v < 4; ++v) {
+        if (h->mix_state[v] < 0) return -1;
+        if (h->mix_state[v] > 0) any = 1;
+    }
+    return any;
+}
+
 extern "C" int he_device_status(he_handle h)
 {
     if (!h) return he_fail(HE_ERR_ARG, "null handle", __FILE__, __LINE__);
@@ -295,6 +314,9 @@ extern "C" int he_create(he_handle *out, int n, int nc, int nt, const int *ptr, 
         s = upload_plan<double>(h, &h->p64, &h->coef64);
         if (!s && h->has32) s = upload_plan<float>(h, &h->p32, &h->coef32);
         h->tiled = !s;
+        bool dipole_real = true;
+        for (long long k = 0; k < 3LL * nd; ++k) dipole_real = dipole_real && dcoef[2 * k + 1] == 0.0;
+        h->mix_src = he::mix_source(h->plan, dipole_real, -2);
     }
     if (s) { delete h; g_status = s; return s; }
     *out = h;
@@ -312,7 +334,8 @@ extern "C" int he_info(he_handle h, long long *values, int count)
     if (!h || !values) return he_fail(HE_ERR_ARG, "null argument", __FILE__, __LINE__);
     const long long all[] = {h->n, h->nc, h->nt, h->nv, h->nd, h->nlam, h->separable, h->has32, h->device,
                              h->tiled, h->path, h->plan.ne, h->plan.ntile, h->plan.ng,
-                             (long long)h->plan.wsrc.size(), (long long)h->plan.dwsrc.size()};
+                             (long long)h->plan.wsrc.size(), (long long)h->plan.dwsrc.size(),
+                             h->b64.ntr > 0, h->k64.ntr > 0};
     for (int k = 0; k < count && k < (int)(sizeof(all) / sizeof(all[0])); ++k) values[k] = all[k];
     return HE_OK;
 }

@@ -566,6 +566,8 @@ int launch_hpsi_tiled(he_operator *h, const DeviceTables<R> &t, const TiledPlan<
 #undef HE_RADIAL
         HE_CUDA_TRY(cudaGetLastError());
     }
+    if (h->mixpath == 1 && jit_mix_prepare(h, (sizeof(R) == 8 ? 0 : 2) + (velocity ? 1 : 0)) == HE_OK)
+        return launch_mix_jit<R>(h, t, psi, out, w1, w2, field, velocity, beta, gamma, stream);
     const size_t nn = (size_t)pl.n * pl.n;
     const size_t ms = mix_smem<R>(pl.nc, pl.nlam, pl.ng, pl.nwide, pl.nwd);
     const size_t ntiles = (nn + MIX_NP - 1) / MIX_NP;

@@ -36,6 +36,24 @@ template <typename R> struct TiledPlan {
 
 }  // namespace he
 
+// Channel-mixing program of the generated kernel (jit_mix.cu): output groups (channels
+// that share Coulomb sources), each with blocks of multipole terms whose sources are
+// loaded once, and the dipole edges per electron.
+struct MixTerm {
+    int lam = 0;
+    std::vector<int> d, s;          // edges: output index in the group, source index in the block
+    std::vector<double> w;          // real Coulomb coefficient
+};
+struct MixBlock {
+    std::vector<int> src;           // source channels loaded for the block
+    std::vector<MixTerm> terms;
+};
+struct MixGroup {
+    std::vector<int> out;           // output channels
+    std::vector<MixBlock> blocks;
+    std::vector<int> dd[2], ds[2], dk[2];   // dipole edges per electron: output index, source channel, edge index
+};
+
 // Host-owned plan (built by he_create when the tables admit it).
 struct he_plan_host {
     bool ok = false;
@@ -43,6 +61,8 @@ struct he_plan_host {
     std::vector<double> blocks, bblocks, wcoef;   // complex as interleaved doubles for blocks
     int ne = 0, ntile = 0, ng = 0, nlam = 0, maxm = 0;
     int blkmax = 0;   // max over tiles and axes of staged block entries (previous row + sum m^2)
+    // generated channel-mixing program
+    std::vector<MixGroup> mix;
     // banded kinetic kernel (FP64 tensor cores, hpsi_kinetic.cu)
     bool band_ok = false;
     int ngroup = 0, bks = 0, bntr = 0, bnct = 0, bbox_r64 = 0, bbox_r32 = 0, bbox_c = 0;

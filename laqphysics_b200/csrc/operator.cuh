@@ -1,5 +1,6 @@
 // Host-side state behind an he_handle.
 #pragma once
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -27,6 +28,10 @@ struct he_operator {
     float2 *w32[2] = {nullptr, nullptr};
     const double2 *tdiag = nullptr;     // diagonal of the kinetic CSR (n entries)
     he_plan_host plan;
+    int mixpath = 1;                    // 1: generated (NVRTC) mixing kernel when it compiles, 0: table-driven kernel
+    std::string mix_src;                // source of the generated mixing kernel (without entry points)
+    int mix_state[4] = {0, 0, 0, 0};    // per variant: 0 not compiled yet, 1 ready, -1 failed (table-driven)
+    void *mix_kern[4] = {nullptr, nullptr, nullptr, nullptr};   // compiled kernels (cudaKernel_t)
     std::vector<void *> allocations;    // every cudaMalloc made for this handle
     ~he_operator();
 };
@@ -47,6 +52,12 @@ template <typename R> bool kinetic_usable(const KineticPlan<R> &kp, const void *
 template <typename R>
 int launch_kinetic(he_operator *h, const DeviceTables<R> &t, const KineticPlan<R> &kp, const cplx<R> *psi,
                    cplx<R> *out, cplx<R> *w1, cplx<R> *w2, R a2, int velocity, cudaStream_t stream);
+std::string mix_source(const he_plan_host &P, bool dipole_real, int variant);
+int jit_mix_prepare(he_operator *h, int variant);
+template <typename R>
+int launch_mix_jit(he_operator *h, const DeviceTables<R> &t, const cplx<R> *psi, cplx<R> *out, const cplx<R> *w1,
+                   const cplx<R> *w2, const double *field, int velocity, cplx<R> beta, cplx<R> gamma,
+                   cudaStream_t stream);
 bool band_usable(const BandPlan<double> &bp, const void *psi);
 int launch_band(he_operator *h, const DeviceTables<double> &t, const BandPlan<double> &bp, const double2 *psi,
                 double2 *out, double2 *w1, double2 *w2, double a2, int velocity, cudaStream_t stream);

@@ -181,6 +181,64 @@ void build_band(he_plan_host &P, int n, const int *ptr, const int *col, const do
     P.band_ok = 2 * P.bbox_r64 <= 256 && P.bbox_c <= 256 && 2 * stage + cfrag + 64 + KIN_STAGE_ALIGN <= 220 * 1024;
 }
 
+// Program of the generated channel-mixing kernel.  Each class of channels that share
+// Coulomb sources is cut into groups of at most MIXJ_OUT outputs; a group's multipoles are
+// ordered by their smallest source and packed into blocks whose sources (at most
+// MIXJ_SRC) are loaded once.  In the coupled basis this puts the even multipoles (sources
+// in the group's own l1-parity class) and the odd ones (the partner class) in separate
+// blocks.
+constexpr int MIXJ_OUT = 8, MIXJ_SRC = 8;
+
+void build_mix_program(he_plan_host &P, const std::vector<std::vector<int>> &classes, const int *vptr, const int *vc,
+                       const int *vl, const double *vcoef, int nlam, const int *dptr, const int *dc, const int *de)
+{
+    P.mix.clear();
+    for (const auto &cls : classes)
+        for (size_t g0 = 0; g0 < cls.size(); g0 += MIXJ_OUT) {
+            MixGroup G;
+            G.out.assign(cls.begin() + g0, cls.begin() + std::min(cls.size(), g0 + (size_t)MIXJ_OUT));
+            // multipoles with edges, each with its sorted source set
+            std::vector<std::pair<int, int>> order;   // (smallest source, lambda)
+            std::vector<std::set<int>> srcs(nlam);
+            for (int d = 0; d < (int)G.out.size(); ++d)
+                for (int k = vptr[G.out[d]]; k < vptr[G.out[d] + 1]; ++k) srcs[vl[k]].insert(vc[k]);
+            for (int lam = 0; lam < nlam; ++lam)
+                if (!srcs[lam].empty()) order.push_back({*srcs[lam].begin(), lam});
+            std::sort(order.begin(), order.end());
+            MixBlock B;
+            std::set<int> bsrc;
+            auto close = [&]() {
+                if (B.terms.empty()) return;
+                B.src.assign(bsrc.begin(), bsrc.end());
+                for (auto &T : B.terms)
+                    for (auto &si : T.s) si = (int)(std::lower_bound(B.src.begin(), B.src.end(), si) - B.src.begin());
+                G.blocks.push_back(B);
+                B = MixBlock();
+                bsrc.clear();
+            };
+            for (const auto &o : order) {
+                const int lam = o.second;
+                std::set<int> merged = bsrc;
+                merged.insert(srcs[lam].begin(), srcs[lam].end());
+                if ((int)merged.size() > MIXJ_SRC && !B.terms.empty()) { close(); merged = srcs[lam]; }
+                bsrc = merged;
+                MixTerm T;
+                T.lam = lam;
+                for (int d = 0; d < (int)G.out.size(); ++d)
+                    for (int k = vptr[G.out[d]]; k < vptr[G.out[d] + 1]; ++k)
+                        if (vl[k] == lam) { T.d.push_back(d); T.s.push_back(vc[k]); T.w.push_back(vcoef[2 * k]); }
+                B.terms.push_back(T);
+            }
+            close();
+            for (int d = 0; d < (int)G.out.size(); ++d)
+                for (int k = dptr[G.out[d]]; k < dptr[G.out[d] + 1]; ++k) {
+                    const int e = de[k] == 1 ? 0 : 1;
+                    G.dd[e].push_back(d); G.ds[e].push_back(dc[k]); G.dk[e].push_back(k);
+                }
+            P.mix.push_back(G);
+        }
+}
+
 }  // namespace
 
 // Build the tiled plan from the reference's tables.  Returns false (and the generic
@@ -279,6 +337,11 @@ bool he_build_plan(he_plan_host &P, int n, int nc, const int *ptr, const int *co
         }
     std::map<std::pair<int, int>, std::vector<int>> classes;
     for (int c = 0; c < nc; ++c) classes[{component.find(c), even.find(c)}].push_back(c);
+    {
+        std::vector<std::vector<int>> cls;
+        for (auto &kv : classes) cls.push_back(kv.second);
+        build_mix_program(P, cls, vptr, vc, vl, vcoef, nlam, dptr, dc, de);
+    }
     std::vector<std::vector<int>> groups;
     for (auto &kv : classes)
         for (size_t i = 0; i < kv.second.size(); i += MIX_GROUP)

@@ -95,11 +95,13 @@ class B200Hamiltonian:
         self.diagonal = torch.empty(self.size, dtype=torch.complex128, device=self.device)
         check(LIB.he_diagonal(self.op.handle, ct.c_void_p(self.diagonal.data_ptr()), _stream(self.device)), 'he_diagonal')
         self.apply_count = 0
-        info = (ct.c_longlong * 16)()
-        check(LIB.he_info(self.op.handle, info, 16), 'he_info')
+        info = (ct.c_longlong * 18)()
+        check(LIB.he_info(self.op.handle, info, 18), 'he_info')
         self.tiled = bool(info[9])
+        self.path = int(info[10])
         self.plan_info = {'elements': int(info[11]), 'tiles_per_axis': int(info[12]), 'groups': int(info[13]),
-                          'wide_edges': int(info[14]), 'wide_dipole_edges': int(info[15])}
+                          'wide_edges': int(info[14]), 'wide_dipole_edges': int(info[15]),
+                          'band_kernel': bool(info[16]), 'kinetic_kernel': bool(info[17])}
         if hasattr(h, 'surface_indices'):
             self._prepare_flux()
 
@@ -113,6 +115,20 @@ class B200Hamiltonian:
         check(LIB.he_set_path(self.op.handle, int(path)), 'he_set_path')
         self.tiled = path != 0
         self.path = int(path)
+
+    def kernels(self, precision='complex128'):
+        """Names of the kernels one apply launches on the current path."""
+        if not self.tiled:
+            return ['hpsi_gather_kernel']
+        if self.path == 2:
+            radial = 'hpsi_radial_kernel'
+        elif self.path == 1 and precision == 'complex128' and self.plan_info['band_kernel']:
+            radial = 'hpsi_band_kernel'
+        elif self.plan_info['kinetic_kernel']:
+            radial = 'hpsi_kinetic_kernel'
+        else:
+            radial = 'hpsi_radial_kernel'
+        return [radial, 'hpsi_mix_kernel']
 
     @property
     def launches_per_apply(self):
