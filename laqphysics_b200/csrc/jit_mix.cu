@@ -77,6 +77,8 @@ std::string mix_entry(int v);
 // real, so field-contracted coefficients are real (length) or imaginary (velocity).
 std::string mix_source(const he_plan_host &P, bool dipole_real, int variant)
 {
+    // The groups are __noinline__ functions: each is register-allocated on its own, so the
+    // loads of one group are not hoisted into another (no spills at two CTAs of 128 per SM).
     std::ostringstream o;
     o << kPrelude;
     o << "template <typename R, bool VEL>\n__device__ __forceinline__ void mix_body(\n"
@@ -100,8 +102,12 @@ std::string mix_source(const he_plan_host &P, bool dipole_real, int variant)
          "    __syncthreads();\n"
          "    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;\n"
          "    if (p >= nn) return;\n"
-         "    const C Z = mk<R>(0, 0);\n"
          "    const C re1 = rt[p % n], re2 = rt[p / n];\n";
+    for (size_t g = 0; g < P.mix.size(); ++g)
+        o << "    mix_group" << g << "<R, VEL>(psi, out, rad, w1, w2, K, KW, p, nn, re1, re2, beta, gamma);\n";
+    o << "}\n";
+    const std::string body = o.str().substr(std::string(kPrelude).size());
+    o.str("");
     // coefficient use: real part (length, dipole_real), imaginary part (velocity, dipole_real) or full complex
     auto dip_term = [&](const char *acc, const char *kref, const char *x) {
         std::ostringstream t;
@@ -114,6 +120,14 @@ std::string mix_source(const he_plan_host &P, bool dipole_real, int variant)
     };
     for (size_t g = 0; g < P.mix.size(); ++g) {
         const MixGroup &G = P.mix[g];
+        o << "template <typename R, bool VEL>\n__device__ __noinline__ void mix_group" << g
+          << "(const typename cx<R>::T *__restrict__ psi, typename cx<R>::T *__restrict__ out,\n"
+             "    const typename cx<R>::T *__restrict__ rad, const typename cx<R>::T *__restrict__ w1,\n"
+             "    const typename cx<R>::T *__restrict__ w2, const typename cx<R>::T *K, const typename cx<R>::T *KW,\n"
+             "    long long p, long long nn, typename cx<R>::T re1, typename cx<R>::T re2, typename cx<R>::T beta,\n"
+             "    typename cx<R>::T gamma)\n{\n"
+             "    typedef typename cx<R>::T C;\n"
+             "    const C Z = mk<R>(0, 0);\n";
         o << "    {   // group " << g << "\n";
         for (size_t d = 0; d < G.out.size(); ++d) o << "        C a" << d << " = out[p + nn * " << G.out[d] << "LL];\n";
         for (const MixBlock &B : G.blocks) {
@@ -165,9 +179,11 @@ std::string mix_source(const he_plan_host &P, bool dipole_real, int variant)
         for (size_t d = 0; d < G.out.size(); ++d)
             o << "        out[p + nn * " << G.out[d] << "LL] = cfma<R>(gamma, a" << d << ", cmul<R>(beta, psi[p + nn * "
               << G.out[d] << "LL]));\n";
-        o << "    }\n";
+        o << "    }\n}\n";
     }
-    o << "}\n";
+    const std::string group_fns = o.str();
+    o.str("");
+    o << kPrelude << group_fns << body;
     if (variant == -1)
         for (int v = 0; v < 4; ++v) o << mix_entry(v);
     else if (variant >= 0)
@@ -182,7 +198,7 @@ std::string mix_entry(int v)
     const bool dbl = v < 2, vel = v & 1;
     const char *R = dbl ? "double" : "float", *C = dbl ? "cd" : "cf";
     std::ostringstream o;
-    o << "extern \"C\" __global__ void __launch_bounds__(128, 4) " << names[v] << "(const " << C << " *psi, " << C
+    o << "extern \"C\" __global__ void __launch_bounds__(128, 2) " << names[v] << "(const " << C << " *psi, " << C
       << " *out, const " << C << " *rad, const " << C << " *rt, const " << C << " *w1, const " << C << " *w2, const "
       << C << " *dcoef, const " << R << " *ldiff, long long nn, int n, int nd, " << R << " f0, " << R << " f1, " << R
       << " f2, " << C << " beta, " << C << " gamma)\n{ mix_body<" << R << ", " << (vel ? "true" : "false")
