@@ -4,7 +4,7 @@
 // The Coulomb multipoles (src/kernels.f90:132-143: sum_lam rad(i,j,lam) sum_c' vcoef
 // psi(i,j,c')) and the dipole couplings (:145-168) are the same for every point of the
 // radial grid, so the generated kernel unrolls every edge with its coefficient as an
-// exact literal: one thread per point, output channels of a group in registers, each
+// exact literal: one thread per (point, output group), the group's output channels in registers, each
 // source loaded once per block of multipoles, no coefficient loads and no padded slots.
 // The dipole coefficients depend on the field; each CTA contracts them once into shared
 // memory (zero below 1e-30, the skip of src/kernels.f90:145).
@@ -100,12 +100,16 @@ std::string mix_source(const he_plan_host &P, bool dipole_real, int variant)
          "        if (VEL) KW[k] = iv;\n"
          "    }\n"
          "    __syncthreads();\n"
-         "    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;\n"
-         "    if (p >= nn) return;\n"
-         "    const C re1 = rt[p % n], re2 = rt[p / n];\n";
+         "    // grid: x = output group (fastest, so the groups of one point block share L2), y = point blocks\n"
+         "    for (long long pb = blockIdx.y; pb * blockDim.x < nn; pb += gridDim.y) {\n"
+         "        const long long p = pb * blockDim.x + threadIdx.x;\n"
+         "        if (p >= nn) return;\n"
+         "        const C re1 = rt[p % n], re2 = rt[p / n];\n"
+         "        switch (blockIdx.x) {\n";
     for (size_t g = 0; g < P.mix.size(); ++g)
-        o << "    mix_group" << g << "<R, VEL>(psi, out, rad, w1, w2, K, KW, p, nn, re1, re2, beta, gamma);\n";
-    o << "}\n";
+        o << "        case " << g << ": mix_group" << g
+          << "<R, VEL>(psi, out, rad, w1, w2, K, KW, p, nn, re1, re2, beta, gamma); break;\n";
+    o << "        }\n    }\n}\n";
     const std::string body = o.str().substr(std::string(kPrelude).size());
     o.str("");
     // coefficient use: real part (length, dipole_real), imaginary part (velocity, dipole_real) or full complex
@@ -343,9 +347,10 @@ int launch_mix_jit(he_operator *h, const DeviceTables<R> &t, const cplx<R> *psi,
     const R *ldiff = t.ldiff;
     void *args[] = {(void *)&psi, (void *)&out, (void *)&t.rad, (void *)&rt, (void *)&w1, (void *)&w2,
                     (void *)&dcoef, (void *)&ldiff, &nn, &n, &nd, &f0, &f1, &f2, &beta, &gamma};
-    const unsigned blocks = (unsigned)((nn + 127) / 128);
+    const unsigned point_blocks = (unsigned)std::min<long long>((nn + 127) / 128, 65535);
     const size_t smem = 2 * (size_t)std::max(nd, 1) * sizeof(cplx<R>);
-    HE_CUDA_TRY(cudaLaunchKernel(reinterpret_cast<const void *>(k), dim3(blocks), dim3(128), args, smem, stream));
+    const dim3 grid((unsigned)h->plan.mix.size(), point_blocks);
+    HE_CUDA_TRY(cudaLaunchKernel(reinterpret_cast<const void *>(k), grid, dim3(128), args, smem, stream));
     return HE_OK;
 }
 
