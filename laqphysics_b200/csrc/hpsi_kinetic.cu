@@ -539,6 +539,9 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
     return fn;
 }
 
+}  // namespace
+
+// Multiprocessor count of a device (cached; 148 on B200 when the query fails).
 int sm_count(int device)
 {
     static int counts[64] = {0};
@@ -550,8 +553,6 @@ int sm_count(int device)
     }
     return counts[device];
 }
-
-}  // namespace
 
 // True when the kinetic kernel can stage `psi` with TMA: 16-byte aligned base and rows
 // (the r1 extent in bytes) a multiple of 16 bytes.

@@ -4,7 +4,7 @@
 // The Coulomb multipoles (src/kernels.f90:132-143: sum_lam rad(i,j,lam) sum_c' vcoef
 // psi(i,j,c')) and the dipole couplings (:145-168) are the same for every point of the
 // radial grid, so the generated kernel unrolls every edge with its coefficient as an
-// exact literal: one thread per (point, output group), the group's output channels in registers, each
+// exact literal: one thread per point (or per point and output group on small grids), the group's output channels in registers, each
 // source loaded once per block of multipoles, no coefficient loads and no padded slots.
 // The dipole coefficients depend on the field; each CTA contracts them once into shared
 // memory (zero below 1e-30, the skip of src/kernels.f90:145).
@@ -70,6 +70,10 @@ std::string lit(double v)
 
 }  // namespace
 
+// CTAs of 128 threads per SM the generated kernels are compiled for (register budget):
+// the complex128 groups need more registers than the complex64 ones.
+constexpr int MIXJ_MIN_BLOCKS_D = 2, MIXJ_MIN_BLOCKS_F = 4;
+
 std::string mix_entry(int v);
 
 // CUDA source of the generated kernel for a plan (variant -1: all four entry points,
@@ -100,16 +104,20 @@ std::string mix_source(const he_plan_host &P, bool dipole_real, int variant)
          "        if (VEL) KW[k] = iv;\n"
          "    }\n"
          "    __syncthreads();\n"
-         "    // grid: x = output group (fastest, so the groups of one point block share L2), y = point blocks\n"
+         "    // grid y = point blocks; grid x = 1: a thread runs every output group of its point (large\n"
+         "    // grids), else x = output group (small grids; fastest axis, so one point block's groups share L2)\n"
          "    for (long long pb = blockIdx.y; pb * blockDim.x < nn; pb += gridDim.y) {\n"
          "        const long long p = pb * blockDim.x + threadIdx.x;\n"
          "        if (p >= nn) return;\n"
          "        const C re1 = rt[p % n], re2 = rt[p / n];\n"
-         "        switch (blockIdx.x) {\n";
+         "        if (gridDim.x == 1) {\n";
     for (size_t g = 0; g < P.mix.size(); ++g)
-        o << "        case " << g << ": mix_group" << g
+        o << "            mix_group" << g << "<R, VEL>(psi, out, rad, w1, w2, K, KW, p, nn, re1, re2, beta, gamma);\n";
+    o << "        } else {\n            switch (blockIdx.x) {\n";
+    for (size_t g = 0; g < P.mix.size(); ++g)
+        o << "            case " << g << ": mix_group" << g
           << "<R, VEL>(psi, out, rad, w1, w2, K, KW, p, nn, re1, re2, beta, gamma); break;\n";
-    o << "        }\n    }\n}\n";
+    o << "            }\n        }\n    }\n}\n";
     const std::string body = o.str().substr(std::string(kPrelude).size());
     o.str("");
     // coefficient use: real part (length, dipole_real), imaginary part (velocity, dipole_real) or full complex
@@ -202,7 +210,8 @@ std::string mix_entry(int v)
     const bool dbl = v < 2, vel = v & 1;
     const char *R = dbl ? "double" : "float", *C = dbl ? "cd" : "cf";
     std::ostringstream o;
-    o << "extern \"C\" __global__ void __launch_bounds__(128, 2) " << names[v] << "(const " << C << " *psi, " << C
+    o << "extern \"C\" __global__ void __launch_bounds__(128, " << (dbl ? MIXJ_MIN_BLOCKS_D : MIXJ_MIN_BLOCKS_F) << ") "
+      << names[v] << "(const " << C << " *psi, " << C
       << " *out, const " << C << " *rad, const " << C << " *rt, const " << C << " *w1, const " << C << " *w2, const "
       << C << " *dcoef, const " << R << " *ldiff, long long nn, int n, int nd, " << R << " f0, " << R << " f1, " << R
       << " f2, " << C << " beta, " << C << " gamma)\n{ mix_body<" << R << ", " << (vel ? "true" : "false")
@@ -349,7 +358,8 @@ int launch_mix_jit(he_operator *h, const DeviceTables<R> &t, const cplx<R> *psi,
                     (void *)&dcoef, (void *)&ldiff, &nn, &n, &nd, &f0, &f1, &f2, &beta, &gamma};
     const unsigned point_blocks = (unsigned)std::min<long long>((nn + 127) / 128, 65535);
     const size_t smem = 2 * (size_t)std::max(nd, 1) * sizeof(cplx<R>);
-    const dim3 grid((unsigned)h->plan.mix.size(), point_blocks);
+    const bool one_thread_per_point = point_blocks >= 8u * (unsigned)sm_count(h->device);
+    const dim3 grid(one_thread_per_point ? 1u : (unsigned)h->plan.mix.size(), point_blocks);
     HE_CUDA_TRY(cudaLaunchKernel(reinterpret_cast<const void *>(k), grid, dim3(128), args, smem, stream));
     return HE_OK;
 }

@@ -52,6 +52,7 @@ template <typename R> bool kinetic_usable(const KineticPlan<R> &kp, const void *
 template <typename R>
 int launch_kinetic(he_operator *h, const DeviceTables<R> &t, const KineticPlan<R> &kp, const cplx<R> *psi,
                    cplx<R> *out, cplx<R> *w1, cplx<R> *w2, R a2, int velocity, cudaStream_t stream);
+int sm_count(int device);
 std::string mix_source(const he_plan_host &P, bool dipole_real, int variant);
 int jit_mix_prepare(he_operator *h, int variant);
 template <typename R>
