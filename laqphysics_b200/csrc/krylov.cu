@@ -175,11 +175,13 @@ __global__ void start_kernel(const double *__restrict__ norm_partial, int nb, Kr
     if (st->beta == 0) { st->done = 1; st->converged = 1; st->m = 0; }
 }
 
-// y = sum_{k < m} Q_k c_k with m taken from the status word (or from `mfix` >= 0).
+// y = sum_{k < m} Q_k c_k with m taken from the status word (or from `mfix` >= 0).  With
+// the status word (mfix < 0), y is left untouched unless the solve converged.
 __global__ void __launch_bounds__(KRYLOV_THREADS)
 combine_kernel(const double2 *__restrict__ Q, size_t n, const double2 *__restrict__ c, double2 *__restrict__ y,
                const KrylovStatus *st, int mfix, int accumulate)
 {
+    if (mfix < 0 && (st->failed || !st->converged)) return;
     const int m = mfix >= 0 ? mfix : st->m;
     __shared__ double2 cs[KRYLOV_MAXDIM];
     for (int k = threadIdx.x; k < m; k += blockDim.x) cs[k] = c[k];
@@ -550,20 +552,16 @@ int expv_impl(he_krylov *k, he_handle op, const void *x, void *y, const double *
     }
     if (maxdim < 1 || maxdim > k->maxdim) return he_fail(HE_ERR_ARG, "maxdim exceeds the workspace", __FILE__, __LINE__);
     if ((size_t)op->n * op->n * op->nc != k->n) return he_fail(HE_ERR_SHAPE, "workspace size != operator size", __FILE__, __LINE__);
+    // The whole Krylov loop is enqueued without waiting on the device: the check kernel
+    // decides convergence at the reference's check points on the device and sets the
+    // status word, after which every Krylov kernel returns at once.  The host reads the
+    // status once, at the end.  (x = 0 gives beta = 0: done at once with m = 0, and the
+    // combination below writes y = 0 = x.)
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
     int rc = krylov_start(k, static_cast<const double2 *>(x), s);
-    if (!rc) rc = krylov_read_status(k, s);
     if (rc) return rc;
-    if (k->host_status->beta == 0) {
-        HE_CUDA_TRY(cudaMemcpyAsync(y, x, k->n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
-        if (dimension) *dimension = 0;
-        if (estimate) *estimate = 0;
-        return HE_OK;
-    }
     const int ld = k->maxdim + 1;
-    int done = 0, m = 0;
-    double err = 0;
-    for (int j = 0; j < maxdim && !done; ++j) {
+    for (int j = 0; j < maxdim; ++j) {
         double2 *qj = k->Q + (size_t)j * k->n, *v = k->Q + (size_t)(j + 1) * k->n;
         if (precision == HE_C64) {
             krylov_to_c64<<<kGrid, kBlock, 0, s>>>(k->n, qj, k->s32[0]);
@@ -574,27 +572,18 @@ int expv_impl(he_krylov *k, he_handle op, const void *x, void *y, const double *
         }
         if (!rc) rc = krylov_cgs2(k, j + 1, v, k->H + (size_t)j * ld, k->H + (size_t)j * ld + j + 1, s, 1e-13);
         if (rc) break;
-        const bool checkpoint = j >= 3 && ((j + 1) % 4 == 0 || j + 1 == maxdim);
         arnoldi_check_kernel<<<1, 512, 0, s>>>(k->H, ld, j, maxdim, dt, tol, k->coef, k->work, k->status);
         if (j + 1 < maxdim) normalize_kernel<<<kGrid, kBlock, 0, s>>>(v, v, k->n, k->status);
-        if (checkpoint || j + 1 == maxdim) {
-            if ((rc = krylov_read_status(k, s))) break;
-            done = k->host_status->done;
-            m = k->host_status->m;
-            err = k->host_status->estimate;
-        }
     }
     if (rc) return rc;
-    if (!done) {   // a happy breakdown recorded between check points
-        if ((rc = krylov_read_status(k, s))) return rc;
-        done = k->host_status->done; m = k->host_status->m; err = k->host_status->estimate;
-    }
-    if (estimate) *estimate = err;
-    if (dimension) *dimension = m;
+    // y = Q c with m from the status word; y is left as is when the solve failed
+    combine_kernel<<<kGrid, kBlock, 0, s>>>(k->Q, k->n, k->coef, static_cast<double2 *>(y), k->status, -1, 0);
+    HE_CUDA_TRY(cudaGetLastError());
+    if ((rc = krylov_read_status(k, s))) return rc;
+    if (estimate) *estimate = k->host_status->estimate;
+    if (dimension) *dimension = k->host_status->m;
     if (k->host_status->failed || !k->host_status->converged)
         return he_fail(HE_ERR_NOCONV, "Arnoldi did not converge", __FILE__, __LINE__);
-    combine_kernel<<<kGrid, kBlock, 0, s>>>(k->Q, k->n, k->coef, static_cast<double2 *>(y), k->status, m, 0);
-    HE_CUDA_TRY(cudaGetLastError());
     return HE_OK;
 }
 }  // namespace
