@@ -123,6 +123,38 @@ update_kernel(const double2 *__restrict__ Q, size_t n, int kc, const double2 *__
     }
 }
 
+// Second CGS pass fused with the first update: v' = v - sum_k Q_k z_k is written and, in
+// the same sweep, partial[b*ld + k] = sum over the block of conj(Q_k) v' (k < kc <= KT).
+// The second read of each Q_k element comes from cache; per-thread order and block sums are those of
+// update_kernel followed by multidot_kernel, so the results are identical.
+template <int KT>
+__global__ void __launch_bounds__(KRYLOV_THREADS)
+update_multidot_kernel(const double2 *__restrict__ Q, size_t n, int kc, const double2 *__restrict__ z,
+                       double2 *__restrict__ v, double2 *__restrict__ partial, int ld, const KrylovStatus *st)
+{
+    if (st && st->done) return;
+    __shared__ double2 zs[KT];
+    for (int k = threadIdx.x; k < kc; k += blockDim.x) zs[k] = z[k];
+    __syncthreads();
+    double2 acc[KT];
+#pragma unroll
+    for (int k = 0; k < KT; ++k) acc[k] = mk<double>(0, 0);
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        double2 x = v[p];
+#pragma unroll
+        for (int k = 0; k < KT; ++k)
+            if (k < kc) x = cfma<double>(mk<double>(-zs[k].x, -zs[k].y), Q[(size_t)k * n + p], x);
+        v[p] = x;
+#pragma unroll
+        for (int k = 0; k < KT; ++k)
+            if (k < kc) acc[k] = cfma_conj<double>(Q[(size_t)k * n + p], x, acc[k]);
+    }
+    __shared__ double2 res[KT];
+    block_sum<KT>(acc, res);
+    __syncthreads();
+    if (threadIdx.x < kc) partial[(size_t)blockIdx.x * ld + threadIdx.x] = res[threadIdx.x];
+}
+
 // per-block |v|^2
 __global__ void __launch_bounds__(KRYLOV_THREADS)
 norm_kernel(const double2 *__restrict__ v, size_t n, double *__restrict__ norm_partial)
@@ -444,9 +476,19 @@ int krylov_multidot(he_krylov *k, int kc, const double2 *v, double2 *hcol, cudaS
 int krylov_cgs2(he_krylov *k, int kc, double2 *v, double2 *hcol, double2 *hsub, cudaStream_t s, double happy_below)
 {
     int rc;
-    for (int rep = 0; rep < 2; ++rep) {
+    if (kc <= KRYLOV_FUSED) {   // three sweeps: project, update + project, update + norm
+        const int ld = k->maxdim + 1;
         if ((rc = krylov_multidot(k, kc, v, hcol, s, k->status, k->Q))) return rc;
-        update_kernel<<<kGrid, kBlock, 0, s>>>(k->Q, k->n, kc, k->z, v, rep == 1 ? k->norm_partial : nullptr, k->status);
+        update_multidot_kernel<KRYLOV_FUSED><<<kGrid, kBlock, 0, s>>>(k->Q, k->n, kc, k->z, v, k->partial, ld, k->status);
+        reduce_partials_kernel<<<1, 32 * std::max(1, std::min(kc, 16)), 0, s>>>(k->partial, KRYLOV_BLOCKS, ld, kc, k->z,
+                                                                               hcol, k->status);
+        update_kernel<<<kGrid, kBlock, 0, s>>>(k->Q, k->n, kc, k->z, v, k->norm_partial, k->status);
+    } else {
+        for (int rep = 0; rep < 2; ++rep) {
+            if ((rc = krylov_multidot(k, kc, v, hcol, s, k->status, k->Q))) return rc;
+            update_kernel<<<kGrid, kBlock, 0, s>>>(k->Q, k->n, kc, k->z, v, rep == 1 ? k->norm_partial : nullptr,
+                                                   k->status);
+        }
     }
     finish_norm_kernel<<<1, 32, 0, s>>>(k->norm_partial, KRYLOV_BLOCKS, hsub, k->status, happy_below);
     HE_CUDA_TRY(cudaGetLastError());

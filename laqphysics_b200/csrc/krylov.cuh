@@ -23,6 +23,7 @@ constexpr int KRYLOV_BLOCKS = 296;    // 2 CTAs per SM on 148 SMs
 constexpr int KRYLOV_THREADS = 256;
 constexpr int KRYLOV_TILE = 8;        // basis vectors per register tile
 constexpr int KRYLOV_MAXDIM = 64;
+constexpr int KRYLOV_FUSED = 16;      // CGS2 with a fused update + projection sweep up to this many vectors
 
 }  // namespace he
 
