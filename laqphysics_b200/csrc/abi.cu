@@ -1,6 +1,8 @@
 // extern "C" entry points of libhelium_b200.so: operator handles, the drop-in
 // host-pointer `tensor_apply`, and error reporting.
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <complex>
 #include <cstdio>
 #include <cstring>
@@ -217,6 +219,21 @@ template <typename R> int velocity_scratch(he_operator *h, cplx<R> **w)
 he_operator::~he_operator()
 {
     for (void *p : allocations) cudaFree(p);
+}
+
+cudaError_t he_smem_limit(const void *kernel, size_t bytes)
+{
+    static std::mutex mutex;
+    static std::map<std::pair<const void *, int>, size_t> raised;
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mutex);
+    size_t &have = raised[{kernel, device}];
+    if (have >= bytes) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) have = bytes;
+    return e;
 }
 
 extern "C" int he_set_path(he_handle h, int tiled)

@@ -95,3 +95,7 @@ template <typename R> struct DeviceTables {
     } while (0)
 
 void he_set_error(const char* what, const char* file, int line);
+
+// Raise a kernel's dynamic shared-memory limit on the current device, once per kernel,
+// device and size (the attribute call costs microseconds per launch otherwise).
+cudaError_t he_smem_limit(const void* kernel, size_t bytes);

@@ -554,6 +554,31 @@ int sm_count(int device)
     return counts[device];
 }
 
+// TMA map of psi(re/im, r1, r2 channel) with a (2 box_r, box_c, 1) box, from the
+// operator's cache of recently used buffers (a Krylov basis reuses the same few), else
+// encoded now.  Returns null when encoding fails.
+const CUtensorMap *psi_map(he_operator *h, int kind, const void *psi, int n, int nc, int box_r, int box_c,
+                           size_t real_bytes)
+{
+    for (auto &e : h->tmaps)
+        if (e.base == psi && e.kind == kind) return &e.map;
+    auto &e = h->tmaps[h->tmap_next];
+    h->tmap_next = (h->tmap_next + 1) % (int)(sizeof(h->tmaps) / sizeof(h->tmaps[0]));
+    const cuuint64_t dims[3] = {2 * (cuuint64_t)n, (cuuint64_t)n, (cuuint64_t)nc};
+    const cuuint64_t strides[2] = {2 * (cuuint64_t)n * real_bytes, 2 * (cuuint64_t)n * n * real_bytes};
+    const cuuint32_t box[3] = {2 * (cuuint32_t)box_r, (cuuint32_t)box_c, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    e.base = nullptr;
+    const CUresult r = tensor_map_encoder()(&e.map, real_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                                            3, const_cast<void *>(psi), dims, strides, box, es,
+                                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return nullptr;
+    e.base = psi;
+    e.kind = kind;
+    return &e.map;
+}
+
 // True when the kinetic kernel can stage `psi` with TMA: 16-byte aligned base and rows
 // (the r1 extent in bytes) a multiple of 16 bytes.
 template <typename R> bool kinetic_usable(const KineticPlan<R> &kp, const void *psi)
@@ -566,23 +591,16 @@ template <typename R>
 int launch_kinetic(he_operator *h, const DeviceTables<R> &t, const KineticPlan<R> &kp, const cplx<R> *psi,
                    cplx<R> *out, cplx<R> *w1, cplx<R> *w2, R a2, int velocity, cudaStream_t stream)
 {
-    CUtensorMap map;
-    const cuuint64_t dims[3] = {2 * (cuuint64_t)kp.n, (cuuint64_t)kp.n, (cuuint64_t)kp.nc};
-    const cuuint64_t strides[2] = {2 * (cuuint64_t)kp.n * sizeof(R), 2 * (cuuint64_t)kp.n * kp.n * sizeof(R)};
-    const cuuint32_t box[3] = {2 * (cuuint32_t)kp.box_r, (cuuint32_t)kp.box_c, 1};
-    const cuuint32_t es[3] = {1, 1, 1};
-    const CUresult r = tensor_map_encoder()(&map, sizeof(R) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
-                                            3, const_cast<cplx<R> *>(psi), dims, strides, box, es,
-                                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return he_fail(HE_ERR_CUDA, "cuTensorMapEncodeTiled failed", __FILE__, __LINE__);
+    const CUtensorMap *mp = psi_map(h, sizeof(R) == 8 ? 1 : 2, psi, kp.n, kp.nc, kp.box_r, kp.box_c, sizeof(R));
+    if (!mp) return he_fail(HE_ERR_CUDA, "cuTensorMapEncodeTiled failed", __FILE__, __LINE__);
+    const CUtensorMap map = *mp;
     const size_t smem = 2 * (size_t)kp.stage_bytes + KIN_BRIDGE_BYTES + 16 + KIN_STAGE_ALIGN;
     const long long items = (long long)kp.ntr * kp.nct * kp.nc;
     const unsigned grid = (unsigned)std::min<long long>(items, 2LL * sm_count(h->device));
 #define HE_KINETIC(V, S)                                                                                   \
     do {                                                                                                   \
         auto kern = hpsi_kinetic_kernel<R, V, S>;                                                          \
-        HE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));   \
+        HE_CUDA_TRY(he_smem_limit(reinterpret_cast<const void *>(kern), smem));   \
         kern<<<grid, KIN_THREADS, smem, stream>>>(map, t, kp, out, w1, w2, a2);                            \
     } while (0)
     if (velocity) { if (t.diag_separable) HE_KINETIC(true, true); else HE_KINETIC(true, false); }
@@ -600,22 +618,16 @@ bool band_usable(const BandPlan<double> &bp, const void *psi)
 int launch_band(he_operator *h, const DeviceTables<double> &t, const BandPlan<double> &bp, const double2 *psi,
                 double2 *out, double2 *w1, double2 *w2, double a2, int velocity, cudaStream_t stream)
 {
-    CUtensorMap map;
-    const cuuint64_t dims[3] = {2 * (cuuint64_t)bp.n, (cuuint64_t)bp.n, (cuuint64_t)bp.nc};
-    const cuuint64_t strides[2] = {2 * (cuuint64_t)bp.n * sizeof(double), 2 * (cuuint64_t)bp.n * bp.n * sizeof(double)};
-    const cuuint32_t box[3] = {2 * (cuuint32_t)bp.box_r, (cuuint32_t)bp.box_c, 1};
-    const cuuint32_t es[3] = {1, 1, 1};
-    const CUresult r = tensor_map_encoder()(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double2 *>(psi), dims,
-                                            strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return he_fail(HE_ERR_CUDA, "cuTensorMapEncodeTiled failed", __FILE__, __LINE__);
+    const CUtensorMap *mp = psi_map(h, 0, psi, bp.n, bp.nc, bp.box_r, bp.box_c, sizeof(double));
+    if (!mp) return he_fail(HE_ERR_CUDA, "cuTensorMapEncodeTiled failed", __FILE__, __LINE__);
+    const CUtensorMap map = *mp;
     const size_t smem = 2 * (size_t)bp.stage_bytes + (size_t)BAND_CG * BAND_KS * 32 * sizeof(double2) + 16 + KIN_STAGE_ALIGN;
     const long long items = (long long)bp.ntr * bp.nct * bp.nc;
     const unsigned grid = (unsigned)std::min<long long>(items, (long long)sm_count(h->device));
 #define HE_BAND(V, S)                                                                                      \
     do {                                                                                                   \
         auto kern = hpsi_band_kernel<V, S>;                                                                \
-        HE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));   \
+        HE_CUDA_TRY(he_smem_limit(reinterpret_cast<const void *>(kern), smem));   \
         kern<<<grid, BAND_THREADS, smem, stream>>>(map, t, bp, out, w1, w2, a2);                           \
     } while (0)
     if (velocity) { if (t.diag_separable) HE_BAND(true, true); else HE_BAND(true, false); }

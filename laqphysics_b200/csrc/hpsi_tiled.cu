@@ -558,7 +558,7 @@ int launch_hpsi_tiled(he_operator *h, const DeviceTables<R> &t, const TiledPlan<
 #define HE_RADIAL(V, S)                                                                                  \
     do {                                                                                                 \
         auto kern = hpsi_radial_kernel<R, V, S>;                                                         \
-        HE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rs));   \
+        HE_CUDA_TRY(he_smem_limit(reinterpret_cast<const void *>(kern), rs));   \
         kern<<<rgrid, RAD_THREADS, rs, stream>>>(t, pl, psi, out, w1, w2, a2, blkmax);                   \
     } while (0)
         if (velocity) { if (t.diag_separable) HE_RADIAL(true, true); else HE_RADIAL(true, false); }
@@ -575,10 +575,10 @@ int launch_hpsi_tiled(he_operator *h, const DeviceTables<R> &t, const TiledPlan<
     const unsigned blocks = (unsigned)std::min<size_t>(ntiles, (size_t)148 * per_sm);
     const int threads = 32 * std::min(16, std::max(1, pl.ng));
     if (velocity) {
-        HE_CUDA_TRY(cudaFuncSetAttribute(hpsi_mix_kernel<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ms));
+        HE_CUDA_TRY(he_smem_limit(reinterpret_cast<const void *>(hpsi_mix_kernel<R, true>), ms));
         hpsi_mix_kernel<R, true><<<blocks, threads, ms, stream>>>(t, pl, psi, out, w1, w2, f0, f1, f2, beta, gamma);
     } else {
-        HE_CUDA_TRY(cudaFuncSetAttribute(hpsi_mix_kernel<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ms));
+        HE_CUDA_TRY(he_smem_limit(reinterpret_cast<const void *>(hpsi_mix_kernel<R, false>), ms));
         hpsi_mix_kernel<R, false><<<blocks, threads, ms, stream>>>(t, pl, psi, out, w1, w2, f0, f1, f2, beta, gamma);
     }
     HE_CUDA_TRY(cudaGetLastError());

@@ -22,6 +22,13 @@ struct he_operator {
     he::KineticPlan<float> k32{};
     he::BandPlan<double> b64{};         // banded FP64 tensor-core kinetic plan (ntr == 0: not usable)
     int *kerr = nullptr;                // device error word of the kinetic kernel
+    struct TensorMapEntry {             // encoded TMA maps of recently used psi buffers
+        const void *base = nullptr;
+        int kind = -1;                  // 0 banded (complex128), 1 kinetic complex128, 2 kinetic complex64
+        CUtensorMap map;
+    };
+    TensorMapEntry tmaps[16];
+    int tmap_next = 0;
     double2 *coef64 = nullptr;          // field-contracted dipole coefficients (nd)
     float2 *coef32 = nullptr;
     double2 *w64[2] = {nullptr, nullptr};   // velocity gauge B-stencil scratch (n*n*nc each)
