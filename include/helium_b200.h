@@ -79,6 +79,14 @@ int he_info(he_handle h, long long *values, int count);
 int he_apply(he_handle h, const void *psi, void *out, const double *field, int velocity,
              int precision, void *stream);
 
+/* out_b = H(fields[3b..3b+2], gauge) psi_b for count (<= 64) instances that share the
+ * operator; psi and out hold the instances one after another (count x n*n*nc).  With the
+ * banded and generated kernels available the whole batch is one launch per kernel, else
+ * the instances run one at a time.  The reference applies one state at a time
+ * (python/torch_backend.py:109-131); this batches its parameter-scan instances. */
+int he_apply_batched(he_handle h, int count, const void *psi, void *out, const double *fields, int velocity,
+                     int precision, void *stream);
+
 /* out = psi + i*alpha*(H(field) psi - e_ref psi): the shifted Pade operator of
  * python/implicit.py:77-84 (K = H - E_ref, A(y) = y + i alpha K y), alpha complex. */
 int he_apply_shifted(he_handle h, const void *psi, void *out, const double *field, int velocity,

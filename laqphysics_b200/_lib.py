@@ -30,6 +30,7 @@ SIGNATURES = {
     'he_destroy': (I, [P]),
     'he_info': (I, [P, ct.POINTER(ct.c_longlong), I]),
     'he_apply': (I, [P, P, P, P, I, I, P]),
+    'he_apply_batched': (I, [P, I, P, P, P, I, I, P]),
     'he_apply_shifted': (I, [P, P, P, P, I, D, D, D, I, P]),
     'he_diagonal': (I, [P, P, P]),
     'he_flux': (I, [P, P, P, I, I, I, P, P, P, P]),

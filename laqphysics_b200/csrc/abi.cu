@@ -178,39 +178,55 @@ template <typename R> int upload_plan(he_operator *h, he::TiledPlan<R> *pl, cplx
         h->kerr = static_cast<int *>(e);
     }
     if (P.kin_ok && (s = upload_kinetic<R>(h, pl, kp))) return s;
-    if constexpr (sizeof(R) == 8) {   // banded FP64 tensor-core kinetic plan
-        h->b64 = he::BandPlan<double>{};
+    {   // banded tensor-core kinetic plan (FP64 fragments shared by both storage precisions)
+        he::BandPlan<R> *bpp;
+        if constexpr (sizeof(R) == 8) bpp = &h->b64; else bpp = &h->b32;
+        *bpp = he::BandPlan<R>{};
         if (P.band_ok) {
-            he::BandPlan<double> b{};
+            he::BandPlan<R> b{};
             b.n = h->n; b.nc = h->nc; b.ngroup = P.ngroup; b.ntr = P.bntr; b.nct = P.bnct;
-            b.box_r = P.bbox_r64; b.box_c = P.bbox_c;
-            const size_t bytes = (size_t)b.box_r * b.box_c * sizeof(double2);
+            b.box_r = sizeof(R) == 8 ? P.bbox_r64 : P.bbox_r32;
+            b.box_c = P.bbox_c;
+            const size_t bytes = (size_t)b.box_r * b.box_c * sizeof(cplx<R>);
             b.stage_bytes = (int)((bytes + he::KIN_STAGE_ALIGN - 1) / he::KIN_STAGE_ALIGN * he::KIN_STAGE_ALIGN);
-            if ((s = upload(h, P.glo.data(), P.glo.size(), &b.glo))) return s;
-            if ((s = upload(h, P.gks.data(), P.gks.size(), &b.gks))) return s;
-            if ((s = upload(h, P.greal.data(), P.greal.size(), &b.greal))) return s;
-            if ((s = upload(h, P.brbase.data(), P.brbase.size(), &b.brbase))) return s;
-            if ((s = upload(h, P.bcbase.data(), P.bcbase.size(), &b.bcbase))) return s;
-            if ((s = upload_c<double>(h, P.gfrag.data(), P.gfrag.size() / 2, &b.frag))) return s;
-            if ((s = upload_c<double>(h, P.gfragb.data(), P.gfragb.size() / 2, &b.fragb))) return s;
+            if constexpr (sizeof(R) == 4) {   // the fragment and index tables of the complex128 plan are reused
+                b.glo = h->b64.glo; b.gks = h->b64.gks; b.greal = h->b64.greal; b.brbase = h->b64.brbase;
+                b.bcbase = h->b64.bcbase; b.frag = h->b64.frag; b.fragb = h->b64.fragb;
+            } else {
+                if ((s = upload(h, P.glo.data(), P.glo.size(), &b.glo))) return s;
+                if ((s = upload(h, P.gks.data(), P.gks.size(), &b.gks))) return s;
+                if ((s = upload(h, P.greal.data(), P.greal.size(), &b.greal))) return s;
+                if ((s = upload(h, P.brbase.data(), P.brbase.size(), &b.brbase))) return s;
+                if ((s = upload(h, P.bcbase.data(), P.bcbase.size(), &b.bcbase))) return s;
+                if ((s = upload_c<double>(h, P.gfrag.data(), P.gfrag.size() / 2, &b.frag))) return s;
+                if ((s = upload_c<double>(h, P.gfragb.data(), P.gfragb.size() / 2, &b.fragb))) return s;
+            }
             b.err = h->kerr;
-            h->b64 = b;
+            if (sizeof(R) == 8 || h->b64.ntr > 0) *bpp = b;
         }
     }
     return HE_OK;
 }
 
 // Velocity-gauge scratch (two n*n*nc vectors), allocated on first use.
-template <typename R> int velocity_scratch(he_operator *h, cplx<R> **w)
+// Velocity-gauge scratch (two vectors of `count` instances each), grown on demand.
+template <typename R> int velocity_scratch(he_operator *h, cplx<R> **w, int count)
 {
-    if (w[0]) return HE_OK;
-    const size_t bytes = (size_t)h->n * h->n * h->nc * sizeof(cplx<R>);
+    int &cap = sizeof(R) == 8 ? h->wcap64 : h->wcap32;
+    if (w[0] && cap >= count) return HE_OK;
+    const size_t bytes = (size_t)h->n * h->n * h->nc * sizeof(cplx<R>) * count;
     for (int k = 0; k < 2; ++k) {
+        if (w[k]) {   // cudaFree waits for the device, so no kernel still reads the old buffer
+            HE_CUDA_TRY(cudaFree(w[k]));
+            h->allocations.erase(std::find(h->allocations.begin(), h->allocations.end(), (void *)w[k]));
+            w[k] = nullptr;
+        }
         void *p = nullptr;
         HE_CUDA_TRY(cudaMalloc(&p, bytes));
         h->allocations.push_back(p);
         w[k] = static_cast<cplx<R> *>(p);
     }
+    cap = count;
     return HE_OK;
 }
 
@@ -358,38 +374,51 @@ extern "C" int he_info(he_handle h, long long *values, int count)
 }
 
 namespace {
-int apply_common(he_handle h, const void *psi, void *out, const double *field, int velocity, int precision,
+int apply_common(he_handle h, const void *psi, void *out, const he::FieldBatch &fb, int velocity, int precision,
                  double beta_re, double beta_im, double gamma_re, double gamma_im, void *stream)
 {
     g_status = HE_OK;
-    if (!h || !psi || !out || !field) return he_fail(HE_ERR_ARG, "null argument", __FILE__, __LINE__);
+    if (!h || !psi || !out) return he_fail(HE_ERR_ARG, "null argument", __FILE__, __LINE__);
     if (velocity != 0 && velocity != 1) return he_fail(HE_ERR_ARG, "velocity must be 0 or 1", __FILE__, __LINE__);
     if (psi == out) return he_fail(HE_ERR_ARG, "H·psi cannot run in place", __FILE__, __LINE__);
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
-    int s;
+    const size_t N = (size_t)h->n * h->n * h->nc;
+    int s = HE_OK;
     const bool tiled = h->tiled && h->path >= 1;
     if (precision == HE_C128) {
         const double2 beta = mk<double>(beta_re, beta_im), gamma = mk<double>(gamma_re, gamma_im);
-        if (tiled) {
-            if (velocity && (s = velocity_scratch<double>(h, h->w64))) return g_status = s;
-            s = he::launch_hpsi_tiled<double>(h, h->t64, h->p64, h->coef64, h->w64[0], h->w64[1],
-                                              static_cast<const double2 *>(psi), static_cast<double2 *>(out), field,
-                                              velocity, beta, gamma, st);
+        const double2 *x = static_cast<const double2 *>(psi);
+        double2 *y = static_cast<double2 *>(out);
+        if (velocity && tiled && (s = velocity_scratch<double>(h, h->w64, fb.count))) return g_status = s;
+        if (tiled && (fb.count == 1 || he::tiled_batchable<double>(h, psi, velocity))) {
+            s = he::launch_hpsi_tiled<double>(h, h->t64, h->p64, h->coef64, h->w64[0], h->w64[1], x, y, fb, velocity,
+                                              beta, gamma, st);
         } else {
-            s = he::launch_hpsi<double>(h->t64, static_cast<const double2 *>(psi), static_cast<double2 *>(out), field,
-                                        velocity, beta, gamma, st);
+            for (int b = 0; b < fb.count && !s; ++b) {   // one instance at a time
+                he::FieldBatch one{1, {}};
+                for (int a = 0; a < 3; ++a) one.f[0][a] = fb.f[b][a];
+                s = tiled ? he::launch_hpsi_tiled<double>(h, h->t64, h->p64, h->coef64, h->w64[0], h->w64[1],
+                                                          x + b * N, y + b * N, one, velocity, beta, gamma, st)
+                          : he::launch_hpsi<double>(h->t64, x + b * N, y + b * N, one.f[0], velocity, beta, gamma, st);
+            }
         }
     } else if (precision == HE_C64) {
         if (!h->has32) return he_fail(HE_ERR_UNSUPPORTED, "handle built without complex64 tables", __FILE__, __LINE__);
         const float2 beta = mk<float>((float)beta_re, (float)beta_im), gamma = mk<float>((float)gamma_re, (float)gamma_im);
-        if (tiled) {
-            if (velocity && (s = velocity_scratch<float>(h, h->w32))) return g_status = s;
-            s = he::launch_hpsi_tiled<float>(h, h->t32, h->p32, h->coef32, h->w32[0], h->w32[1],
-                                             static_cast<const float2 *>(psi), static_cast<float2 *>(out), field,
-                                             velocity, beta, gamma, st);
+        const float2 *x = static_cast<const float2 *>(psi);
+        float2 *y = static_cast<float2 *>(out);
+        if (velocity && tiled && (s = velocity_scratch<float>(h, h->w32, fb.count))) return g_status = s;
+        if (tiled && (fb.count == 1 || he::tiled_batchable<float>(h, psi, velocity))) {
+            s = he::launch_hpsi_tiled<float>(h, h->t32, h->p32, h->coef32, h->w32[0], h->w32[1], x, y, fb, velocity,
+                                             beta, gamma, st);
         } else {
-            s = he::launch_hpsi<float>(h->t32, static_cast<const float2 *>(psi), static_cast<float2 *>(out), field,
-                                       velocity, beta, gamma, st);
+            for (int b = 0; b < fb.count && !s; ++b) {
+                he::FieldBatch one{1, {}};
+                for (int a = 0; a < 3; ++a) one.f[0][a] = fb.f[b][a];
+                s = tiled ? he::launch_hpsi_tiled<float>(h, h->t32, h->p32, h->coef32, h->w32[0], h->w32[1],
+                                                         x + b * N, y + b * N, one, velocity, beta, gamma, st)
+                          : he::launch_hpsi<float>(h->t32, x + b * N, y + b * N, one.f[0], velocity, beta, gamma, st);
+            }
         }
     } else {
         return he_fail(HE_ERR_ARG, "precision must be HE_C128 or HE_C64", __FILE__, __LINE__);
@@ -397,12 +426,32 @@ int apply_common(he_handle h, const void *psi, void *out, const double *field, i
     g_status = s;
     return s;
 }
+
+he::FieldBatch single_field(const double *field)
+{
+    he::FieldBatch fb{1, {}};
+    for (int a = 0; a < 3; ++a) fb.f[0][a] = field[a];
+    return fb;
+}
 }  // namespace
 
 extern "C" int he_apply(he_handle h, const void *psi, void *out, const double *field, int velocity, int precision,
                         void *stream)
 {
-    return apply_common(h, psi, out, field, velocity, precision, 0.0, 0.0, 1.0, 0.0, stream);
+    if (!field) return he_fail(HE_ERR_ARG, "null argument", __FILE__, __LINE__);
+    return apply_common(h, psi, out, single_field(field), velocity, precision, 0.0, 0.0, 1.0, 0.0, stream);
+}
+
+extern "C" int he_apply_batched(he_handle h, int count, const void *psi, void *out, const double *fields, int velocity,
+                                int precision, void *stream)
+{
+    if (!fields) return he_fail(HE_ERR_ARG, "null argument", __FILE__, __LINE__);
+    if (count < 1 || count > he::HE_BATCH_MAX)
+        return he_fail(HE_ERR_ARG, "batch count must be between 1 and 64", __FILE__, __LINE__);
+    he::FieldBatch fb{count, {}};
+    for (int b = 0; b < count; ++b)
+        for (int a = 0; a < 3; ++a) fb.f[b][a] = fields[3 * b + a];
+    return apply_common(h, psi, out, fb, velocity, precision, 0.0, 0.0, 1.0, 0.0, stream);
 }
 
 extern "C" int he_apply_shifted(he_handle h, const void *psi, void *out, const double *field, int velocity,
@@ -410,7 +459,8 @@ extern "C" int he_apply_shifted(he_handle h, const void *psi, void *out, const d
 {
     // psi + i alpha (H psi - e_ref psi) = (1 - i alpha e_ref) psi + (i alpha) H psi
     const double ga_re = -alpha_im, ga_im = alpha_re;     // i*alpha
-    return apply_common(h, psi, out, field, velocity, precision, 1.0 - ga_re * e_ref, -ga_im * e_ref, ga_re, ga_im,
+    if (!field) return he_fail(HE_ERR_ARG, "null argument", __FILE__, __LINE__);
+    return apply_common(h, psi, out, single_field(field), velocity, precision, 1.0 - ga_re * e_ref, -ga_im * e_ref, ga_re, ga_im,
                         stream);
 }
 

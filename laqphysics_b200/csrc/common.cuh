@@ -74,6 +74,14 @@ __device__ __forceinline__ double2 warp_fixed_sum(const double2* p, int nb, size
 // (the reference's Fortran order, src/kernels.f90:125).
 // ---------------------------------------------------------------------------------
 namespace he {
+// Fields of a batch of instances that share one operator (passed by value to kernels):
+// instance b of a batched apply sees the field f[b][0..2]; a single apply has count 1.
+constexpr int HE_BATCH_MAX = 64;
+struct FieldBatch {
+    int count;
+    double f[HE_BATCH_MAX][3];
+};
+
 template <typename R> struct DeviceTables {
     int n, nc, nt, nv, nd, nlam;
     int diag_separable;                 // 1: diag(i,j,c) = d1(i,c) + d2(j,c)

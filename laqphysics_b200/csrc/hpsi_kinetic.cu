@@ -382,43 +382,61 @@ __device__ __forceinline__ void cmma_ba(double (&cr)[2], double (&ci)[2], double
     }
 }
 
+// S element as complex FP64 (complex64 storage is widened exactly)
+__device__ __forceinline__ double2 s_load(const double2 *p) { return *p; }
+__device__ __forceinline__ double2 s_load(const float2 *p)
+{
+    const float2 v = *p;
+    return make_double2((double)v.x, (double)v.y);
+}
+
 // Electron 1 over the window of this warp's row group: block q covers columns j0 + (0..7).
-__device__ __forceinline__ void band_r1(const double2 *S, int P, int x0, int y0, int j0, int glo, int gks, bool real,
+template <typename C>
+__device__ __forceinline__ void band_r1(const C *S, int P, int x0, int y0, int j0, int glo, int gks, bool real,
                                         const double2 (&rf)[BAND_KS], int lr, int lk, double (&cr)[2], double (&ci)[2])
 {
-    const double2 *a = S + (j0 + lr - y0) * P + (glo + lk - x0);
+    const C *a = S + (j0 + lr - y0) * P + (glo + lk - x0);
 #pragma unroll
     for (int s = 0; s < BAND_KS; ++s)
-        if (s < gks) cmma_ab(cr, ci, a[4 * s], rf[s], real);
+        if (s < gks) cmma_ab(cr, ci, s_load(a + 4 * s), rf[s], real);
 }
 
 // Electron 2 over the window of column group gc, fragments `cf` (k-step major, 32 lanes).
-__device__ __forceinline__ void band_r2(const double2 *S, int P, int x0, int y0, int i0, int glo, int gks, bool real,
+template <typename C>
+__device__ __forceinline__ void band_r2(const C *S, int P, int x0, int y0, int i0, int glo, int gks, bool real,
                                         const double2 *cf, int lane, int lr, int lk, double (&cr)[2], double (&ci)[2])
 {
-    const double2 *b = S + (glo + lk - y0) * P + (i0 + lr - x0);
+    const C *b = S + (glo + lk - y0) * P + (i0 + lr - x0);
 #pragma unroll
     for (int s = 0; s < BAND_KS; ++s)
-        if (s < gks) cmma_ba(cr, ci, cf[s * 32 + lane], b[4 * s * P], real);
+        if (s < gks) cmma_ba(cr, ci, cf[s * 32 + lane], s_load(b + 4 * s * P), real);
 }
 
-template <bool VEL, bool SEP>
+template <typename R> __device__ __forceinline__ cplx<R> narrow(double re, double im) { return mk<R>((R)re, (R)im); }
+
+// Work items are (row tile, column tile, channel of the batch): the batch's instances are
+// consecutive blocks of nc channels, so instance b owns channels [b nc, (b + 1) nc) of the
+// 3-D TMA map and of every array.
+template <typename R, bool VEL, bool SEP>
 __global__ void __launch_bounds__(BAND_THREADS, 1)
-hpsi_band_kernel(const __grid_constant__ CUtensorMap tmap, const DeviceTables<double> t, const BandPlan<double> bp,
-                 double2 *__restrict__ out, double2 *__restrict__ w1, double2 *__restrict__ w2, double a2)
+hpsi_band_kernel(const __grid_constant__ CUtensorMap tmap, const DeviceTables<R> t, const BandPlan<R> bp,
+                 cplx<R> *__restrict__ out, cplx<R> *__restrict__ w1, cplx<R> *__restrict__ w2,
+                 const __grid_constant__ FieldBatch fb)
 {
+    typedef cplx<R> C;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char *smem = smem_raw + ((KIN_STAGE_ALIGN - (smem_u32(smem_raw) & (KIN_STAGE_ALIGN - 1))) & (KIN_STAGE_ALIGN - 1));
     double2 *CF = reinterpret_cast<double2 *>(smem + 2 * (size_t)bp.stage_bytes);   // [BAND_CG][BAND_KS][32]
     uint64_t *bar = reinterpret_cast<uint64_t *>(CF + BAND_CG * BAND_KS * 32);
-    const int n = bp.n, nc = bp.nc, P = bp.box_r, G = bp.ngroup;
+    constexpr int ALIGN = 16 / (int)sizeof(C);   // nodes per 16 bytes (TMA start alignment)
+    const int n = bp.n, nc = bp.nc, P = bp.box_r, G = bp.ngroup, nch = nc * fb.count;
     const size_t nn = (size_t)n * n;
-    const long long items = (long long)bp.ntr * bp.nct * nc;
+    const long long items = (long long)bp.ntr * bp.nct * nch;
     const long long per = (items + gridDim.x - 1) / gridDim.x;
     const long long first = (long long)blockIdx.x * per;
     const long long last = first + per < items ? first + per : items;
     if (first >= last) return;
-    const unsigned box_bytes = (unsigned)((size_t)P * bp.box_c * sizeof(double2));
+    const unsigned box_bytes = (unsigned)((size_t)P * bp.box_c * sizeof(C));
 
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
@@ -427,10 +445,11 @@ hpsi_band_kernel(const __grid_constant__ CUtensorMap tmap, const DeviceTables<do
     }
     __syncthreads();
     auto issue = [&](long long it, int stage) {
-        const long long tile = it / nc;
-        const int c = (int)(it % nc), tr = (int)(tile / bp.nct), tc = (int)(tile % bp.nct);
+        const long long tile = it / nch;
+        const int c = (int)(it % nch), tr = (int)(tile / bp.nct), tc = (int)(tile % bp.nct);
         mbar_expect_tx(bar + stage, box_bytes);
-        tma_load_3d(smem + (size_t)stage * bp.stage_bytes, &tmap, 2 * bp.brbase[tr], bp.bcbase[tc], c, bar + stage);
+        tma_load_3d(smem + (size_t)stage * bp.stage_bytes, &tmap, 2 * (bp.brbase[tr] / ALIGN * ALIGN), bp.bcbase[tc], c,
+                    bar + stage);
     };
     if (threadIdx.x == 0) issue(first, 0);
 
@@ -450,8 +469,9 @@ hpsi_band_kernel(const __grid_constant__ CUtensorMap tmap, const DeviceTables<do
             return;
         }
         if (threadIdx.x == 0 && it + 1 < last) issue(it + 1, stage ^ 1);
-        const long long tile = it / nc;
-        const int c = (int)(it % nc), tr = (int)(tile / bp.nct), tc = (int)(tile % bp.nct);
+        const long long tile = it / nch;
+        const int c = (int)(it % nch), tr = (int)(tile / bp.nct), tc = (int)(tile % bp.nct);
+        const int cc = c % nc, inst = c / nc;   // channel within its instance, instance
         if (tc != cur_tc) {   // CTA-uniform: stage the column groups' fragments
             for (int idx = threadIdx.x; idx < BAND_CG * BAND_KS * 32; idx += BAND_THREADS) {
                 const int g = tc * BAND_CG + idx / (BAND_KS * 32);
@@ -470,8 +490,8 @@ hpsi_band_kernel(const __grid_constant__ CUtensorMap tmap, const DeviceTables<do
             }
         }
         if (gr >= G) continue;
-        const double2 *S = reinterpret_cast<const double2 *>(smem + (size_t)stage * bp.stage_bytes);
-        const int x0 = bp.brbase[tr], y0 = bp.bcbase[tc], i0 = gr * BAND_G;
+        const C *S = reinterpret_cast<const C *>(smem + (size_t)stage * bp.stage_bytes);
+        const int x0 = bp.brbase[tr] / ALIGN * ALIGN, y0 = bp.bcbase[tc], i0 = gr * BAND_G;
         if (VEL) {   // commutator stencils W1 (electron 1), W2 (electron 2) with the B fragments
             double2 bf[BAND_KS];
 #pragma unroll
@@ -486,7 +506,7 @@ hpsi_band_kernel(const __grid_constant__ CUtensorMap tmap, const DeviceTables<do
 #pragma unroll
                 for (int u = 0; u < 2; ++u) {
                     const int i = i0 + 2 * lk + u, j = j0 + lr;
-                    if (i < n && j < n) w1[(size_t)i + (size_t)n * j + nn * c] = make_double2(cr[u], ci[u]);
+                    if (i < n && j < n) w1[(size_t)i + (size_t)n * j + nn * c] = narrow<R>(cr[u], ci[u]);
                 }
                 double dr[2] = {0, 0}, di[2] = {0, 0};
                 band_r2(S, P, x0, y0, i0, bp.glo[gc], bp.gks[gc], (bp.greal[gc] & 2) != 0,
@@ -494,10 +514,12 @@ hpsi_band_kernel(const __grid_constant__ CUtensorMap tmap, const DeviceTables<do
 #pragma unroll
                 for (int u = 0; u < 2; ++u) {
                     const int i = i0 + 2 * lk + u, j = j0 + lr;
-                    if (i < n && j < n) w2[(size_t)i + (size_t)n * j + nn * c] = make_double2(dr[u], di[u]);
+                    if (i < n && j < n) w2[(size_t)i + (size_t)n * j + nn * c] = narrow<R>(dr[u], di[u]);
                 }
             }
         }
+        const double *fv = fb.f[inst];
+        const double a2 = VEL ? fv[0] * fv[0] + fv[1] * fv[1] + fv[2] * fv[2] : 0.0;
 #pragma unroll
         for (int q = 0; q < BAND_CG; ++q) {
             const int gc = tc * BAND_CG + q, j0 = gc * BAND_G;
@@ -510,13 +532,13 @@ hpsi_band_kernel(const __grid_constant__ CUtensorMap tmap, const DeviceTables<do
             for (int u = 0; u < 2; ++u) {
                 const int i = i0 + 2 * lk + u, j = j0 + lr;
                 if (i < n && j < n) {
-                    const double2 x = S[(j - y0) * P + (i - x0)];
-                    const size_t p = (size_t)i + (size_t)n * j + nn * c;
-                    const double2 d = SEP ? cadd<double>(__ldg(t.d1 + i + (size_t)n * c), __ldg(t.d2 + j + (size_t)n * c))
-                                          : __ldg(t.diag + p);
-                    double2 v = cfma<double>(d, x, make_double2(cr[u], ci[u]));
+                    const double2 x = s_load(S + (j - y0) * P + (i - x0));
+                    const size_t p = (size_t)i + (size_t)n * j;
+                    const C dd = SEP ? cadd<R>(ldg<R>(t.d1 + i + (size_t)n * cc), ldg<R>(t.d2 + j + (size_t)n * cc))
+                                     : ldg<R>(t.diag + p + nn * cc);
+                    double2 v = cfma<double>(make_double2((double)dd.x, (double)dd.y), x, make_double2(cr[u], ci[u]));
                     if (VEL) v = rfma<double>(a2, x, v);
-                    out[p] = v;
+                    out[p + nn * c] = narrow<R>(v.x, v.y);
                 }
             }
         }
@@ -554,9 +576,11 @@ int sm_count(int device)
     return counts[device];
 }
 
-// TMA map of psi(re/im, r1, r2 channel) with a (2 box_r, box_c, 1) box, from the
+// TMA map of psi(re/im, r1, r2 channel) over nc channels (every instance of a batch) with a
+// (2 box_r, box_c, 1) box, keyed by (buffer, kind) in the
 // operator's cache of recently used buffers (a Krylov basis reuses the same few), else
-// encoded now.  Returns null when encoding fails.
+// encoded now; `kind` encodes the kernel family, precision and batch size.  Returns null
+// when encoding fails.
 const CUtensorMap *psi_map(he_operator *h, int kind, const void *psi, int n, int nc, int box_r, int box_c,
                            size_t real_bytes)
 {
@@ -610,25 +634,31 @@ int launch_kinetic(he_operator *h, const DeviceTables<R> &t, const KineticPlan<R
     return HE_OK;
 }
 
-bool band_usable(const BandPlan<double> &bp, const void *psi)
+// True when the banded kernel can stage `psi` with TMA: 16-byte aligned base and rows
+// (the r1 extent in bytes) a multiple of 16 bytes.
+template <typename R> bool band_usable(const BandPlan<R> &bp, const void *psi)
 {
-    return bp.ntr > 0 && (reinterpret_cast<uintptr_t>(psi) & 15) == 0 && tensor_map_encoder() != nullptr;
+    return bp.ntr > 0 && (reinterpret_cast<uintptr_t>(psi) & 15) == 0 && ((size_t)bp.n * sizeof(cplx<R>)) % 16 == 0 &&
+           tensor_map_encoder() != nullptr;
 }
 
-int launch_band(he_operator *h, const DeviceTables<double> &t, const BandPlan<double> &bp, const double2 *psi,
-                double2 *out, double2 *w1, double2 *w2, double a2, int velocity, cudaStream_t stream)
+template <typename R>
+int launch_band(he_operator *h, const DeviceTables<R> &t, const BandPlan<R> &bp, const cplx<R> *psi, cplx<R> *out,
+                cplx<R> *w1, cplx<R> *w2, const FieldBatch &fb, int velocity, cudaStream_t stream)
 {
-    const CUtensorMap *mp = psi_map(h, 0, psi, bp.n, bp.nc, bp.box_r, bp.box_c, sizeof(double));
+    const CUtensorMap *mp = psi_map(h, (sizeof(R) == 8 ? 0 : 3) + 8 * fb.count, psi, bp.n, bp.nc * fb.count, bp.box_r,
+                                    bp.box_c, sizeof(R));
     if (!mp) return he_fail(HE_ERR_CUDA, "cuTensorMapEncodeTiled failed", __FILE__, __LINE__);
     const CUtensorMap map = *mp;
     const size_t smem = 2 * (size_t)bp.stage_bytes + (size_t)BAND_CG * BAND_KS * 32 * sizeof(double2) + 16 + KIN_STAGE_ALIGN;
-    const long long items = (long long)bp.ntr * bp.nct * bp.nc;
-    const unsigned grid = (unsigned)std::min<long long>(items, (long long)sm_count(h->device));
+    const long long items = (long long)bp.ntr * bp.nct * bp.nc * fb.count;
+    const int per_sm = std::max(1, (int)((227 * 1024) / (smem + 1024)));
+    const unsigned grid = (unsigned)std::min<long long>(items, (long long)per_sm * sm_count(h->device));
 #define HE_BAND(V, S)                                                                                      \
     do {                                                                                                   \
-        auto kern = hpsi_band_kernel<V, S>;                                                                \
-        HE_CUDA_TRY(he_smem_limit(reinterpret_cast<const void *>(kern), smem));   \
-        kern<<<grid, BAND_THREADS, smem, stream>>>(map, t, bp, out, w1, w2, a2);                           \
+        auto kern = hpsi_band_kernel<R, V, S>;                                                             \
+        HE_CUDA_TRY(he_smem_limit(reinterpret_cast<const void *>(kern), smem));                            \
+        kern<<<grid, BAND_THREADS, smem, stream>>>(map, t, bp, out, w1, w2, fb);                           \
     } while (0)
     if (velocity) { if (t.diag_separable) HE_BAND(true, true); else HE_BAND(true, false); }
     else { if (t.diag_separable) HE_BAND(false, true); else HE_BAND(false, false); }
@@ -637,6 +667,12 @@ int launch_band(he_operator *h, const DeviceTables<double> &t, const BandPlan<do
     return HE_OK;
 }
 
+template bool band_usable<double>(const BandPlan<double> &, const void *);
+template bool band_usable<float>(const BandPlan<float> &, const void *);
+template int launch_band<double>(he_operator *, const DeviceTables<double> &, const BandPlan<double> &, const double2 *,
+                                 double2 *, double2 *, double2 *, const FieldBatch &, int, cudaStream_t);
+template int launch_band<float>(he_operator *, const DeviceTables<float> &, const BandPlan<float> &, const float2 *,
+                                float2 *, float2 *, float2 *, const FieldBatch &, int, cudaStream_t);
 template bool kinetic_usable<double>(const KineticPlan<double> &, const void *);
 template bool kinetic_usable<float>(const KineticPlan<float> &, const void *);
 template int launch_kinetic<double>(he_operator *, const DeviceTables<double> &, const KineticPlan<double> &,

@@ -34,12 +34,14 @@ constexpr int BAND_WARPS = BAND_TR / BAND_G;
 constexpr int BAND_THREADS = 32 * BAND_WARPS;
 constexpr int BAND_CG = BAND_TC / BAND_G;
 
+// Storage precision R (complex128 or complex64 psi); the fragments and the tensor-core
+// arithmetic are FP64 in both.
 template <typename R> struct BandPlan {
     int n, nc, ngroup, ntr, nct, box_r, box_c;
     int stage_bytes;
     const int *glo, *gks, *greal;                // per group
     const int *brbase, *bcbase;                  // per tile
-    const cplx<R> *frag, *fragb;                 // [group][BAND_KS][32]
+    const double2 *frag, *fragb;                 // [group][BAND_KS][32]
     int *err;
 };
 

@@ -532,22 +532,30 @@ template <typename R> size_t mix_smem(int nc, int nlam, int ng, int nwide, int n
     return c + r + i + 64;
 }
 
+// True when a batch of fb.count > 1 instances can run as one launch per kernel (banded
+// kinetic kernel and generated mixing kernel); otherwise the caller applies the
+// instances one at a time.
+template <typename R> bool tiled_batchable(he_operator *h, const void *psi, int velocity)
+{
+    return h->path == 1 && band_usable<R>(band_plan<R>(h), psi) && h->mixpath == 1 &&
+           jit_mix_prepare(h, (sizeof(R) == 8 ? 0 : 2) + (velocity ? 1 : 0)) == HE_OK;
+}
+
 template <typename R>
 int launch_hpsi_tiled(he_operator *h, const DeviceTables<R> &t, const TiledPlan<R> &pl, cplx<R> *coef,
-                      cplx<R> *w1, cplx<R> *w2, const cplx<R> *psi, cplx<R> *out, const double *field, int velocity,
+                      cplx<R> *w1, cplx<R> *w2, const cplx<R> *psi, cplx<R> *out, const FieldBatch &fb, int velocity,
                       cplx<R> beta, cplx<R> gamma, cudaStream_t stream)
 {
     (void)coef;
+    const double *field = fb.f[0];
+    if (fb.count > 1 && !tiled_batchable<R>(h, psi, velocity))
+        return he_fail(HE_ERR_UNSUPPORTED, "batched apply needs the banded and generated kernels", __FILE__, __LINE__);
     const R f0 = (R)field[0], f1 = (R)field[1], f2 = (R)field[2];
     const R a2 = (R)(field[0] * field[0] + field[1] * field[1] + field[2] * field[2]);
     const KineticPlan<R> &kp = kinetic_plan<R>(h);
-    bool band = false;
-    if constexpr (sizeof(R) == 8) band = h->path == 1 && band_usable(h->b64, psi);
-    if (band) {
-        if constexpr (sizeof(R) == 8) {
-            const int s = launch_band(h, t, h->b64, psi, out, w1, w2, a2, velocity, stream);
-            if (s) return s;
-        }
+    if (h->path == 1 && band_usable<R>(band_plan<R>(h), psi)) {
+        const int s = launch_band<R>(h, t, band_plan<R>(h), psi, out, w1, w2, fb, velocity, stream);
+        if (s) return s;
     } else if ((h->path == 1 || h->path == 3) && kinetic_usable<R>(kp, psi)) {
         const int s = launch_kinetic<R>(h, t, kp, psi, out, w1, w2, a2, velocity, stream);
         if (s) return s;
@@ -558,7 +566,7 @@ int launch_hpsi_tiled(he_operator *h, const DeviceTables<R> &t, const TiledPlan<
 #define HE_RADIAL(V, S)                                                                                  \
     do {                                                                                                 \
         auto kern = hpsi_radial_kernel<R, V, S>;                                                         \
-        HE_CUDA_TRY(he_smem_limit(reinterpret_cast<const void *>(kern), rs));   \
+        HE_CUDA_TRY(he_smem_limit(reinterpret_cast<const void *>(kern), rs));                            \
         kern<<<rgrid, RAD_THREADS, rs, stream>>>(t, pl, psi, out, w1, w2, a2, blkmax);                   \
     } while (0)
         if (velocity) { if (t.diag_separable) HE_RADIAL(true, true); else HE_RADIAL(true, false); }
@@ -567,7 +575,7 @@ int launch_hpsi_tiled(he_operator *h, const DeviceTables<R> &t, const TiledPlan<
         HE_CUDA_TRY(cudaGetLastError());
     }
     if (h->mixpath == 1 && jit_mix_prepare(h, (sizeof(R) == 8 ? 0 : 2) + (velocity ? 1 : 0)) == HE_OK)
-        return launch_mix_jit<R>(h, t, psi, out, w1, w2, field, velocity, beta, gamma, stream);
+        return launch_mix_jit<R>(h, t, psi, out, w1, w2, fb, velocity, beta, gamma, stream);
     const size_t nn = (size_t)pl.n * pl.n;
     const size_t ms = mix_smem<R>(pl.nc, pl.nlam, pl.ng, pl.nwide, pl.nwd);
     const size_t ntiles = (nn + MIX_NP - 1) / MIX_NP;
@@ -585,11 +593,13 @@ int launch_hpsi_tiled(he_operator *h, const DeviceTables<R> &t, const TiledPlan<
     return HE_OK;
 }
 
+template bool tiled_batchable<double>(he_operator *, const void *, int);
+template bool tiled_batchable<float>(he_operator *, const void *, int);
 template int launch_hpsi_tiled<double>(he_operator *, const DeviceTables<double> &, const TiledPlan<double> &,
-                                       double2 *, double2 *, double2 *, const double2 *, double2 *, const double *,
+                                       double2 *, double2 *, double2 *, const double2 *, double2 *, const FieldBatch &,
                                        int, double2, double2, cudaStream_t);
 template int launch_hpsi_tiled<float>(he_operator *, const DeviceTables<float> &, const TiledPlan<float> &, float2 *,
-                                      float2 *, float2 *, const float2 *, float2 *, const double *, int, float2,
+                                      float2 *, float2 *, const float2 *, float2 *, const FieldBatch &, int, float2,
                                       float2, cudaStream_t);
 
 // Both kernels must fit in shared memory (one CTA per SM) in complex128.

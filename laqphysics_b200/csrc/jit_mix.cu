@@ -38,6 +38,7 @@ namespace he {
 namespace {
 
 const char *kPrelude = R"(// generated channel-mixing kernel
+struct FieldBatch { int count; double f[HE_BATCH_MAX][3]; };
 struct __align__(16) cd { double x, y; };
 struct __align__(8) cf { float x, y; };
 template <typename R> struct cx;
@@ -90,8 +91,13 @@ std::string mix_source(const he_plan_host &P, bool dipole_real, int variant)
          "    const typename cx<R>::T *__restrict__ rad, const typename cx<R>::T *__restrict__ rt,\n"
          "    const typename cx<R>::T *__restrict__ w1, const typename cx<R>::T *__restrict__ w2,\n"
          "    const typename cx<R>::T *__restrict__ dcoef, const R *__restrict__ ldiff, long long nn, int n, int nd,\n"
-         "    R f0, R f1, R f2, typename cx<R>::T beta, typename cx<R>::T gamma)\n{\n"
+         "    int nc, const FieldBatch &fs, typename cx<R>::T beta, typename cx<R>::T gamma)\n{\n"
          "    typedef typename cx<R>::T C;\n"
+         "    // instance blockIdx.z of a batch: its own field and its block of nc channels\n"
+         "    const long long shift = (long long)blockIdx.z * nc * nn;\n"
+         "    psi += shift; out += shift;\n"
+         "    if (VEL) { w1 += shift; w2 += shift; }\n"
+         "    const R f0 = (R)fs.f[blockIdx.z][0], f1 = (R)fs.f[blockIdx.z][1], f2 = (R)fs.f[blockIdx.z][2];\n"
          "    extern __shared__ __align__(16) unsigned char smem_raw[];\n"
          "    C *K = reinterpret_cast<C *>(smem_raw), *KW = K + nd;\n"
          "    for (int k = threadIdx.x; k < nd; k += blockDim.x) {\n"
@@ -195,7 +201,7 @@ std::string mix_source(const he_plan_host &P, bool dipole_real, int variant)
     }
     const std::string group_fns = o.str();
     o.str("");
-    o << kPrelude << group_fns << body;
+    o << "#define HE_BATCH_MAX " << HE_BATCH_MAX << "\n" << kPrelude << group_fns << body;
     if (variant == -1)
         for (int v = 0; v < 4; ++v) o << mix_entry(v);
     else if (variant >= 0)
@@ -211,11 +217,11 @@ std::string mix_entry(int v)
     const char *R = dbl ? "double" : "float", *C = dbl ? "cd" : "cf";
     std::ostringstream o;
     o << "extern \"C\" __global__ void __launch_bounds__(128, " << (dbl ? MIXJ_MIN_BLOCKS_D : MIXJ_MIN_BLOCKS_F) << ") "
-      << names[v] << "(const " << C << " *psi, " << C
-      << " *out, const " << C << " *rad, const " << C << " *rt, const " << C << " *w1, const " << C << " *w2, const "
-      << C << " *dcoef, const " << R << " *ldiff, long long nn, int n, int nd, " << R << " f0, " << R << " f1, " << R
-      << " f2, " << C << " beta, " << C << " gamma)\n{ mix_body<" << R << ", " << (vel ? "true" : "false")
-      << ">(psi, out, rad, rt, w1, w2, dcoef, ldiff, nn, n, nd, f0, f1, f2, beta, gamma); }\n";
+      << names[v] << "(const " << C << " *psi, " << C << " *out, const " << C << " *rad, const " << C << " *rt, const " << C
+      << " *w1, const " << C << " *w2, const " << C << " *dcoef, const " << R
+      << " *ldiff, long long nn, int n, int nd, int nc, const FieldBatch fs, " << C << " beta, " << C
+      << " gamma)\n{ mix_body<" << R << ", " << (vel ? "true" : "false")
+      << ">(psi, out, rad, rt, w1, w2, dcoef, ldiff, nn, n, nd, nc, fs, beta, gamma); }\n";
     return o.str();
 }
 
@@ -344,31 +350,31 @@ int jit_mix_prepare(he_operator *h, int variant)
 
 template <typename R>
 int launch_mix_jit(he_operator *h, const DeviceTables<R> &t, const cplx<R> *psi, cplx<R> *out, const cplx<R> *w1,
-                   const cplx<R> *w2, const double *field, int velocity, cplx<R> beta, cplx<R> gamma,
+                   const cplx<R> *w2, const FieldBatch &fb, int velocity, cplx<R> beta, cplx<R> gamma,
                    cudaStream_t stream)
 {
     const cudaKernel_t k = static_cast<cudaKernel_t>(h->mix_kern[(sizeof(R) == 8 ? 0 : 2) + (velocity ? 1 : 0)]);
     const cplx<R> *rt = velocity ? t.hinv : t.r;
     long long nn = (long long)t.n * t.n;
-    int n = t.n, nd = t.nd;
-    R f0 = (R)field[0], f1 = (R)field[1], f2 = (R)field[2];
+    int n = t.n, nd = t.nd, nc = t.nc;
     const cplx<R> *dcoef = t.dcoef;
     const R *ldiff = t.ldiff;
     void *args[] = {(void *)&psi, (void *)&out, (void *)&t.rad, (void *)&rt, (void *)&w1, (void *)&w2,
-                    (void *)&dcoef, (void *)&ldiff, &nn, &n, &nd, &f0, &f1, &f2, &beta, &gamma};
+                    (void *)&dcoef, (void *)&ldiff, &nn, &n, &nd, &nc, (void *)&fb, &beta, &gamma};
     const unsigned point_blocks = (unsigned)std::min<long long>((nn + 127) / 128, 65535);
     const size_t smem = 2 * (size_t)std::max(nd, 1) * sizeof(cplx<R>);
-    const bool one_thread_per_point = point_blocks >= 8u * (unsigned)sm_count(h->device);
-    const dim3 grid(one_thread_per_point ? 1u : (unsigned)h->plan.mix.size(), point_blocks);
+    const bool one_thread_per_point = (long long)point_blocks * fb.count >= 8LL * sm_count(h->device);
+    const dim3 grid(one_thread_per_point ? 1u : (unsigned)h->plan.mix.size(), point_blocks, (unsigned)fb.count);
     HE_CUDA_TRY(cudaLaunchKernel(reinterpret_cast<const void *>(k), grid, dim3(128), args, smem, stream));
     return HE_OK;
 }
 
 template int launch_mix_jit<double>(he_operator *, const DeviceTables<double> &, const double2 *, double2 *,
-                                    const double2 *, const double2 *, const double *, int, double2, double2,
+                                    const double2 *, const double2 *, const FieldBatch &, int, double2, double2,
                                     cudaStream_t);
 template int launch_mix_jit<float>(he_operator *, const DeviceTables<float> &, const float2 *, float2 *,
-                                   const float2 *, const float2 *, const double *, int, float2, float2, cudaStream_t);
+                                   const float2 *, const float2 *, const FieldBatch &, int, float2, float2,
+                                   cudaStream_t);
 
 }  // namespace he
 

@@ -21,6 +21,7 @@ struct he_operator {
     he::KineticPlan<double> k64{};      // kinetic-kernel plan (ntr == 0: not usable)
     he::KineticPlan<float> k32{};
     he::BandPlan<double> b64{};         // banded FP64 tensor-core kinetic plan (ntr == 0: not usable)
+    he::BandPlan<float> b32{};          // the same for complex64 storage
     int *kerr = nullptr;                // device error word of the kinetic kernel
     struct TensorMapEntry {             // encoded TMA maps of recently used psi buffers
         const void *base = nullptr;
@@ -33,6 +34,7 @@ struct he_operator {
     float2 *coef32 = nullptr;
     double2 *w64[2] = {nullptr, nullptr};   // velocity gauge B-stencil scratch (n*n*nc each)
     float2 *w32[2] = {nullptr, nullptr};
+    int wcap64 = 0, wcap32 = 0;         // instances the velocity-gauge scratch holds
     const double2 *tdiag = nullptr;     // diagonal of the kinetic CSR (n entries)
     he_plan_host plan;
     int mixpath = 1;                    // 1: generated (NVRTC) mixing kernel when it compiles, 0: table-driven kernel
@@ -52,8 +54,9 @@ bool he_build_plan(he_plan_host &P, int n, int nc, const int *ptr, const int *co
 namespace he {
 template <typename R>
 int launch_hpsi_tiled(he_operator *h, const DeviceTables<R> &t, const TiledPlan<R> &pl, cplx<R> *coef, cplx<R> *w1,
-                      cplx<R> *w2, const cplx<R> *psi, cplx<R> *out, const double *field, int velocity,
+                      cplx<R> *w2, const cplx<R> *psi, cplx<R> *out, const FieldBatch &fb, int velocity,
                       cplx<R> beta, cplx<R> gamma, cudaStream_t stream);
+template <typename R> bool tiled_batchable(he_operator *h, const void *psi, int velocity);
 bool tiled_fits(const he_plan_host &P, int nc, int nd);
 template <typename R> bool kinetic_usable(const KineticPlan<R> &kp, const void *psi);
 template <typename R>
@@ -64,11 +67,15 @@ std::string mix_source(const he_plan_host &P, bool dipole_real, int variant);
 int jit_mix_prepare(he_operator *h, int variant);
 template <typename R>
 int launch_mix_jit(he_operator *h, const DeviceTables<R> &t, const cplx<R> *psi, cplx<R> *out, const cplx<R> *w1,
-                   const cplx<R> *w2, const double *field, int velocity, cplx<R> beta, cplx<R> gamma,
+                   const cplx<R> *w2, const FieldBatch &fb, int velocity, cplx<R> beta, cplx<R> gamma,
                    cudaStream_t stream);
-bool band_usable(const BandPlan<double> &bp, const void *psi);
-int launch_band(he_operator *h, const DeviceTables<double> &t, const BandPlan<double> &bp, const double2 *psi,
-                double2 *out, double2 *w1, double2 *w2, double a2, int velocity, cudaStream_t stream);
+template <typename R> bool band_usable(const BandPlan<R> &bp, const void *psi);
+template <typename R>
+int launch_band(he_operator *h, const DeviceTables<R> &t, const BandPlan<R> &bp, const cplx<R> *psi, cplx<R> *out,
+                cplx<R> *w1, cplx<R> *w2, const FieldBatch &fb, int velocity, cudaStream_t stream);
+template <typename R> inline const BandPlan<R> &band_plan(const he_operator *h);
+template <> inline const BandPlan<double> &band_plan<double>(const he_operator *h) { return h->b64; }
+template <> inline const BandPlan<float> &band_plan<float>(const he_operator *h) { return h->b32; }
 template <typename R> inline const KineticPlan<R> &kinetic_plan(const he_operator *h);
 template <> inline const KineticPlan<double> &kinetic_plan<double>(const he_operator *h) { return h->k64; }
 template <> inline const KineticPlan<float> &kinetic_plan<float>(const he_operator *h) { return h->k32; }

@@ -171,6 +171,22 @@ class B200Hamiltonian:
         return out
 
     @torch.no_grad()
+    def apply_batched(self, x, fields, velocity=True, out=None, precision=None):
+        """out[b] = H(fields[b]) x[b] for a batch of instances sharing this operator:
+        x is (count, size) (or count*size) complex128/complex64, fields is (count, 3)."""
+        code, dtype = PRECISIONS[precision or ('complex128' if x.dtype == torch.complex128 else 'complex64')]
+        f = np.ascontiguousarray(fields, dtype=np.float64).reshape(-1, 3)
+        count = f.shape[0]
+        if x.device != self.device or x.dtype != dtype or not x.is_contiguous() or x.numel() != count * self.size:
+            raise ValueError(f'batch must be a contiguous {dtype} tensor of {count} x {self.size} elements on {self.device}')
+        if out is None:
+            out = torch.empty_like(x)
+        check(LIB.he_apply_batched(self.op.handle, count, ct.c_void_p(x.data_ptr()), ct.c_void_p(out.data_ptr()),
+                                   ptr(f), int(bool(velocity)), code, _stream(self.device)), 'he_apply_batched')
+        self.apply_count += count
+        return out
+
+    @torch.no_grad()
     def apply_shifted(self, x, field, alpha, reference_energy=0., velocity=True, out=None):
         """out = x + i*alpha*(H(field) x - E_ref x): the Pade operator of python/implicit.py:77-84."""
         code, dtype = PRECISIONS['complex128' if x.dtype == torch.complex128 else 'complex64']

@@ -198,3 +198,26 @@ def test_apply_rejects_wrong_dtype_and_size():
         op.apply(torch.zeros(op.size, dtype=torch.complex64, device=DEVICE), precision='complex128')
     with pytest.raises(ValueError):
         op.apply(torch.zeros(op.size + 1, dtype=torch.complex128, device=DEVICE))
+
+
+@pytest.mark.parametrize('velocity', [False, True])
+def test_batched_apply_matches_single_applies(velocity):
+    """he_apply_batched (one launch per kernel for the whole batch) against one apply per
+    instance, complex128 and complex64, instances with different fields."""
+    from laqphysics_b200.workloads import arnoldi_small, seeded_state
+    h = arnoldi_small()
+    op = engine(h)
+    count = 5
+    rng = np.random.default_rng(31)
+    fields = np.zeros((count, 3))
+    fields[:, 2] = rng.uniform(.005, .03, count)
+    x = torch.stack([op.state(seeded_state(h.size, 100 + b)) for b in range(count)])
+    for dtype, precision, tol in ((torch.complex128, 'complex128', 1e-14), (torch.complex64, 'complex64', 1e-6)):
+        xb = x.to(dtype).contiguous()
+        y = op.apply_batched(xb, fields, velocity, precision=precision)
+        for b in range(count):
+            yb = op.apply(xb[b].contiguous(), fields[b], velocity, precision=precision)
+            assert rel_l2(op.host(y[b]).astype(complex), op.host(yb).astype(complex)) < tol, (precision, b)
+        ref = cpu.tensor_apply(h, op.host(x[count - 1]), fields[count - 1], velocity)
+        assert rel_l2(op.host(y[count - 1]).astype(complex), ref) < (1e-13 if precision == 'complex128' else C64_REL_L2)
+    op.synchronize()
