@@ -148,6 +148,19 @@ int he_expv(he_krylov_handle k, he_handle op, const void *x, void *y, const doub
 int he_expv_mixed(he_krylov_handle k, he_handle op, const void *x, void *y, const double *field, int velocity,
                   double dt, double tol, int maxdim, int *dimension, double *estimate, void *stream);
 
+/* Batched Arnoldi exponential: `count` (<= 64) instances that share the operator and the
+ * time step, each with its own field (fields[3b..3b+2]), start vector and Krylov space,
+ * advanced together (one launch per kernel per iteration for the whole batch).  The
+ * workspace comes from he_krylov_create_batched (n = one instance's length); x and y hold
+ * the instances one after another.  dimension/estimate/converged (optional, count
+ * entries) report each instance; HE_ERR_NOCONV when any instance did not converge (its y
+ * is untouched, the others are written).  precision as in he_apply.  The reference steps
+ * one state at a time (python/propagate.py:6-50); this batches its parameter scans. */
+int he_krylov_create_batched(he_krylov_handle *out, long long n, int maxdim, int count);
+int he_expv_batched(he_krylov_handle k, he_handle op, const void *x, void *y, const double *fields, int velocity,
+                    double dt, double tol, int maxdim, int precision, int *dimension, double *estimate,
+                    int *converged, void *stream);
+
 /* ------------------------------------------------------------------------------------
  * GMRES / CF4 building blocks (python/implicit.py:45-109).  The GMRES driver keeps its
  * Krylov basis in an he_krylov workspace (Q, and Z when flexible), orthogonalises with

@@ -43,6 +43,8 @@ SIGNATURES = {
     'he_krylov_combine': (I, [P, I, P, P]),
     'he_expv': (I, [P, P, P, P, P, I, D, D, I, ct.POINTER(I), ct.POINTER(D), P]),
     'he_expv_mixed': (I, [P, P, P, P, P, I, D, D, I, ct.POINTER(I), ct.POINTER(D), P]),
+    'he_krylov_create_batched': (I, [ct.POINTER(P), ct.c_longlong, I, I]),
+    'he_expv_batched': (I, [P, P, P, P, P, I, D, D, I, I, P, P, P, P]),
     'he_set_path': (I, [P, I]),
     'he_device_status': (I, [P]),
     'he_set_mix': (I, [P, I]),

@@ -53,12 +53,20 @@ __device__ __forceinline__ void block_sum(double2 (&acc)[KT], double2 *out)
     }
 }
 
+// Batched workspaces: instance b (blockIdx.y of the vector kernels, blockIdx.x of the
+// one-CTA-per-instance kernels) owns vector k of the basis at Q + k*qs + b*n (qs = count*n,
+// so basis vector k of every instance is one contiguous block), and its own slices of
+// H, partial sums, projections, coefficients, scratch and status.
+
 // partial[b*ld + k0 + k] = sum over this block's elements of conj(Q_{k0+k}) v
 template <int KT>
 __global__ void __launch_bounds__(KRYLOV_THREADS)
-multidot_kernel(const double2 *__restrict__ Q, size_t n, int k0, int kc, const double2 *__restrict__ v,
+multidot_kernel(const double2 *__restrict__ Q, size_t n, size_t qs, int k0, int kc, const double2 *__restrict__ v,
                 double2 *__restrict__ partial, int ld, const KrylovStatus *st)
 {
+    const int inst = blockIdx.y;
+    Q += inst * n; v += inst * n; partial += (size_t)inst * gridDim.x * ld;
+    if (st) st += inst;
     if (st && st->done) return;
     double2 acc[KT];
 #pragma unroll
@@ -67,7 +75,7 @@ multidot_kernel(const double2 *__restrict__ Q, size_t n, int k0, int kc, const d
         const double2 x = v[p];
 #pragma unroll
         for (int k = 0; k < KT; ++k)
-            if (k < kc) acc[k] = cfma_conj<double>(Q[(size_t)(k0 + k) * n + p], x, acc[k]);
+            if (k < kc) acc[k] = cfma_conj<double>(Q[(size_t)(k0 + k) * qs + p], x, acc[k]);
     }
     __shared__ double2 res[KT];
     block_sum<KT>(acc, res);
@@ -78,8 +86,13 @@ multidot_kernel(const double2 *__restrict__ Q, size_t n, int k0, int kc, const d
 // z[k] = sum_b partial[b*ld + k] for k < kc (fixed order, one warp per k); optionally
 // H[k] += z[k].
 __global__ void reduce_partials_kernel(const double2 *__restrict__ partial, int nb, int ld, int kc,
-                                       double2 *__restrict__ z, double2 *__restrict__ hcol, const KrylovStatus *st)
+                                       double2 *__restrict__ z, double2 *__restrict__ hcol, size_t hs,
+                                       const KrylovStatus *st)
 {
+    const int inst = blockIdx.x;
+    partial += (size_t)inst * nb * ld; z += (size_t)inst * ld;
+    if (hcol) hcol += inst * hs;
+    if (st) st += inst;
     if (st && st->done) return;
     const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     for (int k = warp; k < kc; k += nwarps) {
@@ -93,9 +106,13 @@ __global__ void reduce_partials_kernel(const double2 *__restrict__ partial, int 
 
 // v -= sum_k Q_k z_k ; optionally per-block |v|^2 partial sums.
 __global__ void __launch_bounds__(KRYLOV_THREADS)
-update_kernel(const double2 *__restrict__ Q, size_t n, int kc, const double2 *__restrict__ z, double2 *__restrict__ v,
-              double *__restrict__ norm_partial, const KrylovStatus *st)
+update_kernel(const double2 *__restrict__ Q, size_t n, size_t qs, int kc, const double2 *__restrict__ z, int ld,
+              double2 *__restrict__ v, double *__restrict__ norm_partial, const KrylovStatus *st)
 {
+    const int inst = blockIdx.y;
+    Q += inst * n; v += inst * n; z += (size_t)inst * ld;
+    if (norm_partial) norm_partial += (size_t)inst * gridDim.x;
+    if (st) st += inst;
     if (st && st->done) return;
     __shared__ double2 zs[KRYLOV_MAXDIM + 1];
     for (int k = threadIdx.x; k < kc; k += blockDim.x) zs[k] = z[k];
@@ -104,7 +121,7 @@ update_kernel(const double2 *__restrict__ Q, size_t n, int kc, const double2 *__
     for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
         double2 x = v[p];
         for (int k = 0; k < kc; ++k) {
-            const double2 q = Q[(size_t)k * n + p];
+            const double2 q = Q[(size_t)k * qs + p];
             x = cfma<double>(mk<double>(-zs[k].x, -zs[k].y), q, x);
         }
         v[p] = x;
@@ -129,9 +146,12 @@ update_kernel(const double2 *__restrict__ Q, size_t n, int kc, const double2 *__
 // update_kernel followed by multidot_kernel, so the results are identical.
 template <int KT>
 __global__ void __launch_bounds__(KRYLOV_THREADS)
-update_multidot_kernel(const double2 *__restrict__ Q, size_t n, int kc, const double2 *__restrict__ z,
+update_multidot_kernel(const double2 *__restrict__ Q, size_t n, size_t qs, int kc, const double2 *__restrict__ z,
                        double2 *__restrict__ v, double2 *__restrict__ partial, int ld, const KrylovStatus *st)
 {
+    const int inst = blockIdx.y;
+    Q += inst * n; v += inst * n; z += (size_t)inst * ld; partial += (size_t)inst * gridDim.x * ld;
+    if (st) st += inst;
     if (st && st->done) return;
     __shared__ double2 zs[KT];
     for (int k = threadIdx.x; k < kc; k += blockDim.x) zs[k] = z[k];
@@ -143,11 +163,11 @@ update_multidot_kernel(const double2 *__restrict__ Q, size_t n, int kc, const do
         double2 x = v[p];
 #pragma unroll
         for (int k = 0; k < KT; ++k)
-            if (k < kc) x = cfma<double>(mk<double>(-zs[k].x, -zs[k].y), Q[(size_t)k * n + p], x);
+            if (k < kc) x = cfma<double>(mk<double>(-zs[k].x, -zs[k].y), Q[(size_t)k * qs + p], x);
         v[p] = x;
 #pragma unroll
         for (int k = 0; k < KT; ++k)
-            if (k < kc) acc[k] = cfma_conj<double>(Q[(size_t)k * n + p], x, acc[k]);
+            if (k < kc) acc[k] = cfma_conj<double>(Q[(size_t)k * qs + p], x, acc[k]);
     }
     __shared__ double2 res[KT];
     block_sum<KT>(acc, res);
@@ -159,6 +179,7 @@ update_multidot_kernel(const double2 *__restrict__ Q, size_t n, int kc, const do
 __global__ void __launch_bounds__(KRYLOV_THREADS)
 norm_kernel(const double2 *__restrict__ v, size_t n, double *__restrict__ norm_partial)
 {
+    v += blockIdx.y * n; norm_partial += (size_t)blockIdx.y * gridDim.x;
     double nrm = 0;
     for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x)
         nrm += cabs2<double>(v[p]);
@@ -174,9 +195,11 @@ norm_kernel(const double2 *__restrict__ v, size_t n, double *__restrict__ norm_p
 }
 
 // h = sqrt(sum of partials) -> H[j+1, j], status.hnext, happy flag (h < 1e-13).
-__global__ void finish_norm_kernel(const double *__restrict__ norm_partial, int nb, double2 *hsub, KrylovStatus *st,
-                                   double happy_below)
+__global__ void finish_norm_kernel(const double *__restrict__ norm_partial, int nb, double2 *hsub, size_t hs,
+                                   KrylovStatus *st, double happy_below)
 {
+    const int inst = blockIdx.x;
+    norm_partial += (size_t)inst * nb; hsub += inst * hs; st += inst;
     if (st->done) return;
     const double s = warp_fixed_sum(norm_partial, nb, 1);
     if (threadIdx.x != 0) return;
@@ -190,6 +213,7 @@ __global__ void finish_norm_kernel(const double *__restrict__ norm_partial, int 
 __global__ void __launch_bounds__(KRYLOV_THREADS)
 normalize_kernel(const double2 *x, double2 *y, size_t n, const KrylovStatus *st)
 {
+    x += blockIdx.y * n; y += blockIdx.y * n; st += blockIdx.y;
     if (st->done) return;
     const double s = 1.0 / st->hnext;
     for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x)
@@ -199,6 +223,7 @@ normalize_kernel(const double2 *x, double2 *y, size_t n, const KrylovStatus *st)
 // start: beta = ||x||, Q_0 = x / beta (reads beta from the reduced norm)
 __global__ void start_kernel(const double *__restrict__ norm_partial, int nb, KrylovStatus *st)
 {
+    norm_partial += (size_t)blockIdx.x * nb; st += blockIdx.x;
     const double s = warp_fixed_sum(norm_partial, nb, 1);
     if (threadIdx.x != 0) return;
     memset(st, 0, sizeof(KrylovStatus));
@@ -210,9 +235,11 @@ __global__ void start_kernel(const double *__restrict__ norm_partial, int nb, Kr
 // y = sum_{k < m} Q_k c_k with m taken from the status word (or from `mfix` >= 0).  With
 // the status word (mfix < 0), y is left untouched unless the solve converged.
 __global__ void __launch_bounds__(KRYLOV_THREADS)
-combine_kernel(const double2 *__restrict__ Q, size_t n, const double2 *__restrict__ c, double2 *__restrict__ y,
-               const KrylovStatus *st, int mfix, int accumulate)
+combine_kernel(const double2 *__restrict__ Q, size_t n, size_t qs, const double2 *__restrict__ c, int ld,
+               double2 *__restrict__ y, const KrylovStatus *st, int mfix, int accumulate)
 {
+    const int inst = blockIdx.y;
+    Q += inst * n; c += (size_t)inst * ld; y += inst * n; st += inst;
     if (mfix < 0 && (st->failed || !st->converged)) return;
     const int m = mfix >= 0 ? mfix : st->m;
     __shared__ double2 cs[KRYLOV_MAXDIM];
@@ -220,7 +247,7 @@ combine_kernel(const double2 *__restrict__ Q, size_t n, const double2 *__restric
     __syncthreads();
     for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
         double2 acc = accumulate ? y[p] : mk<double>(0, 0);
-        for (int k = 0; k < m; ++k) acc = cfma<double>(cs[k], Q[(size_t)k * n + p], acc);
+        for (int k = 0; k < m; ++k) acc = cfma<double>(cs[k], Q[(size_t)k * qs + p], acc);
         y[p] = acc;
     }
 }
@@ -367,9 +394,11 @@ __device__ void expm_pade13(double2 *A, double2 *R, double2 *work, int m)
 // j >= 3 with (j+1) % 4 == 0 or j+1 == maxdim, form c = expm(-i dt H_m)[:, 0] beta
 // and err = |dt h_{m+1,m} c_{m-1}|; accept if happy or err < tol.
 __global__ void __launch_bounds__(512)
-arnoldi_check_kernel(const double2 *__restrict__ H, int ld, int j, int maxdim, double dt, double tol,
-                     double2 *__restrict__ coef, double2 *__restrict__ work, KrylovStatus *st)
+arnoldi_check_kernel(const double2 *__restrict__ H, int ld, size_t hs, int j, int maxdim, double dt, double tol,
+                     double2 *__restrict__ coef, double2 *__restrict__ work, size_t ws, KrylovStatus *st)
 {
+    const int inst = blockIdx.x;
+    H += inst * hs; coef += (size_t)inst * ld; work += inst * ws; st += inst;
     if (st->done) return;
     const int m = j + 1;
     const bool happy = st->happy;
@@ -410,26 +439,28 @@ he_krylov::~he_krylov()
     if (host_status) cudaFreeHost(host_status);
 }
 
-extern "C" int he_krylov_create(he_krylov **out, long long n, int maxdim, int flexible)
+namespace {
+int krylov_create(he_krylov **out, long long n, int maxdim, int flexible, int count)
 {
     if (!out) return he_fail(HE_ERR_ARG, "null handle pointer", __FILE__, __LINE__);
     *out = nullptr;
     if (n < 1 || maxdim < 1 || maxdim > KRYLOV_MAXDIM)
         return he_fail(HE_ERR_ARG, "Krylov dimension must be in [1, 64] and n >= 1", __FILE__, __LINE__);
+    if (count < 1 || count > HE_BATCH_MAX) return he_fail(HE_ERR_ARG, "batch count must be in [1, 64]", __FILE__, __LINE__);
     he_krylov *k = new he_krylov();
-    k->n = (size_t)n; k->maxdim = maxdim; k->flexible = flexible;
+    k->n = (size_t)n; k->maxdim = maxdim; k->flexible = flexible; k->count = count;
     cudaError_t e = cudaGetDevice(&k->device);
-    const size_t ld = maxdim + 1;
-    if (e == cudaSuccess) e = cudaMalloc(&k->Q, ld * k->n * sizeof(double2));
-    if (e == cudaSuccess && flexible) e = cudaMalloc(&k->Z, (size_t)maxdim * k->n * sizeof(double2));
-    if (e == cudaSuccess) e = cudaMalloc(&k->H, ld * maxdim * sizeof(double2));
-    if (e == cudaSuccess) e = cudaMalloc(&k->partial, (size_t)KRYLOV_BLOCKS * ld * sizeof(double2));
-    if (e == cudaSuccess) e = cudaMalloc(&k->z, ld * sizeof(double2));
-    if (e == cudaSuccess) e = cudaMalloc(&k->coef, ld * sizeof(double2));
-    if (e == cudaSuccess) e = cudaMalloc(&k->work, (size_t)8 * ld * ld * sizeof(double2));
-    if (e == cudaSuccess) e = cudaMalloc(&k->norm_partial, KRYLOV_BLOCKS * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&k->status, sizeof(KrylovStatus));
-    if (e == cudaSuccess) e = cudaMallocHost(&k->host_status, sizeof(KrylovStatus));
+    const size_t ld = maxdim + 1, c = count;
+    if (e == cudaSuccess) e = cudaMalloc(&k->Q, ld * c * k->n * sizeof(double2));
+    if (e == cudaSuccess && flexible) e = cudaMalloc(&k->Z, (size_t)maxdim * c * k->n * sizeof(double2));
+    if (e == cudaSuccess) e = cudaMalloc(&k->H, c * ld * maxdim * sizeof(double2));
+    if (e == cudaSuccess) e = cudaMalloc(&k->partial, c * KRYLOV_BLOCKS * ld * sizeof(double2));
+    if (e == cudaSuccess) e = cudaMalloc(&k->z, c * ld * sizeof(double2));
+    if (e == cudaSuccess) e = cudaMalloc(&k->coef, c * ld * sizeof(double2));
+    if (e == cudaSuccess) e = cudaMalloc(&k->work, c * 8 * ld * ld * sizeof(double2));
+    if (e == cudaSuccess) e = cudaMalloc(&k->norm_partial, c * KRYLOV_BLOCKS * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&k->status, c * sizeof(KrylovStatus));
+    if (e == cudaSuccess) e = cudaMallocHost(&k->host_status, c * sizeof(KrylovStatus));
     if (e != cudaSuccess) {
         he_set_error(cudaGetErrorString(e), __FILE__, __LINE__);
         delete k;
@@ -437,6 +468,17 @@ extern "C" int he_krylov_create(he_krylov **out, long long n, int maxdim, int fl
     }
     *out = k;
     return HE_OK;
+}
+}  // namespace
+
+extern "C" int he_krylov_create(he_krylov **out, long long n, int maxdim, int flexible)
+{
+    return krylov_create(out, n, maxdim, flexible, 1);
+}
+
+extern "C" int he_krylov_create_batched(he_krylov **out, long long n, int maxdim, int count)
+{
+    return krylov_create(out, n, maxdim, 0, count);
 }
 
 extern "C" int he_krylov_destroy(he_krylov *k)
@@ -448,7 +490,7 @@ extern "C" int he_krylov_destroy(he_krylov *k)
 extern "C" int he_krylov_vector(he_krylov *k, int which, int j, void **ptr)
 {
     if (!k || !ptr) return he_fail(HE_ERR_ARG, "null argument", __FILE__, __LINE__);
-    if (which == 0 && j >= 0 && j <= k->maxdim) *ptr = k->Q + (size_t)j * k->n;
+    if (which == 0 && j >= 0 && j <= k->maxdim) *ptr = k->Q + (size_t)j * k->qs();
     else if (which == 1 && k->Z && j >= 0 && j < k->maxdim) *ptr = k->Z + (size_t)j * k->n;
     else return he_fail(HE_ERR_ARG, "basis index out of range", __FILE__, __LINE__);
     return HE_OK;
@@ -456,7 +498,8 @@ extern "C" int he_krylov_vector(he_krylov *k, int which, int j, void **ptr)
 
 namespace he {
 
-static const dim3 kGrid(KRYLOV_BLOCKS), kBlock(KRYLOV_THREADS);
+static const dim3 kBlock(KRYLOV_THREADS);
+inline dim3 bgrid(const he_krylov *k) { return dim3(KRYLOV_BLOCKS, k->count); }   // every instance
 
 int krylov_multidot(he_krylov *k, int kc, const double2 *v, double2 *hcol, cudaStream_t s, const KrylovStatus *st,
                     const double2 *basis)
@@ -464,9 +507,10 @@ int krylov_multidot(he_krylov *k, int kc, const double2 *v, double2 *hcol, cudaS
     const int ld = k->maxdim + 1;
     for (int k0 = 0; k0 < kc; k0 += KRYLOV_TILE) {
         const int t = kc - k0 < KRYLOV_TILE ? kc - k0 : KRYLOV_TILE;
-        multidot_kernel<KRYLOV_TILE><<<kGrid, kBlock, 0, s>>>(basis, k->n, k0, t, v, k->partial, ld, st);
+        multidot_kernel<KRYLOV_TILE><<<bgrid(k), kBlock, 0, s>>>(basis, k->n, k->qs(), k0, t, v, k->partial, ld, st);
     }
-    reduce_partials_kernel<<<1, 32 * std::max(1, std::min(kc, 16)), 0, s>>>(k->partial, KRYLOV_BLOCKS, ld, kc, k->z, hcol, st);
+    reduce_partials_kernel<<<k->count, 32 * std::max(1, std::min(kc, 16)), 0, s>>>(k->partial, KRYLOV_BLOCKS, ld, kc, k->z,
+                                                                                  hcol, k->hs(), st);
     HE_CUDA_TRY(cudaGetLastError());
     return HE_OK;
 }
@@ -479,35 +523,36 @@ int krylov_cgs2(he_krylov *k, int kc, double2 *v, double2 *hcol, double2 *hsub, 
     if (kc <= KRYLOV_FUSED) {   // three sweeps: project, update + project, update + norm
         const int ld = k->maxdim + 1;
         if ((rc = krylov_multidot(k, kc, v, hcol, s, k->status, k->Q))) return rc;
-        update_multidot_kernel<KRYLOV_FUSED><<<kGrid, kBlock, 0, s>>>(k->Q, k->n, kc, k->z, v, k->partial, ld, k->status);
-        reduce_partials_kernel<<<1, 32 * std::max(1, std::min(kc, 16)), 0, s>>>(k->partial, KRYLOV_BLOCKS, ld, kc, k->z,
-                                                                               hcol, k->status);
-        update_kernel<<<kGrid, kBlock, 0, s>>>(k->Q, k->n, kc, k->z, v, k->norm_partial, k->status);
+        update_multidot_kernel<KRYLOV_FUSED><<<bgrid(k), kBlock, 0, s>>>(k->Q, k->n, k->qs(), kc, k->z, v, k->partial, ld,
+                                                                        k->status);
+        reduce_partials_kernel<<<k->count, 32 * std::max(1, std::min(kc, 16)), 0, s>>>(k->partial, KRYLOV_BLOCKS, ld, kc,
+                                                                                      k->z, hcol, k->hs(), k->status);
+        update_kernel<<<bgrid(k), kBlock, 0, s>>>(k->Q, k->n, k->qs(), kc, k->z, ld, v, k->norm_partial, k->status);
     } else {
         for (int rep = 0; rep < 2; ++rep) {
             if ((rc = krylov_multidot(k, kc, v, hcol, s, k->status, k->Q))) return rc;
-            update_kernel<<<kGrid, kBlock, 0, s>>>(k->Q, k->n, kc, k->z, v, rep == 1 ? k->norm_partial : nullptr,
-                                                   k->status);
+            update_kernel<<<bgrid(k), kBlock, 0, s>>>(k->Q, k->n, k->qs(), kc, k->z, k->maxdim + 1, v,
+                                                      rep == 1 ? k->norm_partial : nullptr, k->status);
         }
     }
-    finish_norm_kernel<<<1, 32, 0, s>>>(k->norm_partial, KRYLOV_BLOCKS, hsub, k->status, happy_below);
+    finish_norm_kernel<<<k->count, 32, 0, s>>>(k->norm_partial, KRYLOV_BLOCKS, hsub, k->hs(), k->status, happy_below);
     HE_CUDA_TRY(cudaGetLastError());
     return HE_OK;
 }
 
 int krylov_start(he_krylov *k, const double2 *x, cudaStream_t s)
 {
-    norm_kernel<<<kGrid, kBlock, 0, s>>>(x, k->n, k->norm_partial);
-    start_kernel<<<1, 32, 0, s>>>(k->norm_partial, KRYLOV_BLOCKS, k->status);
-    normalize_kernel<<<kGrid, kBlock, 0, s>>>(x, k->Q, k->n, k->status);
-    HE_CUDA_TRY(cudaMemsetAsync(k->H, 0, sizeof(double2) * (k->maxdim + 1) * k->maxdim, s));
+    norm_kernel<<<bgrid(k), kBlock, 0, s>>>(x, k->n, k->norm_partial);
+    start_kernel<<<k->count, 32, 0, s>>>(k->norm_partial, KRYLOV_BLOCKS, k->status);
+    normalize_kernel<<<bgrid(k), kBlock, 0, s>>>(x, k->Q, k->n, k->status);
+    HE_CUDA_TRY(cudaMemsetAsync(k->H, 0, sizeof(double2) * k->hs() * k->count, s));
     HE_CUDA_TRY(cudaGetLastError());
     return HE_OK;
 }
 
 int krylov_read_status(he_krylov *k, cudaStream_t s)
 {
-    HE_CUDA_TRY(cudaMemcpyAsync(k->host_status, k->status, sizeof(KrylovStatus), cudaMemcpyDeviceToHost, s));
+    HE_CUDA_TRY(cudaMemcpyAsync(k->host_status, k->status, sizeof(KrylovStatus) * k->count, cudaMemcpyDeviceToHost, s));
     HE_CUDA_TRY(cudaStreamSynchronize(s));
     return HE_OK;
 }
@@ -531,7 +576,7 @@ extern "C" int he_krylov_orthogonalize(he_krylov *k, int j, void *stream)
 {
     if (!k || j < 0 || j >= k->maxdim) return he_fail(HE_ERR_ARG, "bad Arnoldi index", __FILE__, __LINE__);
     const int ld = k->maxdim + 1;
-    double2 *v = k->Q + (size_t)(j + 1) * k->n;
+    double2 *v = k->Q + (size_t)(j + 1) * k->qs();
     return krylov_cgs2(k, j + 1, v, k->H + (size_t)j * ld, k->H + (size_t)j * ld + j + 1,
                        static_cast<cudaStream_t>(stream), 1e-13);
 }
@@ -544,9 +589,10 @@ extern "C" int he_expv_check(he_krylov *k, int j, int maxdim, double dt, double 
     if (!k || maxdim < 1 || maxdim > k->maxdim || j < 0 || j >= maxdim)
         return he_fail(HE_ERR_ARG, "bad Arnoldi index", __FILE__, __LINE__);
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
-    arnoldi_check_kernel<<<1, 512, 0, s>>>(k->H, k->maxdim + 1, j, maxdim, dt, tol, k->coef, k->work, k->status);
+    arnoldi_check_kernel<<<k->count, 512, 0, s>>>(k->H, k->maxdim + 1, k->hs(), j, maxdim, dt, tol, k->coef, k->work,
+                                                  k->ws(), k->status);
     if (j + 1 < maxdim)
-        normalize_kernel<<<kGrid, kBlock, 0, s>>>(k->Q + (size_t)(j + 1) * k->n, k->Q + (size_t)(j + 1) * k->n, k->n,
+        normalize_kernel<<<bgrid(k), kBlock, 0, s>>>(k->Q + (size_t)(j + 1) * k->qs(), k->Q + (size_t)(j + 1) * k->qs(), k->n,
                                                   k->status);
     HE_CUDA_TRY(cudaGetLastError());
     if (sync) {
@@ -563,8 +609,8 @@ extern "C" int he_expv_check(he_krylov *k, int j, int maxdim, double dt, double 
 extern "C" int he_krylov_combine(he_krylov *k, int m, void *y, void *stream)
 {
     if (!k || !y || m > k->maxdim) return he_fail(HE_ERR_ARG, "bad combination", __FILE__, __LINE__);
-    combine_kernel<<<kGrid, kBlock, 0, static_cast<cudaStream_t>(stream)>>>(k->Q, k->n, k->coef,
-                                                                             static_cast<double2 *>(y), k->status, m, 0);
+    combine_kernel<<<bgrid(k), kBlock, 0, static_cast<cudaStream_t>(stream)>>>(k->Q, k->n, k->qs(), k->coef, k->maxdim + 1,
+                                                                                static_cast<double2 *>(y), k->status, m, 0);
     HE_CUDA_TRY(cudaGetLastError());
     return HE_OK;
 }
@@ -583,14 +629,18 @@ __global__ void krylov_to_c128(size_t n, const float2 *x, double2 *y)
         y[p] = make_double2((double)x[p].x, (double)x[p].y);
 }
 
-// y = exp(-i dt H) x.  precision HE_C64: H·psi in complex64 (the basis, CGS2, the
-// Hessenberg exponential and the error estimate stay complex128).
-int expv_impl(he_krylov *k, he_handle op, const void *x, void *y, const double *field, int velocity, double dt,
-              double tol, int maxdim, int *dimension, double *estimate, void *stream, int precision)
+// y_b = exp(-i dt H(fields_b)) x_b for every instance of the workspace.  precision HE_C64:
+// H·psi in complex64 (the basis, CGS2, the Hessenberg exponential and the error estimate
+// stay complex128).  Per-instance dimensions, estimates and convergence go to the optional
+// arrays; the status is HE_ERR_NOCONV when any instance did not converge (its y_b is left
+// as it was).
+int expv_impl(he_krylov *k, he_handle op, const void *x, void *y, const double *fields, int velocity, double dt,
+              double tol, int maxdim, int *dimension, double *estimate, int *converged, void *stream, int precision)
 {
-    if (!k || !op || !x || !y || !field) return he_fail(HE_ERR_ARG, "null argument", __FILE__, __LINE__);
+    if (!k || !op || !x || !y || !fields) return he_fail(HE_ERR_ARG, "null argument", __FILE__, __LINE__);
+    const size_t total = k->qs();   // one basis vector of every instance
     if (precision == HE_C64 && !k->s32[0]) {
-        for (int q = 0; q < 2; ++q) HE_CUDA_TRY(cudaMalloc(&k->s32[q], k->n * sizeof(float2)));
+        for (int q = 0; q < 2; ++q) HE_CUDA_TRY(cudaMalloc(&k->s32[q], total * sizeof(float2)));
     }
     if (maxdim < 1 || maxdim > k->maxdim) return he_fail(HE_ERR_ARG, "maxdim exceeds the workspace", __FILE__, __LINE__);
     if ((size_t)op->n * op->n * op->nc != k->n) return he_fail(HE_ERR_SHAPE, "workspace size != operator size", __FILE__, __LINE__);
@@ -603,29 +653,37 @@ int expv_impl(he_krylov *k, he_handle op, const void *x, void *y, const double *
     int rc = krylov_start(k, static_cast<const double2 *>(x), s);
     if (rc) return rc;
     const int ld = k->maxdim + 1;
+    const dim3 cgrid(std::min<size_t>(KRYLOV_BLOCKS * (size_t)k->count, 4096));
     for (int j = 0; j < maxdim; ++j) {
-        double2 *qj = k->Q + (size_t)j * k->n, *v = k->Q + (size_t)(j + 1) * k->n;
+        double2 *qj = k->Q + (size_t)j * total, *v = k->Q + (size_t)(j + 1) * total;
         if (precision == HE_C64) {
-            krylov_to_c64<<<kGrid, kBlock, 0, s>>>(k->n, qj, k->s32[0]);
-            rc = he_apply(op, k->s32[0], k->s32[1], field, velocity, HE_C64, stream);
-            krylov_to_c128<<<kGrid, kBlock, 0, s>>>(k->n, k->s32[1], v);
+            krylov_to_c64<<<cgrid, kBlock, 0, s>>>(total, qj, k->s32[0]);
+            rc = he_apply_batched(op, k->count, k->s32[0], k->s32[1], fields, velocity, HE_C64, stream);
+            krylov_to_c128<<<cgrid, kBlock, 0, s>>>(total, k->s32[1], v);
         } else {
-            rc = he_apply(op, qj, v, field, velocity, HE_C128, stream);   // same kernels as every other apply
+            rc = he_apply_batched(op, k->count, qj, v, fields, velocity, HE_C128, stream);   // the kernels of every apply
         }
         if (!rc) rc = krylov_cgs2(k, j + 1, v, k->H + (size_t)j * ld, k->H + (size_t)j * ld + j + 1, s, 1e-13);
         if (rc) break;
-        arnoldi_check_kernel<<<1, 512, 0, s>>>(k->H, ld, j, maxdim, dt, tol, k->coef, k->work, k->status);
-        if (j + 1 < maxdim) normalize_kernel<<<kGrid, kBlock, 0, s>>>(v, v, k->n, k->status);
+        arnoldi_check_kernel<<<k->count, 512, 0, s>>>(k->H, ld, k->hs(), j, maxdim, dt, tol, k->coef, k->work, k->ws(),
+                                                      k->status);
+        if (j + 1 < maxdim) normalize_kernel<<<bgrid(k), kBlock, 0, s>>>(v, v, k->n, k->status);
     }
     if (rc) return rc;
     // y = Q c with m from the status word; y is left as is when the solve failed
-    combine_kernel<<<kGrid, kBlock, 0, s>>>(k->Q, k->n, k->coef, static_cast<double2 *>(y), k->status, -1, 0);
+    combine_kernel<<<bgrid(k), kBlock, 0, s>>>(k->Q, k->n, k->qs(), k->coef, ld, static_cast<double2 *>(y), k->status, -1, 0);
     HE_CUDA_TRY(cudaGetLastError());
     if ((rc = krylov_read_status(k, s))) return rc;
-    if (estimate) *estimate = k->host_status->estimate;
-    if (dimension) *dimension = k->host_status->m;
-    if (k->host_status->failed || !k->host_status->converged)
-        return he_fail(HE_ERR_NOCONV, "Arnoldi did not converge", __FILE__, __LINE__);
+    bool all = true;
+    for (int b = 0; b < k->count; ++b) {
+        const KrylovStatus &h = k->host_status[b];
+        const bool ok = !h.failed && h.converged;
+        if (estimate) estimate[b] = h.estimate;
+        if (dimension) dimension[b] = h.m;
+        if (converged) converged[b] = ok;
+        all = all && ok;
+    }
+    if (!all) return he_fail(HE_ERR_NOCONV, "Arnoldi did not converge", __FILE__, __LINE__);
     return HE_OK;
 }
 }  // namespace
@@ -633,11 +691,22 @@ int expv_impl(he_krylov *k, he_handle op, const void *x, void *y, const double *
 extern "C" int he_expv(he_krylov *k, he_handle op, const void *x, void *y, const double *field, int velocity,
                        double dt, double tol, int maxdim, int *dimension, double *estimate, void *stream)
 {
-    return expv_impl(k, op, x, y, field, velocity, dt, tol, maxdim, dimension, estimate, stream, HE_C128);
+    if (k && k->count != 1) return he_fail(HE_ERR_ARG, "batched workspace: use he_expv_batched", __FILE__, __LINE__);
+    return expv_impl(k, op, x, y, field, velocity, dt, tol, maxdim, dimension, estimate, nullptr, stream, HE_C128);
 }
 
 extern "C" int he_expv_mixed(he_krylov *k, he_handle op, const void *x, void *y, const double *field, int velocity,
                              double dt, double tol, int maxdim, int *dimension, double *estimate, void *stream)
 {
-    return expv_impl(k, op, x, y, field, velocity, dt, tol, maxdim, dimension, estimate, stream, HE_C64);
+    if (k && k->count != 1) return he_fail(HE_ERR_ARG, "batched workspace: use he_expv_batched", __FILE__, __LINE__);
+    return expv_impl(k, op, x, y, field, velocity, dt, tol, maxdim, dimension, estimate, nullptr, stream, HE_C64);
+}
+
+extern "C" int he_expv_batched(he_krylov *k, he_handle op, const void *x, void *y, const double *fields, int velocity,
+                               double dt, double tol, int maxdim, int precision, int *dimension, double *estimate,
+                               int *converged, void *stream)
+{
+    if (precision != HE_C128 && precision != HE_C64)
+        return he_fail(HE_ERR_ARG, "precision must be HE_C128 or HE_C64", __FILE__, __LINE__);
+    return expv_impl(k, op, x, y, fields, velocity, dt, tol, maxdim, dimension, estimate, converged, stream, precision);
 }

@@ -29,10 +29,12 @@ constexpr int KRYLOV_FUSED = 16;      // CGS2 with a fused update + projection s
 
 struct he_krylov {
     int device = 0;
-    size_t n = 0;                 // vector length (complex elements)
+    size_t n = 0;                 // vector length (complex elements) of one instance
     int maxdim = 0;
     int flexible = 0;
-    double2 *Q = nullptr;         // (maxdim+1) vectors, column j at Q + j*n
+    int count = 1;                // instances solved together (batched Arnoldi); every array below has
+                                  // one slice per instance
+    double2 *Q = nullptr;         // (maxdim+1) vectors; vector j of instance b at Q + (j*count + b)*n
     double2 *Z = nullptr;         // flexible GMRES: preconditioned directions (maxdim vectors)
     double2 *H = nullptr;         // (maxdim+1) x maxdim Hessenberg, column major, ld = maxdim+1
     double2 *partial = nullptr;   // KRYLOV_BLOCKS x (maxdim+1) block partial sums (scratch)
@@ -41,7 +43,10 @@ struct he_krylov {
     double2 *work = nullptr;      // 8 * maxdim^2 complex: small dense scratch (expm / least squares)
     double *norm_partial = nullptr;   // KRYLOV_BLOCKS
     float2 *s32[2] = {nullptr, nullptr};   // complex64 operand/result of mixed-precision applies
-    he::KrylovStatus *status = nullptr;      // device
+    he::KrylovStatus *status = nullptr;      // device, count entries
     he::KrylovStatus *host_status = nullptr; // pinned host mirror
+    size_t qs() const { return (size_t)count * n; }              // distance between basis vectors
+    size_t hs() const { return (size_t)(maxdim + 1) * maxdim; }  // Hessenberg size per instance
+    size_t ws() const { return (size_t)8 * (maxdim + 1) * (maxdim + 1); }   // dense scratch per instance
     ~he_krylov();
 };

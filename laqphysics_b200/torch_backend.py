@@ -162,6 +162,72 @@ def _fused(op, ws, x, dt, tol, maxdim, stream):
     return y, {'dimension': dim.value, 'residual_estimate': float(err.value)}
 
 
+class BatchedWorkspace:
+    """Krylov workspace for ``count`` instances advanced together (he_krylov_create_batched)."""
+
+    def __init__(self, n, maxdim, count, device):
+        self.n, self.maxdim, self.count, self.device = int(n), int(maxdim), int(count), torch.device(device)
+        handle = ct.c_void_p()
+        with torch.cuda.device(self.device):
+            check(LIB.he_krylov_create_batched(ct.byref(handle), self.n, self.maxdim, self.count),
+                  'he_krylov_create_batched')
+        self.handle = handle
+
+    def __del__(self):
+        handle = getattr(self, 'handle', None)
+        if handle is not None and handle.value:
+            LIB.he_krylov_destroy(handle)
+            self.handle = None
+
+
+_BATCHED = {}
+
+
+def batched_workspace(n, maxdim, count, device):
+    device = torch.device(device)
+    key = (device, int(n), int(count))
+    ws = _BATCHED.get(key)
+    if ws is None or ws.maxdim < maxdim:
+        ws = BatchedWorkspace(n, max(maxdim, ws.maxdim if ws else 0), count, device)
+        _BATCHED[key] = ws
+    return ws
+
+
+@torch.no_grad()
+def step_batched(engine, fields_at, x, t, dt, tol=1e-10, maxdim=48, velocity=False, precision='complex128'):
+    """One midpoint Arnoldi step of ``count`` instances sharing ``engine``: x is
+    (count, size) complex128, ``fields_at(t)`` returns the (count, 3) fields.  The batch
+    runs as one device Arnoldi (he_expv_batched); an instance that does not converge at
+    dt is redone alone with the reference's recursive halving (:func:`step`), so every
+    instance gets exactly the result of stepping it by itself.  Returns (y, info) with
+    per-instance dimensions."""
+    count = x.shape[0]
+    if x.dtype != torch.complex128 or not x.is_contiguous() or x.numel() != count * engine.size:
+        raise ValueError('batch must be a contiguous complex128 (count, size) tensor')
+    ws = batched_workspace(engine.size, maxdim, count, x.device)
+    fields = np.ascontiguousarray(fields_at(t + dt / 2), dtype=np.float64).reshape(count, 3)
+    y = torch.empty_like(x)
+    dims = np.zeros(count, np.int32)
+    est = np.zeros(count)
+    conv = np.zeros(count, np.int32)
+    code = {'complex128': 0, 'mixed': 1}[precision]
+    status = LIB.he_expv_batched(ws.handle, engine.op.handle, ct.c_void_p(x.data_ptr()), ct.c_void_p(y.data_ptr()),
+                                 ptr(fields), int(bool(velocity)), float(dt), float(tol), int(maxdim), code,
+                                 ptr(dims), ptr(est), ptr(conv), _stream(x.device))
+    if status != HE_ERR_NOCONV:
+        check(status, 'he_expv_batched')
+    engine.apply_count += int(dims.sum())
+    info = {'dimension': dims.copy(), 'residual_estimate': est.copy(), 'subdivided': np.zeros(count, bool)}
+    for b in np.flatnonzero(conv == 0):   # rare: redo alone with halving, like the reference would
+        schedule = FieldSchedule(engine, lambda tt, b=b: np.asarray(fields_at(tt))[b], velocity, precision)
+        yb, ib = step(schedule, x[b].contiguous(), t, dt, tol, maxdim)
+        y[b].copy_(yb)
+        info['dimension'][b] = ib['dimension']
+        info['residual_estimate'][b] = ib['residual_estimate']
+        info['subdivided'][b] = ib.get('subdivided', False)
+    return y, info
+
+
 def step(apply_at, x, t, dt, tol=1e-10, maxdim=48, depth=0):
     """Midpoint exponential step with recursive halving (python/torch_backend.py:160-167)."""
     try:
@@ -179,5 +245,5 @@ def step(apply_at, x, t, dt, tol=1e-10, maxdim=48, depth=0):
                    'residual_estimate': a['residual_estimate'] + b['residual_estimate'], 'subdivided': True}
 
 
-__all__ = ['TorchHamiltonian', 'B200Hamiltonian', 'exponential_action', 'step', 'FieldOperator', 'FieldSchedule',
-           'HeliumError']
+__all__ = ['TorchHamiltonian', 'B200Hamiltonian', 'exponential_action', 'step', 'step_batched', 'FieldOperator',
+           'FieldSchedule', 'HeliumError']

@@ -129,3 +129,32 @@ def test_fused_and_generic_arnoldi_agree_on_larger_grid():
     assert ia['dimension'] == ib['dimension'] == ic['dimension']
     np.testing.assert_array_equal(op.host(a), op.host(b))
     assert np.linalg.norm(op.host(a) - c) / np.linalg.norm(c) < 1e-12
+
+
+@pytest.mark.parametrize('precision', ['complex128', 'mixed'])
+def test_batched_arnoldi_matches_single_instance_steps(precision):
+    """he_expv_batched (every instance of the batch in one launch per kernel) against the
+    same instances stepped one by one: the per-instance arithmetic is the same, so the
+    states agree to rounding; one instance has dt too large for maxdim and is redone
+    alone with the reference's halving."""
+    from laqphysics_b200.torch_backend import FieldSchedule, step, step_batched
+    from laqphysics_b200.workloads import arnoldi_small, seeded_state
+    h = arnoldi_small()
+    op = engine(h)
+    count = 4
+    peaks = np.array([.005, .01, .02, .03])
+    fields_at = lambda t: np.stack([[0., 0., p * np.sin(1.6 * t)] for p in peaks])
+    x0 = torch.stack([op.state(seeded_state(h.size, 50 + b)) for b in range(count)])
+    x0 /= torch.linalg.vector_norm(x0, dim=1, keepdim=True)
+    dt, tol, maxdim = .01, 1e-10, 12
+    xb = x0.clone()
+    for i in range(3):
+        xb, info = step_batched(op, fields_at, xb, i * dt, dt, tol, maxdim, precision=precision)
+    for b in range(count):
+        schedule = FieldSchedule(op, lambda t, b=b: fields_at(t)[b], velocity=False, precision=precision)
+        xs = x0[b].contiguous()
+        for i in range(3):
+            xs, _ = step(schedule, xs, i * dt, dt, tol, maxdim)
+        err = float(torch.linalg.vector_norm(xb[b] - xs) / torch.linalg.vector_norm(xs))
+        assert err < 1e-13, (b, err)
+    assert (info['dimension'] <= maxdim).all()
