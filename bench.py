@@ -40,7 +40,7 @@ def parse():
     p.add_argument('--impl', choices=['b200', 'reference'], default='b200')
     p.add_argument('--no-cpu-baseline', action='store_true')
     p.add_argument('--no-arnoldi', action='store_true', help='skip the Arnoldi steps/s leg')
-    p.add_argument('--profile', choices=['c128', 'c64', 'arnoldi'], default=None,
+    p.add_argument('--profile', choices=['c128', 'c64', 'arnoldi', 'batched'], default=None,
                    help='run only W+K applications of one precision (for ncu captures); prints no JSON')
     return p.parse_args()
 
@@ -200,6 +200,59 @@ def arnoldi_leg(torch, device, steps, cpu_steps):
     return out
 
 
+def batched_leg(torch, device, steps, count=32):
+    """Batched Arnoldi on the Arnoldi grid (n=132, nc=17): `count` pump-probe-like instances
+    (seeded peak fields 0.005-0.03 a.u., delays inside the 10-cycle pulse) stepped together
+    by he_expv_batched, in complex128 and in mixed precision (complex64 H·psi inside the
+    complex128 Krylov).  Reports instance-steps/s and the mixed-vs-FP64 state difference."""
+    from laqphysics_b200 import workloads
+    from laqphysics_b200.engine import B200Hamiltonian
+    from laqphysics_b200.torch_backend import step_batched
+    h, hreal = workloads.arnoldi_small(), workloads.arnoldi_small_real()
+    E0, g, _ = hreal.ground(tol=1e-9)
+    ratio = np.sqrt(h.grid.weights / hreal.grid.weights)
+    psi0 = (g.reshape(h.shape, order='F') * ratio[:, None, None] * ratio[None, :, None]).ravel(order='F')
+    engine = B200Hamiltonian(h, device)
+    pulse = workloads.length_pulse()
+    rng = np.random.default_rng(2026)
+    peaks = rng.uniform(.005, .03, count)
+    delays = rng.uniform(0., 30., count)
+    scale = peaks / .01   # length_pulse has peak 0.01
+
+    def fields_at(t):
+        f = np.zeros((count, 3))
+        f[:, 2] = scale * np.array([pulse.electric(t + d) for d in delays])
+        return f
+
+    dt, tol, maxdim = .02, 1e-10, 12
+    x0 = engine.state(psi0).repeat(count).reshape(count, -1).contiguous()
+    out = {'workload': f'{count} instances, Arnoldi grid n=132 nc=17, length gauge, maxdim 12, dt 0.02',
+           'count': count}
+    finals = {}
+    for precision in ('complex128', 'mixed'):
+        x = x0.clone()
+        for i in range(3):
+            x, _ = step_batched(engine, fields_at, x, i * dt, dt, tol, maxdim, precision=precision)
+        torch.cuda.synchronize(device)
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        dims = []
+        start.record()
+        for i in range(3, 3 + steps):
+            x, info = step_batched(engine, fields_at, x, i * dt, dt, tol, maxdim, precision=precision)
+            dims.append(float(np.mean(info['dimension'])))
+        stop.record()
+        torch.cuda.synchronize(device)
+        ms = start.elapsed_time(stop)
+        finals[precision] = x
+        out[precision] = {'instance_steps_per_s': count * steps / (ms * 1e-3), 'ms_per_step': ms / steps,
+                          'mean_dimension': float(np.mean(dims))}
+    diff = torch.linalg.vector_norm(finals['mixed'] - finals['complex128'], dim=1)
+    ref = torch.linalg.vector_norm(finals['complex128'], dim=1)
+    out['mixed_vs_fp64_rel_l2_max'] = float((diff / ref).max())
+    out['mixed_norm_error_max'] = float((torch.linalg.vector_norm(finals['mixed'], dim=1) - ref).abs().max())
+    return out
+
+
 def run_reference(args, rank):
     """--impl reference: the CPU oracle of the reference's native H·psi on host cores."""
     if rank != 0:
@@ -259,6 +312,9 @@ def main():
 
     if args.profile == 'arnoldi':   # W + K Arnoldi steps on the small grid, for launch lists
         arnoldi_leg(torch, device, steps=args.steps, cpu_steps=0)
+        return 0
+    if args.profile == 'batched':
+        batched_leg(torch, device, steps=args.steps)
         return 0
     h = workloads.hpsi_microbench()
     engine = B200Hamiltonian(h, device)
@@ -347,6 +403,11 @@ def main():
     if not args.no_arnoldi:
         line['arnoldi'] = arnoldi_leg(torch, device, steps=max(10, min(args.steps, 100)),
                                       cpu_steps=0 if (args.no_cpu_baseline or world > 1 or rank) else 3)
+        line['batched'] = batched_leg(torch, device, steps=max(5, min(args.steps, 30)))
+        line['batched']['speedup_vs_single_fp64'] = (line['batched']['complex128']['instance_steps_per_s'] /
+                                                     line['arnoldi']['steps_per_s'])
+        line['batched']['mixed_speedup_vs_single_fp64'] = (line['batched']['mixed']['instance_steps_per_s'] /
+                                                           line['arnoldi']['steps_per_s'])
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         os.environ.setdefault('OMP_NUM_THREADS', str(os.cpu_count()))
         gbs, cores, sample = cpu_oracle_rate(h, workloads.seeded_state(N, 1234), field, 15.0)

@@ -135,8 +135,7 @@ def test_fused_and_generic_arnoldi_agree_on_larger_grid():
 def test_batched_arnoldi_matches_single_instance_steps(precision):
     """he_expv_batched (every instance of the batch in one launch per kernel) against the
     same instances stepped one by one: the per-instance arithmetic is the same, so the
-    states agree to rounding; one instance has dt too large for maxdim and is redone
-    alone with the reference's halving."""
+    states agree to rounding."""
     from laqphysics_b200.torch_backend import FieldSchedule, step, step_batched
     from laqphysics_b200.workloads import arnoldi_small, seeded_state
     h = arnoldi_small()
