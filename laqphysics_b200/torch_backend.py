@@ -194,13 +194,13 @@ def batched_workspace(n, maxdim, count, device):
 
 
 @torch.no_grad()
-def step_batched(engine, fields_at, x, t, dt, tol=1e-10, maxdim=48, velocity=False, precision='complex128'):
+def step_batched(engine, fields_at, x, t, dt, tol=1e-10, maxdim=48, velocity=False, precision='complex128', depth=0):
     """One midpoint Arnoldi step of ``count`` instances sharing ``engine``: x is
     (count, size) complex128, ``fields_at(t)`` returns the (count, 3) fields.  The batch
-    runs as one device Arnoldi (he_expv_batched); an instance that does not converge at
-    dt is redone alone with the reference's recursive halving (:func:`step`), so every
-    instance gets exactly the result of stepping it by itself.  Returns (y, info) with
-    per-instance dimensions."""
+    runs as one device Arnoldi (he_expv_batched).  Instances that do not converge at dt
+    are redone together with the reference's recursive halving (two half steps, depth
+    <= 8, tolerance halved), so every instance gets the result of stepping it by itself
+    with :func:`step`.  Returns (y, info) with per-instance dimensions."""
     count = x.shape[0]
     if x.dtype != torch.complex128 or not x.is_contiguous() or x.numel() != count * engine.size:
         raise ValueError('batch must be a contiguous complex128 (count, size) tensor')
@@ -218,13 +218,18 @@ def step_batched(engine, fields_at, x, t, dt, tol=1e-10, maxdim=48, velocity=Fal
         check(status, 'he_expv_batched')
     engine.apply_count += int(dims.sum())
     info = {'dimension': dims.copy(), 'residual_estimate': est.copy(), 'subdivided': np.zeros(count, bool)}
-    for b in np.flatnonzero(conv == 0):   # rare: redo alone with halving, like the reference would
-        schedule = FieldSchedule(engine, lambda tt, b=b: np.asarray(fields_at(tt))[b], velocity, precision)
-        yb, ib = step(schedule, x[b].contiguous(), t, dt, tol, maxdim)
-        y[b].copy_(yb)
-        info['dimension'][b] = ib['dimension']
-        info['residual_estimate'][b] = ib['residual_estimate']
-        info['subdivided'][b] = ib.get('subdivided', False)
+    failed = np.flatnonzero(conv == 0)
+    if len(failed):
+        if depth >= 8:
+            raise _not_converged(maxdim, dt, float(est[failed].max()))
+        sub = lambda tt: np.asarray(fields_at(tt)).reshape(count, 3)[failed]
+        xs = x[torch.as_tensor(failed, device=x.device)].contiguous()
+        ys, a = step_batched(engine, sub, xs, t, dt / 2, tol / 2, maxdim, velocity, precision, depth + 1)
+        ys, b = step_batched(engine, sub, ys, t + dt / 2, dt / 2, tol / 2, maxdim, velocity, precision, depth + 1)
+        y[torch.as_tensor(failed, device=x.device)] = ys
+        info['dimension'][failed] = np.maximum(a['dimension'], b['dimension'])
+        info['residual_estimate'][failed] = a['residual_estimate'] + b['residual_estimate']
+        info['subdivided'][failed] = True
     return y, info
 
 
