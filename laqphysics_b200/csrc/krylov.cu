@@ -499,7 +499,7 @@ extern "C" int he_krylov_vector(he_krylov *k, int which, int j, void **ptr)
 namespace he {
 
 static const dim3 kBlock(KRYLOV_THREADS);
-inline dim3 bgrid(const he_krylov *k) { return dim3(KRYLOV_BLOCKS, k->count); }   // every instance
+inline dim3 bgrid(const he_krylov *k) { return dim3(k->kb(), k->count); }   // every instance
 
 int krylov_multidot(he_krylov *k, int kc, const double2 *v, double2 *hcol, cudaStream_t s, const KrylovStatus *st,
                     const double2 *basis)
@@ -509,7 +509,7 @@ int krylov_multidot(he_krylov *k, int kc, const double2 *v, double2 *hcol, cudaS
         const int t = kc - k0 < KRYLOV_TILE ? kc - k0 : KRYLOV_TILE;
         multidot_kernel<KRYLOV_TILE><<<bgrid(k), kBlock, 0, s>>>(basis, k->n, k->qs(), k0, t, v, k->partial, ld, st);
     }
-    reduce_partials_kernel<<<k->count, 32 * std::max(1, std::min(kc, 16)), 0, s>>>(k->partial, KRYLOV_BLOCKS, ld, kc, k->z,
+    reduce_partials_kernel<<<k->count, 32 * std::max(1, std::min(kc, 16)), 0, s>>>(k->partial, k->kb(), ld, kc, k->z,
                                                                                   hcol, k->hs(), st);
     HE_CUDA_TRY(cudaGetLastError());
     return HE_OK;
@@ -525,7 +525,7 @@ int krylov_cgs2(he_krylov *k, int kc, double2 *v, double2 *hcol, double2 *hsub, 
         if ((rc = krylov_multidot(k, kc, v, hcol, s, k->status, k->Q))) return rc;
         update_multidot_kernel<KRYLOV_FUSED><<<bgrid(k), kBlock, 0, s>>>(k->Q, k->n, k->qs(), kc, k->z, v, k->partial, ld,
                                                                         k->status);
-        reduce_partials_kernel<<<k->count, 32 * std::max(1, std::min(kc, 16)), 0, s>>>(k->partial, KRYLOV_BLOCKS, ld, kc,
+        reduce_partials_kernel<<<k->count, 32 * std::max(1, std::min(kc, 16)), 0, s>>>(k->partial, k->kb(), ld, kc,
                                                                                       k->z, hcol, k->hs(), k->status);
         update_kernel<<<bgrid(k), kBlock, 0, s>>>(k->Q, k->n, k->qs(), kc, k->z, ld, v, k->norm_partial, k->status);
     } else {
@@ -535,7 +535,7 @@ int krylov_cgs2(he_krylov *k, int kc, double2 *v, double2 *hcol, double2 *hsub, 
                                                       rep == 1 ? k->norm_partial : nullptr, k->status);
         }
     }
-    finish_norm_kernel<<<k->count, 32, 0, s>>>(k->norm_partial, KRYLOV_BLOCKS, hsub, k->hs(), k->status, happy_below);
+    finish_norm_kernel<<<k->count, 32, 0, s>>>(k->norm_partial, k->kb(), hsub, k->hs(), k->status, happy_below);
     HE_CUDA_TRY(cudaGetLastError());
     return HE_OK;
 }
@@ -543,7 +543,7 @@ int krylov_cgs2(he_krylov *k, int kc, double2 *v, double2 *hcol, double2 *hsub, 
 int krylov_start(he_krylov *k, const double2 *x, cudaStream_t s)
 {
     norm_kernel<<<bgrid(k), kBlock, 0, s>>>(x, k->n, k->norm_partial);
-    start_kernel<<<k->count, 32, 0, s>>>(k->norm_partial, KRYLOV_BLOCKS, k->status);
+    start_kernel<<<k->count, 32, 0, s>>>(k->norm_partial, k->kb(), k->status);
     normalize_kernel<<<bgrid(k), kBlock, 0, s>>>(x, k->Q, k->n, k->status);
     HE_CUDA_TRY(cudaMemsetAsync(k->H, 0, sizeof(double2) * k->hs() * k->count, s));
     HE_CUDA_TRY(cudaGetLastError());

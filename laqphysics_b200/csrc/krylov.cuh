@@ -1,5 +1,7 @@
 // Krylov workspace shared by the Arnoldi exponential and GMRES (krylov.cu, gmres.cu).
 #pragma once
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace he {
@@ -46,6 +48,7 @@ struct he_krylov {
     he::KrylovStatus *status = nullptr;      // device, count entries
     he::KrylovStatus *host_status = nullptr; // pinned host mirror
     size_t qs() const { return (size_t)count * n; }              // distance between basis vectors
+    int kb() const { return count == 1 ? he::KRYLOV_BLOCKS : std::max(8, he::KRYLOV_BLOCKS / count); }   // CTAs per instance
     size_t hs() const { return (size_t)(maxdim + 1) * maxdim; }  // Hessenberg size per instance
     size_t ws() const { return (size_t)8 * (maxdim + 1) * (maxdim + 1); }   // dense scratch per instance
     ~he_krylov();
