@@ -272,6 +272,44 @@ def batched_leg(torch, device, steps, count=32):
     return out
 
 
+def adjoint_leg(torch, device, steps=64, knots=32, checkpoint=32):
+    """Adjoint gradient on the Arnoldi grid widened to l <= 4: `steps` fixed Arnoldi steps
+    (dt 0.02, Krylov tolerance 1e-13, maxdim 30) under a field of `knots` seeded samples
+    (two pulses, peak 0.02 a.u.); objective = probability of electron 2 beyond 20 a.u.
+    Reports the forward and backward times and their ratio."""
+    from laqphysics_b200 import workloads
+    from laqphysics_b200.adjoint import Propagation, check_complex_symmetric
+    from laqphysics_b200.engine import B200Hamiltonian
+    h, hreal = workloads.adjoint_grid(), workloads.adjoint_grid(ecs_angle=0.)
+    _, g, _ = hreal.ground(tol=1e-9)
+    ratio = np.sqrt(h.grid.weights / hreal.grid.weights)
+    psi0 = (g.reshape(h.shape, order='F') * ratio[:, None, None] * ratio[None, :, None]).ravel(order='F')
+    engine = B200Hamiltonian(h, device)
+    check_complex_symmetric(engine)
+    r = np.asarray(h.r).real
+    mask = np.broadcast_to((r > 20.)[None, :, None], h.shape).astype(float).ravel(order='F')
+    dt = .02
+    rng = np.random.default_rng(512)
+    t = np.linspace(0, steps * dt, knots)
+    theta = .02 * (np.exp(-((t - .3 * t[-1]) / (.1 * t[-1])) ** 2) + np.exp(-((t - .7 * t[-1]) / (.1 * t[-1])) ** 2))
+    theta *= rng.uniform(.8, 1.2, knots)
+    prop = Propagation(engine, psi0, dt, steps, t, mask, tol=1e-13, maxdim=30, checkpoint=checkpoint)
+    prop.forward(theta)                                   # warm-up (generated kernels, workspaces)
+    prop.gradient()
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    J = prop.forward(theta)
+    torch.cuda.synchronize(device)
+    t1 = time.perf_counter()
+    grad = prop.gradient()
+    torch.cuda.synchronize(device)
+    t2 = time.perf_counter()
+    return {'workload': f'adjoint gradient: l1,l2<=4 L<=2 (nc={h.nc}, n={h.n}), {steps} Arnoldi steps dt 0.02, '
+                        f'{knots} field samples, checkpoint {checkpoint}, objective P(r2 > 20 a.u.)',
+            'objective': J, 'forward_ms': (t1 - t0) * 1e3, 'backward_ms': (t2 - t1) * 1e3,
+            'backward_over_forward': (t2 - t1) / (t1 - t0), 'gradient_norm': float(np.linalg.norm(grad))}
+
+
 def run_reference(args, rank):
     """--impl reference: the CPU oracle of the reference's native H·psi on host cores."""
     if rank != 0:
@@ -423,6 +461,7 @@ def main():
         line['arnoldi'] = arnoldi_leg(torch, device, steps=max(10, min(args.steps, 100)),
                                       cpu_steps=0 if (args.no_cpu_baseline or world > 1 or rank) else 3)
         line['batched'] = batched_leg(torch, device, steps=max(5, min(args.steps, 30)))
+        line['adjoint'] = adjoint_leg(torch, device)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         os.environ.setdefault('OMP_NUM_THREADS', str(os.cpu_count()))

@@ -40,6 +40,11 @@ def arnoldi_small_real(tail=12):
     return coupled(np.linspace(0, 25, 16), 8, 3, 2, ecs_angle=0., tail=tail, cutoff_radii=(18., 22.))
 
 
+def adjoint_grid(tail=12, ecs_angle=.3):
+    """Adjoint-gradient grid: the Arnoldi grid widened to l1, l2 <= 4 (L <= 2, M = 0)."""
+    return coupled(np.linspace(0, 25, 16), 8, 4, 2, ecs_angle=ecs_angle, tail=tail, cutoff_radii=(18., 22.))
+
+
 def length_pulse():
     """Linear sin^2 pulse, omega 1.6 a.u., 10 cycles, peak field 0.01 a.u."""
     return Pulse(omega=1.6, cycles=10, field=.01)
