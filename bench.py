@@ -274,7 +274,7 @@ def batched_leg(torch, device, steps, count=32):
 
 def adjoint_leg(torch, device, steps=64, knots=32, checkpoint=32):
     """Adjoint gradient on the Arnoldi grid widened to l <= 4: `steps` fixed Arnoldi steps
-    (dt 0.02, Krylov tolerance 1e-13, maxdim 30) under a field of `knots` seeded samples
+    (dt 0.02, Krylov tolerance 1e-12, maxdim 30) under a field of `knots` seeded samples
     (two pulses, peak 0.02 a.u.); objective = probability of electron 2 beyond 20 a.u.
     Reports the forward and backward times and their ratio."""
     from laqphysics_b200 import workloads
@@ -293,7 +293,7 @@ def adjoint_leg(torch, device, steps=64, knots=32, checkpoint=32):
     t = np.linspace(0, steps * dt, knots)
     theta = .02 * (np.exp(-((t - .3 * t[-1]) / (.1 * t[-1])) ** 2) + np.exp(-((t - .7 * t[-1]) / (.1 * t[-1])) ** 2))
     theta *= rng.uniform(.8, 1.2, knots)
-    prop = Propagation(engine, psi0, dt, steps, t, mask, tol=1e-13, maxdim=30, checkpoint=checkpoint)
+    prop = Propagation(engine, psi0, dt, steps, t, mask, tol=1e-12, maxdim=30, checkpoint=checkpoint)
     prop.forward(theta)                                   # warm-up (generated kernels, workspaces)
     prop.gradient()
     torch.cuda.synchronize(device)
