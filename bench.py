@@ -272,9 +272,9 @@ def batched_leg(torch, device, steps, count=32):
     return out
 
 
-def adjoint_leg(torch, device, steps=64, knots=32, checkpoint=32):
+def adjoint_leg(torch, device, steps=128, knots=32, checkpoint=32):
     """Adjoint gradient on the Arnoldi grid widened to l <= 4: `steps` fixed Arnoldi steps
-    (dt 0.02, Krylov tolerance 1e-12, maxdim 30) under a field of `knots` seeded samples
+    (dt 0.005, Krylov tolerance 1e-12, maxdim 30) under a field of `knots` seeded samples
     (two pulses, peak 0.02 a.u.); objective = probability of electron 2 beyond 20 a.u.
     Reports the forward and backward times and their ratio."""
     from laqphysics_b200 import workloads
@@ -288,7 +288,7 @@ def adjoint_leg(torch, device, steps=64, knots=32, checkpoint=32):
     check_complex_symmetric(engine)
     r = np.asarray(h.r).real
     mask = np.broadcast_to((r > 20.)[None, :, None], h.shape).astype(float).ravel(order='F')
-    dt = .02
+    dt = .005
     rng = np.random.default_rng(512)
     t = np.linspace(0, steps * dt, knots)
     theta = .02 * (np.exp(-((t - .3 * t[-1]) / (.1 * t[-1])) ** 2) + np.exp(-((t - .7 * t[-1]) / (.1 * t[-1])) ** 2))
@@ -304,7 +304,7 @@ def adjoint_leg(torch, device, steps=64, knots=32, checkpoint=32):
     grad = prop.gradient()
     torch.cuda.synchronize(device)
     t2 = time.perf_counter()
-    return {'workload': f'adjoint gradient: l1,l2<=4 L<=2 (nc={h.nc}, n={h.n}), {steps} Arnoldi steps dt 0.02, '
+    return {'workload': f'adjoint gradient: l1,l2<=4 L<=2 (nc={h.nc}, n={h.n}), {steps} Arnoldi steps dt 0.005, '
                         f'{knots} field samples, checkpoint {checkpoint}, objective P(r2 > 20 a.u.)',
             'objective': J, 'forward_ms': (t1 - t0) * 1e3, 'backward_ms': (t2 - t1) * 1e3,
             'backward_over_forward': (t2 - t1) / (t1 - t0), 'gradient_norm': float(np.linalg.norm(grad))}
