@@ -275,7 +275,8 @@ def batched_leg(torch, device, steps, count=32):
 def adjoint_leg(torch, device, steps=128, knots=32, checkpoint=32):
     """Adjoint gradient on the Arnoldi grid widened to l <= 4: `steps` fixed Arnoldi steps
     (dt 0.005, Krylov tolerance 1e-12, maxdim 30) under a field of `knots` seeded samples
-    (two pulses, peak 0.02 a.u.); objective = probability of electron 2 beyond 20 a.u.
+    (two pulses, peak 0.02 a.u.); objective = population of the total-L = 1 channels
+    (the dipole-excited part of the two-electron state).
     Reports the forward and backward times and their ratio."""
     from laqphysics_b200 import workloads
     from laqphysics_b200.adjoint import Propagation, check_complex_symmetric
@@ -286,8 +287,8 @@ def adjoint_leg(torch, device, steps=128, knots=32, checkpoint=32):
     psi0 = (g.reshape(h.shape, order='F') * ratio[:, None, None] * ratio[None, :, None]).ravel(order='F')
     engine = B200Hamiltonian(h, device)
     check_complex_symmetric(engine)
-    r = np.asarray(h.r).real
-    mask = np.broadcast_to((r > 20.)[None, :, None], h.shape).astype(float).ravel(order='F')
+    dipole = np.array([float(L == 1) for _, _, L in h.basis])   # channels of total L = 1
+    mask = np.broadcast_to(dipole[None, None, :], h.shape).astype(float).ravel(order='F')
     dt = .005
     rng = np.random.default_rng(512)
     t = np.linspace(0, steps * dt, knots)
@@ -305,7 +306,7 @@ def adjoint_leg(torch, device, steps=128, knots=32, checkpoint=32):
     torch.cuda.synchronize(device)
     t2 = time.perf_counter()
     return {'workload': f'adjoint gradient: l1,l2<=4 L<=2 (nc={h.nc}, n={h.n}), {steps} Arnoldi steps dt 0.005, '
-                        f'{knots} field samples, checkpoint {checkpoint}, objective P(r2 > 20 a.u.)',
+                        f'{knots} field samples, checkpoint {checkpoint}, objective: population of L=1 channels',
             'objective': J, 'forward_ms': (t1 - t0) * 1e3, 'backward_ms': (t2 - t1) * 1e3,
             'backward_over_forward': (t2 - t1) / (t1 - t0), 'gradient_norm': float(np.linalg.norm(grad))}
 
