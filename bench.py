@@ -311,6 +311,33 @@ def adjoint_leg(torch, device, steps=128, knots=32, checkpoint=32):
             'backward_over_forward': (t2 - t1) / (t1 - t0), 'gradient_norm': float(np.linalg.norm(grad))}
 
 
+def spectrum_leg(torch, device):
+    """Channel-resolved tSURFF on the small case of laqphysics_b200.tsurff_run: complex128
+    and mixed-precision propagations with a surface sample every step; spectrum error of
+    the mixed run against the complex128 one, and both wall times."""
+    from laqphysics_b200.tsurff_run import SMALL_CASE, build_case, run, spectrum_error
+    dt = .02
+    engine, contractor, psi0, avec, steps, chi = build_case(SMALL_CASE, device, dt)
+    run(engine, contractor, SMALL_CASE, psi0, avec, dt, 20, chi, 'complex128')   # warm-up (generated kernels)
+    run(engine, contractor, SMALL_CASE, psi0, avec, dt, 20, chi, 'mixed')
+    out = {'workload': f'tSURFF small case: n={engine.n} nc={engine.nc}, {steps} velocity-gauge Arnoldi steps '
+                       f'dt {dt}, surface sample every step, He+ n<=2 channels'}
+    res = {}
+    for precision in ('complex128', 'mixed'):
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        res[precision] = run(engine, contractor, SMALL_CASE, psi0, avec, dt, steps, chi, precision)
+        torch.cuda.synchronize(device)
+        out[precision] = {'steps_per_s': steps / (time.perf_counter() - t0), 'mean_dimension': res[precision][2]}
+    rel, per_label = spectrum_error(res['mixed'][0], res['complex128'][0])
+    p64, p32 = res['complex128'][1], res['mixed'][1]
+    out['spectrum_rel_l2_mixed_vs_fp64'] = rel
+    out['angle_integrated_rel_max_mixed_vs_fp64'] = per_label
+    out['state_rel_l2_mixed_vs_fp64'] = float(torch.linalg.vector_norm(p32 - p64) / torch.linalg.vector_norm(p64))
+    out['norm_error_mixed_vs_fp64'] = float(abs(torch.linalg.vector_norm(p32) - torch.linalg.vector_norm(p64)))
+    return out
+
+
 def run_reference(args, rank):
     """--impl reference: the CPU oracle of the reference's native H·psi on host cores."""
     if rank != 0:
@@ -463,6 +490,7 @@ def main():
                                       cpu_steps=0 if (args.no_cpu_baseline or world > 1 or rank) else 3)
         line['batched'] = batched_leg(torch, device, steps=max(5, min(args.steps, 30)))
         line['adjoint'] = adjoint_leg(torch, device)
+        line['spectrum'] = spectrum_leg(torch, device)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         os.environ.setdefault('OMP_NUM_THREADS', str(os.cpu_count()))

@@ -54,3 +54,44 @@ def spectrum_error(acc_test, acc_ref):
     rel = float(np.linalg.norm(pes_t - pes_r) / np.linalg.norm(pes_r))
     per_label = float(np.max(np.linalg.norm(tot_t - tot_r, axis=1) / np.linalg.norm(tot_r, axis=1)))
     return rel, per_label
+
+
+# A small channel-resolved case (the spectrum test and the bench's spectrum leg):
+# 8 elements of order 4 to 12 a.u. + 8-point ECS tail, coupled l <= 1, L <= 1, surface at
+# 8 a.u., 2-cycle sin^2 pulse omega 2.0 a.u. with peak field 0.3 a.u., He+ n <= 2 labels.
+SMALL_CASE = {'radial': {'edges': [0, 1, 2, 3, 4, 6, 8, 10, 12], 'order': 4, 'tail': 8, 'ecs_angle': .3},
+              'lmax': 1, 'M': 0, 'total_Lmax': 1, 'cutoff_radii': [3, 4], 'surface': 8.,
+              'pulses': [{'pulse': {'omega': 2.0, 'cycles': 2, 'field': .3}, 'polarization': 'z'}],
+              'ionic_channels': [[1, 0, 0], [2, 0, 0], [2, 1, 0]],
+              'spectrum_energy': [.3, 2.3, 21], 'spectrum': {'theta_points': 4, 'phi_points': 1}}
+
+
+def build_case(config, device, dt=.02, after=1.0):
+    """Engine, contractor, initial state (scaled ground state, python/run3d.py:134-136),
+    vector potential, step count (pulse + `after` a.u.) and channel functions of a config."""
+    from .engine import B200Hamiltonian
+    from .pulses import Pulse
+    from .surface3d import Ionic
+    from .surface_contract import SurfaceContractor
+    from .workloads import coupled
+    rc = config['radial']
+    build = lambda angle: coupled(rc['edges'], rc['order'], config['lmax'], config['total_Lmax'], ecs_angle=angle,
+                                  tail=rc['tail'], cutoff_radii=tuple(config['cutoff_radii']))
+    h, hreal = build(rc['ecs_angle']), build(0.)
+    base = h.uncoupled
+    base.prepare_surface(config['surface'])
+    h.prepare_surface(config['surface'])
+    labels = [tuple(x) for x in config['ionic_channels']]
+    unique = list(dict.fromkeys((n, l, abs(m)) for n, l, m in labels))
+    columns = [unique.index((n, l, abs(m))) for n, l, m in labels]
+    ion = Ionic(base, {m for n, l, m in unique})
+    contractor = SurfaceContractor(base, ion, labels, unique, columns, True, h.transform, device)
+    pulse = Pulse(**config['pulses'][0]['pulse'])
+    avec = lambda t: np.array([0., 0., float(pulse.vector(t))])
+    _, g, _ = hreal.ground(tol=1e-10)
+    ratio = np.sqrt(h.grid.weights / hreal.grid.weights)
+    psi0 = (g.reshape(h.shape, order='F') * ratio[:, None, None] * ratio[None, :, None]).ravel(order='F')
+    engine = B200Hamiltonian(h, device)
+    steps = int(round((pulse.duration + after) / dt))
+    chi = ionic_channel_functions(ion, unique, avec, dt, steps)
+    return engine, contractor, psi0, avec, steps, chi
