@@ -68,57 +68,64 @@ def profile_traffic(name):
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle sampling while the timed region runs."""
-    QUERY = ('clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,'
-             'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,'
-             'clocks_event_reasons.sw_power_cap')
+    """SM clock and clock-event reasons sampled through NVML (read-only queries) every
+    millisecond while the timed region runs; falls back to nvidia-smi polling."""
+    REASONS = {'hw_slowdown': 0x8, 'hw_thermal_slowdown': 0x40, 'sw_thermal_slowdown': 0x20, 'sw_power_cap': 0x4}
 
     def __init__(self, gpu_id):
         self.gpu_id = gpu_id
-        self.proc = None
-        self.lines = []
+        self.samples, self.reason_bits, self.max_mhz = [], 0, None
+        self.stop = threading.Event()
+        self.nvml = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            if isinstance(gpu_id, str) and gpu_id.startswith('GPU-'):
+                self.handle = pynvml.nvmlDeviceGetHandleByUUID(gpu_id)
+            else:
+                self.handle = pynvml.nvmlDeviceGetHandleByIndex(int(gpu_id))
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM))
+            self.nvml = pynvml
+        except Exception:
+            self.nvml = None
 
     def __enter__(self):
-        try:
-            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.gpu_id), f'--query-gpu={self.QUERY}',
-                                          '--format=csv,noheader,nounits', '-lms', '50'],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
-        except (OSError, FileNotFoundError):
-            self.proc = None
+        self.stop.clear()
+        self.thread = threading.Thread(target=self._poll if self.nvml else self._smi, daemon=True)
+        self.thread.start()
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _poll(self):
+        nv = self.nvml
+        while not self.stop.is_set():
+            try:
+                self.samples.append(float(nv.nvmlDeviceGetClockInfo(self.handle, nv.NVML_CLOCK_SM)))
+                self.reason_bits |= int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.handle))
+            except Exception:
+                return
+            time.sleep(0.001)
+
+    def _smi(self):
+        query = 'clocks.sm,clocks.max.sm,clocks_event_reasons.active'
+        while not self.stop.is_set():
+            try:
+                out = subprocess.run(['nvidia-smi', '-i', str(self.gpu_id), f'--query-gpu={query}',
+                                      '--format=csv,noheader,nounits'], capture_output=True, text=True, timeout=5)
+                sm, mx, active = [x.strip() for x in out.stdout.split(',')[:3]]
+                self.samples.append(float(sm))
+                self.max_mhz = float(mx)
+                self.reason_bits |= int(active, 16) if active.startswith('0x') else 0
+            except Exception:
+                return
 
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-            self.thread.join(timeout=2)
+        self.stop.set()
+        self.thread.join(timeout=5)
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
-        for line in self.lines:
-            parts = [x.strip() for x in line.split(',')]
-            if len(parts) < 8:
-                continue
-            try:
-                sm.append(float(parts[0]))
-                mx = float(parts[1])
-            except ValueError:
-                continue
-            for name, flag in zip(names, parts[4:8]):
-                if flag.lower() in ('active', '1'):
-                    reasons.add(name)
-        return {'sm_mhz': float(np.median(sm)) if sm else None, 'sm_max_mhz': mx, 'samples': len(sm),
-                'reasons': sorted(reasons)}
+        reasons = sorted(name for name, bit in self.REASONS.items() if self.reason_bits & bit)
+        return {'sm_mhz': float(np.median(self.samples)) if self.samples else None, 'sm_max_mhz': self.max_mhz,
+                'samples': len(self.samples), 'reasons': reasons, 'source': 'nvml' if self.nvml else 'nvidia-smi'}
 
 
 def gpu_identifier(torch, device):
