@@ -255,12 +255,17 @@ int he_device_status(he_handle h);
  * on the first tiled apply and cached by source); 0 uses the table-driven kernel.
  * he_mix_status: 0 not compiled yet, 1 generated kernel in use, -1 it failed to compile
  * (the table-driven kernel runs instead; he_last_error has the log).
+ * he_set_mix_blocks(h, precision, b): size the generated kernel's register budget for b
+ *   CTAs of 128 threads per SM (1..8; defaults 2 for HE_C128, 4 for HE_C64); the kernel is
+ *   recompiled (or taken from the cache) on the next apply.  The autotuner of
+ *   laqphysics_b200.engine (B200Hamiltonian.autotune) times the choices.
  * he_plan_mix_source / he_plan_mix_program / he_nvrtc_check: the generated source and the
  * mixing program (JSON) of a planner handle, and an NVRTC compile check for sm_100a
  * (host only).
  * ---------------------------------------------------------------------------------- */
 int he_set_mix(he_handle h, int generated);
 int he_mix_status(he_handle h);
+int he_set_mix_blocks(he_handle h, int precision, int blocks);
 long long he_plan_mix_source(void *plan, int dipole_real, char *buf, long long cap);
 long long he_plan_mix_program(void *plan, char *buf, long long cap);
 int he_nvrtc_check(const char *src, char *log, long long cap);

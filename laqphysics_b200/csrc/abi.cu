@@ -269,6 +269,23 @@ extern "C" int he_set_mix(he_handle h, int generated)
     return HE_OK;
 }
 
+extern "C" int he_set_mix_blocks(he_handle h, int precision, int blocks)
+{
+    if (!h) return he_fail(HE_ERR_ARG, "null handle", __FILE__, __LINE__);
+    if (precision != HE_C128 && precision != HE_C64)
+        return he_fail(HE_ERR_ARG, "precision must be HE_C128 or HE_C64", __FILE__, __LINE__);
+    if (blocks < 1 || blocks > 8) return he_fail(HE_ERR_ARG, "blocks per SM must be in [1, 8]", __FILE__, __LINE__);
+    const int p = precision == HE_C128 ? 0 : 1;
+    if (h->mix_blocks[p] != blocks) {
+        h->mix_blocks[p] = blocks;
+        for (int v = 2 * p; v < 2 * p + 2; ++v) {   // recompiled (or found in the cache) on the next apply
+            h->mix_state[v] = 0;
+            h->mix_kern[v] = nullptr;
+        }
+    }
+    return HE_OK;
+}
+
 extern "C" int he_mix_status(he_handle h)
 {
     if (!h) return he_fail(HE_ERR_ARG, "null handle", __FILE__, __LINE__);

@@ -412,6 +412,39 @@ __device__ __forceinline__ void band_r2(const C *S, int P, int x0, int y0, int i
         if (s < gks) cmma_ba(cr, ci, cf[s * 32 + lane], s_load(b + 4 * s * P), real);
 }
 
+// The same two sweeps for all BAND_CG column groups of the tile at once: the k-step loop
+// is outermost, so every k-step issues 2 * BAND_CG independent accumulation chains (the
+// DMMA latency of one chain is hidden behind the others).  Column group q covers columns
+// j0 + 8 q + (0..7); groups past the grid have gks_c[q] = 0 (and zero fragments).
+template <typename C>
+__device__ __forceinline__ void band_r1_tile(const C *S, int P, int x0, int y0, int j0, int glo, int gks, bool real,
+                                             const double2 (&rf)[BAND_KS], int lr, int lk,
+                                             double (&cr)[BAND_CG][2], double (&ci)[BAND_CG][2])
+{
+    const C *a = S + (j0 + lr - y0) * P + (glo + lk - x0);
+#pragma unroll
+    for (int s = 0; s < BAND_KS; ++s)
+        if (s < gks) {
+#pragma unroll
+            for (int q = 0; q < BAND_CG; ++q) cmma_ab(cr[q], ci[q], s_load(a + 8 * q * P + 4 * s), rf[s], real);
+        }
+}
+
+template <typename C>
+__device__ __forceinline__ void band_r2_tile(const C *S, int P, int x0, int y0, int i0, const int (&glo_c)[BAND_CG],
+                                             const int (&gks_c)[BAND_CG], const bool (&real_c)[BAND_CG],
+                                             const double2 *cf, size_t cf_stride, int lane, int lr, int lk,
+                                             double (&cr)[BAND_CG][2], double (&ci)[BAND_CG][2])
+{
+#pragma unroll
+    for (int s = 0; s < BAND_KS; ++s)
+#pragma unroll
+        for (int q = 0; q < BAND_CG; ++q)
+            if (s < gks_c[q])
+                cmma_ba(cr[q], ci[q], cf[q * cf_stride + s * 32 + lane],
+                        s_load(S + (glo_c[q] + lk + 4 * s - y0) * P + (i0 + lr - x0)), real_c[q]);
+}
+
 template <typename R> __device__ __forceinline__ cplx<R> narrow(double re, double im) { return mk<R>((R)re, (R)im); }
 
 // Work items are (row tile, column tile, channel of the batch): the batch's instances are
@@ -427,7 +460,8 @@ hpsi_band_kernel(const __grid_constant__ CUtensorMap tmap, const DeviceTables<R>
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char *smem = smem_raw + ((KIN_STAGE_ALIGN - (smem_u32(smem_raw) & (KIN_STAGE_ALIGN - 1))) & (KIN_STAGE_ALIGN - 1));
     double2 *CF = reinterpret_cast<double2 *>(smem + 2 * (size_t)bp.stage_bytes);   // [BAND_CG][BAND_KS][32]
-    uint64_t *bar = reinterpret_cast<uint64_t *>(CF + BAND_CG * BAND_KS * 32);
+    double2 *CFB = CF + BAND_CG * BAND_KS * 32;   // velocity gauge: the B fragments of the same groups
+    uint64_t *bar = reinterpret_cast<uint64_t *>(CFB + (VEL ? BAND_CG * BAND_KS * 32 : 0));
     constexpr int ALIGN = 16 / (int)sizeof(C);   // nodes per 16 bytes (TMA start alignment)
     const int n = bp.n, nc = bp.nc, P = bp.box_r, G = bp.ngroup, nch = nc * fb.count;
     const size_t nn = (size_t)n * n;
@@ -476,6 +510,8 @@ hpsi_band_kernel(const __grid_constant__ CUtensorMap tmap, const DeviceTables<R>
             for (int idx = threadIdx.x; idx < BAND_CG * BAND_KS * 32; idx += BAND_THREADS) {
                 const int g = tc * BAND_CG + idx / (BAND_KS * 32);
                 CF[idx] = g < G ? bp.frag[(size_t)g * BAND_KS * 32 + idx % (BAND_KS * 32)] : make_double2(0, 0);
+                if (VEL)
+                    CFB[idx] = g < G ? bp.fragb[(size_t)g * BAND_KS * 32 + idx % (BAND_KS * 32)] : make_double2(0, 0);
             }
             cur_tc = tc;
             __syncthreads();
@@ -492,56 +528,58 @@ hpsi_band_kernel(const __grid_constant__ CUtensorMap tmap, const DeviceTables<R>
         if (gr >= G) continue;
         const C *S = reinterpret_cast<const C *>(smem + (size_t)stage * bp.stage_bytes);
         const int x0 = bp.brbase[tr] / ALIGN * ALIGN, y0 = bp.bcbase[tc], i0 = gr * BAND_G;
+        int glo_c[BAND_CG], gks_c[BAND_CG];
+        bool real_c[BAND_CG], breal_c[BAND_CG];
+#pragma unroll
+        for (int q = 0; q < BAND_CG; ++q) {
+            const int gc = tc * BAND_CG + q;
+            const bool in = gc < G;
+            glo_c[q] = in ? bp.glo[gc] : 0;
+            gks_c[q] = in ? bp.gks[gc] : 0;
+            real_c[q] = in ? (bp.greal[gc] & 1) != 0 : true;
+            breal_c[q] = in ? (bp.greal[gc] & 2) != 0 : true;
+        }
+        const int j0 = tc * BAND_TC;
         if (VEL) {   // commutator stencils W1 (electron 1), W2 (electron 2) with the B fragments
             double2 bf[BAND_KS];
 #pragma unroll
             for (int s = 0; s < BAND_KS; ++s) bf[s] = bp.fragb[((size_t)gr * BAND_KS + s) * 32 + lane];
             const bool breal_r = (bp.greal[gr] & 2) != 0;
+            double cr[BAND_CG][2] = {}, ci[BAND_CG][2] = {};
+            band_r1_tile(S, P, x0, y0, j0, glo_r, gks_r, breal_r, bf, lr, lk, cr, ci);
+            double dr[BAND_CG][2] = {}, di[BAND_CG][2] = {};
+            band_r2_tile(S, P, x0, y0, i0, glo_c, gks_c, breal_c, CFB, (size_t)BAND_KS * 32, lane, lr, lk, dr, di);
 #pragma unroll
-            for (int q = 0; q < BAND_CG; ++q) {
-                const int gc = tc * BAND_CG + q, j0 = gc * BAND_G;
-                if (gc >= G) break;
-                double cr[2] = {0, 0}, ci[2] = {0, 0};
-                band_r1(S, P, x0, y0, j0, glo_r, gks_r, breal_r, bf, lr, lk, cr, ci);
-#pragma unroll
-                for (int u = 0; u < 2; ++u) {
-                    const int i = i0 + 2 * lk + u, j = j0 + lr;
-                    if (i < n && j < n) w1[(size_t)i + (size_t)n * j + nn * c] = narrow<R>(cr[u], ci[u]);
-                }
-                double dr[2] = {0, 0}, di[2] = {0, 0};
-                band_r2(S, P, x0, y0, i0, bp.glo[gc], bp.gks[gc], (bp.greal[gc] & 2) != 0,
-                        bp.fragb + (size_t)gc * BAND_KS * 32, lane, lr, lk, dr, di);
+            for (int q = 0; q < BAND_CG; ++q)
 #pragma unroll
                 for (int u = 0; u < 2; ++u) {
-                    const int i = i0 + 2 * lk + u, j = j0 + lr;
-                    if (i < n && j < n) w2[(size_t)i + (size_t)n * j + nn * c] = narrow<R>(dr[u], di[u]);
+                    const int i = i0 + 2 * lk + u, j = j0 + 8 * q + lr;
+                    if (i < n && j < n) {
+                        w1[(size_t)i + (size_t)n * j + nn * c] = narrow<R>(cr[q][u], ci[q][u]);
+                        w2[(size_t)i + (size_t)n * j + nn * c] = narrow<R>(dr[q][u], di[q][u]);
+                    }
                 }
-            }
         }
         const double *fv = fb.f[inst];
         const double a2 = VEL ? fv[0] * fv[0] + fv[1] * fv[1] + fv[2] * fv[2] : 0.0;
+        double cr[BAND_CG][2] = {}, ci[BAND_CG][2] = {};
+        band_r1_tile(S, P, x0, y0, j0, glo_r, gks_r, real_r, rf, lr, lk, cr, ci);
+        band_r2_tile(S, P, x0, y0, i0, glo_c, gks_c, real_c, CF, (size_t)BAND_KS * 32, lane, lr, lk, cr, ci);
 #pragma unroll
-        for (int q = 0; q < BAND_CG; ++q) {
-            const int gc = tc * BAND_CG + q, j0 = gc * BAND_G;
-            if (gc >= G) break;
-            double cr[2] = {0, 0}, ci[2] = {0, 0};
-            band_r1(S, P, x0, y0, j0, glo_r, gks_r, real_r, rf, lr, lk, cr, ci);
-            band_r2(S, P, x0, y0, i0, bp.glo[gc], bp.gks[gc], (bp.greal[gc] & 1) != 0, CF + q * BAND_KS * 32, lane,
-                    lr, lk, cr, ci);
+        for (int q = 0; q < BAND_CG; ++q)
 #pragma unroll
             for (int u = 0; u < 2; ++u) {
-                const int i = i0 + 2 * lk + u, j = j0 + lr;
+                const int i = i0 + 2 * lk + u, j = j0 + 8 * q + lr;
                 if (i < n && j < n) {
                     const double2 x = s_load(S + (j - y0) * P + (i - x0));
                     const size_t p = (size_t)i + (size_t)n * j;
                     const C dd = SEP ? cadd<R>(ldg<R>(t.d1 + i + (size_t)n * cc), ldg<R>(t.d2 + j + (size_t)n * cc))
                                      : ldg<R>(t.diag + p + nn * cc);
-                    double2 v = cfma<double>(make_double2((double)dd.x, (double)dd.y), x, make_double2(cr[u], ci[u]));
+                    double2 v = cfma<double>(make_double2((double)dd.x, (double)dd.y), x, make_double2(cr[q][u], ci[q][u]));
                     if (VEL) v = rfma<double>(a2, x, v);
                     out[p + nn * c] = narrow<R>(v.x, v.y);
                 }
             }
-        }
     }
 }
 
@@ -650,7 +688,8 @@ int launch_band(he_operator *h, const DeviceTables<R> &t, const BandPlan<R> &bp,
                                     bp.box_c, sizeof(R));
     if (!mp) return he_fail(HE_ERR_CUDA, "cuTensorMapEncodeTiled failed", __FILE__, __LINE__);
     const CUtensorMap map = *mp;
-    const size_t smem = 2 * (size_t)bp.stage_bytes + (size_t)BAND_CG * BAND_KS * 32 * sizeof(double2) + 16 + KIN_STAGE_ALIGN;
+    const size_t smem = 2 * (size_t)bp.stage_bytes + (velocity ? 2 : 1) * (size_t)BAND_CG * BAND_KS * 32 * sizeof(double2) +
+                        16 + KIN_STAGE_ALIGN;
     const long long items = (long long)bp.ntr * bp.nct * bp.nc * fb.count;
     const int per_sm = std::max(1, (int)((227 * 1024) / (smem + 1024)));
     const unsigned grid = (unsigned)std::min<long long>(items, (long long)per_sm * sm_count(h->device));

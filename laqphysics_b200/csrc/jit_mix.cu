@@ -75,7 +75,7 @@ std::string lit(double v)
 // the complex128 groups need more registers than the complex64 ones.
 constexpr int MIXJ_MIN_BLOCKS_D = 2, MIXJ_MIN_BLOCKS_F = 4;
 
-std::string mix_entry(int v);
+std::string mix_entry(int v, int min_blocks);
 
 // CUDA source of the generated kernel for a plan (variant -1: all four entry points,
 // -2: none, 0..3: one).  `dipole_real`: every dcoef entry is
@@ -203,20 +203,22 @@ std::string mix_source(const he_plan_host &P, bool dipole_real, int variant)
     o.str("");
     o << "#define HE_BATCH_MAX " << HE_BATCH_MAX << "\n" << kPrelude << group_fns << body;
     if (variant == -1)
-        for (int v = 0; v < 4; ++v) o << mix_entry(v);
+        for (int v = 0; v < 4; ++v) o << mix_entry(v, 0);
     else if (variant >= 0)
-        o << mix_entry(variant);
+        o << mix_entry(variant, 0);
     return o.str();
 }
 
-// Entry point of one variant: 0/1 complex128 length/velocity, 2/3 complex64.
-std::string mix_entry(int v)
+// Entry point of one variant: 0/1 complex128 length/velocity, 2/3 complex64; min_blocks
+// (> 0) overrides the default CTAs per SM of the register budget.
+std::string mix_entry(int v, int min_blocks)
 {
     const char *names[4] = {"he_mix_d0", "he_mix_d1", "he_mix_f0", "he_mix_f1"};
     const bool dbl = v < 2, vel = v & 1;
     const char *R = dbl ? "double" : "float", *C = dbl ? "cd" : "cf";
     std::ostringstream o;
-    o << "extern \"C\" __global__ void __launch_bounds__(128, " << (dbl ? MIXJ_MIN_BLOCKS_D : MIXJ_MIN_BLOCKS_F) << ") "
+    const int blocks = min_blocks > 0 ? min_blocks : (dbl ? MIXJ_MIN_BLOCKS_D : MIXJ_MIN_BLOCKS_F);
+    o << "extern \"C\" __global__ void __launch_bounds__(128, " << blocks << ") "
       << names[v] << "(const " << C << " *psi, " << C << " *out, const " << C << " *rad, const " << C << " *rt, const " << C
       << " *w1, const " << C << " *w2, const " << C << " *dcoef, const " << R
       << " *ldiff, long long nn, int n, int nd, int nc, const FieldBatch fs, " << C << " beta, " << C
@@ -328,7 +330,7 @@ int jit_mix_prepare(he_operator *h, int variant)
 {
     if (h->mix_state[variant] != 0) return h->mix_state[variant] > 0 ? HE_OK : HE_ERR_UNSUPPORTED;
     std::lock_guard<std::mutex> lock(g_jit_mutex);
-    const std::string src = h->mix_src + mix_entry(variant);
+    const std::string src = h->mix_src + mix_entry(variant, h->mix_blocks[variant < 2 ? 0 : 1]);
     auto it = g_jit_cache.find(src);
     if (it == g_jit_cache.end()) {
         std::string log;

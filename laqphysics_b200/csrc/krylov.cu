@@ -390,16 +390,13 @@ __device__ void expm_pade13(double2 *A, double2 *R, double2 *work, int m)
     }
 }
 
-// Arnoldi check at iteration j (python/propagate.py:28-38): on happy breakdown or at
-// j >= 3 with (j+1) % 4 == 0 or j+1 == maxdim, form c = expm(-i dt H_m)[:, 0] beta
-// and err = |dt h_{m+1,m} c_{m-1}|; accept if happy or err < tol.
-__global__ void __launch_bounds__(512)
-arnoldi_check_kernel(const double2 *__restrict__ H, int ld, size_t hs, int j, int maxdim, double dt, double tol,
-                     double2 *__restrict__ coef, double2 *__restrict__ work, size_t ws, KrylovStatus *st)
+// Arnoldi check at iteration j (python/propagate.py:28-38) by the whole calling block: on
+// happy breakdown or at j >= 3 with (j+1) % 4 == 0 or j+1 == maxdim, form
+// c = expm(-i dt H_m)[:, 0] beta and err = |dt h_{m+1,m} c_{m-1}|; accept if happy or
+// err < tol.  H, coef, work and st are this instance's slices.
+__device__ __noinline__ void arnoldi_check_block(const double2 *__restrict__ H, int ld, int j, int maxdim, double dt, double tol,
+                                    double2 *__restrict__ coef, double2 *__restrict__ work, KrylovStatus *st)
 {
-    const int inst = blockIdx.x;
-    H += inst * hs; coef += (size_t)inst * ld; work += inst * ws; st += inst;
-    if (st->done) return;
     const int m = j + 1;
     const bool happy = st->happy;
     const bool check = happy || (j >= 3 && ((j + 1) % 4 == 0 || j + 1 == maxdim));
@@ -425,6 +422,196 @@ arnoldi_check_kernel(const double2 *__restrict__ H, int ld, size_t hs, int j, in
     }
 }
 
+__global__ void __launch_bounds__(512)
+arnoldi_check_kernel(const double2 *__restrict__ H, int ld, size_t hs, int j, int maxdim, double dt, double tol,
+                     double2 *__restrict__ coef, double2 *__restrict__ work, size_t ws, KrylovStatus *st)
+{
+    const int inst = blockIdx.x;
+    H += inst * hs; coef += (size_t)inst * ld; work += inst * ws; st += inst;
+    if (st->done) return;
+    arnoldi_check_block(H, ld, j, maxdim, dt, tol, coef, work, st);
+}
+
+// ---------------------------------------------------------------------------------
+// One Arnoldi iteration in three sweeps (kc = j + 1 <= KRYLOV_FUSED basis vectors):
+//   project:  z = Q^H v                                    (H[:, j] += z)
+//   reorth:   v' = v - Q z; z' = Q^H v'; |v'|^2             (H[:, j] += z')
+//             h = sqrt(|v'|^2 - |z'|^2) = |v' - Q z'|        (H[j+1, j], happy flag)
+//             + the Arnoldi check on the same block
+//   next:     Q_{j+1} = (v' - Q z') / h                       (skipped once done)
+// Each reduction ends in the last block to finish (ticket counter): it sums the block
+// partials in a fixed order (lane l adds blocks l, l+32, ... in sequence, then a butterfly),
+// so results do not depend on timing.  |v'' |^2 = |v'|^2 - |z'|^2 holds because Q has
+// orthonormal columns; after the first sweep |z'| is at rounding level, so the subtraction
+// loses nothing.
+// ---------------------------------------------------------------------------------
+constexpr int KRYLOV_LANE_LOADS = (KRYLOV_BLOCKS + 31) / 32;
+
+// Fixed-order sum of nb <= KRYLOV_BLOCKS partials p[b * ld] by one warp (all loads issued
+// before the adds; L1 bypassed, the partials come from other SMs).
+__device__ __forceinline__ double2 ordered_partial_sum(const double2 *p, int nb, int ld)
+{
+    const int lane = threadIdx.x & 31;
+    double2 v[KRYLOV_LANE_LOADS];
+#pragma unroll
+    for (int i = 0; i < KRYLOV_LANE_LOADS; ++i) {
+        const int b = lane + 32 * i;
+        v[i] = b < nb ? __ldcg(p + (size_t)b * ld) : mk<double>(0, 0);
+    }
+    double2 s = mk<double>(0, 0);
+#pragma unroll
+    for (int i = 0; i < KRYLOV_LANE_LOADS; ++i) s = cadd<double>(s, v[i]);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        s.x += __shfl_xor_sync(0xffffffffu, s.x, off);
+        s.y += __shfl_xor_sync(0xffffffffu, s.y, off);
+    }
+    return s;
+}
+
+// Every thread has written its partials; returns true in the last block to arrive (which
+// then sees every block's partials).  No waiting: the other blocks just return.
+__device__ __forceinline__ bool arrive_last(unsigned int *ticket)
+{
+    __shared__ int s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (s_last) __threadfence();
+    return s_last;
+}
+
+// project: partials of conj(Q_k) v, last block -> z, H[:, j] += z.  With src32, v is first
+// filled from the complex64 operator result (mixed precision).
+template <int KT>
+__global__ void __launch_bounds__(KRYLOV_THREADS)
+arnoldi_project_kernel(const double2 *__restrict__ Q, size_t n, size_t qs, int kc, double2 *__restrict__ v,
+                       const float2 *__restrict__ src32, double2 *__restrict__ partial, int ld,
+                       unsigned int *__restrict__ ticket, double2 *__restrict__ z, double2 *__restrict__ H, size_t hs,
+                       int j, const KrylovStatus *st)
+{
+    const int inst = blockIdx.y;
+    Q += inst * n; v += inst * n; partial += (size_t)inst * gridDim.x * ld; st += inst;
+    z += (size_t)inst * ld; H += inst * hs; ticket += inst;
+    if (src32) src32 += inst * n;
+    if (st->done) return;
+    double2 acc[KT];
+#pragma unroll
+    for (int k = 0; k < KT; ++k) acc[k] = mk<double>(0, 0);
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        double2 x;
+        if (src32) {
+            const float2 f = src32[p];
+            x = mk<double>((double)f.x, (double)f.y);
+            v[p] = x;
+        } else {
+            x = v[p];
+        }
+#pragma unroll
+        for (int k = 0; k < KT; ++k)
+            if (k < kc) acc[k] = cfma_conj<double>(Q[(size_t)k * qs + p], x, acc[k]);
+    }
+    __shared__ double2 res[KT];
+    block_sum<KT>(acc, res);
+    __syncthreads();
+    if (threadIdx.x < kc) partial[(size_t)blockIdx.x * ld + threadIdx.x] = res[threadIdx.x];
+    if (!arrive_last(ticket)) return;
+    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (int k = warp; k < kc; k += nwarps) {
+        const double2 s = ordered_partial_sum(partial + k, gridDim.x, ld);
+        if ((threadIdx.x & 31) == 0) {
+            z[k] = s;
+            H[k + (size_t)j * ld] = cadd<double>(H[k + (size_t)j * ld], s);
+        }
+    }
+    if (threadIdx.x == 0) *ticket = 0;
+}
+
+// reorth: v' = v - Q z written; partials of conj(Q_k) v' and |v'|^2 (column kc); last
+// block -> z' (into z), H[:, j] += z', h, happy flag, then the Arnoldi check.
+template <int KT>
+__global__ void __launch_bounds__(KRYLOV_THREADS)
+arnoldi_reorth_kernel(const double2 *__restrict__ Q, size_t n, size_t qs, int kc, double2 *__restrict__ z,
+                      double2 *__restrict__ v, double2 *__restrict__ partial, int ld, unsigned int *__restrict__ ticket,
+                      double2 *__restrict__ H, size_t hs, int j, int maxdim, double dt, double tol,
+                      double2 *__restrict__ coef, double2 *__restrict__ work, size_t ws, KrylovStatus *st,
+                      double happy_below)
+{
+    const int inst = blockIdx.y;
+    Q += inst * n; v += inst * n; partial += (size_t)inst * gridDim.x * ld; st += inst;
+    z += (size_t)inst * ld; H += inst * hs; ticket += inst; coef += (size_t)inst * ld; work += inst * ws;
+    if (st->done) return;
+    __shared__ double2 zs[KT];
+    for (int k = threadIdx.x; k < kc; k += blockDim.x) zs[k] = z[k];
+    __syncthreads();
+    double2 acc[KT + 1];
+#pragma unroll
+    for (int k = 0; k <= KT; ++k) acc[k] = mk<double>(0, 0);
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        double2 x = v[p];
+#pragma unroll
+        for (int k = 0; k < KT; ++k)
+            if (k < kc) x = cfma<double>(mk<double>(-zs[k].x, -zs[k].y), Q[(size_t)k * qs + p], x);
+        v[p] = x;
+#pragma unroll
+        for (int k = 0; k < KT; ++k)
+            if (k < kc) acc[k] = cfma_conj<double>(Q[(size_t)k * qs + p], x, acc[k]);
+        acc[KT].x += cabs2<double>(x);
+    }
+    __shared__ double2 res[KT + 1];
+    block_sum<KT + 1>(acc, res);
+    __syncthreads();
+    if (threadIdx.x < kc) partial[(size_t)blockIdx.x * ld + threadIdx.x] = res[threadIdx.x];
+    if (threadIdx.x == kc) partial[(size_t)blockIdx.x * ld + kc] = res[KT];
+    if (!arrive_last(ticket)) return;
+    __shared__ double2 tot[KT + 1];
+    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (int k = warp; k <= kc; k += nwarps) {
+        const double2 s = ordered_partial_sum(partial + k, gridDim.x, ld);
+        if ((threadIdx.x & 31) == 0) tot[k] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double h2 = tot[kc].x;
+        for (int k = 0; k < kc; ++k) {
+            z[k] = tot[k];
+            H[k + (size_t)j * ld] = cadd<double>(H[k + (size_t)j * ld], tot[k]);
+            h2 -= cabs2<double>(tot[k]);
+        }
+        const double h = sqrt(fmax(h2, 0.0));
+        H[j + 1 + (size_t)j * ld] = mk<double>(h, 0);
+        st->hnext = h;
+        st->happy = h < happy_below;
+        *ticket = 0;
+    }
+    __syncthreads();
+    arnoldi_check_block(H, ld, j, maxdim, dt, tol, coef, work, st);
+}
+
+// next: Q_{j+1} = (v' - Q z') / h in place (and its complex64 copy for the next
+// mixed-precision apply); nothing once the solve is done.
+__global__ void __launch_bounds__(KRYLOV_THREADS)
+arnoldi_next_kernel(const double2 *__restrict__ Q, size_t n, size_t qs, int kc, const double2 *__restrict__ z, int ld,
+                    double2 *__restrict__ v, float2 *__restrict__ out32, const KrylovStatus *st)
+{
+    const int inst = blockIdx.y;
+    Q += inst * n; v += inst * n; z += (size_t)inst * ld; st += inst;
+    if (out32) out32 += inst * n;
+    if (st->done) return;
+    __shared__ double2 zs[KRYLOV_MAXDIM + 1];
+    for (int k = threadIdx.x; k < kc; k += blockDim.x) zs[k] = z[k];
+    __syncthreads();
+    const double s = 1.0 / st->hnext;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        double2 x = v[p];
+        for (int k = 0; k < kc; ++k) x = cfma<double>(mk<double>(-zs[k].x, -zs[k].y), Q[(size_t)k * qs + p], x);
+        x = cscale<double>(s, x);
+        v[p] = x;
+        if (out32) out32[p] = make_float2((float)x.x, (float)x.y);
+    }
+}
+
 }  // namespace he
 
 // =====================================================================================
@@ -435,7 +622,7 @@ using namespace he;
 he_krylov::~he_krylov()
 {
     cudaFree(Q); cudaFree(Z); cudaFree(H); cudaFree(partial); cudaFree(z); cudaFree(coef); cudaFree(work);
-    cudaFree(norm_partial); cudaFree(status); cudaFree(s32[0]); cudaFree(s32[1]);
+    cudaFree(norm_partial); cudaFree(status); cudaFree(ticket); cudaFree(s32[0]); cudaFree(s32[1]);
     if (host_status) cudaFreeHost(host_status);
 }
 
@@ -460,6 +647,8 @@ int krylov_create(he_krylov **out, long long n, int maxdim, int flexible, int co
     if (e == cudaSuccess) e = cudaMalloc(&k->work, c * 8 * ld * ld * sizeof(double2));
     if (e == cudaSuccess) e = cudaMalloc(&k->norm_partial, c * KRYLOV_BLOCKS * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&k->status, c * sizeof(KrylovStatus));
+    if (e == cudaSuccess) e = cudaMalloc(&k->ticket, c * sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMemset(k->ticket, 0, c * sizeof(unsigned int));
     if (e == cudaSuccess) e = cudaMallocHost(&k->host_status, c * sizeof(KrylovStatus));
     if (e != cudaSuccess) {
         he_set_error(cudaGetErrorString(e), __FILE__, __LINE__);
@@ -629,6 +818,31 @@ __global__ void krylov_to_c128(size_t n, const float2 *x, double2 *y)
         y[p] = make_double2((double)x[p].x, (double)x[p].y);
 }
 
+// project + reorth(+ check) sweeps of one fused Arnoldi iteration, with the register tile
+// sized to the basis (4, 8, 12 or 16 vectors).
+template <int KT>
+void launch_fused_sweeps(he_krylov *k, int kc, double2 *v, const float2 *src32, int j, int maxdim, double dt,
+                         double tol, cudaStream_t s)
+{
+    const int ld = k->maxdim + 1;
+    arnoldi_project_kernel<KT><<<bgrid(k), kBlock, 0, s>>>(k->Q, k->n, k->qs(), kc, v, src32, k->partial, ld, k->ticket,
+                                                          k->z, k->H, k->hs(), j, k->status);
+    arnoldi_reorth_kernel<KT><<<bgrid(k), kBlock, 0, s>>>(k->Q, k->n, k->qs(), kc, k->z, v, k->partial, ld, k->ticket,
+                                                         k->H, k->hs(), j, maxdim, dt, tol, k->coef, k->work, k->ws(),
+                                                         k->status, 1e-13);
+}
+
+int fused_sweeps(he_krylov *k, int kc, double2 *v, const float2 *src32, int j, int maxdim, double dt, double tol,
+                 cudaStream_t s)
+{
+    if (kc <= 4) launch_fused_sweeps<4>(k, kc, v, src32, j, maxdim, dt, tol, s);
+    else if (kc <= 8) launch_fused_sweeps<8>(k, kc, v, src32, j, maxdim, dt, tol, s);
+    else if (kc <= 12) launch_fused_sweeps<12>(k, kc, v, src32, j, maxdim, dt, tol, s);
+    else launch_fused_sweeps<KRYLOV_FUSED>(k, kc, v, src32, j, maxdim, dt, tol, s);
+    HE_CUDA_TRY(cudaGetLastError());
+    return HE_OK;
+}
+
 // y_b = exp(-i dt H(fields_b)) x_b for every instance of the workspace.  precision HE_C64:
 // H·psi in complex64 (the basis, CGS2, the Hessenberg exponential and the error estimate
 // stay complex128).  Per-instance dimensions, estimates and convergence go to the optional
@@ -652,18 +866,36 @@ int expv_impl(he_krylov *k, he_handle op, const void *x, void *y, const double *
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
     int rc = krylov_start(k, static_cast<const double2 *>(x), s);
     if (rc) return rc;
+    HE_CUDA_TRY(cudaMemsetAsync(k->ticket, 0, sizeof(unsigned int) * k->count, s));
     const int ld = k->maxdim + 1;
     const dim3 cgrid(std::min<size_t>(KRYLOV_BLOCKS * (size_t)k->count, 4096));
+    const bool mixed = precision == HE_C64;
+    bool have32 = false;   // s32[0] holds the complex64 copy of Q_j (written by the previous iteration)
     for (int j = 0; j < maxdim; ++j) {
         double2 *qj = k->Q + (size_t)j * total, *v = k->Q + (size_t)(j + 1) * total;
-        if (precision == HE_C64) {
-            krylov_to_c64<<<cgrid, kBlock, 0, s>>>(total, qj, k->s32[0]);
+        const int kc = j + 1;
+        const bool fused = kc <= KRYLOV_FUSED;
+        if (mixed) {
+            if (!have32) krylov_to_c64<<<cgrid, kBlock, 0, s>>>(total, qj, k->s32[0]);
             rc = he_apply_batched(op, k->count, k->s32[0], k->s32[1], fields, velocity, HE_C64, stream);
-            krylov_to_c128<<<cgrid, kBlock, 0, s>>>(total, k->s32[1], v);
+            if (!fused) krylov_to_c128<<<cgrid, kBlock, 0, s>>>(total, k->s32[1], v);
         } else {
             rc = he_apply_batched(op, k->count, qj, v, fields, velocity, HE_C128, stream);   // the kernels of every apply
         }
-        if (!rc) rc = krylov_cgs2(k, j + 1, v, k->H + (size_t)j * ld, k->H + (size_t)j * ld + j + 1, s, 1e-13);
+        if (rc) break;
+        have32 = false;
+        if (fused) {   // three sweeps, the check in the second one's last block
+            rc = fused_sweeps(k, kc, v, mixed ? k->s32[1] : nullptr, j, maxdim, dt, tol, s);
+            if (rc) break;
+            if (j + 1 < maxdim) {
+                arnoldi_next_kernel<<<bgrid(k), kBlock, 0, s>>>(k->Q, k->n, k->qs(), kc, k->z, ld, v,
+                                                               mixed ? k->s32[0] : nullptr, k->status);
+                have32 = mixed;
+            }
+            HE_CUDA_TRY(cudaGetLastError());
+            continue;
+        }
+        rc = krylov_cgs2(k, kc, v, k->H + (size_t)j * ld, k->H + (size_t)j * ld + j + 1, s, 1e-13);
         if (rc) break;
         arnoldi_check_kernel<<<k->count, 512, 0, s>>>(k->H, ld, k->hs(), j, maxdim, dt, tol, k->coef, k->work, k->ws(),
                                                       k->status);

@@ -45,6 +45,7 @@ struct he_krylov {
     double2 *work = nullptr;      // 8 * maxdim^2 complex: small dense scratch (expm / least squares)
     double *norm_partial = nullptr;   // KRYLOV_BLOCKS
     float2 *s32[2] = {nullptr, nullptr};   // complex64 operand/result of mixed-precision applies
+    unsigned int *ticket = nullptr;          // device, count entries: last-block counters (0 between kernels)
     he::KrylovStatus *status = nullptr;      // device, count entries
     he::KrylovStatus *host_status = nullptr; // pinned host mirror
     size_t qs() const { return (size_t)count * n; }              // distance between basis vectors

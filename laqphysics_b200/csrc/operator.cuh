@@ -41,6 +41,8 @@ struct he_operator {
     std::string mix_src;                // source of the generated mixing kernel (without entry points)
     int mix_state[4] = {0, 0, 0, 0};    // per variant: 0 not compiled yet, 1 ready, -1 failed (table-driven)
     void *mix_kern[4] = {nullptr, nullptr, nullptr, nullptr};   // compiled kernels (cudaKernel_t)
+    int mix_blocks[2] = {2, 4};         // generated mixing kernel: CTAs of 128 threads per SM the register
+                                        // budget is sized for (complex128, complex64)
     std::vector<void *> allocations;    // every cudaMalloc made for this handle
     ~he_operator();
 };

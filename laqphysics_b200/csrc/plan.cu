@@ -178,7 +178,8 @@ void build_band(he_plan_host &P, int n, const int *ptr, const int *col, const do
     P.bbox_r32 = pad(P.bbox_r32);
     const size_t stage = ((size_t)P.bbox_r64 * P.bbox_c * 16 + KIN_STAGE_ALIGN - 1) / KIN_STAGE_ALIGN * KIN_STAGE_ALIGN;
     const size_t cfrag = (size_t)BAND_CG * BAND_KS * 32 * 16;
-    P.band_ok = 2 * P.bbox_r64 <= 256 && P.bbox_c <= 256 && 2 * stage + cfrag + 64 + KIN_STAGE_ALIGN <= 220 * 1024;
+    // two stages + the column groups' T and B fragments (B: velocity gauge) + barriers
+    P.band_ok = 2 * P.bbox_r64 <= 256 && P.bbox_c <= 256 && 2 * stage + 2 * cfrag + 64 + KIN_STAGE_ALIGN <= 220 * 1024;
 }
 
 // Program of the generated channel-mixing kernel.  Each class of channels that share

@@ -98,6 +98,7 @@ class B200Hamiltonian:
         info = (ct.c_longlong * 18)()
         check(LIB.he_info(self.op.handle, info, 18), 'he_info')
         self.tiled = bool(info[9])
+        self.mix_blocks = {'complex128': 2, 'complex64': 4}
         self.path = int(info[10])
         self.plan_info = {'elements': int(info[11]), 'tiles_per_axis': int(info[12]), 'groups': int(info[13]),
                           'wide_edges': int(info[14]), 'wide_dipole_edges': int(info[15]),
@@ -129,6 +130,45 @@ class B200Hamiltonian:
         else:
             radial = 'hpsi_radial_kernel'
         return [radial, 'hpsi_mix_kernel']
+
+    def set_mix_blocks(self, precision, blocks):
+        """Register budget of the generated mixing kernel: sized for `blocks` CTAs of 128
+        threads per SM (more CTAs, fewer registers per thread)."""
+        check(LIB.he_set_mix_blocks(self.op.handle, PRECISIONS[precision][0], int(blocks)), 'he_set_mix_blocks')
+        self.mix_blocks[precision] = int(blocks)
+
+    @torch.no_grad()
+    def autotune(self, field=(0., 0., .02), velocity=False, precisions=('complex128', 'complex64'),
+                 candidates=(1, 2, 3, 4, 6), reps=10, seed=0):
+        """Pick, per precision, the mixing kernel's CTAs per SM (register budget) that gives
+        the fastest apply on this operator: each candidate is compiled (or read from the
+        kernel cache), warmed up and timed with CUDA events over `reps` applies of a seeded
+        state; the fastest stays selected.  Returns {precision: {blocks: ms per apply}}."""
+        if not self.tiled:
+            return {}
+        rng = np.random.default_rng(seed)
+        x128 = self.state(rng.normal(size=self.size) + 1j * rng.normal(size=self.size))
+        timings = {}
+        for precision in precisions:
+            x = x128 if precision == 'complex128' else x128.to(torch.complex64)
+            out = torch.empty_like(x)
+            result = {}
+            for blocks in candidates:
+                self.set_mix_blocks(precision, blocks)
+                for _ in range(2):
+                    self.apply(x, field, velocity, out=out, precision=precision)
+                torch.cuda.synchronize(self.device)
+                start = torch.cuda.Event(enable_timing=True)
+                stop = torch.cuda.Event(enable_timing=True)
+                start.record()
+                for _ in range(reps):
+                    self.apply(x, field, velocity, out=out, precision=precision)
+                stop.record()
+                self.synchronize()
+                result[blocks] = start.elapsed_time(stop) / reps
+            self.set_mix_blocks(precision, min(result, key=result.get))
+            timings[precision] = result
+        return timings
 
     @property
     def launches_per_apply(self):

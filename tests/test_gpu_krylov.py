@@ -127,7 +127,9 @@ def test_fused_and_generic_arnoldi_agree_on_larger_grid():
     c, ic = arnoldi.exponential_action(lambda v: cpu.tensor_apply(h, v, f, False), op.host(x), .005, tol=1e-10,
                                        maxdim=16)
     assert ia['dimension'] == ib['dimension'] == ic['dimension']
-    np.testing.assert_array_equal(op.host(a), op.host(b))
+    # the fused loop takes h_{j+1,j} from the second CGS sweep (|v'|^2 - |z'|^2), the host
+    # loop from a separate norm: equal up to rounding
+    assert np.linalg.norm(op.host(a) - op.host(b)) / np.linalg.norm(op.host(b)) < 1e-13
     assert np.linalg.norm(op.host(a) - c) / np.linalg.norm(c) < 1e-12
 
 
