@@ -181,6 +181,7 @@ def arnoldi_leg(torch, device, steps, cpu_steps):
         state, _ = step(apply_at, state, i * dt, dt, tol, maxdim)
     torch.cuda.synchronize(device)
     dims = []
+    applies0 = engine.apply_count
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     start.record()
     t0 = time.perf_counter()
@@ -192,7 +193,8 @@ def arnoldi_leg(torch, device, steps, cpu_steps):
     ms = start.elapsed_time(stop)
     out = {'workload': 'Arnoldi FP64 length gauge: n=132 nc=17 (N=296,208), maxdim 12, dt 0.02, ground-state start',
            'steps': steps, 'steps_per_s': steps / (ms * 1e-3), 'ms_per_step': ms / steps,
-           'mean_dimension': float(np.mean(dims)), 'ground_energy': E0}
+           'mean_dimension': float(np.mean(dims)), 'ground_energy': E0,
+           'hpsi_per_step': (engine.apply_count - applies0) / steps}
     if cpu_steps:
         from oracle import arnoldi, cpu
         from threadpoolctl import threadpool_limits
@@ -247,6 +249,7 @@ def batched_leg(torch, device, steps, count=32):
         torch.cuda.synchronize(device)
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         dims = []
+        applies0 = engine.apply_count
         start.record()
         for i in range(3, 3 + steps):
             x, info = step_batched(engine, fields_at, x, i * dt, dt, tol, maxdim, precision=precision)
@@ -256,7 +259,8 @@ def batched_leg(torch, device, steps, count=32):
         ms = start.elapsed_time(stop)
         finals[precision] = x
         out[precision] = {'instance_steps_per_s': count * steps / (ms * 1e-3), 'ms_per_step': ms / steps,
-                          'mean_dimension': float(np.mean(dims))}
+                          'mean_dimension': float(np.mean(dims)),
+                          'hpsi_per_instance_step': (engine.apply_count - applies0) / (count * steps)}
     # the same instances stepped one at a time by the plain FP64 engine (same start, same
     # fields, same first steps), for the like-for-like speed-up of batching
     from laqphysics_b200.torch_backend import FieldSchedule, step
@@ -476,6 +480,11 @@ def main():
     e2e = world * bytes128 / (per_e2e * 1e-3) / 1e9
     hbm, _, peak_kind = peaks()
     flops = workloads.hpsi_flops(h)
+    parts = workloads.hpsi_flop_parts(h)
+    from laqphysics_b200.engine import fp64_peaks
+    fp64 = fp64_peaks(device)
+    # compute floor of one apply: kinetic on the FP64 tensor pipe, the rest on the FMA pipe
+    floor_ms = (parts['kinetic'] / (fp64['dmma'] * 1e12) + (flops - parts['kinetic']) / (fp64['dfma'] * 1e12)) * 1e3
     achieved = bytes128 / (per128 * 1e-3) / 1e9
     line = {
         'metric': METRIC, 'value': value, 'unit': 'GB/s', 'n_gpus': world, 'steps': args.steps,
@@ -489,6 +498,10 @@ def main():
                      'kernel': ' + '.join(engine.kernels()) + ' (one apply)',
                      'plan': engine.plan_info,
                      'fp64_tflops': flops / (per128 * 1e-3) / 1e12, 'flops_per_apply': flops},
+        'roofline_fp64': {'bound': 'fp64 (kinetic: DMMA pipe, mixing: DFMA pipe)', 'unit': 'TFLOP/s',
+                          'achieved': flops / (per128 * 1e-3) / 1e12, 'peak_dmma': fp64['dmma'],
+                          'peak_dfma': fp64['dfma'], 'peak_kind': 'measured in this run (he_fp64_peak)',
+                          'flops_per_apply': parts, 'compute_floor_ms': floor_ms, 'frac': floor_ms / per128},
         'complex64': {'value': value64, 'unit': 'GB/s', 'ms_per_step': per64,
                       'frac': value64 / world / hbm, 'speedup_vs_complex128': per128 / per64},
         'e2e': {'value': e2e, 'unit': 'GB/s', 'ms_per_step': per_e2e, 'steps': e2e_steps,

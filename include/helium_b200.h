@@ -161,6 +161,12 @@ int he_expv_batched(he_krylov_handle k, he_handle op, const void *x, void *y, co
                     double dt, double tol, int maxdim, int precision, int *dimension, double *estimate,
                     int *converged, void *stream);
 
+/* FP64 throughput of the current device, for the compute roofline of H·psi: kind 0 = the
+ * FP64 tensor pipe (mma.sync m8n8k4 f64, as in hpsi_band_kernel), kind 1 = FP64 FMA (as in
+ * the mixing kernel).  Runs `iters` iterations of 8 independent chains on 4 CTAs per SM
+ * and blocks until done.  Not part of the reference's interface. */
+int he_fp64_peak(int kind, int iters, double *tflops, void *stream);
+
 /* ------------------------------------------------------------------------------------
  * GMRES / CF4 building blocks (python/implicit.py:45-109).  The GMRES driver keeps its
  * Krylov basis in an he_krylov workspace (Q, and Z when flexible), orthogonalises with

@@ -401,6 +401,10 @@ __device__ __noinline__ void arnoldi_check_block(const double2 *__restrict__ H, 
     const bool happy = st->happy;
     const bool check = happy || (j >= 3 && ((j + 1) % 4 == 0 || j + 1 == maxdim));
     if (!check) return;
+    // the 8 small matrices of the exponential in shared memory when they fit (m <= 16)
+    constexpr int SMALL = 16;
+    __shared__ double2 small[8 * SMALL * SMALL];
+    if (m <= SMALL) work = small;
     double2 *A = work, *R = work + m * m, *scratch = work + 2 * m * m;
     for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
         const int r = idx % m, c = idx / m;

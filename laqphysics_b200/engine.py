@@ -40,6 +40,18 @@ def _host_tables(h):
     return t
 
 
+def fp64_peaks(device='cuda:0', iters=4096):
+    """Measured FP64 throughput of a device in TFLOP/s: {'dmma': tensor pipe (mma.sync
+    m8n8k4 f64), 'dfma': FMA pipe} (he_fp64_peak)."""
+    out = {}
+    with torch.cuda.device(torch.device(device)):
+        for kind, name in ((0, 'dmma'), (1, 'dfma')):
+            v = ct.c_double()
+            check(LIB.he_fp64_peak(kind, int(iters), ct.byref(v), _stream(torch.device(device))), 'he_fp64_peak')
+            out[name] = v.value
+    return out
+
+
 class OperatorHandle:
     """Owns one ``he_handle`` (device tables) for a Hamiltonian table object ``h``."""
 

@@ -156,6 +156,7 @@ def _fused(op, ws, x, dt, tol, maxdim, stream):
                          ptr(op.field), int(op.velocity), float(dt), float(tol), int(maxdim), ct.byref(dim),
                          ct.byref(err), stream)
     if status == HE_ERR_NOCONV:
+        op.engine.apply_count += int(maxdim)   # the attempt ran to maxdim
         raise _not_converged(maxdim, dt, err.value)
     check(status, 'he_expv')
     op.engine.apply_count += dim.value

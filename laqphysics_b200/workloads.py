@@ -57,14 +57,16 @@ def seeded_state(size, seed, dtype=np.complex128):
     return (x / np.linalg.norm(x)).astype(dtype)
 
 
-def hpsi_flops(h):
-    """Algorithmic real flops of one complex H·psi (complex MAC = 8 flops): kinetic on
-    both electrons, Coulomb edges (complex coefficient x complex radial x complex psi =
-    2 complex products), length-gauge dipole edges and the diagonal."""
+def hpsi_flop_parts(h):
+    """Algorithmic real flops of one complex H·psi (complex MAC = 8 flops), by part:
+    kinetic on both electrons, Coulomb edges (complex coefficient x complex radial x
+    complex psi = 2 complex products), length-gauge dipole edges and the diagonal."""
     n2 = h.n * h.n
     nnz = int(h.ptr[-1])
-    kinetic = 2 * nnz * h.n * h.nc * 8
-    coulomb = len(h.vc) * n2 * 14
-    dipole = len(h.dc) * n2 * 14
-    diagonal = h.nc * n2 * 8
-    return kinetic + coulomb + dipole + diagonal
+    return {'kinetic': 2 * nnz * h.n * h.nc * 8, 'coulomb': len(h.vc) * n2 * 14, 'dipole': len(h.dc) * n2 * 14,
+            'diagonal': h.nc * n2 * 8}
+
+
+def hpsi_flops(h):
+    """Total algorithmic real flops of one complex H·psi (see hpsi_flop_parts)."""
+    return sum(hpsi_flop_parts(h).values())

@@ -221,3 +221,26 @@ def test_batched_apply_matches_single_applies(velocity):
         ref = cpu.tensor_apply(h, op.host(x[count - 1]), fields[count - 1], velocity)
         assert rel_l2(op.host(y[count - 1]).astype(complex), ref) < (1e-13 if precision == 'complex128' else C64_REL_L2)
     op.synchronize()
+
+
+def test_fp64_peak_probes():
+    from laqphysics_b200.engine import fp64_peaks
+    p = fp64_peaks(DEVICE, iters=256)
+    assert p['dmma'] > 1.0 and p['dfma'] > 1.0
+
+
+def test_mixing_kernel_occupancy_choices_agree():
+    """The autotuner's candidates (register budgets of the generated mixing kernel) give
+    the same H·psi; the fastest one stays selected."""
+    from laqphysics_b200.workloads import arnoldi_small, seeded_state
+    h = arnoldi_small()
+    op = engine(h)
+    x = op.state(seeded_state(h.size, 41))
+    f = (0., 0., .02)
+    ref = op.host(op.apply(x, f, False))
+    timings = op.autotune(f, False, precisions=('complex128',), candidates=(2, 4), reps=2)
+    assert set(timings['complex128']) == {2, 4}
+    for blocks in (2, 4):
+        op.set_mix_blocks('complex128', blocks)
+        np.testing.assert_array_equal(op.host(op.apply(x, f, False)), ref)
+    op.synchronize()
