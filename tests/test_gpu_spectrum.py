@@ -3,8 +3,9 @@ gauge Arnoldi propagation from the ground state through a short pulse, a surface
 every step, He+ (n <= 2) channel spectra.  The mixed run applies H·psi in complex64 inside
 the complex128 Krylov; everything on the surface stays complex128.
 
-Stated tolerances (mixed vs complex128): photoelectron spectrum relative L2 error <= 1e-5,
-final-state relative L2 error <= 1e-5, norm difference <= 1e-7."""
+Stated tolerances (mixed vs complex128): photoelectron spectrum relative L2 error <= 1e-6
+(the mixed-precision target), final-state relative L2 error <= 2e-6, norm difference
+<= 1e-8."""
 import numpy as np
 import pytest
 import torch
@@ -22,7 +23,7 @@ def test_mixed_precision_tsurff_spectrum_against_complex128():
     rel, per_label = spectrum_error(acc32, acc64)
     pes, _ = acc64.spectrum()
     assert np.isfinite(pes).all() and pes.max() > 0
-    assert rel <= 1e-5, rel
+    assert rel <= 1e-6, rel
     state = float(torch.linalg.vector_norm(psi32 - psi64) / torch.linalg.vector_norm(psi64))
-    assert state <= 1e-5, state
-    assert abs(float(torch.linalg.vector_norm(psi32)) - float(torch.linalg.vector_norm(psi64))) <= 1e-7
+    assert state <= 2e-6, state
+    assert abs(float(torch.linalg.vector_norm(psi32)) - float(torch.linalg.vector_norm(psi64))) <= 1e-8
