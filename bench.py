@@ -40,7 +40,7 @@ def parse():
     p.add_argument('--impl', choices=['b200', 'reference'], default='b200')
     p.add_argument('--no-cpu-baseline', action='store_true')
     p.add_argument('--no-arnoldi', action='store_true', help='skip the Arnoldi steps/s leg')
-    p.add_argument('--profile', choices=['c128', 'c64', 'arnoldi', 'batched'], default=None,
+    p.add_argument('--profile', choices=['c128', 'c64', 'arnoldi', 'batched', 'cf4'], default=None,
                    help='run only W+K applications of one precision (for ncu captures); prints no JSON')
     return p.parse_args()
 
@@ -326,6 +326,60 @@ def adjoint_leg(torch, device, steps=128, knots=32, checkpoint=32):
             'backward_over_forward': (t2 - t1) / (t1 - t0), 'gradient_norm': float(np.linalg.norm(grad))}
 
 
+def cf4_leg(torch, device, steps=10):
+    """CF4 Magnus steps, each exponential a [2/2] Pade pair of shifted solves by right-
+    preconditioned GMRES (the reference's implicit.py:45-109 path), on the Arnoldi grid
+    (n=132, nc=17), velocity gauge, sin^2 pulse omega 1.6 a.u. peak 0.02 a.u., dt 0.05,
+    ground-state start, reference energy = ground energy, GMRES tolerance 1e-10; separable
+    ionic preconditioner in complex128 (GMRES(32)) and in complex64 (flexible GMRES(16)).
+    Also times the preconditioner alone (4 n^3 complex GEMMs per channel)."""
+    from laqphysics_b200 import workloads
+    from laqphysics_b200.engine import B200Hamiltonian
+    from laqphysics_b200.implicit import SeparablePreconditioner, cf4_step
+    from laqphysics_b200.pulses import Pulse
+    h, hreal = workloads.arnoldi_small(), workloads.arnoldi_small_real()
+    E0, g, _ = hreal.ground(tol=1e-9)
+    ratio = np.sqrt(h.grid.weights / hreal.grid.weights)
+    psi0 = (g.reshape(h.shape, order='F') * ratio[:, None, None] * ratio[None, :, None]).ravel(order='F')
+    engine = B200Hamiltonian(h, device)
+    pulse = Pulse(omega=1.6, cycles=10, field=.02)
+    avec = lambda t: np.array([0., 0., float(pulse.vector(t))])
+    dt, tol = .05, 1e-10
+    out = {'workload': 'CF4 + [2/2] Pade / GMRES, Arnoldi grid n=132 nc=17, velocity gauge, dt 0.05, tol 1e-10, '
+                       'separable preconditioner', 'steps': steps}
+    gemm_flops = 32 * h.n ** 3 * h.nc
+    for precision in ('complex128', 'complex64'):
+        engine.separable = SeparablePreconditioner(engine, precision)
+        x = engine.state(psi0)
+        for i in range(2):
+            x, _ = cf4_step(engine, x, avec, i * dt, dt, E0, tol=tol)
+        torch.cuda.synchronize(device)
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        iterations = 0
+        start.record()
+        for i in range(2, 2 + steps):
+            x, info = cf4_step(engine, x, avec, i * dt, dt, E0, tol=tol)
+            iterations += info['linear_iterations']
+        stop.record()
+        torch.cuda.synchronize(device)
+        ms = start.elapsed_time(stop)
+        y = x   # complex128 in and out; the complex64 preconditioner converts inside
+        for _ in range(3):
+            engine.separable.apply(y, dt / 6, .01)
+        torch.cuda.synchronize(device)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(20):
+            engine.separable.apply(y, dt / 6, .01)
+        b.record()
+        torch.cuda.synchronize(device)
+        pre_ms = a.elapsed_time(b) / 20
+        out[precision] = {'steps_per_s': steps / (ms * 1e-3), 'ms_per_step': ms / steps,
+                          'gmres_iterations_per_step': iterations / steps,
+                          'preconditioner_ms': pre_ms, 'preconditioner_tflops': gemm_flops / (pre_ms * 1e-3) / 1e12}
+    return out
+
+
 def spectrum_leg(torch, device):
     """Channel-resolved tSURFF on the small case of laqphysics_b200.tsurff_run: complex128
     and mixed-precision propagations with a surface sample every step; spectrum error of
@@ -415,6 +469,9 @@ def main():
         return 0
     if args.profile == 'batched':
         batched_leg(torch, device, steps=args.steps)
+        return 0
+    if args.profile == 'cf4':
+        print(json.dumps(cf4_leg(torch, device, steps=args.steps)), flush=True)
         return 0
     h = workloads.hpsi_microbench()
     engine = B200Hamiltonian(h, device)
@@ -515,6 +572,7 @@ def main():
         line['batched'] = batched_leg(torch, device, steps=max(5, min(args.steps, 30)))
         line['adjoint'] = adjoint_leg(torch, device)
         line['spectrum'] = spectrum_leg(torch, device)
+        line['cf4'] = cf4_leg(torch, device)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         os.environ.setdefault('OMP_NUM_THREADS', str(os.cpu_count()))
