@@ -254,6 +254,12 @@ int he_vec_norms_noalloc(long long n, int count, const void *x, long long ld, do
  * ---------------------------------------------------------------------------------- */
 int he_set_path(he_handle h, int tiled);
 int he_device_status(he_handle h);
+/* Length-gauge form of the banded kinetic kernel for one precision: stages 1 keeps one TMA
+ * stage with the register budget of two CTAs per SM, 2 keeps two stages (the next box loads
+ * during the current one).  Defaults: 1 for HE_C128, 2 for HE_C64 (the faster on B200).
+ * Results are identical; the autotuner (B200Hamiltonian.autotune) times both.  No
+ * counterpart in the reference. */
+int he_set_band_stages(he_handle h, int precision, int stages);
 
 /* ------------------------------------------------------------------------------------
  * Channel mixing: he_set_mix(h, 1) (default) uses the kernel generated for the handle's

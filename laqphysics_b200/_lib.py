@@ -50,6 +50,7 @@ SIGNATURES = {
     'he_set_mix': (I, [P, I]),
     'he_mix_status': (I, [P]),
     'he_set_mix_blocks': (I, [P, I, I]),
+    'he_set_band_stages': (I, [P, I, I]),
     'he_fp64_peak': (I, [I, I, ct.POINTER(ct.c_double), P]),
     'he_plan_mix_source': (ct.c_longlong, [P, I, ct.c_char_p, ct.c_longlong]),
     'he_nvrtc_check': (I, [ct.c_char_p, ct.c_char_p, ct.c_longlong]),

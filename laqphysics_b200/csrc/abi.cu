@@ -286,6 +286,16 @@ extern "C" int he_set_mix_blocks(he_handle h, int precision, int blocks)
     return HE_OK;
 }
 
+extern "C" int he_set_band_stages(he_handle h, int precision, int stages)
+{
+    if (!h) return he_fail(HE_ERR_ARG, "null handle", __FILE__, __LINE__);
+    if (precision != HE_C128 && precision != HE_C64)
+        return he_fail(HE_ERR_ARG, "precision must be HE_C128 or HE_C64", __FILE__, __LINE__);
+    if (stages != 1 && stages != 2) return he_fail(HE_ERR_ARG, "band kernel stages must be 1 or 2", __FILE__, __LINE__);
+    h->band_stages[precision == HE_C128 ? 0 : 1] = stages;
+    return HE_OK;
+}
+
 extern "C" int he_mix_status(he_handle h)
 {
     if (!h) return he_fail(HE_ERR_ARG, "null handle", __FILE__, __LINE__);

@@ -450,8 +450,11 @@ template <typename R> __device__ __forceinline__ cplx<R> narrow(double re, doubl
 // Work items are (row tile, column tile, channel of the batch): the batch's instances are
 // consecutive blocks of nc channels, so instance b owns channels [b nc, (b + 1) nc) of the
 // 3-D TMA map and of every array.
-template <typename R, bool VEL, bool SEP>
-__global__ void __launch_bounds__(BAND_THREADS, 1)
+// NST = 2: two TMA stages (the next item's box lands while this one is computed), one CTA
+// per SM; NST = 1: one stage, the next box is requested after the item, and the register
+// budget admits two CTAs per SM, which hide each other's waits.
+template <typename R, bool VEL, bool SEP, int NST>
+__global__ void __launch_bounds__(BAND_THREADS, NST == 1 ? 2 : 1)
 hpsi_band_kernel(const __grid_constant__ CUtensorMap tmap, const DeviceTables<R> t, const BandPlan<R> bp,
                  cplx<R> *__restrict__ out, cplx<R> *__restrict__ w1, cplx<R> *__restrict__ w2,
                  const __grid_constant__ FieldBatch fb)
@@ -459,7 +462,7 @@ hpsi_band_kernel(const __grid_constant__ CUtensorMap tmap, const DeviceTables<R>
     typedef cplx<R> C;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char *smem = smem_raw + ((KIN_STAGE_ALIGN - (smem_u32(smem_raw) & (KIN_STAGE_ALIGN - 1))) & (KIN_STAGE_ALIGN - 1));
-    double2 *CF = reinterpret_cast<double2 *>(smem + 2 * (size_t)bp.stage_bytes);   // [BAND_CG][BAND_KS][32]
+    double2 *CF = reinterpret_cast<double2 *>(smem + NST * (size_t)bp.stage_bytes);   // [BAND_CG][BAND_KS][32]
     double2 *CFB = CF + BAND_CG * BAND_KS * 32;   // velocity gauge: the B fragments of the same groups
     uint64_t *bar = reinterpret_cast<uint64_t *>(CFB + (VEL ? BAND_CG * BAND_KS * 32 : 0));
     constexpr int ALIGN = 16 / (int)sizeof(C);   // nodes per 16 bytes (TMA start alignment)
@@ -493,16 +496,17 @@ hpsi_band_kernel(const __grid_constant__ CUtensorMap tmap, const DeviceTables<R>
     int glo_r = 0, gks_r = 0;
     bool real_r = true;
     for (long long it = first; it < last; ++it) {
-        const int k = (int)(it - first), stage = k & 1;
-        const bool ok = mbar_wait_bounded(bar + stage, (unsigned)((k >> 1) & 1));
+        const int k = (int)(it - first), stage = NST == 2 ? (k & 1) : 0;
+        const unsigned parity = NST == 2 ? (unsigned)((k >> 1) & 1) : (unsigned)(k & 1);
+        const bool ok = mbar_wait_bounded(bar + stage, parity);
         if (__syncthreads_or(!ok)) {
             if (threadIdx.x == 0) {
                 atomicExch(bp.err, 1);
-                mbar_wait_bounded(bar + stage, (unsigned)((k >> 1) & 1));
+                mbar_wait_bounded(bar + stage, parity);
             }
             return;
         }
-        if (threadIdx.x == 0 && it + 1 < last) issue(it + 1, stage ^ 1);
+        if (NST == 2 && threadIdx.x == 0 && it + 1 < last) issue(it + 1, stage ^ 1);
         const long long tile = it / nch;
         const int c = (int)(it % nch), tr = (int)(tile / bp.nct), tc = (int)(tile % bp.nct);
         const int cc = c % nc, inst = c / nc;   // channel within its instance, instance
@@ -525,7 +529,7 @@ hpsi_band_kernel(const __grid_constant__ CUtensorMap tmap, const DeviceTables<R>
                 glo_r = bp.glo[gr]; gks_r = bp.gks[gr]; real_r = bp.greal[gr] & 1;
             }
         }
-        if (gr >= G) continue;
+        if (gr < G) {   // warps past the last row group only keep the CTA's barriers
         const C *S = reinterpret_cast<const C *>(smem + (size_t)stage * bp.stage_bytes);
         const int x0 = bp.brbase[tr] / ALIGN * ALIGN, y0 = bp.bcbase[tc], i0 = gr * BAND_G;
         int glo_c[BAND_CG], gks_c[BAND_CG];
@@ -580,6 +584,11 @@ hpsi_band_kernel(const __grid_constant__ CUtensorMap tmap, const DeviceTables<R>
                     out[p + nn * c] = narrow<R>(v.x, v.y);
                 }
             }
+        }
+        if (NST == 1) {   // every warp is done with the stage: request the next box into it
+            __syncthreads();
+            if (threadIdx.x == 0 && it + 1 < last) issue(it + 1, 0);
+        }
     }
 }
 
@@ -612,6 +621,24 @@ int sm_count(int device)
         counts[device] = v;
     }
     return counts[device];
+}
+
+// CTAs of one kernel that fit on an SM at a block size and dynamic shared memory (occupancy
+// calculator, cached per kernel and size; at least 1).
+int resident_ctas(const void *kernel, int threads, size_t smem)
+{
+    struct Entry { const void *k; int threads; size_t smem; int device; int n; };
+    static thread_local Entry cache[16];
+    static thread_local int next = 0;
+    int device = 0;
+    cudaGetDevice(&device);
+    for (const Entry &e : cache)
+        if (e.k == kernel && e.threads == threads && e.smem == smem && e.device == device) return e.n;
+    int n = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem) != cudaSuccess || n < 1) n = 1;
+    cache[next] = {kernel, threads, smem, device, n};
+    next = (next + 1) % 16;
+    return n;
 }
 
 // TMA map of psi(re/im, r1, r2 channel) over nc channels (every instance of a batch) with a
@@ -688,19 +715,23 @@ int launch_band(he_operator *h, const DeviceTables<R> &t, const BandPlan<R> &bp,
                                     bp.box_c, sizeof(R));
     if (!mp) return he_fail(HE_ERR_CUDA, "cuTensorMapEncodeTiled failed", __FILE__, __LINE__);
     const CUtensorMap map = *mp;
-    const size_t smem = 2 * (size_t)bp.stage_bytes + (velocity ? 2 : 1) * (size_t)BAND_CG * BAND_KS * 32 * sizeof(double2) +
-                        16 + KIN_STAGE_ALIGN;
+    // length gauge: the single-stage form at two CTAs per SM when the operator asks for it
+    // (he_set_band_stages); the velocity gauge needs the registers of one CTA per SM
+    const int nst = (!velocity && h->band_stages[sizeof(R) == 8 ? 0 : 1] == 1) ? 1 : 2;
+    const size_t smem = nst * (size_t)bp.stage_bytes +
+                        (velocity ? 2 : 1) * (size_t)BAND_CG * BAND_KS * 32 * sizeof(double2) + 16 + KIN_STAGE_ALIGN;
     const long long items = (long long)bp.ntr * bp.nct * bp.nc * fb.count;
-    const int per_sm = std::max(1, (int)((227 * 1024) / (smem + 1024)));
-    const unsigned grid = (unsigned)std::min<long long>(items, (long long)per_sm * sm_count(h->device));
-#define HE_BAND(V, S)                                                                                      \
+#define HE_BAND(V, S, N)                                                                                   \
     do {                                                                                                   \
-        auto kern = hpsi_band_kernel<R, V, S>;                                                             \
+        auto kern = hpsi_band_kernel<R, V, S, N>;                                                          \
         HE_CUDA_TRY(he_smem_limit(reinterpret_cast<const void *>(kern), smem));                            \
+        const int per_sm = resident_ctas(reinterpret_cast<const void *>(kern), BAND_THREADS, smem);        \
+        const unsigned grid = (unsigned)std::min<long long>(items, (long long)per_sm * sm_count(h->device)); \
         kern<<<grid, BAND_THREADS, smem, stream>>>(map, t, bp, out, w1, w2, fb);                           \
     } while (0)
-    if (velocity) { if (t.diag_separable) HE_BAND(true, true); else HE_BAND(true, false); }
-    else { if (t.diag_separable) HE_BAND(false, true); else HE_BAND(false, false); }
+    if (velocity) { if (t.diag_separable) HE_BAND(true, true, 2); else HE_BAND(true, false, 2); }
+    else if (nst == 1) { if (t.diag_separable) HE_BAND(false, true, 1); else HE_BAND(false, false, 1); }
+    else { if (t.diag_separable) HE_BAND(false, true, 2); else HE_BAND(false, false, 2); }
 #undef HE_BAND
     HE_CUDA_TRY(cudaGetLastError());
     return HE_OK;

@@ -41,6 +41,9 @@ struct he_operator {
     std::string mix_src;                // source of the generated mixing kernel (without entry points)
     int mix_state[4] = {0, 0, 0, 0};    // per variant: 0 not compiled yet, 1 ready, -1 failed (table-driven)
     void *mix_kern[4] = {nullptr, nullptr, nullptr, nullptr};   // compiled kernels (cudaKernel_t)
+    int band_stages[2] = {1, 2};        // hpsi_band_kernel, length gauge, per precision (complex128,
+                                        // complex64): 1 TMA stage with the registers of two CTAs per SM,
+                                        // or 2 stages (he_set_band_stages; defaults = the faster on B200)
     int mix_blocks[2] = {2, 4};         // generated mixing kernel: CTAs of 128 threads per SM the register
                                         // budget is sized for (complex128, complex64)
     std::vector<void *> allocations;    // every cudaMalloc made for this handle

@@ -111,6 +111,7 @@ class B200Hamiltonian:
         check(LIB.he_info(self.op.handle, info, 18), 'he_info')
         self.tiled = bool(info[9])
         self.mix_blocks = {'complex128': 2, 'complex64': 4}
+        self.band_stages = {'complex128': 1, 'complex64': 2}
         self.path = int(info[10])
         self.plan_info = {'elements': int(info[11]), 'tiles_per_axis': int(info[12]), 'groups': int(info[13]),
                           'wide_edges': int(info[14]), 'wide_dipole_edges': int(info[15]),
@@ -149,13 +150,34 @@ class B200Hamiltonian:
         check(LIB.he_set_mix_blocks(self.op.handle, PRECISIONS[precision][0], int(blocks)), 'he_set_mix_blocks')
         self.mix_blocks[precision] = int(blocks)
 
+    def set_band_stages(self, precision, stages):
+        """Length-gauge banded kinetic kernel of one precision: 2 TMA stages at one CTA per
+        SM, or 1 stage with the registers of two CTAs per SM (same results)."""
+        check(LIB.he_set_band_stages(self.op.handle, PRECISIONS[precision][0], int(stages)), 'he_set_band_stages')
+        self.band_stages[precision] = int(stages)
+
+    def _time_apply(self, x, out, field, velocity, precision, reps):
+        for _ in range(2):
+            self.apply(x, field, velocity, out=out, precision=precision)
+        torch.cuda.synchronize(self.device)
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        start.record()
+        for _ in range(reps):
+            self.apply(x, field, velocity, out=out, precision=precision)
+        stop.record()
+        self.synchronize()
+        return start.elapsed_time(stop) / reps
+
     @torch.no_grad()
     def autotune(self, field=(0., 0., .02), velocity=False, precisions=('complex128', 'complex64'),
-                 candidates=(1, 2, 3, 4, 6), reps=10, seed=0):
-        """Pick, per precision, the mixing kernel's CTAs per SM (register budget) that gives
-        the fastest apply on this operator: each candidate is compiled (or read from the
-        kernel cache), warmed up and timed with CUDA events over `reps` applies of a seeded
-        state; the fastest stays selected.  Returns {precision: {blocks: ms per apply}}."""
+                 candidates=(1, 2, 3, 4, 6), stages=(1, 2), reps=10, seed=0):
+        """Pick, per precision, the launch shapes that give the fastest apply on this
+        operator: the banded kinetic kernel's form (`stages`; length gauge only), then the
+        mixing kernel's CTAs per SM (register budget).  Each candidate is compiled (or read
+        from the kernel cache), warmed up and timed with CUDA events over `reps` applies of a
+        seeded state; the fastest stays selected.  Returns {precision: {'band_stages':
+        {stages: ms}, 'mix_blocks': {blocks: ms per apply}}}."""
         if not self.tiled:
             return {}
         rng = np.random.default_rng(seed)
@@ -164,22 +186,20 @@ class B200Hamiltonian:
         for precision in precisions:
             x = x128 if precision == 'complex128' else x128.to(torch.complex64)
             out = torch.empty_like(x)
+            timings[precision] = {}
+            if not velocity and stages:
+                result = {}
+                for st in stages:
+                    self.set_band_stages(precision, st)
+                    result[st] = self._time_apply(x, out, field, velocity, precision, reps)
+                self.set_band_stages(precision, min(result, key=result.get))
+                timings[precision]['band_stages'] = result
             result = {}
             for blocks in candidates:
                 self.set_mix_blocks(precision, blocks)
-                for _ in range(2):
-                    self.apply(x, field, velocity, out=out, precision=precision)
-                torch.cuda.synchronize(self.device)
-                start = torch.cuda.Event(enable_timing=True)
-                stop = torch.cuda.Event(enable_timing=True)
-                start.record()
-                for _ in range(reps):
-                    self.apply(x, field, velocity, out=out, precision=precision)
-                stop.record()
-                self.synchronize()
-                result[blocks] = start.elapsed_time(stop) / reps
+                result[blocks] = self._time_apply(x, out, field, velocity, precision, reps)
             self.set_mix_blocks(precision, min(result, key=result.get))
-            timings[precision] = result
+            timings[precision]['mix_blocks'] = result
         return timings
 
     @property

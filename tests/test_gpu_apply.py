@@ -239,8 +239,31 @@ def test_mixing_kernel_occupancy_choices_agree():
     f = (0., 0., .02)
     ref = op.host(op.apply(x, f, False))
     timings = op.autotune(f, False, precisions=('complex128',), candidates=(2, 4), reps=2)
-    assert set(timings['complex128']) == {2, 4}
+    assert set(timings['complex128']['mix_blocks']) == {2, 4} and set(timings['complex128']['band_stages']) == {1, 2}
     for blocks in (2, 4):
         op.set_mix_blocks('complex128', blocks)
         np.testing.assert_array_equal(op.host(op.apply(x, f, False)), ref)
     op.synchronize()
+
+
+@pytest.mark.parametrize('precision', ['complex128', 'complex64'])
+def test_band_kernel_single_and_double_stage_forms_agree(precision):
+    """The one-stage, two-CTA form of the banded kinetic kernel gives bit-identical H·psi to
+    the two-stage form, on a grid with a ragged last tile and on a batch of instances."""
+    from laqphysics_b200.workloads import arnoldi_small, seeded_state
+    h = _coupled(np.linspace(0, 24, 7), 6, .3, 24, 2, 1, cut=(12., 15.))
+    dtype = torch.complex128 if precision == 'complex128' else torch.complex64
+    for hh in (h, arnoldi_small()):
+        op = engine(hh)
+        x = op.state(seeded_state(hh.size, 43)).to(dtype)
+        f = (0., 0., .03)
+        fields = np.array([[0., 0., .01], [0., 0., .02], [0., 0., .03]])
+        xb = torch.stack([x, 2 * x, -x]).contiguous()
+        results = {}
+        for stages in (2, 1):
+            op.set_band_stages(precision, stages)
+            results[stages] = (op.host(op.apply(x, f, False, precision=precision)),
+                               op.host(op.apply_batched(xb, fields, False, precision=precision)))
+        op.synchronize()
+        np.testing.assert_array_equal(results[1][0], results[2][0])
+        np.testing.assert_array_equal(results[1][1], results[2][1])
