@@ -473,6 +473,15 @@ __device__ __forceinline__ double2 ordered_partial_sum(const double2 *p, int nb,
     return s;
 }
 
+// Load that the compiler may neither merge with an earlier load of the same address nor
+// move: a value read again instead of being held in a register.
+__device__ __forceinline__ double2 reload(const double2 *p)
+{
+    double2 v;
+    asm volatile("ld.global.ca.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+    return v;
+}
+
 // Every thread has written its partials; returns true in the last block to arrive (which
 // then sees every block's partials).  No waiting: the other blocks just return.
 __device__ __forceinline__ bool arrive_last(unsigned int *ticket)
@@ -558,9 +567,11 @@ arnoldi_reorth_kernel(const double2 *__restrict__ Q, size_t n, size_t qs, int kc
         for (int k = 0; k < KT; ++k)
             if (k < kc) x = cfma<double>(mk<double>(-zs[k].x, -zs[k].y), Q[(size_t)k * qs + p], x);
         v[p] = x;
+        // second use of the basis elements: read again (from L1) rather than kept in
+        // registers, so that the kernel keeps its occupancy
 #pragma unroll
         for (int k = 0; k < KT; ++k)
-            if (k < kc) acc[k] = cfma_conj<double>(Q[(size_t)k * qs + p], x, acc[k]);
+            if (k < kc) acc[k] = cfma_conj<double>(reload(Q + (size_t)k * qs + p), x, acc[k]);
         acc[KT].x += cabs2<double>(x);
     }
     __shared__ double2 res[KT + 1];
@@ -641,6 +652,10 @@ int krylov_create(he_krylov **out, long long n, int maxdim, int flexible, int co
     he_krylov *k = new he_krylov();
     k->n = (size_t)n; k->maxdim = maxdim; k->flexible = flexible; k->count = count;
     cudaError_t e = cudaGetDevice(&k->device);
+    // one instance: KRYLOV_BLOCKS CTAs; a batch: about four CTAs per SM over all instances
+    // (the sweeps of a batch stream from HBM and need the warps to keep enough loads in flight)
+    if (count > 1)
+        k->blocks = std::min(KRYLOV_BLOCKS, std::max(8, 4 * sm_count(k->device) / count));
     const size_t ld = maxdim + 1, c = count;
     if (e == cudaSuccess) e = cudaMalloc(&k->Q, ld * c * k->n * sizeof(double2));
     if (e == cudaSuccess && flexible) e = cudaMalloc(&k->Z, (size_t)maxdim * c * k->n * sizeof(double2));

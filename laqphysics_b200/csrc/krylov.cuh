@@ -49,7 +49,8 @@ struct he_krylov {
     he::KrylovStatus *status = nullptr;      // device, count entries
     he::KrylovStatus *host_status = nullptr; // pinned host mirror
     size_t qs() const { return (size_t)count * n; }              // distance between basis vectors
-    int kb() const { return count == 1 ? he::KRYLOV_BLOCKS : std::max(8, he::KRYLOV_BLOCKS / count); }   // CTAs per instance
+    int blocks = he::KRYLOV_BLOCKS;   // CTAs per instance of the vector kernels (set at creation)
+    int kb() const { return blocks; }
     size_t hs() const { return (size_t)(maxdim + 1) * maxdim; }  // Hessenberg size per instance
     size_t ws() const { return (size_t)8 * (maxdim + 1) * (maxdim + 1); }   // dense scratch per instance
     ~he_krylov();
