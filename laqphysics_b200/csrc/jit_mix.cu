@@ -58,6 +58,16 @@ template <typename R> __device__ __forceinline__ typename cx<R>::T ifma(R s, typ
 { c.x = f3(-s, b.y, c.x); c.y = f3(s, b.x, c.y); return c; }
 template <typename R> __device__ __forceinline__ typename cx<R>::T cmul(typename cx<R>::T a, typename cx<R>::T b)
 { return mk<R>(f3(a.x, b.x, -a.y * b.y), f3(a.x, b.y, a.y * b.x)); }
+// streaming (evict-first) access to the output, read once and written once per point, so
+// that L1 keeps the channels of psi and the multipoles that several groups read
+__device__ __forceinline__ cd ld_stream(const cd *p)
+{ cd v; asm volatile("ld.global.cs.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p)); return v; }
+__device__ __forceinline__ cf ld_stream(const cf *p)
+{ cf v; asm volatile("ld.global.cs.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p)); return v; }
+__device__ __forceinline__ void st_stream(cd *p, cd v)
+{ asm volatile("st.global.cs.v2.f64 [%0], {%1, %2};" :: "l"(p), "d"(v.x), "d"(v.y) : "memory"); }
+__device__ __forceinline__ void st_stream(cf *p, cf v)
+{ asm volatile("st.global.cs.v2.f32 [%0], {%1, %2};" :: "l"(p), "f"(v.x), "f"(v.y) : "memory"); }
 )";
 
 std::string lit(double v)
@@ -147,7 +157,7 @@ std::string mix_source(const he_plan_host &P, bool dipole_real, int variant)
              "    typedef typename cx<R>::T C;\n"
              "    const C Z = mk<R>(0, 0);\n";
         o << "    {   // group " << g << "\n";
-        for (size_t d = 0; d < G.out.size(); ++d) o << "        C a" << d << " = out[p + nn * " << G.out[d] << "LL];\n";
+        for (size_t d = 0; d < G.out.size(); ++d) o << "        C a" << d << " = ld_stream(out + p + nn * " << G.out[d] << "LL);\n";
         for (const MixBlock &B : G.blocks) {
             o << "        {\n";
             for (size_t s = 0; s < B.src.size(); ++s)
@@ -195,8 +205,8 @@ std::string mix_source(const he_plan_host &P, bool dipole_real, int variant)
             o << "            }\n        }\n";
         }
         for (size_t d = 0; d < G.out.size(); ++d)
-            o << "        out[p + nn * " << G.out[d] << "LL] = cfma<R>(gamma, a" << d << ", cmul<R>(beta, psi[p + nn * "
-              << G.out[d] << "LL]));\n";
+            o << "        st_stream(out + p + nn * " << G.out[d] << "LL, cfma<R>(gamma, a" << d << ", cmul<R>(beta, psi[p + nn * "
+              << G.out[d] << "LL])));\n";
         o << "    }\n}\n";
     }
     const std::string group_fns = o.str();
