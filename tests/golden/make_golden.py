@@ -135,6 +135,35 @@ def coupled_case():
          **tables(c), **gold)
 
 
+def bipolar_case():
+    # Bipolar all-M basis (python/bipolar.py): the reference's own tables, and H·psi from two
+    # paths that do not use the native library: the Kronecker assembly of the product basis
+    # projected by the bipolar isometry (U^T H_product U x), and TorchHamiltonian on the
+    # bipolar tables.  Field with all three Cartesian components (circular/elliptic probes).
+    from bipolar import BipolarHelium
+    args = dict(edges=[0, .5, 1, 2, 4, 6, 8], order=3, ecs_angle=.4, tail=6)
+    g = make_grid(**args)
+    b = BipolarHelium(g, lmax=2, total_Lmax=2, M=None, cutoff_radii=[1, 2])
+    product = Helium(g, 2, M=None, cutoff_radii=[1, 2])
+    U = b.transform.toarray()
+    n2 = b.n * b.n
+    rng = np.random.default_rng(733)
+    x = rng.normal(size=b.size) + 1j * rng.normal(size=b.size)
+    f = np.array([.11, -.07, .15])
+    op = TorchHamiltonian(b, 'cpu')
+    gold = {}
+    for velocity in (False, True):
+        key = 'velocity' if velocity else 'length'
+        up = (x.reshape(n2, b.nc, order='F') @ U.T).ravel(order='F')
+        hp = product.reference_sparse(f, velocity) @ up
+        gold[f'kron_{key}'] = (hp.reshape(n2, product.nc, order='F') @ U).ravel(order='F')
+        gold[f'torch_{key}'] = op.host(op.apply(op.state(x), f, velocity))
+    save('apply_bipolar', x=x, field=f, shape=np.array(b.shape), lmax=2, total_Lmax=2, cutoff=np.array([1., 2.]),
+         grid=json.dumps(args), basis=np.array(b.basis, np.int32), transform=U, exchange_sign=b.exchange_sign,
+         product_channels=np.array([[a[0], a[1], c[0], c[1]] for a, c in product.ch], np.int32),
+         **tables(b), **gold)
+
+
 def arnoldi_dense():
     # python tests/test_kernels.py:42-47.
     from scipy.linalg import expm
@@ -289,6 +318,7 @@ if __name__ == '__main__':
     grids()
     product_cases()
     coupled_case()
+    bipolar_case()
     arnoldi_dense()
     length_gauge_run()
     cf4_cases()
