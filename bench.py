@@ -398,6 +398,18 @@ def spectrum_leg(torch, device):
         res[precision] = run(engine, contractor, SMALL_CASE, psi0, avec, dt, steps, chi, precision)
         torch.cuda.synchronize(device)
         out[precision] = {'steps_per_s': steps / (time.perf_counter() - t0), 'mean_dimension': res[precision][2]}
+    # the He+ channel functions of the run: backward CF4 on the device (laqphysics_b200.ionic_adjoint)
+    from laqphysics_b200.ionic_adjoint import channel_functions
+    from laqphysics_b200.surface3d import Ionic
+    ion = Ionic(engine.h.uncoupled, {0})
+    unique = [(1, 0, 0), (2, 0, 0), (2, 1, 0)]
+    times = dt * np.arange(steps + 1)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    channel_functions(ion, unique, avec, times, device)
+    torch.cuda.synchronize(device)
+    out['ionic_channel_functions'] = {'frames': steps + 1, 'ms': (time.perf_counter() - t0) * 1e3,
+                                      'method': 'backward CF4 + Pade/GMRES (tol 1e-12) on the device'}
     rel, per_label = spectrum_error(res['mixed'][0], res['complex128'][0])
     p64, p32 = res['complex128'][1], res['mixed'][1]
     out['spectrum_rel_l2_mixed_vs_fp64'] = rel

@@ -192,6 +192,28 @@ int he_krylov_combine_coef(he_krylov_handle k, int which, int m, const void *coe
                            void *stream);
 
 /* ------------------------------------------------------------------------------------
+ * He+ operator for the backward propagation of the tSURFF channel functions chi_c(t)
+ * (replaces IonicAdjoint, python/ionic_adjoint.py:12-52, the device counterpart of the
+ * sparse-LU SparseCF4 of python/implicit.py:111-123 used by python/streaming_surface.py:
+ * 125-146).  H(c) = sum_k c_k M_k over nmat (<= 16) CSR planes sharing one pattern (ptr:
+ * ndof+1, col: nnz, data: nmat x nnz interleaved complex), applied to nrhs (<= 16)
+ * right-hand sides stored row-major x[row * nrhs + rhs].  he_ionic_apply: y = H(c) x, or
+ * with shifted != 0 y = x + i alpha (H(c) x - shift x) (the shifted Pade operator).
+ * he_ionic_set_preconditioner: na blocks of n rows (na n = ndof) with column-major n x n
+ * eigenvectors S, inverses Si and eigenvalues E of each block of M_0;
+ * he_ionic_precondition: y_a = S_a [(Si_a x_a) / (1 + i alpha (E_a + shift))].
+ * ---------------------------------------------------------------------------------- */
+typedef struct he_ionic *he_ionic_handle;
+int he_ionic_create(he_ionic_handle *out, int ndof, int nrhs, int nmat, long long nnz, const int *ptr, const int *col,
+                    const double *data);
+int he_ionic_set_preconditioner(he_ionic_handle h, int na, int n, const double *S, const double *Si, const double *E);
+int he_ionic_apply(he_ionic_handle h, const double *coef, int ncoef, const void *x, void *y, double alpha_re,
+                   double alpha_im, double shift, int shifted, void *stream);
+int he_ionic_precondition(he_ionic_handle h, const void *x, void *y, double alpha_re, double alpha_im, double shift,
+                          void *stream);
+int he_ionic_destroy(he_ionic_handle h);
+
+/* ------------------------------------------------------------------------------------
  * Separable ionic resolvent preconditioner.  Replaces SeparablePreconditioner
  * (python/implicit.py:13-39): for channel c with one-electron momenta (l1[c], l2[c]),
  * Y_c = S_{l1} [ (S_{l1}^-1 Psi_c S_{l2}^-T) / (1 + i alpha (e_{l1}(i) + e_{l2}(j) + shift)) ] S_{l2}^T.

@@ -52,6 +52,11 @@ SIGNATURES = {
     'he_set_mix_blocks': (I, [P, I, I]),
     'he_set_band_stages': (I, [P, I, I]),
     'he_fp64_peak': (I, [I, I, ct.POINTER(ct.c_double), P]),
+    'he_ionic_create': (I, [ct.POINTER(P), I, I, I, ct.c_longlong, P, P, P]),
+    'he_ionic_set_preconditioner': (I, [P, I, I, P, P, P]),
+    'he_ionic_apply': (I, [P, P, I, P, P, D, D, D, I, P]),
+    'he_ionic_precondition': (I, [P, P, P, D, D, D, P]),
+    'he_ionic_destroy': (I, [P]),
     'he_plan_mix_source': (ct.c_longlong, [P, I, ct.c_char_p, ct.c_longlong]),
     'he_nvrtc_check': (I, [ct.c_char_p, ct.c_char_p, ct.c_longlong]),
     'he_plan_mix_program': (ct.c_longlong, [P, ct.c_char_p, ct.c_longlong]),

@@ -8,26 +8,21 @@ so that a complex128 run and a mixed-precision run (complex64 H·psi inside the 
 Krylov, every surface quantity in complex128) can be compared on equal terms.
 
 The ionic channel functions chi_c(t) are the dual final He+ states propagated backward
-with the ionic Hamiltonian, chi(t_k) = exp(+i dt H_ion(A(t_k + dt/2))^dagger) chi(t_{k+1})
-(python/streaming_surface.py:125-146 propagates the same duals backward with CF4); they
-are computed once on the host (scipy) and shared by every run.
+with the adjoint ionic Hamiltonian by the reference's CF4 formula
+(python/streaming_surface.py:125-146), on the device (laqphysics_b200.ionic_adjoint); they
+are computed once per run and shared by the complex128 and mixed-precision runs.
 """
 import numpy as np
 import torch
-from scipy.sparse.linalg import expm_multiply
 
+from .ionic_adjoint import channel_functions
 from .streaming_surface import SurfaceSampler, VolkovAccumulator
 from .torch_backend import FieldSchedule, step
 
 
-def ionic_channel_functions(ion, unique, avec, dt, steps):
-    """chi at t_k = k dt, k = 0..steps: (steps+1, na*n, len(unique)) complex."""
-    chi = np.zeros((steps + 1, ion.na * ion.n, len(unique)), complex)
-    chi[steps] = ion.dual_final_states(unique)
-    for k in range(steps - 1, -1, -1):
-        H = ion.matrix(avec((k + 0.5) * dt))
-        chi[k] = expm_multiply(1j * dt * H.conj().T, chi[k + 1])
-    return chi
+def ionic_channel_functions(ion, unique, avec, dt, steps, device='cuda:0'):
+    """chi at t_k = k dt, k = 0..steps: device tensor (steps+1, na*n, len(unique))."""
+    return channel_functions(ion, unique, avec, dt * np.arange(steps + 1), device)
 
 
 def run(engine, contractor, config, psi0, avec, dt, steps, chi, precision='complex128', tol=1e-10, maxdim=16):
@@ -93,5 +88,5 @@ def build_case(config, device, dt=.02, after=1.0):
     psi0 = (g.reshape(h.shape, order='F') * ratio[:, None, None] * ratio[None, :, None]).ravel(order='F')
     engine = B200Hamiltonian(h, device)
     steps = int(round((pulse.duration + after) / dt))
-    chi = ionic_channel_functions(ion, unique, avec, dt, steps)
+    chi = ionic_channel_functions(ion, unique, avec, dt, steps, device)
     return engine, contractor, psi0, avec, steps, chi

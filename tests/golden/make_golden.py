@@ -164,6 +164,29 @@ def bipolar_case():
          **tables(b), **gold)
 
 
+def ionic_adjoint_case():
+    # Backward CF4-Pade propagation of the dual He+ channel functions with the ionic
+    # Hamiltonian's adjoint (python/streaming_surface.py:125-146 with sparse LU,
+    # python/implicit.py:111-123), velocity gauge, from t = 1.8 back to 1.0 in steps of 0.02.
+    from surface3d import Ionic
+    from streaming_surface import AdjointStepper
+    args = dict(edges=[0, 1, 2, 3, 4, 6, 8, 10, 12], order=4, ecs_angle=.3, tail=8)
+    base = Helium(make_grid(**args), 1, M=0, cutoff_radii=[3, 4])
+    ion = Ionic(base, {0})
+    unique = [(1, 0, 0), (2, 0, 0), (2, 1, 0)]
+    pulse = Pulse(omega=2.0, cycles=2, field=.3)
+    avec = lambda t: np.array([0., 0., float(pulse.vector(t))])
+    stepper = AdjointStepper(ion, avec, 'cf4', 'lu')
+    chi = ion.dual_final_states(unique)
+    stepper.reset(chi)
+    dt, t_end, steps = .02, 1.8, 40
+    states = [chi]
+    for i in range(steps):
+        states.append(stepper.step(t_end - i * dt, -dt).copy())
+    save('ionic_adjoint', grid=json.dumps(args), cutoff=np.array([3., 4.]), unique=np.array(unique),
+         pulse=json.dumps(dict(omega=2.0, cycles=2, field=.3)), dt=dt, t_end=t_end, states=np.array(states))
+
+
 def arnoldi_dense():
     # python tests/test_kernels.py:42-47.
     from scipy.linalg import expm
@@ -319,6 +342,7 @@ if __name__ == '__main__':
     product_cases()
     coupled_case()
     bipolar_case()
+    ionic_adjoint_case()
     arnoldi_dense()
     length_gauge_run()
     cf4_cases()
