@@ -183,6 +183,8 @@ int he_vec_jacobi(long long n, const void *diag, double alpha_re, double alpha_i
                   void *y, void *stream);
 /* Q_j (which = 0) or Z_j (which = 1) *= s. */
 int he_krylov_scale(he_krylov_handle k, int which, int j, double s, void *stream);
+/* Q_j /= h_{j,j-1} as left on the device by he_krylov_orthogonalize(j - 1) (no host read). */
+int he_krylov_normalize(he_krylov_handle k, int j, void *stream);
 /* Copy H[0:rows, j] (interleaved complex) to host memory `out`.  Blocks. */
 int he_krylov_hessenberg(he_krylov_handle k, int j, int rows, void *out, void *stream);
 /* H = 0 and a fresh status word (start of a GMRES cycle). */

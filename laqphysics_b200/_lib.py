@@ -64,6 +64,7 @@ SIGNATURES = {
     'he_vec_residual_norm': (I, [ct.c_longlong, P, P, P, ct.POINTER(D), P]),
     'he_vec_jacobi': (I, [ct.c_longlong, P, D, D, D, P, P, P]),
     'he_krylov_scale': (I, [P, I, I, D, P]),
+    'he_krylov_normalize': (I, [P, I, P]),
     'he_krylov_hessenberg': (I, [P, I, I, P, P]),
     'he_krylov_reset': (I, [P, P]),
     'he_krylov_combine_coef': (I, [P, I, I, P, P, I, P]),

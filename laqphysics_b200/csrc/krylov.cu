@@ -814,6 +814,17 @@ extern "C" int he_expv_check(he_krylov *k, int j, int maxdim, double dt, double 
     return HE_OK;
 }
 
+// Q_j /= h_{j,j-1} from the status word (the norm of the last orthogonalisation), on the
+// device: the GMRES driver reads the Hessenberg only at its check points.
+extern "C" int he_krylov_normalize(he_krylov *k, int j, void *stream)
+{
+    if (!k || j < 1 || j > k->maxdim) return he_fail(HE_ERR_ARG, "bad basis index", __FILE__, __LINE__);
+    double2 *q = k->Q + (size_t)j * k->qs();
+    normalize_kernel<<<bgrid(k), kBlock, 0, static_cast<cudaStream_t>(stream)>>>(q, q, k->n, k->status);
+    HE_CUDA_TRY(cudaGetLastError());
+    return HE_OK;
+}
+
 extern "C" int he_krylov_combine(he_krylov *k, int m, void *y, void *stream)
 {
     if (!k || !y || m > k->maxdim) return he_fail(HE_ERR_ARG, "bad combination", __FILE__, __LINE__);

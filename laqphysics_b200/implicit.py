@@ -139,6 +139,7 @@ def gmres(apply, b, preconditioner, x0=None, tol=1e-11, restart=32, max_restarts
         check(LIB.he_krylov_reset(ws.handle, stream), 'reset')
         hostH[:] = 0
         column = np.zeros(2 * (restart + 1))
+        read = 0   # Hessenberg columns read so far; the rest stay on the device until a check point
         for j in range(restart):
             z = M(ws.vector(j))
             if flexible:
@@ -146,37 +147,47 @@ def gmres(apply, b, preconditioner, x0=None, tol=1e-11, restart=32, max_restarts
             ws.vector(j + 1).copy_(apply(z))
             iterations += 1
             check(LIB.he_krylov_orthogonalize(ws.handle, j, stream), 'orthogonalize')
-            check(LIB.he_krylov_hessenberg(ws.handle, j, j + 2, column.ctypes.data, stream), 'hessenberg')
-            hostH[:j + 2, j] = column[:2 * (j + 2)].view(complex)
+            if (j + 1) % (2 if flexible else 4) != 0 and j + 1 != restart:
+                check(LIB.he_krylov_normalize(ws.handle, j + 1, stream), 'normalize')
+                continue
+            # check point: read the pending columns; a breakdown (h < 1e-14) in one of them ends
+            # the cycle there, with the same least squares as an immediate check would use
+            for c in range(read, j + 1):
+                check(LIB.he_krylov_hessenberg(ws.handle, c, c + 2, column.ctypes.data, stream), 'hessenberg')
+                hostH[:c + 2, c] = column[:2 * (c + 2)].view(complex)
+            read = j + 1
+            broken = [c for c in range(j + 1) if hostH[c + 1, c].real < 1e-14]
+            if broken:
+                iterations -= j - broken[0]
+                j = broken[0]
             hnorm = hostH[j + 1, j].real
-            if hnorm < 1e-14 or (j + 1) % (2 if flexible else 4) == 0 or j + 1 == restart:
-                m = j + 1
-                small = hostH[:m + 1, :m]
-                rhs = np.zeros(m + 1, complex)
-                rhs[0] = beta
-                y = np.linalg.lstsq(small, rhs, rcond=None)[0]
-                estimate = np.linalg.norm(rhs - small @ y)
-                if estimate < tol * bnorm or hnorm < 1e-14 or m == restart:
-                    coef = np.ascontiguousarray(y, dtype=complex)
-                    if flexible:
-                        candidate = x.clone()
-                        check(LIB.he_krylov_combine_coef(ws.handle, 1, m, coef.ctypes.data, _vp(candidate), 1, stream),
-                              'combine')
-                    else:
-                        direction = torch.empty_like(x)
-                        check(LIB.he_krylov_combine_coef(ws.handle, 0, m, coef.ctypes.data, _vp(direction), 0, stream),
-                              'combine')
-                        candidate = axpby(1, x, 1, M(direction))
-                    res = ct.c_double()
-                    check(LIB.he_vec_residual_norm(n, _vp(b), _vp(apply(candidate)), None, ct.byref(res), stream),
-                          'true residual')
-                    true = res.value / bnorm
-                    if true <= tol:
-                        return candidate, {'iterations': iterations, 'relative_residual': true}
-                    if hnorm < 1e-14 or m == restart:
-                        x = candidate
-                        break
-            check(LIB.he_krylov_scale(ws.handle, 0, j + 1, 1.0 / hnorm, stream), 'scale')
+            m = j + 1
+            small = hostH[:m + 1, :m]
+            rhs = np.zeros(m + 1, complex)
+            rhs[0] = beta
+            y = np.linalg.lstsq(small, rhs, rcond=None)[0]
+            estimate = np.linalg.norm(rhs - small @ y)
+            if estimate < tol * bnorm or hnorm < 1e-14 or m == restart:
+                coef = np.ascontiguousarray(y, dtype=complex)
+                if flexible:
+                    candidate = x.clone()
+                    check(LIB.he_krylov_combine_coef(ws.handle, 1, m, coef.ctypes.data, _vp(candidate), 1, stream),
+                          'combine')
+                else:
+                    direction = torch.empty_like(x)
+                    check(LIB.he_krylov_combine_coef(ws.handle, 0, m, coef.ctypes.data, _vp(direction), 0, stream),
+                          'combine')
+                    candidate = axpby(1, x, 1, M(direction))
+                res = ct.c_double()
+                check(LIB.he_vec_residual_norm(n, _vp(b), _vp(apply(candidate)), None, ct.byref(res), stream),
+                      'true residual')
+                true = res.value / bnorm
+                if true <= tol:
+                    return candidate, {'iterations': iterations, 'relative_residual': true}
+                if hnorm < 1e-14 or m == restart:
+                    x = candidate
+                    break
+            check(LIB.he_krylov_normalize(ws.handle, j + 1, stream), 'normalize')
     raise RuntimeError(f'GMRES did not converge: residual={true:.3e}, iterations={iterations}')
 
 
