@@ -515,15 +515,20 @@ def main():
 
     step128 = lambda k: engine.apply(inputs[k % 2], field, False, out=out)
     step64 = lambda k: engine.apply(in64[k % 2], field, False, out=out64)
-    host_in = torch.empty(N, dtype=torch.complex128).pin_memory()
-    host_in.copy_(inputs[0].cpu())
-    host_out = torch.empty_like(host_in).pin_memory()
+    host_in = [torch.empty(N, dtype=torch.complex128).pin_memory() for _ in range(2)]
+    for k in range(2):
+        host_in[k].copy_(inputs[k].cpu())
+    host_out = [torch.empty_like(host_in[0]).pin_memory() for _ in range(2)]
     dev_in = torch.empty_like(inputs[0])
 
-    def step_e2e(k):
-        dev_in.copy_(host_in, non_blocking=True)
+    def step_e2e(k):   # one state at a time: H2D, apply, D2H in sequence
+        dev_in.copy_(host_in[k % 2], non_blocking=True)
         engine.apply(dev_in, field, False, out=out)
-        host_out.copy_(out, non_blocking=True)
+        host_out[k % 2].copy_(out, non_blocking=True)
+
+    def e2e_stream(count):   # B200Hamiltonian.apply_host_stream: transfers overlapped with compute
+        engine.apply_host_stream([host_in[k % 2] for k in range(count)], field, False,
+                                 [host_out[k % 2] for k in range(count)])
 
     if args.profile:
         step = step128 if args.profile == 'c128' else step64
@@ -533,6 +538,7 @@ def main():
         return 0
     for k in range(max(3, args.warmup)):
         step128(k); step64(k); step_e2e(k)
+    e2e_stream(3)
     torch.cuda.synchronize(device)
     launches0 = engine.apply_count
     with ClockSampler(gpu_identifier(torch, device)) as clocks:
@@ -540,10 +546,12 @@ def main():
         launches = (engine.apply_count - launches0) * engine.launches_per_apply
         ms64 = timed(step64, args.steps)
         e2e_steps = max(3, min(args.steps, 20))
-        ms_e2e = timed(step_e2e, e2e_steps)
+        ms_e2e_seq = timed(step_e2e, e2e_steps)
+        ms_e2e = timed(lambda k: e2e_stream(e2e_steps) if k == 0 else None, 1)
     per128 = ms128 / args.steps
     per64 = ms64 / args.steps
     per_e2e = ms_e2e / e2e_steps
+    per_e2e_seq = ms_e2e_seq / e2e_steps
     value = world * bytes128 / (per128 * 1e-3) / 1e9
     value64 = world * (2 * N * 8) / (per64 * 1e-3) / 1e9
     e2e = world * bytes128 / (per_e2e * 1e-3) / 1e9
@@ -575,7 +583,10 @@ def main():
                       'frac': value64 / world / hbm, 'speedup_vs_complex128': per128 / per64},
         'e2e': {'value': e2e, 'unit': 'GB/s', 'ms_per_step': per_e2e, 'steps': e2e_steps,
                 'h2d_bytes_per_step': N * 16, 'd2h_bytes_per_step': N * 16,
-                'path': 'pinned host psi -> H2D -> B200Hamiltonian.apply -> D2H pinned host'},
+                'path': 'B200Hamiltonian.apply_host_stream over pinned host states: H2D of state k+1 and D2H '
+                        'of state k-1 overlap the apply of state k',
+                'sequential': {'value': world * bytes128 / (per_e2e_seq * 1e-3) / 1e9, 'ms_per_step': per_e2e_seq,
+                               'path': 'pinned host psi -> H2D -> B200Hamiltonian.apply -> D2H, one state at a time'}},
         'clocks': clocks.summary(),
     }
     if not args.no_arnoldi:

@@ -243,6 +243,51 @@ class B200Hamiltonian:
         return out
 
     @torch.no_grad()
+    def apply_host_stream(self, xs, field=(0., 0., 0.), velocity=True, outs=None, precision=None):
+        """outs[k] = H(field) xs[k] for a sequence of host states (pinned CPU tensors), with
+        the transfers overlapped: while state k is applied, state k+1 is copied in on one
+        stream and the result of state k-1 is copied out on another (the two directions use
+        separate copy engines), through two device buffers each way.  Returns `outs`
+        (allocated pinned when None) after the last copy has landed."""
+        code, dtype = PRECISIONS[precision or ('complex128' if xs[0].dtype == torch.complex128 else 'complex64')]
+        for x in xs:
+            if x.device.type != 'cpu' or x.dtype != dtype or x.numel() != self.size:
+                raise ValueError(f'host states must be {dtype} CPU tensors of {self.size} elements')
+        if outs is None:
+            outs = [torch.empty(self.size, dtype=dtype).pin_memory() for _ in xs]
+        dev_in = [torch.empty(self.size, dtype=dtype, device=self.device) for _ in range(2)]
+        dev_out = [torch.empty_like(dev_in[0]) for _ in range(2)]
+        compute = torch.cuda.current_stream(self.device)
+        h2d, d2h = torch.cuda.Stream(self.device), torch.cuda.Stream(self.device)
+        h2d.wait_stream(compute)
+        d2h.wait_stream(compute)
+        loaded = [torch.cuda.Event() for _ in range(2)]
+        applied = [torch.cuda.Event() for _ in range(2)]
+        drained = [torch.cuda.Event() for _ in range(2)]
+        for k, x in enumerate(xs):
+            b = k % 2
+            with torch.cuda.stream(h2d):
+                if k >= 2:
+                    h2d.wait_event(applied[b])      # state k-2 no longer reads dev_in[b]
+                dev_in[b].copy_(x, non_blocking=True)
+                loaded[b].record(h2d)
+            compute.wait_event(loaded[b])
+            if k >= 2:
+                compute.wait_event(drained[b])      # result k-2 has left dev_out[b]
+            self.apply(dev_in[b], field, velocity, out=dev_out[b], precision=precision)
+            applied[b].record(compute)
+            with torch.cuda.stream(d2h):
+                d2h.wait_event(applied[b])
+                outs[k].copy_(dev_out[b], non_blocking=True)
+                drained[b].record(d2h)
+        compute.wait_stream(d2h)
+        compute.wait_stream(h2d)
+        for t in dev_in + dev_out:
+            t.record_stream(compute)
+        torch.cuda.current_stream(self.device).synchronize()
+        return outs
+
+    @torch.no_grad()
     def apply_batched(self, x, fields, velocity=True, out=None, precision=None):
         """out[b] = H(fields[b]) x[b] for a batch of instances sharing this operator:
         x is (count, size) (or count*size) complex128/complex64, fields is (count, 3)."""

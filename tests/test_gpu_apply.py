@@ -267,3 +267,21 @@ def test_band_kernel_single_and_double_stage_forms_agree(precision):
         op.synchronize()
         np.testing.assert_array_equal(results[1][0], results[2][0])
         np.testing.assert_array_equal(results[1][1], results[2][1])
+
+
+def test_host_stream_apply_matches_device_apply():
+    """apply_host_stream (H2D, apply and D2H of consecutive host states overlapped on three
+    streams) returns exactly the per-state device results, for more states than buffers."""
+    from laqphysics_b200.workloads import arnoldi_small, seeded_state
+    h = arnoldi_small()
+    op = engine(h)
+    xs = [torch.as_tensor(seeded_state(h.size, 60 + k)).pin_memory() for k in range(5)]
+    f = (0., 0., .02)
+    outs = op.apply_host_stream(xs, f, False)
+    for x, y in zip(xs, outs):
+        ref = op.host(op.apply(x.to(DEVICE), f, False))
+        np.testing.assert_array_equal(y.numpy(), ref)
+    outs64 = op.apply_host_stream([x.to(torch.complex64).pin_memory() for x in xs], f, True, precision='complex64')
+    ref = op.host(op.apply(xs[3].to(DEVICE).to(torch.complex64), f, True, precision='complex64'))
+    np.testing.assert_array_equal(outs64[3].numpy(), ref)
+    op.synchronize()
