@@ -290,8 +290,8 @@ def batched_leg(torch, device, steps, count=32):
 def adjoint_leg(torch, device, steps=128, knots=32, checkpoint=32):
     """Adjoint gradient on the Arnoldi grid widened to l <= 4: `steps` fixed Arnoldi steps
     (dt 0.005, Krylov tolerance 1e-12, maxdim 30) under a field of `knots` seeded samples
-    (two pulses, peak 0.02 a.u.); objective = population of the total-L = 1 channels
-    (the dipole-excited part of the two-electron state).
+    (two pulses, peak 0.02 a.u.); objective = He+(n = 2) channel yield with the second
+    electron beyond 5 a.u. (adjoint.ChannelYield).
     Reports the forward and backward times and their ratio."""
     from laqphysics_b200 import workloads
     from laqphysics_b200.adjoint import Propagation, check_complex_symmetric
@@ -302,14 +302,14 @@ def adjoint_leg(torch, device, steps=128, knots=32, checkpoint=32):
     psi0 = (g.reshape(h.shape, order='F') * ratio[:, None, None] * ratio[None, :, None]).ravel(order='F')
     engine = B200Hamiltonian(h, device)
     check_complex_symmetric(engine)
-    dipole = np.array([float(L == 1) for _, _, L in h.basis])   # channels of total L = 1
-    mask = np.broadcast_to(dipole[None, None, :], h.shape).astype(float).ravel(order='F')
+    from laqphysics_b200.adjoint import ChannelYield
+    objective = ChannelYield(h, device, shell=2, radius=5.)
     dt = .005
     rng = np.random.default_rng(512)
     t = np.linspace(0, steps * dt, knots)
     theta = .02 * (np.exp(-((t - .3 * t[-1]) / (.1 * t[-1])) ** 2) + np.exp(-((t - .7 * t[-1]) / (.1 * t[-1])) ** 2))
     theta *= rng.uniform(.8, 1.2, knots)
-    prop = Propagation(engine, psi0, dt, steps, t, mask, tol=1e-12, maxdim=30, checkpoint=checkpoint)
+    prop = Propagation(engine, psi0, dt, steps, t, objective, tol=1e-12, maxdim=30, checkpoint=checkpoint)
     prop.forward(theta)                                   # warm-up (generated kernels, workspaces)
     prop.gradient()
     torch.cuda.synchronize(device)
@@ -321,7 +321,8 @@ def adjoint_leg(torch, device, steps=128, knots=32, checkpoint=32):
     torch.cuda.synchronize(device)
     t2 = time.perf_counter()
     return {'workload': f'adjoint gradient: l1,l2<=4 L<=2 (nc={h.nc}, n={h.n}), {steps} Arnoldi steps dt 0.005, '
-                        f'{knots} field samples, checkpoint {checkpoint}, objective: population of L=1 channels',
+                        f'{knots} field samples, checkpoint {checkpoint}, objective: He+(n=2) yield, '
+                        f'second electron beyond 5 a.u.',
             'objective': J, 'forward_ms': (t1 - t0) * 1e3, 'backward_ms': (t2 - t1) * 1e3,
             'backward_over_forward': (t2 - t1) / (t1 - t0), 'gradient_norm': float(np.linalg.norm(grad))}
 

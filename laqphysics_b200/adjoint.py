@@ -7,8 +7,10 @@ propagation of python/propagate.py:41-50 (midpoint field, fixed dt).  The forwar
     H(E) = H0 + E D  (length gauge along z, src/kernels.f90:147-152),
     E(t) = sum_k theta_k phi_k(t)  (piecewise-linear hat functions on K knots),
 
-and the objective is J = <psi_N | P | psi_N> with P a real diagonal mask (for example
-the probability of one electron beyond a radius, or the population of a set of channels).
+and the objective is J = <psi_N | P | psi_N> with P Hermitian: a real diagonal mask (the
+probability of one electron beyond a radius, the population of a set of channels) or the
+ion-channel yield :class:`ChannelYield` (He+ left in shell n with the other electron beyond
+a radius).
 
 Backward pass (exact for the discrete map, up to the Krylov tolerance):
 
@@ -20,7 +22,8 @@ Backward pass (exact for the discrete map, up to the Krylov tolerance):
   exponential applied to conj(lambda_n) gives both the costate step
   lambda_{n-1} = exp(A^dagger) lambda_n (bottom block, conjugated back) and the
   gradient term dJ/dE_n = 2 Re <L(A^dagger, B^dagger) lambda_n | psi_{n-1}> (top block).
-* lambda_N = P psi_N; dJ/dtheta = sum_n (dJ/dE_n) phi_k(t_{n-1} + dt/2).
+* lambda_N = P psi_N (dJ = 2 Re <P psi_N | d psi_N> for Hermitian P);
+  dJ/dtheta = sum_n (dJ/dE_n) phi_k(t_{n-1} + dt/2).
 * States are kept every `checkpoint` steps and each segment is recomputed forward
   before its backward sweep.  The block system's H·psi products run as one batched
   apply of three instances (H u, H w, H(E+1) w; D w = H(E+1) w - H(E) w).
@@ -30,7 +33,35 @@ Backward pass (exact for the discrete map, up to the Krylov tolerance):
 import numpy as np
 import torch
 
+from .angular import radial_hydrogen
 from .torch_backend import FieldOperator, exponential_action
+
+
+class ChannelYield:
+    """P = sum_c |phi_{n, l1(c)}><phi_{n, l1(c)}| (electron 1) x Theta(r2 > radius): the
+    probability of finding He+ in shell n (every l < n that the channels carry) with the
+    second electron beyond `radius`, the box form of an ion-channel yield.  phi_{n l} is the
+    hydrogenic Z = 2 radial function on the grid (r R_nl(r) sqrt(w), normalised on the grid);
+    channels whose electron-1 momentum has no state in shell n contribute nothing."""
+
+    def __init__(self, h, device, shell=2, radius=8.):
+        r, w = np.asarray(h.r), np.asarray(h.grid.weights)
+        phi = {}
+        for l in range(shell):
+            v = r * radial_hydrogen(shell, l, r, 2.0) * np.sqrt(w)
+            phi[l] = v / np.linalg.norm(v)
+        labels = [c[0] for c in h.basis] if hasattr(h, 'basis') else [a[0] for a, _ in h.ch]
+        Phi = np.array([phi[l] if l in phi else np.zeros(h.n, complex) for l in labels])
+        self.n, self.nc = h.n, h.nc
+        self.Phi = torch.as_tensor(Phi, dtype=torch.complex128, device=device)            # (nc, n) over r1
+        self.outer = torch.as_tensor((np.asarray(r).real > radius).astype(float), dtype=torch.complex128,
+                                     device=device)                                          # over r2
+
+    def __call__(self, psi):
+        """P psi for a Fortran-order state psi(i, j, c) (viewed as u[c, j, i])."""
+        u = psi.reshape(self.nc, self.n, self.n)
+        a = torch.einsum('ci,cji->cj', self.Phi.conj(), u) * self.outer[None, :]
+        return torch.einsum('ci,cj->cji', self.Phi, a).reshape(-1)
 
 
 def hat_weights(knots, t):
@@ -67,7 +98,8 @@ class Propagation:
     """Fixed-step length-gauge Arnoldi propagation of one state under a sampled field.
 
     engine: B200Hamiltonian; psi0: initial state (numpy or device tensor); dt, steps;
-    knots: K sample times of E(t); mask: real diagonal of P (numpy, engine.size);
+    knots: K sample times of E(t); mask: the objective's P, a real diagonal (numpy,
+    engine.size) or a callable psi -> P psi on the device (Hermitian, e.g. ChannelYield);
     tol/maxdim: Krylov controls (no dt halving: the gradient is that of this exact map,
     so a step that does not converge raises)."""
 
@@ -78,7 +110,11 @@ class Propagation:
         self.knots = np.asarray(knots, float)
         self.tmid = self.dt * (np.arange(self.steps) + 0.5)
         self.W = hat_weights(self.knots, self.tmid)                       # (steps, K)
-        self.mask = torch.as_tensor(np.asarray(mask, float), device=engine.device).to(torch.complex128)
+        if callable(mask):
+            self.P = mask
+        else:
+            diagonal = torch.as_tensor(np.asarray(mask, float), device=engine.device).to(torch.complex128)
+            self.P = lambda psi: diagonal * psi
 
     def fields(self, theta):
         return self.W @ np.asarray(theta, float)
@@ -99,7 +135,7 @@ class Propagation:
                 self._checkpoints[n + 1] = psi.clone()
         self._final = psi
         self._E = E
-        return float(torch.sum(self.mask * (psi.conj() * psi)).real)
+        return float(torch.sum(psi.conj() * self.P(psi)).real)
 
     def _block_apply(self, e):
         engine, size = self.engine, self.engine.size
@@ -117,7 +153,7 @@ class Propagation:
         if self._checkpoints is None:
             raise RuntimeError('run forward(theta, keep=True) first')
         size, E = self.engine.size, self._E
-        lam = self.mask * self._final                                  # dJ/dpsi_N (up to the factor 2 in Re)
+        lam = self.P(self._final)                                      # dJ/dpsi_N (up to the factor 2 in Re)
         gE = np.zeros(self.steps)
         starts = sorted(self._checkpoints)
         for s in reversed(starts):

@@ -83,3 +83,41 @@ def test_adjoint_gradient_matches_oracle_fp64_gradient():
                         for e in np.eye(len(theta))])
     assert np.abs(ref).max() > 0
     assert np.abs(g - ref).max() <= 1e-6 * np.abs(ref).max(), (g, ref)
+
+
+def test_channel_yield_gradient_matches_device_and_oracle_differences():
+    """Objective = He+(n = 2) yield with the second electron beyond 6 a.u. (a Hermitian,
+    non-diagonal P): adjoint gradient against central differences of the device propagation
+    and of the CPU oracle propagation (h = 1e-5), 1e-6 of the largest component."""
+    from threadpoolctl import threadpool_limits
+    from oracle import arnoldi, cpu
+    from laqphysics_b200.adjoint import ChannelYield, Propagation
+    prop0, theta, h, psi0, _ = setup(with_tables=True)
+    P = ChannelYield(h, DEVICE, shell=2, radius=6.)
+    prop = Propagation(prop0.engine, psi0, prop0.dt, prop0.steps, prop0.knots, P, tol=1e-13, maxdim=30, checkpoint=8)
+    J = prop.forward(theta)
+    g = prop.gradient()
+    assert J > 0 and np.abs(g).max() > 0
+    step = 1e-5
+    fd = np.array([(prop.forward(theta + step * e, keep=False) - prop.forward(theta - step * e, keep=False)) / (2 * step)
+                   for e in np.eye(len(theta))])
+    assert np.abs(g - fd).max() <= 1e-6 * np.abs(g).max(), (g, fd)
+    Phi = P.Phi.cpu().numpy()
+    outer = P.outer.cpu().numpy().real
+    tables = cpu.host_tables(h)
+
+    def objective(th):
+        E = prop.fields(th)
+        x = psi0.copy()
+        for n in range(prop.steps):
+            x, _ = arnoldi.exponential_action(
+                lambda y, e=E[n]: cpu.tensor_apply(h, y, (0., 0., e), False, tables=tables), x, prop.dt, 1e-13, 30)
+        u = x.reshape((h.n, h.n, h.nc), order='F')
+        a = np.einsum('ci,ijc->jc', Phi.conj(), u)
+        return float(np.sum(outer[:, None] * np.abs(a) ** 2))
+
+    with threadpool_limits(limits=1, user_api='blas'):
+        assert abs(objective(theta) - J) <= 1e-10 * J
+        ref = np.array([(objective(theta + step * e) - objective(theta - step * e)) / (2 * step)
+                        for e in np.eye(len(theta))])
+    assert np.abs(g - ref).max() <= 1e-6 * np.abs(ref).max(), (g, ref)
