@@ -194,6 +194,21 @@ int he_krylov_combine_coef(he_krylov_handle k, int which, int m, const void *coe
                            void *stream);
 
 /* ------------------------------------------------------------------------------------
+ * Mixed length/velocity gauge (replaces MixedHamiltonian, python/mixed_gauge.py:73-117).
+ * he_set_mixed_gauge attaches, once per handle, the gauge-function profiles on the radial
+ * grid (complex, n each: q = r (1 - f), qr2h = q / (2 r^2), F = r f, c0 = (1 - f)^2,
+ * c2 = q'^2 - (1 - f)^2) and the quadratic angular edges per output channel (qptr: nc + 1,
+ * source qc, electron qe (1 or 2), qcoef: 6 complex per edge = the projected
+ * rhat_x^2, rhat_y^2, rhat_z^2, rhat_x rhat_y, rhat_x rhat_z, rhat_y rhat_z).
+ * he_apply_mixed_terms adds to `out` (complex128, holding the field-free H psi) the
+ * gauge terms of field = (A_x, A_y, A_z, E_x, E_y, E_z, then the six A_a A_b coefficients,
+ * off-diagonal ones doubled), using the handle's dipole edges.
+ * ---------------------------------------------------------------------------------- */
+int he_set_mixed_gauge(he_handle h, const double *q, const double *qr2h, const double *F, const double *c0,
+                       const double *c2, int nq, const int *qptr, const int *qc, const int *qe, const double *qcoef);
+int he_apply_mixed_terms(he_handle h, const void *psi, void *out, const double *field, void *stream);
+
+/* ------------------------------------------------------------------------------------
  * He+ operator for the backward propagation of the tSURFF channel functions chi_c(t)
  * (replaces IonicAdjoint, python/ionic_adjoint.py:12-52, the device counterpart of the
  * sparse-LU SparseCF4 of python/implicit.py:111-123 used by python/streaming_surface.py:

@@ -52,6 +52,8 @@ SIGNATURES = {
     'he_set_mix_blocks': (I, [P, I, I]),
     'he_set_band_stages': (I, [P, I, I]),
     'he_fp64_peak': (I, [I, I, ct.POINTER(ct.c_double), P]),
+    'he_set_mixed_gauge': (I, [P, P, P, P, P, P, I, P, P, P, P]),
+    'he_apply_mixed_terms': (I, [P, P, P, P, P]),
     'he_ionic_create': (I, [ct.POINTER(P), I, I, I, ct.c_longlong, P, P, P]),
     'he_ionic_set_preconditioner': (I, [P, I, I, P, P, P]),
     'he_ionic_apply': (I, [P, P, I, P, P, D, D, D, I, P]),

@@ -46,6 +46,12 @@ struct he_operator {
                                         // or 2 stages (he_set_band_stages; defaults = the faster on B200)
     int mix_blocks[2] = {2, 4};         // generated mixing kernel: CTAs of 128 threads per SM the register
                                         // budget is sized for (complex128, complex64)
+    struct MixedGaugeTables {           // he_set_mixed_gauge (device, complex128; freed with the handle)
+        bool ready = false;
+        double2 *q = nullptr, *qr2h = nullptr, *F = nullptr, *c0 = nullptr, *c2 = nullptr, *qcoef = nullptr;
+        int *qptr = nullptr, *qc = nullptr, *qe = nullptr;
+        int nq = 0;
+    } mg;
     std::vector<void *> allocations;    // every cudaMalloc made for this handle
     ~he_operator();
 };

@@ -187,6 +187,31 @@ def ionic_adjoint_case():
          pulse=json.dumps(dict(omega=2.0, cycles=2, field=.3)), dt=dt, t_end=t_end, states=np.array(states))
 
 
+def mixed_gauge_case():
+    # Mixed length/velocity gauge operator (python/mixed_gauge.py:73-117) on CPU torch: the
+    # coupled M = 0 case with a z field and the bipolar all-M case with a general field;
+    # field = (A, E, six quadratic coefficients A_a A_b) as python/mixed_gauge.py:30-33 forms it.
+    from mixed_gauge import MixedHamiltonian, parameters
+    from bipolar import BipolarHelium
+    out = {}
+    args = dict(edges=[0, .5, 1, 2, 4, 6, 8], order=3, ecs_angle=.4, tail=6)
+    g = make_grid(**args)
+    cases = {'coupled': (CoupledHelium(Helium(g, 2, M=0, cutoff_radii=[1, 2]), 2), lambda t: np.array([0, 0, .21]),
+                         lambda t: np.array([0, 0, -.13])),
+             'bipolar': (BipolarHelium(g, lmax=1, total_Lmax=2, M=None, cutoff_radii=[1, 2]),
+                         lambda t: np.array([.11, -.07, .15]), lambda t: np.array([-.05, .09, .04]))}
+    for key, (h, avec, efunc) in cases.items():
+        op = MixedHamiltonian(h, 'cpu', inner=1.5, outer=3.5)
+        rng = np.random.default_rng(811)
+        x = rng.normal(size=h.size) + 1j * rng.normal(size=h.size)
+        field = parameters(avec, efunc, 0.)
+        out[f'{key}_x'] = x
+        out[f'{key}_field'] = field
+        out[f'{key}_y'] = op.host(op.apply(op.state(x), field))
+        out[f'{key}_y0'] = op.host(op.apply(op.state(x), np.zeros(12)))
+    save('mixed_gauge', grid=json.dumps(args), cutoff=np.array([1., 2.]), inner=1.5, outer=3.5, **out)
+
+
 def arnoldi_dense():
     # python tests/test_kernels.py:42-47.
     from scipy.linalg import expm
@@ -343,6 +368,7 @@ if __name__ == '__main__':
     coupled_case()
     bipolar_case()
     ionic_adjoint_case()
+    mixed_gauge_case()
     arnoldi_dense()
     length_gauge_run()
     cf4_cases()
