@@ -6,7 +6,7 @@ Clebsch-Gordan coefficients and the folded-m masks — as one entry list per lab
 (frame column, inner ionic state, real coefficient, outer state).  ``__call__`` then
 computes q[label, outer, s] = sum_entries coef sum_r conj(chi[inner, r, column]) frame(r, s, col)
 in one device launch (python/surface_contract.py:41-56).  Sparse (bipolar) transforms
-are not supported yet and raise.
+contribute one entry per non-zero, as the reference's sparse path does.
 """
 import ctypes as ct
 
@@ -26,10 +26,11 @@ class SurfaceContractor:
         self.outerstates = sorted({h.ch[c][1] for c in active})
         outerindex = {x: i for i, x in enumerate(self.outerstates)}
         self.shape = (len(labels), len(self.outerstates), len(h.surface_indices))
-        if angular_transform is not None and issparse(angular_transform):
-            raise NotImplementedError('sparse (bipolar) angular transforms are not supported by the device contractor')
+        sparse = angular_transform is not None and issparse(angular_transform)
+        if sparse:   # bipolar transforms: every non-zero becomes an entry (python/surface_contract.py:29-32)
+            angular_transform = angular_transform.toarray()
         self.transform = angular_transform
-        self.fast = bool(angular_transform is not None and folded)
+        self.fast = bool(angular_transform is not None and folded and not sparse)
         entries = [[] for _ in labels]          # (frame column, inner, coef, outer)
         if self.fast:
             U = angular_transform

@@ -212,6 +212,26 @@ def mixed_gauge_case():
     save('mixed_gauge', grid=json.dumps(args), cutoff=np.array([1., 2.]), inner=1.5, outer=3.5, **out)
 
 
+def bipolar_contraction_case():
+    # Ionic contraction of a surface frame in the bipolar all-M basis (sparse angular
+    # transform, unfolded labels): python/surface_contract.py:29-37 and 49-56.
+    from bipolar import BipolarHelium
+    from surface3d import Ionic
+    from surface_contract import SurfaceContractor as RefContractor
+    args = dict(edges=[0, 1, 2, 3, 4, 6, 8, 10, 12], order=4, ecs_angle=.3, tail=8)
+    h = BipolarHelium(make_grid(**args), lmax=1, total_Lmax=1, M=None, cutoff_radii=[3, 4])
+    base = h.uncoupled
+    idx = base.prepare_surface(8.)
+    ion = Ionic(base, None)
+    labels = [(1, 0, 0), (2, 0, 0), (2, 1, -1), (2, 1, 0), (2, 1, 1)]
+    contract = RefContractor(base, ion, labels, labels, list(range(len(labels))), False, h.transform)
+    rng = np.random.default_rng(97)
+    chi = rng.normal(size=(ion.na * h.n, len(labels))) + 1j * rng.normal(size=(ion.na * h.n, len(labels)))
+    frame = rng.normal(size=(h.n, len(idx), h.nc)) + 1j * rng.normal(size=(h.n, len(idx), h.nc))
+    save('bipolar_contraction', grid=json.dumps(args), cutoff=np.array([3., 4.]), surface=8., labels=np.array(labels),
+         chi=chi, frame=frame, q=contract(chi, frame), outer=np.array(contract.outerstates))
+
+
 def arnoldi_dense():
     # python tests/test_kernels.py:42-47.
     from scipy.linalg import expm
@@ -369,6 +389,7 @@ if __name__ == '__main__':
     bipolar_case()
     ionic_adjoint_case()
     mixed_gauge_case()
+    bipolar_contraction_case()
     arnoldi_dense()
     length_gauge_run()
     cf4_cases()

@@ -71,3 +71,27 @@ def test_bipolar_surface_flux_and_arnoldi_step():
     ref, rinfo = arnoldi.exponential_action(lambda v: cpu.tensor_apply(b, v, f, False), x, .01, tol=1e-11, maxdim=24)
     assert info['dimension'] == rinfo['dimension']
     assert rel_l2(op.host(y), ref) < 1e-12
+
+
+def test_bipolar_surface_contraction_matches_reference():
+    """Ionic contraction of a surface frame in the bipolar all-M basis (unfolded He+ labels
+    with m = -1, 0, 1) against the reference's sparse-transform contraction, 1e-12."""
+    import json as js
+    from scipy.sparse import csr_matrix
+    from conftest import golden
+    from laqphysics_b200.bipolar import BipolarHelium
+    from laqphysics_b200.fedvr import make_grid
+    from laqphysics_b200.surface3d import Ionic
+    from laqphysics_b200.surface_contract import SurfaceContractor
+    g = golden('bipolar_contraction')
+    h = BipolarHelium(make_grid(**js.loads(str(g['grid']))), lmax=1, total_Lmax=1, M=None,
+                      cutoff_radii=tuple(g['cutoff']))
+    base = h.uncoupled
+    base.prepare_surface(float(g['surface']))
+    ion = Ionic(base, None)
+    labels = [tuple(int(v) for v in x) for x in g['labels']]
+    for transform in (h.transform, csr_matrix(h.transform)):
+        contract = SurfaceContractor(base, ion, labels, labels, list(range(len(labels))), False, transform, DEVICE)
+        assert contract.outerstates == [tuple(int(v) for v in x) for x in g['outer']]
+        q = contract(g['chi'], g['frame'])
+        np.testing.assert_allclose(q, g['q'], rtol=1e-12, atol=1e-12)
