@@ -40,7 +40,10 @@ def parse():
     p.add_argument('--impl', choices=['b200', 'reference'], default='b200')
     p.add_argument('--no-cpu-baseline', action='store_true')
     p.add_argument('--no-arnoldi', action='store_true', help='skip the Arnoldi steps/s leg')
-    p.add_argument('--profile', choices=['c128', 'c64', 'arnoldi', 'batched', 'cf4'], default=None,
+    p.add_argument('--adjoint-steps', type=int, default=128, help='adjoint leg: Arnoldi steps (dt 0.005)')
+    p.add_argument('--adjoint-knots', type=int, default=32, help='adjoint leg: field samples')
+    p.add_argument('--adjoint-checkpoint', type=int, default=32, help='adjoint leg: steps between checkpoints')
+    p.add_argument('--profile', choices=['c128', 'c64', 'arnoldi', 'batched', 'cf4', 'adjoint'], default=None,
                    help='run only W+K applications of one precision (for ncu captures); prints no JSON')
     return p.parse_args()
 
@@ -486,6 +489,10 @@ def main():
     if args.profile == 'cf4':
         print(json.dumps(cf4_leg(torch, device, steps=args.steps)), flush=True)
         return 0
+    if args.profile == 'adjoint':
+        print(json.dumps(adjoint_leg(torch, device, args.adjoint_steps, args.adjoint_knots, args.adjoint_checkpoint)),
+              flush=True)
+        return 0
     h = workloads.hpsi_microbench()
     engine = B200Hamiltonian(h, device)
     field = (0., 0., .02)
@@ -594,7 +601,7 @@ def main():
         line['arnoldi'] = arnoldi_leg(torch, device, steps=max(10, min(args.steps, 100)),
                                       cpu_steps=0 if (args.no_cpu_baseline or world > 1 or rank) else 3)
         line['batched'] = batched_leg(torch, device, steps=max(5, min(args.steps, 30)))
-        line['adjoint'] = adjoint_leg(torch, device)
+        line['adjoint'] = adjoint_leg(torch, device, args.adjoint_steps, args.adjoint_knots, args.adjoint_checkpoint)
         line['spectrum'] = spectrum_leg(torch, device)
         line['cf4'] = cf4_leg(torch, device)
 
