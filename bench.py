@@ -43,7 +43,8 @@ def parse():
     p.add_argument('--adjoint-steps', type=int, default=128, help='adjoint leg: Arnoldi steps (dt 0.005)')
     p.add_argument('--adjoint-knots', type=int, default=32, help='adjoint leg: field samples')
     p.add_argument('--adjoint-checkpoint', type=int, default=32, help='adjoint leg: steps between checkpoints')
-    p.add_argument('--profile', choices=['c128', 'c64', 'arnoldi', 'batched', 'cf4', 'adjoint'], default=None,
+    p.add_argument('--profile', choices=['c128', 'c64', 'arnoldi', 'batched', 'cf4', 'adjoint', 'concurrent'],
+                   default=None,
                    help='run only W+K applications of one precision (for ncu captures); prints no JSON')
     return p.parse_args()
 
@@ -330,6 +331,48 @@ def adjoint_leg(torch, device, steps=128, knots=32, checkpoint=32):
             'backward_over_forward': (t2 - t1) / (t1 - t0), 'gradient_norm': float(np.linalg.norm(grad))}
 
 
+def concurrent_leg(torch, device, count=8, steps=3):
+    """Instances of different operators (Arnoldi-type grids with 8-15 tail points, l <= 2
+    or 3, L <= 2; own fields) stepped together by laqphysics_b200.concurrent (one stream and
+    host thread each) against the same instances stepped one after another; maxdim 12,
+    dt 0.02, tol 1e-10, seeded states.  Wall time around synchronized regions."""
+    from laqphysics_b200.concurrent import ConcurrentStepper
+    from laqphysics_b200.engine import B200Hamiltonian
+    from laqphysics_b200.torch_backend import FieldSchedule, step
+    from laqphysics_b200 import workloads
+    schedules, states, sizes = [], [], []
+    for k in range(count):
+        h = workloads.coupled(np.linspace(0, 25, 16), 8, 2 + k % 2, 2, ecs_angle=.3, tail=8 + k, cutoff_radii=(18., 22.))
+        e = B200Hamiltonian(h, device)
+        amp = .005 + .003 * k
+        schedules.append(FieldSchedule(e, lambda t, a=amp: (0., 0., a * np.sin(1.6 * t)), velocity=False))
+        x = workloads.seeded_state(h.size, 90 + k)
+        states.append(e.state(x / np.linalg.norm(x)))
+        sizes.append(h.size)
+    stepper = ConcurrentStepper(schedules, device)
+    dt, tol, maxdim = .02, 1e-10, 12
+    stepper.step(states, 0., dt, tol, maxdim)            # warm-up (generated kernels, workspaces)
+    for sch, x in zip(schedules, states):
+        step(sch, x, 0., dt, tol, maxdim)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    xs = states
+    for i in range(steps):
+        xs, _ = stepper.step(xs, (i + 1) * dt, dt, tol, maxdim)
+    torch.cuda.synchronize(device)
+    together = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for sch, x in zip(schedules, states):
+        for i in range(steps):
+            x, _ = step(sch, x, (i + 1) * dt, dt, tol, maxdim)
+    torch.cuda.synchronize(device)
+    alone = time.perf_counter() - t0
+    stepper.close()
+    return {'workload': f'{count} instances of different operators (N = {min(sizes)}..{max(sizes)}), {steps} Arnoldi '
+                        f'steps each, maxdim 12, dt 0.02', 'instance_steps_per_s': count * steps / together,
+            'one_after_another_instance_steps_per_s': count * steps / alone, 'speedup': alone / together}
+
+
 def cf4_leg(torch, device, steps=10):
     """CF4 Magnus steps, each exponential a [2/2] Pade pair of shifted solves by right-
     preconditioned GMRES (the reference's implicit.py:45-109 path), on the Arnoldi grid
@@ -489,6 +532,9 @@ def main():
     if args.profile == 'cf4':
         print(json.dumps(cf4_leg(torch, device, steps=args.steps)), flush=True)
         return 0
+    if args.profile == 'concurrent':
+        print(json.dumps(concurrent_leg(torch, device)), flush=True)
+        return 0
     if args.profile == 'adjoint':
         print(json.dumps(adjoint_leg(torch, device, args.adjoint_steps, args.adjoint_knots, args.adjoint_checkpoint)),
               flush=True)
@@ -604,6 +650,7 @@ def main():
         line['adjoint'] = adjoint_leg(torch, device, args.adjoint_steps, args.adjoint_knots, args.adjoint_checkpoint)
         line['spectrum'] = spectrum_leg(torch, device)
         line['cf4'] = cf4_leg(torch, device)
+        line['concurrent'] = concurrent_leg(torch, device)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         os.environ.setdefault('OMP_NUM_THREADS', str(os.cpu_count()))

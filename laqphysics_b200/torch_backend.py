@@ -65,9 +65,10 @@ def _device_view(address, n, device):
 
 
 def workspace(n, maxdim, device, flexible=False):
-    """Cached workspace with at least ``maxdim`` Krylov vectors for vectors of length n."""
+    """Cached workspace with at least ``maxdim`` Krylov vectors for vectors of length n, one
+    per CUDA stream (solves running concurrently on different streams never share one)."""
     device = torch.device(device)
-    key = (device, int(n), bool(flexible))
+    key = (device, int(n), bool(flexible), torch.cuda.current_stream(device).cuda_stream)
     ws = _WORKSPACES.get(key)
     if ws is None or ws.maxdim < maxdim:
         ws = KrylovWorkspace(n, max(maxdim, ws.maxdim if ws else 0), device, flexible)
@@ -186,7 +187,7 @@ _BATCHED = {}
 
 def batched_workspace(n, maxdim, count, device):
     device = torch.device(device)
-    key = (device, int(n), int(count))
+    key = (device, int(n), int(count), torch.cuda.current_stream(device).cuda_stream)
     ws = _BATCHED.get(key)
     if ws is None or ws.maxdim < maxdim:
         ws = BatchedWorkspace(n, max(maxdim, ws.maxdim if ws else 0), count, device)
