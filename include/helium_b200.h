@@ -284,9 +284,10 @@ int he_vec_norms_noalloc(long long n, int count, const void *x, long long ld, do
 
 /* ------------------------------------------------------------------------------------
  * Operator set-up options and planner inspection (host only, no device work).
- * he_set_path: 1 = tiled kernels (default when the tables admit them; the radial part
- *   runs on the TMA-staged kinetic kernel when psi is 16-byte aligned), 2 = tiled kernels
- *   with the shared-memory radial kernel (no TMA), 0 = generic gather kernel.
+ * he_set_path: 1 = tiled kernels (default when the tables admit them; the kinetic part
+ *   runs on the banded FP64 tensor-core kernel, TMA-staged, when psi is 16-byte aligned),
+ *   3 = tiled kernels with the TMA-staged FMA kinetic kernel, 2 = tiled kernels with the
+ *   shared-memory radial kernel (no TMA), 0 = generic gather kernel.
  * he_device_status: waits for the handle's device work and reports HE_ERR_DEVICE once
  *   (then clears it) when a bounded device-side wait of a kernel ran out.
  * he_plan_build / he_plan_array / he_plan_free expose the tiled plan of a set of tables.

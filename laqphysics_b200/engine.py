@@ -136,7 +136,7 @@ class B200Hamiltonian:
             return ['hpsi_gather_kernel']
         if self.path == 2:
             radial = 'hpsi_radial_kernel'
-        elif self.path == 1 and precision == 'complex128' and self.plan_info['band_kernel']:
+        elif self.path == 1 and self.plan_info['band_kernel']:
             radial = 'hpsi_band_kernel'
         elif self.plan_info['kinetic_kernel']:
             radial = 'hpsi_kinetic_kernel'
