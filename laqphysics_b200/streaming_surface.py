@@ -115,14 +115,16 @@ class VolkovAccumulator:
         pes = abs(amp) ** 2 * self.k[None, :, None]
         return pes, np.sum(pes * self.solid_angle_weights[None, None, :], axis=2)
 
-    def write(self, path, signature=''):
+    def write(self, path, signature='', max_file_bytes=4_000_000_000):
+        """The spectrum file of python/streaming_surface.py:74-82 (same keys, atomic capped write)."""
+        from .checkpoint import capped_npz
         pes, total = self.spectrum()
-        np.savez(path, energy=self.energy, theta=self.theta, phi=self.phi,
-                 solid_angle_weights=self.solid_angle_weights, amplitudes=self.amplitude.cpu().numpy(), pes=pes,
-                 angle_integrated=total, labels=self.labels, source_signature=signature,
-                 extraction_end_time=self.time, projection_final_time=self.time,
-                 spectrum_scope='single ionization into the explicitly recorded bound ionic channels',
-                 angular_rule='gauss', storage_method='online device accumulation')
+        capped_npz(path, max_file_bytes, energy=self.energy, theta=self.theta, phi=self.phi,
+                   solid_angle_weights=self.solid_angle_weights, amplitudes=self.amplitude.cpu().numpy(), pes=pes,
+                   angle_integrated=total, labels=self.labels, source_signature=signature,
+                   extraction_end_time=self.time, projection_final_time=self.time,
+                   spectrum_scope='single ionization into the explicitly recorded bound ionic channels',
+                   angular_rule='gauss', storage_method='online device accumulation')
 
 
 TorchVolkovAccumulator = VolkovAccumulator
