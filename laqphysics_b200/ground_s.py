@@ -3,8 +3,8 @@
 Same method as the reference's ``GroundS`` (python/ground_s.py:15-89): the S
 state sum_m (-1)^(l-m) Y_lm Y_l,-m / sqrt(2l+1) reduces the problem to lmax+1
 radial channels; LOBPCG is preconditioned by the exact separable inverse built
-from the eigenvectors of each one-electron radial Hamiltonian.  The matvec is
-this package's GPU ``tensor_apply`` through the C-ABI.
+from the eigenvectors of each one-electron radial Hamiltonian.  The matvec runs in this
+package's GPU kernels with the tables resident on the device for the whole solve.
 """
 import hashlib
 import os
@@ -53,8 +53,13 @@ class GroundS:
         self.ldiff = np.zeros(0)
 
     def apply(self, x):
-        from .native import tensor_apply
-        return tensor_apply(self, x)
+        """H x in the compressed basis on the GPU: the tables stay resident in one engine
+        for the whole solve (only x and H x cross the bus per product)."""
+        engine = getattr(self, '_engine', None)
+        if engine is None:
+            from .engine import B200Hamiltonian
+            engine = self._engine = B200Hamiltonian(self, 'cuda:0')
+        return engine.host(engine.apply(engine.state(x), (0., 0., 0.), False))
 
     def expand(self, x):
         u = np.asarray(x).reshape(self.shape, order='F')
