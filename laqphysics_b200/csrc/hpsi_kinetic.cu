@@ -60,7 +60,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity
     return false;
 }
 
-// Tiled TMA load of one box (no multicast) completing on `bar`.
+// Tiled TMA load of one box into this CTA's shared memory, completing on `bar`.
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar)
 {
     asm volatile(
