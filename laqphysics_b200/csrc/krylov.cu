@@ -848,6 +848,17 @@ __global__ void krylov_to_c128(size_t n, const float2 *x, double2 *y)
         y[p] = make_double2((double)x[p].x, (double)x[p].y);
 }
 
+// Grid of a fused sweep: one instance keeps KRYLOV_BLOCKS CTAs; a batch gets as many CTAs
+// per instance as fill the SMs in one wave at the kernel's own occupancy (the sweeps of a
+// batch stream from HBM), at most KRYLOV_BLOCKS (the size of the partial-sum slices).
+dim3 sweep_grid(const he_krylov *k, const void *kernel)
+{
+    if (k->count == 1) return bgrid(k);
+    const int per_sm = resident_ctas(kernel, KRYLOV_THREADS, 0);
+    const int blocks = std::min(KRYLOV_BLOCKS, std::max(8, per_sm * sm_count(k->device) / k->count));
+    return dim3(blocks, k->count);
+}
+
 // project + reorth(+ check) sweeps of one fused Arnoldi iteration, with the register tile
 // sized to the basis (4, 8, 12 or 16 vectors).
 template <int KT>
@@ -855,9 +866,10 @@ void launch_fused_sweeps(he_krylov *k, int kc, double2 *v, const float2 *src32, 
                          double tol, cudaStream_t s)
 {
     const int ld = k->maxdim + 1;
-    arnoldi_project_kernel<KT><<<bgrid(k), kBlock, 0, s>>>(k->Q, k->n, k->qs(), kc, v, src32, k->partial, ld, k->ticket,
+    arnoldi_project_kernel<KT><<<sweep_grid(k, reinterpret_cast<const void *>(arnoldi_project_kernel<KT>)), kBlock, 0, s>>>(k->Q, k->n, k->qs(), kc, v, src32, k->partial, ld, k->ticket,
                                                           k->z, k->H, k->hs(), j, k->status);
-    arnoldi_reorth_kernel<KT><<<bgrid(k), kBlock, 0, s>>>(k->Q, k->n, k->qs(), kc, k->z, v, k->partial, ld, k->ticket,
+    arnoldi_reorth_kernel<KT><<<sweep_grid(k, reinterpret_cast<const void *>(arnoldi_reorth_kernel<KT>)), kBlock, 0, s>>>(
+        k->Q, k->n, k->qs(), kc, k->z, v, k->partial, ld, k->ticket,
                                                          k->H, k->hs(), j, maxdim, dt, tol, k->coef, k->work, k->ws(),
                                                          k->status, 1e-13);
 }
@@ -918,7 +930,8 @@ int expv_impl(he_krylov *k, he_handle op, const void *x, void *y, const double *
             rc = fused_sweeps(k, kc, v, mixed ? k->s32[1] : nullptr, j, maxdim, dt, tol, s);
             if (rc) break;
             if (j + 1 < maxdim) {
-                arnoldi_next_kernel<<<bgrid(k), kBlock, 0, s>>>(k->Q, k->n, k->qs(), kc, k->z, ld, v,
+                arnoldi_next_kernel<<<sweep_grid(k, reinterpret_cast<const void *>(arnoldi_next_kernel)), kBlock, 0, s>>>(
+                    k->Q, k->n, k->qs(), kc, k->z, ld, v,
                                                                mixed ? k->s32[0] : nullptr, k->status);
                 have32 = mixed;
             }

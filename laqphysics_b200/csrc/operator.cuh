@@ -74,6 +74,7 @@ template <typename R>
 int launch_kinetic(he_operator *h, const DeviceTables<R> &t, const KineticPlan<R> &kp, const cplx<R> *psi,
                    cplx<R> *out, cplx<R> *w1, cplx<R> *w2, R a2, int velocity, cudaStream_t stream);
 int sm_count(int device);
+int resident_ctas(const void *kernel, int threads, size_t smem);
 std::string mix_source(const he_plan_host &P, bool dipole_real, int variant);
 int jit_mix_prepare(he_operator *h, int variant);
 template <typename R>
