@@ -544,7 +544,7 @@ arnoldi_project_kernel(const double2 *__restrict__ Q, size_t n, size_t qs, int k
 // reorth: v' = v - Q z written; partials of conj(Q_k) v' and |v'|^2 (column kc); last
 // block -> z' (into z), H[:, j] += z', h, happy flag, then the Arnoldi check.
 template <int KT>
-__global__ void __launch_bounds__(KRYLOV_THREADS)
+__global__ void __launch_bounds__(KRYLOV_THREADS, 3)
 arnoldi_reorth_kernel(const double2 *__restrict__ Q, size_t n, size_t qs, int kc, double2 *__restrict__ z,
                       double2 *__restrict__ v, double2 *__restrict__ partial, int ld, unsigned int *__restrict__ ticket,
                       double2 *__restrict__ H, size_t hs, int j, int maxdim, double dt, double tol,
