@@ -43,7 +43,8 @@ def parse():
     p.add_argument('--adjoint-steps', type=int, default=128, help='adjoint leg: Arnoldi steps (dt 0.005)')
     p.add_argument('--adjoint-knots', type=int, default=32, help='adjoint leg: field samples')
     p.add_argument('--adjoint-checkpoint', type=int, default=32, help='adjoint leg: steps between checkpoints')
-    p.add_argument('--profile', choices=['c128', 'c64', 'arnoldi', 'batched', 'cf4', 'adjoint', 'concurrent'],
+    p.add_argument('--profile', choices=['c128', 'c64', 'arnoldi', 'batched', 'batched-attempt', 'cf4', 'adjoint',
+                                         'concurrent'],
                    default=None,
                    help='run only W+K applications of one precision (for ncu captures); prints no JSON')
     return p.parse_args()
@@ -531,6 +532,24 @@ def main():
         return 0
     if args.profile == 'cf4':
         print(json.dumps(cf4_leg(torch, device, steps=args.steps)), flush=True)
+        return 0
+    if args.profile == 'batched-attempt':   # two 12-iteration attempts of 32 instances (every one runs to maxdim)
+        from laqphysics_b200 import workloads
+        from laqphysics_b200.engine import B200Hamiltonian
+        from laqphysics_b200.torch_backend import step_batched
+        h = workloads.arnoldi_small()
+        engine = B200Hamiltonian(h, device)
+        x = engine.state(workloads.seeded_state(h.size, 1))
+        x /= torch.linalg.vector_norm(x)
+        xb = x.repeat(32).reshape(32, -1).contiguous()
+        fields = np.zeros((32, 3))
+        fields[:, 2] = .01
+        for _ in range(2):
+            try:
+                step_batched(engine, lambda t: fields, xb, 0., .02, 1e-300, 12, depth=8)
+            except RuntimeError:
+                pass
+        torch.cuda.synchronize(device)
         return 0
     if args.profile == 'concurrent':
         print(json.dumps(concurrent_leg(torch, device)), flush=True)
