@@ -43,8 +43,8 @@ def parse():
     p.add_argument('--adjoint-steps', type=int, default=128, help='adjoint leg: Arnoldi steps (dt 0.005)')
     p.add_argument('--adjoint-knots', type=int, default=32, help='adjoint leg: field samples')
     p.add_argument('--adjoint-checkpoint', type=int, default=32, help='adjoint leg: steps between checkpoints')
-    p.add_argument('--profile', choices=['c128', 'c64', 'arnoldi', 'batched', 'batched-attempt', 'cf4', 'adjoint',
-                                         'concurrent'],
+    p.add_argument('--profile', choices=['c128', 'c64', 'arnoldi', 'arnoldi-split', 'batched', 'batched-attempt', 'cf4',
+                                         'adjoint', 'concurrent'],
                    default=None,
                    help='run only W+K applications of one precision (for ncu captures); prints no JSON')
     return p.parse_args()
@@ -532,6 +532,51 @@ def main():
         return 0
     if args.profile == 'cf4':
         print(json.dumps(cf4_leg(torch, device, steps=args.steps)), flush=True)
+        return 0
+    if args.profile == 'arnoldi-split':   # CUDA-event cost of one H·psi and of 12-iteration attempts
+        from laqphysics_b200 import workloads
+        from laqphysics_b200.engine import B200Hamiltonian
+        from laqphysics_b200.torch_backend import FieldOperator, exponential_action, step_batched
+        h = workloads.arnoldi_small()
+        engine = B200Hamiltonian(h, device)
+        x = engine.state(workloads.seeded_state(h.size, 1))
+        x /= torch.linalg.vector_norm(x)
+
+        def per_call_us(fn, reps):
+            for _ in range(3):
+                fn()
+            torch.cuda.synchronize(device)
+            start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record()
+            for _ in range(reps):
+                fn()
+            stop.record()
+            torch.cuda.synchronize(device)
+            return start.elapsed_time(stop) / reps * 1e3
+
+        def attempt(count, precision):
+            if count == 1:
+                op = FieldOperator(engine, (0., 0., .01), velocity=False, precision=precision)
+                call = lambda: exponential_action(op, x, .02, 1e-300, 12)
+            else:
+                xb = x.repeat(count).reshape(count, -1).contiguous()
+                fields = np.zeros((count, 3))
+                fields[:, 2] = .01
+                call = lambda: step_batched(engine, lambda t: fields, xb, 0., .02, 1e-300, 12, precision=precision,
+                                            depth=8)
+
+            def run():
+                try:
+                    call()
+                except RuntimeError:   # tol 1e-300: every attempt runs to maxdim and reports non-convergence
+                    pass
+            return run
+
+        out = {'apply_us': per_call_us(lambda: engine.apply(x, (0., 0., .01), False), 200)}
+        for count in (1, 2, 4, 8, 16, 32):
+            for precision in ('complex128', 'mixed'):
+                out[f'attempt12_us_per_instance_{precision}_x{count}'] = per_call_us(attempt(count, precision), 10) / count
+        print(json.dumps(out), flush=True)
         return 0
     if args.profile == 'batched-attempt':   # two 12-iteration attempts of 32 instances (every one runs to maxdim)
         from laqphysics_b200 import workloads
