@@ -40,6 +40,8 @@ def parse():
     p.add_argument('--impl', choices=['b200', 'reference'], default='b200')
     p.add_argument('--no-cpu-baseline', action='store_true')
     p.add_argument('--no-arnoldi', action='store_true', help='skip the Arnoldi steps/s leg')
+    p.add_argument('--path', type=int, default=1, choices=[0, 1, 2, 3],
+                   help='H·psi kernel path of the microbenchmark operator (he_set_path; 1 = default fused kernels)')
     p.add_argument('--adjoint-steps', type=int, default=128, help='adjoint leg: Arnoldi steps (dt 0.005)')
     p.add_argument('--adjoint-knots', type=int, default=32, help='adjoint leg: field samples')
     p.add_argument('--adjoint-checkpoint', type=int, default=32, help='adjoint leg: steps between checkpoints')
@@ -605,6 +607,8 @@ def main():
         return 0
     h = workloads.hpsi_microbench()
     engine = B200Hamiltonian(h, device)
+    if args.path != 1:
+        engine.set_path(args.path)
     field = (0., 0., .02)
     N = h.size
     bytes128 = 2 * N * 16
