@@ -370,10 +370,34 @@ def concurrent_leg(torch, device, count=8, steps=3):
             x, _ = step(sch, x, (i + 1) * dt, dt, tol, maxdim)
     torch.cuda.synchronize(device)
     alone = time.perf_counter() - t0
+    out = {'workload': f'{count} instances of different operators (N = {min(sizes)}..{max(sizes)}), {steps} Arnoldi '
+                       f'steps each, maxdim 12, dt 0.02', 'instance_steps_per_s': count * steps / together,
+           'one_after_another_instance_steps_per_s': count * steps / alone, 'speedup': alone / together}
+    # the same instances under CF4 + Pade/GMRES steps (velocity gauge, dt 0.05, each with its
+    # own separable preconditioner in complex64 and its own pulse)
+    from laqphysics_b200.implicit import SeparablePreconditioner, cf4_step
+    avecs = [lambda t, a=.01 + .003 * k: np.array([0., 0., a * np.cos(1.6 * t)]) for k in range(count)]
+    for sch in schedules:
+        sch.engine.separable = SeparablePreconditioner(sch.engine, 'complex64')
+    e_ref = [-2.9] * count
+    xs, _ = stepper.cf4(states, avecs, 0., .05, e_ref, 1e-10)            # warm-up
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    for i in range(steps):
+        xs, _ = stepper.cf4(xs, avecs, (i + 1) * .05, .05, e_ref, 1e-10)
+    torch.cuda.synchronize(device)
+    together = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for sch, av, x in zip(schedules, avecs, states):
+        for i in range(steps):
+            x, _ = cf4_step(sch.engine, x, av, (i + 1) * .05, .05, -2.9, 1e-10)
+    torch.cuda.synchronize(device)
+    alone = time.perf_counter() - t0
     stepper.close()
-    return {'workload': f'{count} instances of different operators (N = {min(sizes)}..{max(sizes)}), {steps} Arnoldi '
-                        f'steps each, maxdim 12, dt 0.02', 'instance_steps_per_s': count * steps / together,
-            'one_after_another_instance_steps_per_s': count * steps / alone, 'speedup': alone / together}
+    out['cf4'] = {'workload': f'the same instances, {steps} CF4 + Pade/GMRES steps each (dt 0.05, complex64 '
+                              f'separable preconditioners)', 'instance_steps_per_s': count * steps / together,
+                  'one_after_another_instance_steps_per_s': count * steps / alone, 'speedup': alone / together}
+    return out
 
 
 def cf4_leg(torch, device, steps=10):

@@ -27,10 +27,10 @@ class ConcurrentStepper:
         self.streams = [torch.cuda.Stream(self.device) for _ in self.schedules]
         self.pool = ThreadPoolExecutor(max_workers=len(self.schedules))
 
-    def step(self, states, t, dt, tol=1e-10, maxdim=48):
-        """One midpoint step of every instance from time t; returns (states, infos)."""
-        if len(states) != len(self.schedules):
-            raise ValueError('one state per instance')
+    def map(self, fn):
+        """fn(i) -> (state, info) for every instance i, each on its own stream and host
+        thread; returns ([states], [infos]) once every stream's work is ordered before the
+        caller's stream."""
         current = torch.cuda.current_stream(self.device)
 
         def run(i):
@@ -38,7 +38,7 @@ class ConcurrentStepper:
             with torch.cuda.device(self.device):
                 stream.wait_stream(current)
                 with torch.cuda.stream(stream):
-                    y, info = step(self.schedules[i], states[i], t, dt, tol, maxdim)
+                    y, info = fn(i)
                 y.record_stream(current)
             return y, info
 
@@ -46,6 +46,21 @@ class ConcurrentStepper:
         for stream in self.streams:
             current.wait_stream(stream)
         return [r[0] for r in results], [r[1] for r in results]
+
+    def step(self, states, t, dt, tol=1e-10, maxdim=48):
+        """One midpoint Arnoldi step of every instance from time t; returns (states, infos)."""
+        if len(states) != len(self.schedules):
+            raise ValueError('one state per instance')
+        return self.map(lambda i: step(self.schedules[i], states[i], t, dt, tol, maxdim))
+
+    def cf4(self, states, avecs, t, dt, reference_energies, tol=1e-11):
+        """One CF4 Magnus + Pade/GMRES step of every instance (implicit.cf4_step with each
+        engine's own preconditioner, field and reference energy)."""
+        from .implicit import cf4_step
+        if not len(states) == len(avecs) == len(reference_energies) == len(self.schedules):
+            raise ValueError('one state, field and reference energy per instance')
+        return self.map(lambda i: cf4_step(self.schedules[i].engine, states[i], avecs[i], t, dt,
+                                           reference_energies[i], tol))
 
     def close(self):
         self.pool.shutdown()
