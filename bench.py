@@ -44,7 +44,8 @@ def parse():
                    help='H·psi kernel path of the microbenchmark operator (he_set_path; 1 = default fused kernels)')
     p.add_argument('--adjoint-steps', type=int, default=128, help='adjoint leg: Arnoldi steps (dt 0.005)')
     p.add_argument('--adjoint-knots', type=int, default=32, help='adjoint leg: field samples')
-    p.add_argument('--adjoint-checkpoint', type=int, default=32, help='adjoint leg: steps between checkpoints')
+    p.add_argument('--adjoint-checkpoint', type=int, default=None,
+                   help='adjoint leg: steps between kept states (default: every state resident in HBM)')
     p.add_argument('--profile', choices=['c128', 'c64', 'arnoldi', 'arnoldi-split', 'batched', 'batched-attempt', 'cf4',
                                          'adjoint', 'concurrent'],
                    default=None,
@@ -294,12 +295,13 @@ def batched_leg(torch, device, steps, count=32):
     return out
 
 
-def adjoint_leg(torch, device, steps=128, knots=32, checkpoint=32):
+def adjoint_leg(torch, device, steps=128, knots=32, checkpoint=None):
     """Adjoint gradient on the Arnoldi grid widened to l <= 4: `steps` fixed Arnoldi steps
     (dt 0.005, Krylov tolerance 1e-12, maxdim 30) under a field of `knots` seeded samples
     (two pulses, peak 0.02 a.u.); objective = He+(n = 2) channel yield with the second
     electron beyond 5 a.u. (adjoint.ChannelYield).
-    Reports the forward and backward times and their ratio."""
+    Reports the forward and backward times and their ratio with every state resident (the
+    default) and with states kept every 32 steps (segments recomputed)."""
     from laqphysics_b200 import workloads
     from laqphysics_b200.adjoint import Propagation, check_complex_symmetric
     from laqphysics_b200.engine import B200Hamiltonian
@@ -316,22 +318,30 @@ def adjoint_leg(torch, device, steps=128, knots=32, checkpoint=32):
     t = np.linspace(0, steps * dt, knots)
     theta = .02 * (np.exp(-((t - .3 * t[-1]) / (.1 * t[-1])) ** 2) + np.exp(-((t - .7 * t[-1]) / (.1 * t[-1])) ** 2))
     theta *= rng.uniform(.8, 1.2, knots)
-    prop = Propagation(engine, psi0, dt, steps, t, objective, tol=1e-12, maxdim=30, checkpoint=checkpoint)
-    prop.forward(theta)                                   # warm-up (generated kernels, workspaces)
-    prop.gradient()
-    torch.cuda.synchronize(device)
-    t0 = time.perf_counter()
-    J = prop.forward(theta)
-    torch.cuda.synchronize(device)
-    t1 = time.perf_counter()
-    grad = prop.gradient()
-    torch.cuda.synchronize(device)
-    t2 = time.perf_counter()
+
+    def run(every):
+        prop = Propagation(engine, psi0, dt, steps, t, objective, tol=1e-12, maxdim=30, checkpoint=every)
+        prop.forward(theta)                               # warm-up (generated kernels, workspaces, graphs)
+        prop.gradient()
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        J = prop.forward(theta)
+        torch.cuda.synchronize(device)
+        t1 = time.perf_counter()
+        grad = prop.gradient()
+        torch.cuda.synchronize(device)
+        t2 = time.perf_counter()
+        return prop, J, grad, t1 - t0, t2 - t1
+
+    prop, J, grad, fwd, bwd = run(checkpoint)
+    _, _, grad32, fwd32, bwd32 = run(32)
     return {'workload': f'adjoint gradient: l1,l2<=4 L<=2 (nc={h.nc}, n={h.n}), {steps} Arnoldi steps dt 0.005, '
-                        f'{knots} field samples, checkpoint {checkpoint}, objective: He+(n=2) yield, '
-                        f'second electron beyond 5 a.u.',
-            'objective': J, 'forward_ms': (t1 - t0) * 1e3, 'backward_ms': (t2 - t1) * 1e3,
-            'backward_over_forward': (t2 - t1) / (t1 - t0), 'gradient_norm': float(np.linalg.norm(grad))}
+                        f'{knots} field samples, objective: He+(n=2) yield, second electron beyond 5 a.u.',
+            'checkpoint': prop.checkpoint, 'objective': J, 'forward_ms': fwd * 1e3, 'backward_ms': bwd * 1e3,
+            'backward_over_forward': bwd / fwd, 'gradient_norm': float(np.linalg.norm(grad)),
+            'checkpoint_32': {'forward_ms': fwd32 * 1e3, 'backward_ms': bwd32 * 1e3,
+                              'backward_over_forward': bwd32 / fwd32,
+                              'gradient_rel_diff': float(np.linalg.norm(grad32 - grad) / np.linalg.norm(grad))}}
 
 
 def concurrent_leg(torch, device, count=8, steps=3):
@@ -602,6 +612,12 @@ def main():
         for count in (1, 2, 4, 8, 16, 32):
             for precision in ('complex128', 'mixed'):
                 out[f'attempt12_us_per_instance_{precision}_x{count}'] = per_call_us(attempt(count, precision), 10) / count
+        from laqphysics_b200 import torch_backend
+        torch_backend.use_cuda_graphs(False)   # the same solves launched kernel by kernel
+        for count in (1, 32):
+            out[f'attempt12_us_per_instance_complex128_x{count}_no_graph'] = per_call_us(attempt(count, 'complex128'),
+                                                                                        10) / count
+        torch_backend.use_cuda_graphs(True)
         print(json.dumps(out), flush=True)
         return 0
     if args.profile == 'batched-attempt':   # two 12-iteration attempts of 32 instances (every one runs to maxdim)

@@ -139,7 +139,9 @@ int he_expv_check(he_krylov_handle k, int j, int maxdim, double dt, double tol, 
 int he_krylov_combine(he_krylov_handle k, int m, void *y, void *stream);
 
 /* Fused y = exp(-i dt H(field)) x with the device operator `op` (no host work between
- * Krylov vectors).  x, y: n*n*nc complex128 device vectors, y != x. */
+ * Krylov vectors).  x, y: n*n*nc complex128 device vectors, y != x.  All maxdim iterations
+ * are enqueued; once the solve converges on the device, the remaining H·psi launches return
+ * without work. */
 int he_expv(he_krylov_handle k, he_handle op, const void *x, void *y, const double *field, int velocity,
             double dt, double tol, int maxdim, int *dimension, double *estimate, void *stream);
 /* Mixed precision: as he_expv, but each H·psi runs in complex64 with FP32 accumulation
@@ -157,6 +159,20 @@ int he_expv_mixed(he_krylov_handle k, he_handle op, const void *x, void *y, cons
  * is untouched, the others are written).  precision as in he_apply.  The reference steps
  * one state at a time (python/propagate.py:6-50); this batches its parameter scans. */
 int he_krylov_create_batched(he_krylov_handle *out, long long n, int maxdim, int count);
+/* enable != 0: he_expv / he_expv_mixed / he_expv_batched / he_expv_field_derivative calls
+ * that repeat the previous call's configuration (operator, precision, gauge, maxdim) are
+ * captured once on an internal stream and replayed on the caller's stream as one CUDA graph, updated in place
+ * for new states, fields and step sizes; results are identical.  Off by default. */
+int he_krylov_set_graphs(he_krylov_handle k, int enable);
+/* Field derivative of one step: y = exp(-i dt B) x for the block operator
+ * B = [[H(field), direction . d], [0, H(field)]] (length gauge, complex128) on x = [u; w], so
+ * y = [e^{-i dt H} u + L w; e^{-i dt H} w] with L the derivative of e^{-i dt H(field)} along
+ * `direction` (d the dipole couplings).  The workspace holds vectors of 2 N.  Same fused
+ * Arnoldi, checks and messages as he_expv.  Not part of the reference's interface: the
+ * adjoint field gradient (one call per step of the backward sweep). */
+int he_expv_field_derivative(he_krylov_handle k, he_handle op, const void *x, void *y, const double *field,
+                             const double *direction, double dt, double tol, int maxdim, int *dimension,
+                             double *estimate, void *stream);
 int he_expv_batched(he_krylov_handle k, he_handle op, const void *x, void *y, const double *fields, int velocity,
                     double dt, double tol, int maxdim, int precision, int *dimension, double *estimate,
                     int *converged, void *stream);
@@ -207,6 +223,9 @@ int he_krylov_combine_coef(he_krylov_handle k, int which, int m, const void *coe
 int he_set_mixed_gauge(he_handle h, const double *q, const double *qr2h, const double *F, const double *c0,
                        const double *c2, int nq, const int *qptr, const int *qc, const int *qe, const double *qcoef);
 int he_apply_mixed_terms(he_handle h, const void *psi, void *out, const double *field, void *stream);
+/* out += (direction . d) psi: the length-gauge dipole coupling of both electrons, i.e.
+ * H(f + direction) psi - H(f) psi, complex128 (the field derivative of the Hamiltonian). */
+int he_apply_dipole(he_handle h, const void *psi, void *out, const double *direction, void *stream);
 
 /* ------------------------------------------------------------------------------------
  * He+ operator for the backward propagation of the tSURFF channel functions chi_c(t)

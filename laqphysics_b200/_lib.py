@@ -54,6 +54,7 @@ SIGNATURES = {
     'he_fp64_peak': (I, [I, I, ct.POINTER(ct.c_double), P]),
     'he_set_mixed_gauge': (I, [P, P, P, P, P, P, I, P, P, P, P]),
     'he_apply_mixed_terms': (I, [P, P, P, P, P]),
+    'he_apply_dipole': (I, [P, P, P, P, P]),
     'he_ionic_create': (I, [ct.POINTER(P), I, I, I, ct.c_longlong, P, P, P]),
     'he_ionic_set_preconditioner': (I, [P, I, I, P, P, P]),
     'he_ionic_apply': (I, [P, P, I, P, P, D, D, D, I, P]),
@@ -67,6 +68,8 @@ SIGNATURES = {
     'he_vec_jacobi': (I, [ct.c_longlong, P, D, D, D, P, P, P]),
     'he_krylov_scale': (I, [P, I, I, D, P]),
     'he_krylov_normalize': (I, [P, I, P]),
+    'he_krylov_set_graphs': (I, [P, I]),
+    'he_expv_field_derivative': (I, [P, P, P, P, P, P, D, D, I, ct.POINTER(I), ct.POINTER(D), P]),
     'he_krylov_hessenberg': (I, [P, I, I, P, P]),
     'he_krylov_reset': (I, [P, P]),
     'he_krylov_combine_coef': (I, [P, I, I, P, P, I, P]),

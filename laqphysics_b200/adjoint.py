@@ -24,9 +24,12 @@ Backward pass (exact for the discrete map, up to the Krylov tolerance):
   gradient term dJ/dE_n = 2 Re <L(A^dagger, B^dagger) lambda_n | psi_{n-1}> (top block).
 * lambda_N = P psi_N (dJ = 2 Re <P psi_N | d psi_N> for Hermitian P);
   dJ/dtheta = sum_n (dJ/dE_n) phi_k(t_{n-1} + dt/2).
-* States are kept every `checkpoint` steps and each segment is recomputed forward
-  before its backward sweep.  The block system's H·psi products run as one batched
-  apply of three instances (H u, H w, H(E+1) w; D w = H(E+1) w - H(E) w).
+* The block exponential is one fused device solve (he_expv_field_derivative): per Krylov
+  vector one batched apply of the two halves (H u, H w) and one dipole pass (D w), so a
+  backward step costs about two forward steps.
+* Every forward state stays in device memory when the states fit a quarter of the free
+  memory (no recompute); otherwise states are kept every `checkpoint` steps and each
+  segment is recomputed forward before its backward sweep.
 
 :class:`AdjointObjective` wraps the pair as a ``torch.autograd.Function``.
 """
@@ -34,7 +37,7 @@ import numpy as np
 import torch
 
 from .angular import radial_hydrogen
-from .torch_backend import FieldOperator, exponential_action
+from .torch_backend import FieldOperator, exponential_action, field_derivative_action
 
 
 class ChannelYield:
@@ -101,11 +104,16 @@ class Propagation:
     knots: K sample times of E(t); mask: the objective's P, a real diagonal (numpy,
     engine.size) or a callable psi -> P psi on the device (Hermitian, e.g. ChannelYield);
     tol/maxdim: Krylov controls (no dt halving: the gradient is that of this exact map,
-    so a step that does not converge raises)."""
+    so a step that does not converge raises); checkpoint: steps between kept states (None:
+    every state when all fit a quarter of the free device memory, else 64)."""
 
-    def __init__(self, engine, psi0, dt, steps, knots, mask, tol=1e-13, maxdim=30, checkpoint=64):
+    def __init__(self, engine, psi0, dt, steps, knots, mask, tol=1e-13, maxdim=30, checkpoint=None):
         self.engine, self.dt, self.steps = engine, float(dt), int(steps)
-        self.tol, self.maxdim, self.checkpoint = float(tol), int(maxdim), int(checkpoint)
+        self.tol, self.maxdim = float(tol), int(maxdim)
+        if checkpoint is None:
+            free, _ = torch.cuda.mem_get_info(engine.device)
+            checkpoint = 1 if (self.steps + 1) * engine.size * 16 <= free // 4 else 64
+        self.checkpoint = max(1, int(checkpoint))
         self.psi0 = psi0 if torch.is_tensor(psi0) else engine.state(psi0)
         self.knots = np.asarray(knots, float)
         self.tmid = self.dt * (np.arange(self.steps) + 0.5)
@@ -132,20 +140,30 @@ class Propagation:
         for n in range(self.steps):
             psi = self._step(psi, E[n])
             if keep and (n + 1) % self.checkpoint == 0 and n + 1 < self.steps:
-                self._checkpoints[n + 1] = psi.clone()
+                self._checkpoints[n + 1] = psi            # each step returns a new tensor
         self._final = psi
         self._E = E
         return float(torch.sum(psi.conj() * self.P(psi)).real)
 
     def _block_apply(self, e):
+        """z = [u; w] -> [H(E) u + D w; H(E) w] with D w = H(E+1) w - H(E) w, as a callable
+        for the host-looped exponential_action (the form the fused derivative solve is
+        tested against); the result buffer is reused (the caller copies it)."""
+        from .implicit import axpby
         engine, size = self.engine, self.engine.size
-        fields = np.array([[0., 0., e], [0., 0., e], [0., 0., e + 1.]])
+        fields = np.array([[0., 0., e], [0., 0., e]])
+        shifted = (0., 0., e + 1.)
+        pair = torch.empty((2, size), dtype=torch.complex128, device=engine.device)
+        out = torch.empty(2 * size, dtype=torch.complex128, device=engine.device)
+        top, bottom = out[:size], out[size:]
 
         def apply(z):
-            u, w = z[:size], z[size:]
-            batch = torch.stack([u, w, w])
-            out = engine.apply_batched(batch, fields, False)
-            return torch.cat([out[0] + (out[2] - out[1]), out[1]])
+            engine.apply_batched(z.view(2, size), fields, False, out=pair)
+            engine.apply(z[size:], shifted, False, out=top)
+            axpby(1, top, -1, pair[1], out=top)            # D w
+            axpby(1, pair[0], 1, top, out=top)             # H(E) u + D w
+            bottom.copy_(pair[1])
+            return out
         return apply
 
     def gradient(self):
@@ -163,8 +181,8 @@ class Propagation:
                 states.append(self._step(states[-1], E[n]))
             for n in range(stop - 1, s - 1, -1):                       # step n maps psi_n -> psi_{n+1}
                 z = torch.cat([torch.zeros_like(lam), lam.conj()])
-                op = self._block_apply(E[n])
-                y, _ = exponential_action(op, z, self.dt, self.tol, self.maxdim)
+                y, _ = field_derivative_action(self.engine, z, (0., 0., float(E[n])), (0., 0., 1.), self.dt,
+                                               self.tol, self.maxdim)
                 top, bottom = y[:size], y[size:]
                 gE[n] = 2.0 * float(torch.sum(top * states[n - s]).real)
                 lam = bottom.conj()

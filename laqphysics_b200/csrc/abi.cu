@@ -422,7 +422,7 @@ int apply_common(he_handle h, const void *psi, void *out, const he::FieldBatch &
                                               beta, gamma, st);
         } else {
             for (int b = 0; b < fb.count && !s; ++b) {   // one instance at a time
-                he::FieldBatch one{1, {}};
+                he::FieldBatch one{1, {}, fb.skip};
                 for (int a = 0; a < 3; ++a) one.f[0][a] = fb.f[b][a];
                 s = tiled ? he::launch_hpsi_tiled<double>(h, h->t64, h->p64, h->coef64, h->w64[0], h->w64[1],
                                                           x + b * N, y + b * N, one, velocity, beta, gamma, st)
@@ -440,7 +440,7 @@ int apply_common(he_handle h, const void *psi, void *out, const he::FieldBatch &
                                              beta, gamma, st);
         } else {
             for (int b = 0; b < fb.count && !s; ++b) {
-                he::FieldBatch one{1, {}};
+                he::FieldBatch one{1, {}, fb.skip};
                 for (int a = 0; a < 3; ++a) one.f[0][a] = fb.f[b][a];
                 s = tiled ? he::launch_hpsi_tiled<float>(h, h->t32, h->p32, h->coef32, h->w32[0], h->w32[1],
                                                          x + b * N, y + b * N, one, velocity, beta, gamma, st)
@@ -469,16 +469,25 @@ extern "C" int he_apply(he_handle h, const void *psi, void *out, const double *f
     return apply_common(h, psi, out, single_field(field), velocity, precision, 0.0, 0.0, 1.0, 0.0, stream);
 }
 
-extern "C" int he_apply_batched(he_handle h, int count, const void *psi, void *out, const double *fields, int velocity,
-                                int precision, void *stream)
+namespace he {
+int apply_batched_gated(he_handle h, int count, const void *psi, void *out, const double *fields, int velocity,
+                        int precision, const int *skip, cudaStream_t stream)
 {
     if (!fields) return he_fail(HE_ERR_ARG, "null argument", __FILE__, __LINE__);
     if (count < 1 || count > he::HE_BATCH_MAX)
         return he_fail(HE_ERR_ARG, "batch count must be between 1 and 64", __FILE__, __LINE__);
-    he::FieldBatch fb{count, {}};
+    he::FieldBatch fb{count, {}, skip};
     for (int b = 0; b < count; ++b)
         for (int a = 0; a < 3; ++a) fb.f[b][a] = fields[3 * b + a];
     return apply_common(h, psi, out, fb, velocity, precision, 0.0, 0.0, 1.0, 0.0, stream);
+}
+}  // namespace he
+
+extern "C" int he_apply_batched(he_handle h, int count, const void *psi, void *out, const double *fields, int velocity,
+                                int precision, void *stream)
+{
+    return he::apply_batched_gated(h, count, psi, out, fields, velocity, precision, nullptr,
+                                   static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int he_apply_shifted(he_handle h, const void *psi, void *out, const double *field, int velocity,

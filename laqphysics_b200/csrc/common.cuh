@@ -76,10 +76,14 @@ __device__ __forceinline__ double2 warp_fixed_sum(const double2* p, int nb, size
 namespace he {
 // Fields of a batch of instances that share one operator (passed by value to kernels):
 // instance b of a batched apply sees the field f[b][0..2]; a single apply has count 1.
+// skip (optional): a device flag that, when non-zero at launch, makes the banded kinetic and
+// generated mixing kernels return without work (the done word of a Krylov solve, so the
+// applies a fused solve enqueues past its convergence cost one empty launch each).
 constexpr int HE_BATCH_MAX = 64;
 struct FieldBatch {
     int count;
     double f[HE_BATCH_MAX][3];
+    const int *skip;
 };
 
 template <typename R> struct DeviceTables {

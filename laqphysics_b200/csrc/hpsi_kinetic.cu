@@ -466,6 +466,7 @@ hpsi_band_kernel(const __grid_constant__ CUtensorMap tmap, const DeviceTables<R>
     double2 *CFB = CF + BAND_CG * BAND_KS * 32;   // velocity gauge: the B fragments of the same groups
     uint64_t *bar = reinterpret_cast<uint64_t *>(CFB + (VEL ? BAND_CG * BAND_KS * 32 : 0));
     constexpr int ALIGN = 16 / (int)sizeof(C);   // nodes per 16 bytes (TMA start alignment)
+    if (fb.skip && *fb.skip) return;   // the solve that enqueued this apply has converged
     const int n = bp.n, nc = bp.nc, P = bp.box_r, G = bp.ngroup, nch = nc * fb.count;
     const size_t nn = (size_t)n * n;
     const long long items = (long long)bp.ntr * bp.nct * nch;

@@ -38,7 +38,7 @@ namespace he {
 namespace {
 
 const char *kPrelude = R"(// generated channel-mixing kernel
-struct FieldBatch { int count; double f[HE_BATCH_MAX][3]; };
+struct FieldBatch { int count; double f[HE_BATCH_MAX][3]; const int *skip; };
 struct __align__(16) cd { double x, y; };
 struct __align__(8) cf { float x, y; };
 template <typename R> struct cx;
@@ -103,6 +103,7 @@ std::string mix_source(const he_plan_host &P, bool dipole_real, int variant)
          "    const typename cx<R>::T *__restrict__ dcoef, const R *__restrict__ ldiff, long long nn, int n, int nd,\n"
          "    int nc, const FieldBatch &fs, typename cx<R>::T beta, typename cx<R>::T gamma)\n{\n"
          "    typedef typename cx<R>::T C;\n"
+         "    if (fs.skip && *fs.skip) return;   // the solve that enqueued this apply has converged\n"
          "    // instance blockIdx.z of a batch: its own field and its block of nc channels\n"
          "    const long long shift = (long long)blockIdx.z * nc * nn;\n"
          "    psi += shift; out += shift;\n"

@@ -638,6 +638,8 @@ he_krylov::~he_krylov()
 {
     cudaFree(Q); cudaFree(Z); cudaFree(H); cudaFree(partial); cudaFree(z); cudaFree(coef); cudaFree(work);
     cudaFree(norm_partial); cudaFree(status); cudaFree(ticket); cudaFree(s32[0]); cudaFree(s32[1]);
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (capture_stream) cudaStreamDestroy(capture_stream);
     if (host_status) cudaFreeHost(host_status);
 }
 
@@ -687,6 +689,14 @@ extern "C" int he_krylov_create(he_krylov **out, long long n, int maxdim, int fl
 extern "C" int he_krylov_create_batched(he_krylov **out, long long n, int maxdim, int count)
 {
     return krylov_create(out, n, maxdim, 0, count);
+}
+
+extern "C" int he_krylov_set_graphs(he_krylov *k, int enable)
+{
+    if (!k) return he_fail(HE_ERR_ARG, "null handle", __FILE__, __LINE__);
+    k->graphs = enable != 0;
+    k->graph_key = 0;
+    return HE_OK;
 }
 
 extern "C" int he_krylov_destroy(he_krylov *k)
@@ -890,39 +900,46 @@ int fused_sweeps(he_krylov *k, int kc, double2 *v, const float2 *src32, int j, i
 // stay complex128).  Per-instance dimensions, estimates and convergence go to the optional
 // arrays; the status is HE_ERR_NOCONV when any instance did not converge (its y_b is left
 // as it was).
-int expv_impl(he_krylov *k, he_handle op, const void *x, void *y, const double *fields, int velocity, double dt,
-              double tol, int maxdim, int *dimension, double *estimate, int *converged, void *stream, int precision)
+// Every kernel of one Arnoldi solve, enqueued on s without waiting on the device: the check
+// decides convergence at the reference's check points on the device and sets the status
+// word, after which every Krylov kernel returns at once.  (x = 0 gives beta = 0: done at
+// once with m = 0, and the combination writes y = 0 = x.)
+// Iterations j0 .. j1-1 of the solve (j0 = 0 starts it), then y = Q c if it has converged.
+// The kernels see the solve's maxdim whatever the segment, so a solve enqueued in segments
+// runs exactly the launches of one enqueued whole.
+// direction != null: the field-derivative block operator of he_expv_field_derivative on
+// x = [u; w] (k->n = 2 N): B [u; w] = [H u + (direction . d) w; H w], one batched apply of the
+// two halves and the dipole coupling added to the upper half.
+int enqueue_expv(he_krylov *k, he_handle op, const void *x, void *y, const double *fields, int velocity, double dt,
+                 double tol, int maxdim, cudaStream_t s, int precision, const double *direction, int j0, int j1)
 {
-    if (!k || !op || !x || !y || !fields) return he_fail(HE_ERR_ARG, "null argument", __FILE__, __LINE__);
     const size_t total = k->qs();   // one basis vector of every instance
-    if (precision == HE_C64 && !k->s32[0]) {
-        for (int q = 0; q < 2; ++q) HE_CUDA_TRY(cudaMalloc(&k->s32[q], total * sizeof(float2)));
+    int rc = HE_OK;
+    if (j0 == 0) {
+        if ((rc = krylov_start(k, static_cast<const double2 *>(x), s))) return rc;
+        HE_CUDA_TRY(cudaMemsetAsync(k->ticket, 0, sizeof(unsigned int) * k->count, s));
     }
-    if (maxdim < 1 || maxdim > k->maxdim) return he_fail(HE_ERR_ARG, "maxdim exceeds the workspace", __FILE__, __LINE__);
-    if ((size_t)op->n * op->n * op->nc != k->n) return he_fail(HE_ERR_SHAPE, "workspace size != operator size", __FILE__, __LINE__);
-    // The whole Krylov loop is enqueued without waiting on the device: the check kernel
-    // decides convergence at the reference's check points on the device and sets the
-    // status word, after which every Krylov kernel returns at once.  The host reads the
-    // status once, at the end.  (x = 0 gives beta = 0: done at once with m = 0, and the
-    // combination below writes y = 0 = x.)
-    const cudaStream_t s = static_cast<cudaStream_t>(stream);
-    int rc = krylov_start(k, static_cast<const double2 *>(x), s);
-    if (rc) return rc;
-    HE_CUDA_TRY(cudaMemsetAsync(k->ticket, 0, sizeof(unsigned int) * k->count, s));
     const int ld = k->maxdim + 1;
     const dim3 cgrid(std::min<size_t>(KRYLOV_BLOCKS * (size_t)k->count, 4096));
     const bool mixed = precision == HE_C64;
-    bool have32 = false;   // s32[0] holds the complex64 copy of Q_j (written by the previous iteration)
-    for (int j = 0; j < maxdim; ++j) {
+    // a single solve's applies return at once after its convergence
+    const int *gate = k->count == 1 ? &k->status->done : nullptr;
+    // s32[0] holds the complex64 copy of Q_j (written by the previous iteration when it was fused)
+    bool have32 = mixed && j0 >= 1 && j0 <= KRYLOV_FUSED;
+    for (int j = j0; j < j1; ++j) {
         double2 *qj = k->Q + (size_t)j * total, *v = k->Q + (size_t)(j + 1) * total;
         const int kc = j + 1;
         const bool fused = kc <= KRYLOV_FUSED;
         if (mixed) {
             if (!have32) krylov_to_c64<<<cgrid, kBlock, 0, s>>>(total, qj, k->s32[0]);
-            rc = he_apply_batched(op, k->count, k->s32[0], k->s32[1], fields, velocity, HE_C64, stream);
+            rc = he::apply_batched_gated(op, k->count, k->s32[0], k->s32[1], fields, velocity, HE_C64, gate, s);
             if (!fused) krylov_to_c128<<<cgrid, kBlock, 0, s>>>(total, k->s32[1], v);
+        } else if (direction) {
+            const double pair[6] = {fields[0], fields[1], fields[2], fields[0], fields[1], fields[2]};
+            rc = he::apply_batched_gated(op, 2, qj, v, pair, 0, HE_C128, gate, s);
+            if (!rc) rc = he::dipole_accumulate(op, qj + k->n / 2, v, direction, gate, s);
         } else {
-            rc = he_apply_batched(op, k->count, qj, v, fields, velocity, HE_C128, stream);   // the kernels of every apply
+            rc = he::apply_batched_gated(op, k->count, qj, v, fields, velocity, HE_C128, gate, s);
         }
         if (rc) break;
         have32 = false;
@@ -948,11 +965,82 @@ int expv_impl(he_krylov *k, he_handle op, const void *x, void *y, const double *
     // y = Q c with m from the status word; y is left as is when the solve failed
     combine_kernel<<<bgrid(k), kBlock, 0, s>>>(k->Q, k->n, k->qs(), k->coef, ld, static_cast<double2 *>(y), k->status, -1, 0);
     HE_CUDA_TRY(cudaGetLastError());
+    return HE_OK;
+}
+
+int expv_impl(he_krylov *k, he_handle op, const void *x, void *y, const double *fields, int velocity, double dt,
+              double tol, int maxdim, int *dimension, double *estimate, int *converged, void *stream, int precision,
+              const double *direction = nullptr)
+{
+    if (!k || !op || !x || !y || !fields) return he_fail(HE_ERR_ARG, "null argument", __FILE__, __LINE__);
+    const size_t total = k->qs();   // one basis vector of every instance
+    if (precision == HE_C64 && !k->s32[0]) {
+        for (int q = 0; q < 2; ++q) HE_CUDA_TRY(cudaMalloc(&k->s32[q], total * sizeof(float2)));
+    }
+    if (maxdim < 1 || maxdim > k->maxdim) return he_fail(HE_ERR_ARG, "maxdim exceeds the workspace", __FILE__, __LINE__);
+    if ((size_t)op->n * op->n * op->nc * (direction ? 2 : 1) != k->n)
+        return he_fail(HE_ERR_SHAPE, "workspace size != operator size", __FILE__, __LINE__);
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // With graphs on, a solve whose configuration (operator, precision, gauge, maxdim) repeats
+    // the previous one is captured on the workspace's own stream and replayed on the caller's
+    // stream as one graph (the previous, uncaptured solve compiled and allocated everything
+    // it needs); changed pointers and fields update the instantiated graph in place.
+    const long long config = (long long)(reinterpret_cast<uintptr_t>(op) ^ ((uintptr_t)precision << 1) ^
+                                         ((uintptr_t)velocity << 3) ^ ((uintptr_t)(direction != nullptr) << 4) ^
+                                         ((uintptr_t)maxdim << 8));
+    // Only the iterations a solve is likely to need are enqueued: two past the largest
+    // dimension that solves of this configuration have converged at.  When the status read
+    // after them shows a solve still running, the rest (up to maxdim) follow; the launches,
+    // and so the results, are those of one solve enqueued to maxdim.
+    if (k->hint_key != config) {
+        k->hint_key = config;
+        k->dim_seen = 0;
+    }
+    const int first = k->dim_seen > 0 ? std::min(maxdim, k->dim_seen + 2) : maxdim;
+    const long long key = config ^ ((long long)first << 40);
+    int rc;
+    if (k->graphs && k->graph_key == key) {
+        if (!k->capture_stream) HE_CUDA_TRY(cudaStreamCreateWithFlags(&k->capture_stream, cudaStreamNonBlocking));
+        HE_CUDA_TRY(cudaStreamBeginCapture(k->capture_stream, cudaStreamCaptureModeRelaxed));
+        rc = enqueue_expv(k, op, x, y, fields, velocity, dt, tol, maxdim, k->capture_stream, precision, direction, 0,
+                          first);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ended = cudaStreamEndCapture(k->capture_stream, &g);
+        if (!rc && ended != cudaSuccess) rc = he_fail(HE_ERR_CUDA, cudaGetErrorString(ended), __FILE__, __LINE__);
+        if (!rc) {
+            bool updated = false;
+            if (k->graph_exec) {
+                cudaGraphExecUpdateResultInfo info;
+                updated = cudaGraphExecUpdate(k->graph_exec, g, &info) == cudaSuccess;
+                if (!updated) {
+                    cudaGetLastError();
+                    cudaGraphExecDestroy(k->graph_exec);
+                    k->graph_exec = nullptr;
+                }
+            }
+            cudaError_t e = updated ? cudaSuccess : cudaGraphInstantiate(&k->graph_exec, g, 0);
+            if (e == cudaSuccess) e = cudaGraphLaunch(k->graph_exec, s);
+            if (e != cudaSuccess) rc = he_fail(HE_ERR_CUDA, cudaGetErrorString(e), __FILE__, __LINE__);
+        }
+        if (g) cudaGraphDestroy(g);
+    } else {
+        rc = enqueue_expv(k, op, x, y, fields, velocity, dt, tol, maxdim, s, precision, direction, 0, first);
+    }
+    if (rc) return rc;
+    k->graph_key = key;
     if ((rc = krylov_read_status(k, s))) return rc;
+    bool pending = false;
+    for (int b = 0; b < k->count; ++b) pending = pending || !k->host_status[b].done;
+    if (pending && first < maxdim) {
+        rc = enqueue_expv(k, op, x, y, fields, velocity, dt, tol, maxdim, s, precision, direction, first, maxdim);
+        if (rc) return rc;
+        if ((rc = krylov_read_status(k, s))) return rc;
+    }
     bool all = true;
     for (int b = 0; b < k->count; ++b) {
         const KrylovStatus &h = k->host_status[b];
         const bool ok = !h.failed && h.converged;
+        if (ok) k->dim_seen = std::max(k->dim_seen, h.m);
         if (estimate) estimate[b] = h.estimate;
         if (dimension) dimension[b] = h.m;
         if (converged) converged[b] = ok;
@@ -984,4 +1072,18 @@ extern "C" int he_expv_batched(he_krylov *k, he_handle op, const void *x, void *
     if (precision != HE_C128 && precision != HE_C64)
         return he_fail(HE_ERR_ARG, "precision must be HE_C128 or HE_C64", __FILE__, __LINE__);
     return expv_impl(k, op, x, y, fields, velocity, dt, tol, maxdim, dimension, estimate, converged, stream, precision);
+}
+
+// exp(-i dt B) x for B = [[H(field), direction . d], [0, H(field)]] (length gauge) on x = [u; w]
+// (2 N complex128 values, a workspace of that length): y = [e^{-i dt H} u + L w; e^{-i dt H} w],
+// L the derivative of e^{-i dt H(field)} along `direction` (the Frechet derivative of the
+// exponential in the direction -i dt direction . d).  The fused Arnoldi of he_expv on the block
+// operator: each Krylov vector costs one two-instance apply and one dipole pass.
+extern "C" int he_expv_field_derivative(he_krylov *k, he_handle op, const void *x, void *y, const double *field,
+                                        const double *direction, double dt, double tol, int maxdim, int *dimension,
+                                        double *estimate, void *stream)
+{
+    if (!direction) return he_fail(HE_ERR_ARG, "null argument", __FILE__, __LINE__);
+    if (k && k->count != 1) return he_fail(HE_ERR_ARG, "the derivative takes a single-instance workspace", __FILE__, __LINE__);
+    return expv_impl(k, op, x, y, field, 0, dt, tol, maxdim, dimension, estimate, nullptr, stream, HE_C128, direction);
 }

@@ -50,6 +50,12 @@ struct he_krylov {
     he::KrylovStatus *host_status = nullptr; // pinned host mirror
     size_t qs() const { return (size_t)count * n; }              // distance between basis vectors
     int blocks = he::KRYLOV_BLOCKS;   // CTAs per instance of the vector kernels (set at creation)
+    bool graphs = false;              // he_krylov_set_graphs: replay repeated solves as one CUDA graph
+    long long graph_key = 0;          // configuration of the last solve (0: none)
+    cudaStream_t capture_stream = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    long long hint_key = 0;           // configuration the dimension hint belongs to
+    int dim_seen = 0;                 // largest converged dimension of solves with that configuration
     int kb() const { return blocks; }
     size_t hs() const { return (size_t)(maxdim + 1) * maxdim; }  // Hessenberg size per instance
     size_t ws() const { return (size_t)8 * (maxdim + 1) * (maxdim + 1); }   // dense scratch per instance

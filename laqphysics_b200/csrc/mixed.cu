@@ -66,6 +66,30 @@ __global__ void mixed_gauge_kernel(he::DeviceTables<double> t, const double2 *__
     out[p + nn * c] = cadd<double>(out[p + nn * c], val);
 }
 
+// out(p, c) += sum over the dipole edges k of channel c of (direction . d_k) r(a) psi(p, src_k), a the
+// coordinate of the edge's electron (i for electron 1, j for electron 2): the length-gauge field
+// coupling of both electrons, i.e. H(f + direction) psi - H(f) psi.  One thread per point and
+// output channel; returns at once while *skip != 0.
+__global__ void dipole_kernel(he::DeviceTables<double> t, double dx, double dy, double dz,
+                              const double2 *__restrict__ psi, double2 *__restrict__ out, const int *skip)
+{
+    if (skip && *skip) return;
+    const int n = t.n, c = blockIdx.y;
+    const size_t nn = (size_t)n * n;
+    const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nn || t.dptr[c] == t.dptr[c + 1]) return;
+    const int i = (int)(p % n), j = (int)(p / n);
+    double2 val = mk<double>(0, 0);
+    for (int k = t.dptr[c]; k < t.dptr[c + 1]; ++k) {
+        const double2 *dk = t.dcoef + 3 * (size_t)k;
+        double2 coef = cscale<double>(dx, dk[0]);
+        coef = rfma<double>(dy, dk[1], coef);
+        coef = rfma<double>(dz, dk[2], coef);
+        val = cfma<double>(cmul<double>(coef, t.r[t.de[k] == 1 ? i : j]), psi[p + nn * t.dc[k]], val);
+    }
+    out[p + nn * c] = cadd<double>(out[p + nn * c], val);
+}
+
 template <typename T> int upload(he_operator *h, T **dst, const void *src, size_t count)
 {
     *dst = nullptr;
@@ -115,4 +139,25 @@ extern "C" int he_apply_mixed_terms(he_handle h, const void *psi, void *out, con
         static_cast<const double2 *>(psi), static_cast<double2 *>(out));
     HE_CUDA_TRY(cudaGetLastError());
     return HE_OK;
+}
+
+namespace he {
+int dipole_accumulate(he_operator *h, const double2 *psi, double2 *out, const double direction[3], const int *skip,
+                      cudaStream_t stream)
+{
+    if (!h->t64.r || h->nd < 1) return he_fail(HE_ERR_UNSUPPORTED, "operator has no dipole couplings", __FILE__, __LINE__);
+    const size_t nn = (size_t)h->n * h->n;
+    const dim3 grid((unsigned)((nn + 255) / 256), h->nc);
+    dipole_kernel<<<grid, 256, 0, stream>>>(h->t64, direction[0], direction[1], direction[2], psi, out, skip);
+    HE_CUDA_TRY(cudaGetLastError());
+    return HE_OK;
+}
+}  // namespace he
+
+extern "C" int he_apply_dipole(he_handle h, const void *psi, void *out, const double *direction, void *stream)
+{
+    if (!h || !psi || !out || !direction) return he_fail(HE_ERR_ARG, "null argument", __FILE__, __LINE__);
+    if (psi == out) return he_fail(HE_ERR_ARG, "the dipole coupling cannot run in place", __FILE__, __LINE__);
+    return he::dipole_accumulate(h, static_cast<const double2 *>(psi), static_cast<double2 *>(out), direction, nullptr,
+                                 static_cast<cudaStream_t>(stream));
 }

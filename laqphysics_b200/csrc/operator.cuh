@@ -91,4 +91,11 @@ template <> inline const BandPlan<float> &band_plan<float>(const he_operator *h)
 template <typename R> inline const KineticPlan<R> &kinetic_plan(const he_operator *h);
 template <> inline const KineticPlan<double> &kinetic_plan<double>(const he_operator *h) { return h->k64; }
 template <> inline const KineticPlan<float> &kinetic_plan<float>(const he_operator *h) { return h->k32; }
+// he_apply_batched whose kernels return without work while *skip != 0 (skip may be null).
+int apply_batched_gated(he_operator *h, int count, const void *psi, void *out, const double *fields, int velocity,
+                        int precision, const int *skip, cudaStream_t stream);
+// out += (direction . d) psi: the length-gauge dipole coupling of both electrons (the field
+// derivative of H(field) along `direction`), complex128, one instance; skipped while *skip != 0.
+int dipole_accumulate(he_operator *h, const double2 *psi, double2 *out, const double direction[3], const int *skip,
+                      cudaStream_t stream);
 }  // namespace he

@@ -23,6 +23,19 @@ from .engine import B200Hamiltonian, _stream
 TorchHamiltonian = B200Hamiltonian
 
 _WORKSPACES = {}
+_GRAPHS = [True]
+
+
+def use_cuda_graphs(flag=True):
+    """Replay repeated Arnoldi solves (same operator, precision, gauge and maxdim as the
+    previous solve on the workspace) as one captured CUDA graph (he_krylov_set_graphs; on
+    by default); applies to existing and future workspaces.  Results are identical either
+    way.  Returns the previous setting."""
+    previous = _GRAPHS[0]
+    _GRAPHS[0] = bool(flag)
+    for ws in list(_WORKSPACES.values()) + list(_BATCHED.values()):
+        check(LIB.he_krylov_set_graphs(ws.handle, int(flag)), 'he_krylov_set_graphs')
+    return previous
 
 
 class KrylovWorkspace:
@@ -35,6 +48,8 @@ class KrylovWorkspace:
             check(LIB.he_krylov_create(ct.byref(handle), self.n, self.maxdim, int(flexible)), 'he_krylov_create')
         self.handle = handle
         self._views = {}
+        if _GRAPHS[0] and not flexible:
+            check(LIB.he_krylov_set_graphs(handle, 1), 'he_krylov_set_graphs')
 
     def vector(self, j, which=0):
         """torch view of basis vector j (which=0: Q, which=1: Z of flexible GMRES)."""
@@ -164,6 +179,31 @@ def _fused(op, ws, x, dt, tol, maxdim, stream):
     return y, {'dimension': dim.value, 'residual_estimate': float(err.value)}
 
 
+@torch.no_grad()
+def field_derivative_action(engine, x, field, direction, dt, tol=1e-10, maxdim=48):
+    """exp(-i dt B) x for B = [[H(field), direction . d], [0, H(field)]] on x = [u; w], a
+    complex128 device vector of 2 engine.size values (length gauge, he_expv_field_derivative):
+    the lower half of the result is exp(-i dt H) w, the upper half exp(-i dt H) u + L w with L
+    the derivative of exp(-i dt H(field)) along the field direction.  One fused Arnoldi on the
+    block operator (a two-instance apply and one dipole pass per Krylov vector)."""
+    if x.dtype != torch.complex128 or x.device.type != 'cuda' or x.numel() != 2 * engine.size:
+        raise ValueError('field_derivative_action needs a complex128 CUDA vector of 2 engine.size values')
+    x = x.contiguous()
+    ws = workspace(x.numel(), maxdim, x.device)
+    y = torch.empty_like(x)
+    f = np.ascontiguousarray(field, dtype=np.float64)
+    d = np.ascontiguousarray(direction, dtype=np.float64)
+    dim, err = ct.c_int(0), ct.c_double(0.)
+    status = LIB.he_expv_field_derivative(ws.handle, engine.op.handle, ct.c_void_p(x.data_ptr()),
+                                          ct.c_void_p(y.data_ptr()), ptr(f), ptr(d), float(dt), float(tol),
+                                          int(maxdim), ct.byref(dim), ct.byref(err), _stream(x.device))
+    if status == HE_ERR_NOCONV:
+        raise _not_converged(maxdim, dt, err.value)
+    check(status, 'he_expv_field_derivative')
+    engine.apply_count += 2 * dim.value
+    return y, {'dimension': dim.value, 'residual_estimate': float(err.value)}
+
+
 class BatchedWorkspace:
     """Krylov workspace for ``count`` instances advanced together (he_krylov_create_batched)."""
 
@@ -174,6 +214,8 @@ class BatchedWorkspace:
             check(LIB.he_krylov_create_batched(ct.byref(handle), self.n, self.maxdim, self.count),
                   'he_krylov_create_batched')
         self.handle = handle
+        if _GRAPHS[0]:
+            check(LIB.he_krylov_set_graphs(handle, 1), 'he_krylov_set_graphs')
 
     def __del__(self):
         handle = getattr(self, 'handle', None)

@@ -57,6 +57,47 @@ def test_autograd_function_and_checkpoint_length_do_not_change_the_gradient():
     prop2, _ = setup(checkpoint=64)
     prop2.forward(theta)
     np.testing.assert_allclose(t.grad.numpy(), prop2.gradient(), rtol=1e-10, atol=1e-14)
+    prop3, _ = setup(checkpoint=None)            # every state resident: no recompute
+    assert prop3.checkpoint == 1
+    prop3.forward(theta)
+    np.testing.assert_allclose(prop3.gradient(), prop2.gradient(), rtol=1e-10, atol=1e-14)
+
+
+def test_dipole_pass_is_the_field_difference_of_h():
+    """he_apply_dipole adds (direction . d) psi = H(f + direction) psi - H(f) psi (length gauge)."""
+    import ctypes as ct
+    from laqphysics_b200._lib import LIB, check, ptr
+    from laqphysics_b200.engine import _stream
+    from laqphysics_b200.workloads import seeded_state
+    prop, _ = setup()
+    engine = prop.engine
+    x = engine.state(seeded_state(engine.size, 3))
+    f, d = np.array([0.01, -0.02, 0.03]), np.array([0.3, -0.5, 1.0])
+    diff = engine.apply(x, f + d, False) - engine.apply(x, f, False)
+    base = torch.randn(engine.size, dtype=torch.complex128, device=DEVICE)
+    out = base.clone()
+    check(LIB.he_apply_dipole(engine.op.handle, ct.c_void_p(x.data_ptr()), ct.c_void_p(out.data_ptr()),
+                              ptr(np.ascontiguousarray(d)), _stream(engine.device)), 'he_apply_dipole')
+    err = torch.linalg.norm(out - base - diff) / torch.linalg.norm(diff)
+    assert err < 1e-12, float(err)
+
+
+def test_fused_derivative_solve_matches_host_block_exponential():
+    """he_expv_field_derivative (fused block Arnoldi: batched apply + dipole pass) against the
+    host-looped Arnoldi over the explicit block operator [[H, H(E+1) - H(E)], [0, H]]."""
+    from laqphysics_b200.torch_backend import exponential_action, field_derivative_action
+    from laqphysics_b200.workloads import seeded_state
+    prop, _ = setup()
+    engine, size = prop.engine, prop.engine.size
+    z = torch.cat([engine.state(seeded_state(size, 5)), engine.state(seeded_state(size, 6))])
+    E = 0.07
+    ref, info_ref = exponential_action(prop._block_apply(E), z, prop.dt, 1e-13, 30)
+    ref = ref.clone()
+    for _ in range(2):                      # the second call replays the captured graph
+        y, info = field_derivative_action(engine, z, (0., 0., E), (0., 0., 1.), prop.dt, 1e-13, 30)
+        err = torch.linalg.norm(y - ref) / torch.linalg.norm(ref)
+        assert err < 1e-11, float(err)
+        assert info['dimension'] <= info_ref['dimension']
 
 
 def test_adjoint_gradient_matches_oracle_fp64_gradient():

@@ -159,3 +159,70 @@ def test_batched_arnoldi_matches_single_instance_steps(precision):
         err = float(torch.linalg.vector_norm(xb[b] - xs) / torch.linalg.vector_norm(xs))
         assert err < 1e-13, (b, err)
     assert (info['dimension'] <= maxdim).all()
+
+
+@pytest.mark.parametrize('precision', ['complex128', 'mixed'])
+def test_graph_replayed_arnoldi_steps_match_direct_launches(precision):
+    """Repeated solves replayed as one captured CUDA graph (new state, field and dt each
+    time) give bit-identical results to the directly launched solves, single and batched."""
+    from laqphysics_b200 import torch_backend as tb
+    from laqphysics_b200.torch_backend import FieldSchedule, step, step_batched
+    from laqphysics_b200.workloads import arnoldi_small, seeded_state
+    h = arnoldi_small()
+    op = engine(h)
+    x0 = op.state(seeded_state(h.size, 5))
+    x0 /= torch.linalg.vector_norm(x0)
+    field = lambda t: (0., 0., .01 * np.sin(t + .3))
+    fields = lambda t: np.array([[0., 0., .01 * np.sin(t + .3 * b)] for b in range(3)])
+    runs = {}
+    previous = tb.use_cuda_graphs(True)
+    for graphs in (False, True):
+        tb.use_cuda_graphs(graphs)
+        try:
+            sched = FieldSchedule(op, field, velocity=False, precision=precision)
+            x, xb = x0.clone(), x0.repeat(3).reshape(3, -1).contiguous()
+            for i in range(4):
+                x, _ = step(sched, x, i * .005, .005, 1e-10, 16)
+                xb, _ = step_batched(op, fields, xb, i * .005, .005, 1e-10, 16, precision=precision)
+            runs[graphs] = (op.host(x), xb.cpu().numpy())
+        finally:
+            tb.use_cuda_graphs(previous)
+    np.testing.assert_array_equal(runs[True][0], runs[False][0])
+    np.testing.assert_array_equal(runs[True][1], runs[False][1])
+    op.synchronize()
+
+
+@pytest.mark.parametrize('precision', ['complex128', 'mixed'])
+def test_applies_past_convergence_do_no_work(precision):
+    """A fused solve enqueues all maxdim iterations; the H·psi launches after its device-side
+    convergence return without work.  The result and dimension do not depend on maxdim, and
+    the extra iterations cost far less than applies (timed with CUDA events)."""
+    from laqphysics_b200.torch_backend import FieldOperator, exponential_action
+    from laqphysics_b200.workloads import arnoldi_small, seeded_state
+    h = arnoldi_small()
+    op = engine(h)
+    x = op.state(seeded_state(h.size, 9))
+    x /= torch.linalg.vector_norm(x)
+    apply = FieldOperator(op, (0., 0., .01), velocity=False, precision=precision)
+    loose, info = exponential_action(apply, x, .002, 1e-8, 48)
+    small = info['dimension'] + 1
+    assert small < 40
+    tight, info2 = exponential_action(apply, x, .002, 1e-8, small)
+    assert info['dimension'] == info2['dimension']
+    np.testing.assert_allclose(op.host(loose), op.host(tight), rtol=1e-14, atol=1e-16)
+
+    def timed(run, reps=5):
+        run()
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        for _ in range(reps):
+            run()
+        stop.record()
+        torch.cuda.synchronize()
+        return start.elapsed_time(stop) / reps
+
+    t_small = timed(lambda: exponential_action(apply, x, .002, 1e-8, small))
+    t48 = timed(lambda: exponential_action(apply, x, .002, 1e-8, 48))
+    t_apply = timed(lambda: apply(x), reps=20)
+    # each extra iteration is a handful of empty launches, not an apply
+    assert (t48 - t_small) / (48 - small) < 0.6 * t_apply, (t_small, t48, t_apply)
