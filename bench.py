@@ -176,7 +176,9 @@ def arnoldi_leg(torch, device, steps, cpu_steps):
     from laqphysics_b200.engine import B200Hamiltonian
     from laqphysics_b200.torch_backend import FieldSchedule, step
     h, hreal = workloads.arnoldi_small(), workloads.arnoldi_small_real()
-    E0, g, _ = hreal.ground(tol=1e-9)
+    t_ground = time.perf_counter()
+    E0, g, _ = hreal.ground(tol=1e-9)                    # device LOBPCG (laqphysics_b200.ground_s)
+    t_ground = time.perf_counter() - t_ground
     ratio = np.sqrt(h.grid.weights / hreal.grid.weights)
     psi0 = (g.reshape(h.shape, order='F') * ratio[:, None, None] * ratio[None, :, None]).ravel(order='F')
     engine = B200Hamiltonian(h, device)
@@ -201,7 +203,7 @@ def arnoldi_leg(torch, device, steps, cpu_steps):
     ms = start.elapsed_time(stop)
     out = {'workload': 'Arnoldi FP64 length gauge: n=132 nc=17 (N=296,208), maxdim 12, dt 0.02, ground-state start',
            'steps': steps, 'steps_per_s': steps / (ms * 1e-3), 'ms_per_step': ms / steps,
-           'mean_dimension': float(np.mean(dims)), 'ground_energy': E0,
+           'mean_dimension': float(np.mean(dims)), 'ground_energy': E0, 'ground_state_s': t_ground,
            'hpsi_per_step': (engine.apply_count - applies0) / steps}
     if cpu_steps:
         from oracle import arnoldi, cpu
@@ -230,7 +232,9 @@ def batched_leg(torch, device, steps, count=32):
     from laqphysics_b200.engine import B200Hamiltonian
     from laqphysics_b200.torch_backend import step_batched
     h, hreal = workloads.arnoldi_small(), workloads.arnoldi_small_real()
-    E0, g, _ = hreal.ground(tol=1e-9)
+    t_ground = time.perf_counter()
+    E0, g, _ = hreal.ground(tol=1e-9)                    # device LOBPCG (laqphysics_b200.ground_s)
+    t_ground = time.perf_counter() - t_ground
     ratio = np.sqrt(h.grid.weights / hreal.grid.weights)
     psi0 = (g.reshape(h.shape, order='F') * ratio[:, None, None] * ratio[None, :, None]).ravel(order='F')
     engine = B200Hamiltonian(h, device)
