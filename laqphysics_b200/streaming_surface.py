@@ -132,16 +132,24 @@ TorchVolkovAccumulator = VolkovAccumulator
 
 class SurfaceSampler:
     """One tSURFF surface sample on the device: flux frame (engine), ionic contraction
-    with the device channel functions chi, Volkov accumulation."""
+    with the device channel functions chi, Volkov accumulation.  Optional storage in the
+    reference's sharded layout (surface_storage.ShardedArray): `projected` keeps q of every
+    sample (storage mode 'projected', python/streaming_surface.py:255), `raw` the flux frame
+    (mode 'raw_shards', python/run3d.py:139-141)."""
 
-    def __init__(self, engine, contractor, accumulator):
+    def __init__(self, engine, contractor, accumulator, projected=None, raw=None):
         self.engine, self.contractor, self.accumulator = engine, contractor, accumulator
+        self.projected, self.raw = projected, raw
 
     @torch.no_grad()
     def record(self, index, time, state, field, chi):
         frame = self.engine.surface.frame(state, field)
+        if self.raw is not None:
+            self.raw[index] = frame
         if not torch.is_tensor(chi):
             chi = torch.as_tensor(np.ascontiguousarray(chi, dtype=complex), device=self.engine.device)
         q = self.contractor.contract(chi, frame)
         self.accumulator.add(index, time, q)
+        if self.projected is not None:
+            self.projected[index] = q
         return q

@@ -382,7 +382,28 @@ def pulses():
     save('pulses', t=ts, **arrays)
 
 
+def sharded_case():
+    """A (7, 3, 2) complex128 array written frame by frame (in reverse order) through the
+    reference's ShardedArray with a 4400-byte cap (three frames per shard, three shards)."""
+    import shutil
+    from surface_storage import ShardedArray
+    folder = Path(__file__).resolve().parent / 'shards'
+    if folder.exists():
+        shutil.rmtree(folder)
+    shape = (7, 3, 2)
+    values = (np.arange(np.prod(shape)).reshape(shape) * (1 + 2j) - 3.5j).astype(complex)
+    a = ShardedArray(folder, shape, mode='w+', max_file_bytes=4400)
+    for i in reversed(range(shape[0])):
+        a[i] = values[i]
+    a.close()
+    save('shards_values', values=values)
+
+
 if __name__ == '__main__':
+    if len(sys.argv) > 1:          # named cases only, e.g. `make_golden.py sharded_case`
+        for name in sys.argv[1:]:
+            globals()[name]()
+        sys.exit(0)
     grids()
     product_cases()
     coupled_case()
@@ -397,3 +418,4 @@ if __name__ == '__main__':
     volkov_case()
     ground_case()
     pulses()
+    sharded_case()

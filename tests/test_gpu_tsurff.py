@@ -99,3 +99,35 @@ def test_fused_surface_sample_from_device_state():
         ref_acc.add(i, t, q_ref)
     np.testing.assert_allclose(sampler.accumulator.amplitude.cpu().numpy(), ref_acc.amplitude.cpu().numpy(),
                                rtol=1e-11, atol=1e-13)
+
+
+def test_sampler_keeps_projected_and_raw_history_in_shards(tmp_path):
+    """SurfaceSampler with the reference's 'projected' and 'raw_shards' storage: every q and
+    every flux frame lands in capped NPY shards (surface_storage.ShardedArray) that read back
+    equal to the device values and to the host flux."""
+    from laqphysics_b200.engine import B200Hamiltonian
+    from laqphysics_b200.streaming_surface import SurfaceSampler, VolkovAccumulator
+    from laqphysics_b200.surface_storage import ShardedArray, load_flux
+    from laqphysics_b200.workloads import seeded_state
+    g = golden('volkov')
+    h, base, ion, contractor, avec = _setup()
+    op = B200Hamiltonian(h, DEVICE)
+    count = 5
+    frame_shape = tuple(op.surface.frame(op.state(seeded_state(h.size, 1)), avec(0.)).shape)
+    q_shape = tuple(contractor.contract(torch.as_tensor(g['chi'][0], device=DEVICE),
+                                        op.surface.frame(op.state(seeded_state(h.size, 1)), avec(0.))).shape)
+    raw = ShardedArray(tmp_path / 'run' / 'flux_shards', (count, *frame_shape), mode='w+', max_file_bytes=2 * 16 * int(np.prod(frame_shape)) + 4200)
+    projected = ShardedArray(tmp_path / 'run' / 'projected', (count, *q_shape), mode='w+', max_file_bytes=100000)
+    sampler = SurfaceSampler(op, contractor, VolkovAccumulator(contractor, CONFIG, avec, device=DEVICE),
+                             projected=projected, raw=raw)
+    qs = []
+    for i, t in enumerate(g['times'][:count]):
+        x = seeded_state(h.size, 100 + i)
+        qs.append(sampler.record(i, t, op.state(x), avec(t), g['chi'][i]).cpu().numpy())
+    raw.close()
+    projected.close()
+    flux = load_flux(tmp_path / 'run')
+    assert len(list((tmp_path / 'run' / 'flux_shards').glob('part_*.npy'))) == 3
+    for i, t in enumerate(g['times'][:count]):
+        np.testing.assert_allclose(flux[i], h.flux(seeded_state(h.size, 100 + i), avec(t)), rtol=1e-12, atol=1e-14)
+    np.testing.assert_array_equal(ShardedArray(tmp_path / 'run' / 'projected')[:], np.array(qs))
