@@ -419,8 +419,10 @@ def cf4_leg(torch, device, steps=10):
     preconditioned GMRES (the reference's implicit.py:45-109 path), on the Arnoldi grid
     (n=132, nc=17), velocity gauge, sin^2 pulse omega 1.6 a.u. peak 0.02 a.u., dt 0.05,
     ground-state start, reference energy = ground energy, GMRES tolerance 1e-10; separable
-    ionic preconditioner in complex128 (GMRES(32)) and in complex64 (flexible GMRES(16)).
-    Also times the preconditioner alone (4 n^3 complex GEMMs per channel)."""
+    ionic preconditioner in complex128 (GMRES(32)) and in complex64 (flexible GMRES(16)), and
+    the mixed form (complex128 defect correction around complex64 inner solves) with the
+    state error against the complex128 run.  Also times the preconditioner alone (4 n^3
+    complex GEMMs per channel)."""
     from laqphysics_b200 import workloads
     from laqphysics_b200.engine import B200Hamiltonian
     from laqphysics_b200.implicit import SeparablePreconditioner, cf4_step
@@ -436,19 +438,23 @@ def cf4_leg(torch, device, steps=10):
     out = {'workload': 'CF4 + [2/2] Pade / GMRES, Arnoldi grid n=132 nc=17, velocity gauge, dt 0.05, tol 1e-10, '
                        'separable preconditioner', 'steps': steps}
     gemm_flops = 32 * h.n ** 3 * h.nc
-    for precision in ('complex128', 'complex64'):
+    finals = {}
+    for variant in ('complex128', 'complex64', 'mixed'):
+        precision = 'complex128' if variant == 'complex128' else 'complex64'     # of the preconditioner
+        solve = 'mixed' if variant == 'mixed' else 'complex128'                  # of H·psi in the solves
         engine.separable = SeparablePreconditioner(engine, precision)
         x = engine.state(psi0)
         for i in range(2):
-            x, _ = cf4_step(engine, x, avec, i * dt, dt, E0, tol=tol)
+            x, _ = cf4_step(engine, x, avec, i * dt, dt, E0, tol=tol, precision=solve)
         torch.cuda.synchronize(device)
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         iterations = 0
         start.record()
         for i in range(2, 2 + steps):
-            x, info = cf4_step(engine, x, avec, i * dt, dt, E0, tol=tol)
+            x, info = cf4_step(engine, x, avec, i * dt, dt, E0, tol=tol, precision=solve)
             iterations += info['linear_iterations']
         stop.record()
+        finals[variant] = x
         torch.cuda.synchronize(device)
         ms = start.elapsed_time(stop)
         y = x   # complex128 in and out; the complex64 preconditioner converts inside
@@ -462,9 +468,14 @@ def cf4_leg(torch, device, steps=10):
         b.record()
         torch.cuda.synchronize(device)
         pre_ms = a.elapsed_time(b) / 20
-        out[precision] = {'steps_per_s': steps / (ms * 1e-3), 'ms_per_step': ms / steps,
-                          'gmres_iterations_per_step': iterations / steps,
-                          'preconditioner_ms': pre_ms, 'preconditioner_tflops': gemm_flops / (pre_ms * 1e-3) / 1e12}
+        out[variant] = {'steps_per_s': steps / (ms * 1e-3), 'ms_per_step': ms / steps,
+                        'gmres_iterations_per_step': iterations / steps,
+                        'preconditioner_ms': pre_ms, 'preconditioner_tflops': gemm_flops / (pre_ms * 1e-3) / 1e12}
+    ref = finals['complex128']
+    out['mixed']['solve'] = ('complex128 defect correction around complex64 inner GMRES solves '
+                             '(complex64 H·psi, complex64 separable preconditioner)')
+    out['mixed']['state_rel_l2_vs_complex128'] = float(torch.linalg.vector_norm(finals['mixed'] - ref) /
+                                                       torch.linalg.vector_norm(ref))
     return out
 
 

@@ -13,6 +13,9 @@ reference (python/implicit.py:13-109):
 * ``pade_step`` / ``cf4_step``: the two Pade roots 3 +- i sqrt(3), CF4 fields at the
   Gauss points, the scalar |A|^2 and E_ref phases, and dt halving (depth <= 6) on
   'GMRES did not converge'.
+* ``precision='mixed'`` (pade_step / cf4_step): complex128 defect correction around
+  complex64 inner GMRES solves (complex64 H·psi with FP32 accumulation); an addition, the
+  reference has one precision.
 The operator y + i alpha (H - E_ref) y is one fused launch of the engine.
 """
 import ctypes as ct
@@ -191,10 +194,39 @@ def gmres(apply, b, preconditioner, x0=None, tol=1e-11, restart=32, max_restarts
     raise RuntimeError(f'GMRES did not converge: residual={true:.3e}, iterations={iterations}')
 
 
+INNER_TOLERANCE = 1e-5   # relative residual of each complex64 inner solve of a mixed Pade solve
+
+
+def defect_corrected_solve(A, A32, b, M, tol, flexible, restart, corrections=8):
+    """Solve A s = b to a complex128 relative residual <= tol by defect correction: each
+    sweep solves A32 d = r by GMRES with the complex64 operator A32 (FP32 accumulation)
+    to INNER_TOLERANCE, adds d to s and recomputes r = b - A s with the complex128
+    operator.  Each sweep gains about five digits while that stays above the complex64
+    operator's own error, so a 1e-11 solve takes two or three sweeps.  Raises the
+    reference's 'GMRES did not converge' message when the sweeps run out."""
+    s = torch.zeros_like(b)
+    r = b
+    bnorm = norm(b)
+    iterations, relative = 0, 1.
+    for sweep in range(corrections):
+        d, info = gmres(A32, r, M, tol=max(INNER_TOLERANCE, tol), flexible=flexible, restart=restart)
+        iterations += info['iterations']
+        s = axpby(1, s, 1, d, out=s)
+        r = axpby(1, b, -1, A(s))
+        relative = norm(r) / bnorm
+        if relative <= tol:
+            return s, {'iterations': iterations, 'relative_residual': relative, 'corrections': sweep + 1}
+    raise RuntimeError(f'GMRES did not converge: residual={relative:.3e}, iterations={iterations}')
+
+
 @torch.no_grad()
-def pade_step(engine, x, field, dt, reference_energy=0., tol=1e-11):
+def pade_step(engine, x, field, dt, reference_energy=0., tol=1e-11, precision='complex128'):
     """Two shifted solves (I + i alpha K) s = x, x <- 2 s - x, alpha = dt / (3 +- i sqrt 3)
-    (python/implicit.py:76-89)."""
+    (python/implicit.py:76-89).  precision='mixed': each solve is a complex128 defect
+    correction around complex64 inner GMRES solves (:func:`defect_corrected_solve`); the
+    state, the residuals and the step stay complex128."""
+    if precision not in ('complex128', 'mixed'):
+        raise ValueError("precision must be 'complex128' or 'mixed'")
     a2 = getattr(engine, 'a2_coefficient', 1.)
     squared = a2 * sum(float(a) ** 2 for a in field)
     iterations, residual = 0, 0.
@@ -210,7 +242,13 @@ def pade_step(engine, x, field, dt, reference_energy=0., tol=1e-11):
             M = (lambda y, alpha=alpha: separable.apply(y, alpha, squared - reference_energy))
         else:
             M = _jacobi(engine.diagonal, alpha, squared - reference_energy)
-        s, info = gmres(A, x, M, tol=tol, flexible=flexible, restart=16 if flexible else 32)
+        if precision == 'mixed':
+            def A32(y, alpha=alpha):
+                return engine.apply_shifted(y.to(torch.complex64), field, alpha, reference_energy,
+                                            velocity=True).to(torch.complex128)
+            s, info = defect_corrected_solve(A, A32, x, M, tol, flexible, 16 if flexible else 32)
+        else:
+            s, info = gmres(A, x, M, tol=tol, flexible=flexible, restart=16 if flexible else 32)
         x = axpby(2, s, -1, x)
         iterations += info['iterations']
         residual = max(residual, info['relative_residual'])
@@ -218,8 +256,9 @@ def pade_step(engine, x, field, dt, reference_energy=0., tol=1e-11):
 
 
 @torch.no_grad()
-def cf4_step(engine, x, avec, t, dt, reference_energy=0., tol=1e-11, depth=0):
-    """Commutator-free 4th-order Magnus step (python/implicit.py:91-109)."""
+def cf4_step(engine, x, avec, t, dt, reference_energy=0., tol=1e-11, depth=0, precision='complex128'):
+    """Commutator-free 4th-order Magnus step (python/implicit.py:91-109); precision as in
+    :func:`pade_step`."""
     fields = np.array([avec(t + C1 * dt), avec(t + C2 * dt)], float)
     iterations, residual, original = 0, 0., x
     a2 = getattr(engine, 'a2_coefficient', 1.)
@@ -227,7 +266,7 @@ def cf4_step(engine, x, avec, t, dt, reference_energy=0., tol=1e-11, depth=0):
         for w in ((A2, A1), (A1, A2)):
             effective = 2 * np.einsum('a,aj->j', w, fields)
             correction = a2 * (np.dot(w, np.sum(fields ** 2, axis=1)) - .5 * np.dot(effective, effective))
-            x, info = pade_step(engine, x, effective, dt / 2, reference_energy, tol)
+            x, info = pade_step(engine, x, effective, dt / 2, reference_energy, tol, precision)
             phase = np.exp(-1j * dt * (correction + reference_energy / 2))
             x = axpby(phase, x, 0, x, out=x)
             iterations += info['linear_iterations']
@@ -237,8 +276,8 @@ def cf4_step(engine, x, avec, t, dt, reference_energy=0., tol=1e-11, depth=0):
     except RuntimeError as error:
         if 'GMRES did not converge' not in str(error) or depth >= 6:
             raise
-        x, a = cf4_step(engine, original, avec, t, dt / 2, reference_energy, tol / 2, depth + 1)
-        x, b = cf4_step(engine, x, avec, t + dt / 2, dt / 2, reference_energy, tol / 2, depth + 1)
+        x, a = cf4_step(engine, original, avec, t, dt / 2, reference_energy, tol / 2, depth + 1, precision)
+        x, b = cf4_step(engine, x, avec, t + dt / 2, dt / 2, reference_energy, tol / 2, depth + 1, precision)
         return x, {'linear_iterations': a['linear_iterations'] + b['linear_iterations'],
                    'linear_residual': max(a['linear_residual'], b['linear_residual']), 'dimension': 0,
                    'residual_estimate': None, 'subdivided': True}
