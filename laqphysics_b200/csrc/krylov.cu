@@ -1006,8 +1006,15 @@ int expv_impl(he_krylov *k, he_handle op, const void *x, void *y, const double *
                           first);
         cudaGraph_t g = nullptr;
         const cudaError_t ended = cudaStreamEndCapture(k->capture_stream, &g);
-        if (!rc && ended != cudaSuccess) rc = he_fail(HE_ERR_CUDA, cudaGetErrorString(ended), __FILE__, __LINE__);
-        if (!rc) {
+        if (rc || ended != cudaSuccess || !g) {
+            // The capture can be invalidated by work outside this solve (another host thread
+            // loading its kernels, for instance): nothing captured has run, so drop it and
+            // enqueue the solve directly.  A genuine error repeats there and is returned.
+            if (g) cudaGraphDestroy(g);
+            g = nullptr;
+            cudaGetLastError();
+            rc = enqueue_expv(k, op, x, y, fields, velocity, dt, tol, maxdim, s, precision, direction, 0, first);
+        } else {
             bool updated = false;
             if (k->graph_exec) {
                 cudaGraphExecUpdateResultInfo info;
