@@ -744,7 +744,7 @@ def main():
         'metric': METRIC, 'value': value, 'unit': 'GB/s', 'n_gpus': world, 'steps': args.steps,
         'warmup': args.warmup, 'ms_per_step': per128, 'higher_is_better': True, 'scaling': 'weak',
         'vs_baseline': None, 'dtype': 'complex128', 'data': 'synthetic (seeded complex Gaussian state)',
-        'config': {'workload': WORKLOAD, 'field': 'length gauge, Ez=0.02', 'parallelism': f'replicas x{world}',
+        'config': {'workload': WORKLOAD, 'field': 'length gauge, Ez=0.02', 'parallelism': 'replicas',
                    'l2': 'two rotating 216 MB input states (> 126 MB L2)'},
         'gpu_launches': launches,
         'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': hbm, 'unit': 'GB/s', 'frac': achieved / hbm,

@@ -50,6 +50,9 @@ void tensor_apply(int n, int nc, int nt, const int *ptr, const int *col, const d
 int he_last_status(void);
 const char *he_last_error(void);
 int he_version(void);
+/* binaryVersion of this library's kernels as loaded on the current device (100 = sm_100a);
+ * a diagnostic of the build, no counterpart in the reference. */
+int he_binary_version(int *version);
 
 /* ------------------------------------------------------------------------------------
  * Device operator handle.
@@ -294,10 +297,14 @@ int he_volkov_add(int nlab, int nouter, int ns, int ne, int nang, const void *q,
  * allocator, a host runtime that forbids allocations outside its own allocator).
  * norms[v] = ||x + v*ld|| for v < count, count <= 64 (larger counts are rejected with
  * HE_ERR_ARG); x: complex128 device vectors of n elements; norms: host memory.  The
- * scratch is a fixed file-scope device array (152,064 bytes, held by every GPU that loads
- * the library until exit), shared by all calls: calls that overlap on the GPU race.  The
- * first call on a device looks up that array's address and should come before any
- * stream capture on the device.  Blocks the host until the norms are ready.
+ * scratch is a fixed file-scope device array of 152,064 bytes, shared by all calls: calls
+ * that overlap on the GPU race.  Under CUDA's default lazy module loading the driver
+ * allocates that array on a device when the library first looks up its address there:
+ * in he_create for the operator's device, else at the first he_vec_norms_noalloc call on
+ * the device.  Make one of those before a pool allocator takes the device's memory and
+ * before any stream capture on it (CUDA_MODULE_LOADING=EAGER allocates the array when
+ * the context is created).  After that no call allocates device memory; the array stays
+ * until the process exits.  Blocks the host until the norms are ready.
  * ---------------------------------------------------------------------------------- */
 int he_vec_norms_noalloc(long long n, int count, const void *x, long long ld, double *norms, void *stream);
 

@@ -26,6 +26,7 @@ SIGNATURES = {
     'he_last_status': (I, []),
     'he_last_error': (ct.c_char_p, []),
     'he_version': (I, []),
+    'he_binary_version': (I, [ct.POINTER(I)]),
     'he_create': (I, [ct.POINTER(P), I, I, I, P, P, P, P, P, P, I, P, P, P, P, P, I, I, P, P, P, P, P, P, I]),
     'he_destroy': (I, [P]),
     'he_info': (I, [P, ct.POINTER(ct.c_longlong), I]),

@@ -9,6 +9,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
@@ -18,8 +19,9 @@ LIBRARY = LIBDIR / 'libhelium_b200.so'
 INCLUDE = HERE.parent / 'include'
 
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
-FLAGS = ['-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC', '-shared', '--expt-relaxed-constexpr',
-         '-Xcompiler', '-Wall']
+FLAGS = ['-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC', '--expt-relaxed-constexpr', '-Xcompiler', '-Wall']
+COMPILE_FLAGS = FLAGS
+LIBS = ['-lcublas', '-lnvrtc']
 
 
 def nvcc():
@@ -44,19 +46,33 @@ def up_to_date():
     return all(p.stat().st_mtime <= stamp for p in dependencies())
 
 
-def build(force=False, verbose=False):
-    if not force and up_to_date():
-        return LIBRARY
-    LIBDIR.mkdir(exist_ok=True)
-    tmp = LIBRARY.with_suffix('.so.tmp')
-    cmd = [nvcc(), *ARCH, *FLAGS, f'-I{INCLUDE}', *map(str, sources()), '-o', str(tmp), '-lcublas', '-lnvrtc']
+def _compile(source, objdir, verbose):
+    obj = objdir / (source.stem + '.o')
+    cmd = [nvcc(), *ARCH, *COMPILE_FLAGS, f'-I{INCLUDE}', '-c', str(source), '-o', str(obj)]
     if verbose:
         cmd.insert(1, '-Xptxas=-v')
     result = subprocess.run(cmd, capture_output=True, text=True)
     if result.returncode != 0:
-        raise RuntimeError('nvcc failed:\n' + result.stdout + result.stderr)
+        raise RuntimeError(f'nvcc failed on {source.name}:\n' + result.stdout + result.stderr)
     if verbose:
         sys.stderr.write(result.stderr)
+    return obj
+
+
+def build(force=False, verbose=False):
+    """Compile every source to an object file in parallel (one nvcc per file), then link."""
+    if not force and up_to_date():
+        return LIBRARY
+    LIBDIR.mkdir(exist_ok=True)
+    objdir = LIBDIR / 'obj'
+    objdir.mkdir(exist_ok=True)
+    with ThreadPoolExecutor(max_workers=max(1, min(len(sources()), os.cpu_count() or 1))) as pool:
+        objects = list(pool.map(lambda src: _compile(src, objdir, verbose), sources()))
+    tmp = LIBRARY.with_suffix('.so.tmp')
+    cmd = [nvcc(), *ARCH, '-shared', '-Xcompiler', '-fPIC', *map(str, objects), '-o', str(tmp), *LIBS]
+    result = subprocess.run(cmd, capture_output=True, text=True)
+    if result.returncode != 0:
+        raise RuntimeError('nvcc link failed:\n' + result.stdout + result.stderr)
     os.replace(tmp, LIBRARY)
     return LIBRARY
 

@@ -19,22 +19,30 @@ CHECKPOINT_KEYS = ('psi', 'step', 'signature', 'ground_energy', 'ground', 'groun
                    'maximum_linear_residual_all_segments', 'linear_iterations_all_segments')
 
 
+def _npz_estimate(arrays):
+    """Upper estimate of an uncompressed NPZ: the payloads plus 1 KiB per member for its
+    NPY header and zip entry, plus 4 KiB for the zip directory."""
+    return 4096 + sum(1024 + np.asarray(v).nbytes for v in arrays.values())
+
+
 def capped_npz(path, max_file_bytes=DEFAULT_FILE_BYTES, **arrays):
-    """np.savez to a temporary file beside `path`, refused above `max_file_bytes` (checked
-    before and after writing), then renamed over `path`."""
+    """Write an uncompressed NPZ atomically, refusing it above `max_file_bytes`: the size
+    is estimated before writing and measured after, then the staged file is renamed over
+    `path` (a refused write leaves `path` untouched)."""
     path = Path(path)
-    limit = int(max_file_bytes)
-    if limit <= 0:
-        raise ValueError('file cap must be positive')
-    estimate = sum(np.asarray(v).nbytes + 1024 for v in arrays.values()) + 4096
-    if estimate > limit:
-        raise ValueError(f'{path.name}: checkpoint needs about {estimate} bytes, above file cap {limit}')
-    temporary = path.with_name(path.stem + '.tmp.npz')
-    np.savez(temporary, **arrays)
-    if temporary.stat().st_size > limit:
-        temporary.unlink()
-        raise ValueError('NPZ exceeds configured file cap')
-    os.replace(temporary, path)
+    cap = int(max_file_bytes)
+    if cap <= 0:
+        raise ValueError(f'file cap must be positive, got {cap}')
+    needed = _npz_estimate(arrays)
+    if needed > cap:
+        raise ValueError(f'{path.name}: about {needed} bytes would exceed the {cap}-byte file cap')
+    staged = path.parent / (path.stem + '.tmp.npz')
+    np.savez(staged, **arrays)
+    written = staged.stat().st_size
+    if written > cap:
+        staged.unlink()
+        raise ValueError(f'{path.name}: {written} bytes written, above the {cap}-byte file cap')
+    os.replace(staged, path)
 
 
 def write_checkpoint(path, psi, step, signature, ground_energy, ground, ground_residual, surface_generation=-1,

@@ -1,121 +1,72 @@
-"""Coupled (l1, l2, L), M=0 channels with natural parity (host setup).
+"""Coupled (l1, l2, L) channels of total M = 0 and natural parity (host setup).
 
-Same basis, tables and change-of-basis as the reference's ``CoupledHelium``
-(python/coupled_angular.py:13-82): the coupled channels are an exact
-Clebsch-Gordan isometry U of the product M=0 channels; Coulomb multipoles and
-z dipoles are projected as U^T A U and re-emitted as edge lists with the
-reference's 1e-13 pruning, so the device kernel consumes exactly the same
-format for either basis.
+Drop-in for the reference's ``CoupledHelium(uncoupled, total_Lmax)``
+(python/coupled_angular.py:13-82): the same channel list (l1, l2 <= lmax, natural parity
+l1 + l2 + L even, L <= total_Lmax), the same tables in the same format, the same
+``transform``, ``exchange``/``exchange_sign``, ``expand``/``project``/``ground``/
+``exchange_error``.  The tables are built by this package's projection module: the
+product operator of ``uncoupled`` (an M = 0 ``Helium``) is projected through the
+Clebsch-Gordan isometry in one contraction per table, and the edges are emitted in the
+coupled layout (dipole edges ordered by source, then electron).
 """
 import numpy as np
-from sympy.physics.wigner import wigner_3j
 
-from .helium3d import Helium, separable_diagonal
+from .helium3d import Helium
+from .projection import ProjectedChannels, check_isometry, isometry, project_tables
 
 
-class CoupledHelium:
+def natural_parity_channels(lmax, total_Lmax):
+    """(l1, l2, L) with l1, l2 <= lmax, |l1 - l2| <= L <= min(l1 + l2, total_Lmax), l1 + l2 + L even."""
+    out = []
+    for l1 in range(lmax + 1):
+        for l2 in range(lmax + 1):
+            out += [(l1, l2, L) for L in range(abs(l1 - l2), min(l1 + l2, total_Lmax) + 1, 2)]
+    return out
+
+
+class CoupledHelium(ProjectedChannels):
     def __init__(self, uncoupled, total_Lmax):
-        h = uncoupled
-        self.uncoupled = h
-        if any(a[1] + b[1] != 0 for a, b in h.ch):
-            raise ValueError('coupled backend currently requires M=0')
-        self.lmax = max(a[0] for a, _ in h.ch)
+        product = uncoupled
+        total_m = {a[1] + b[1] for a, b in product.ch}
+        if total_m != {0}:
+            raise ValueError(f'the coupled basis is built from an M = 0 product basis (got total M {sorted(total_m)})')
+        self.uncoupled = product
+        self.lmax = max(l1 for (l1, _), _ in product.ch)
         self.total_Lmax = total_Lmax
-        L1 = range(self.lmax + 1)
-        self.basis = [(l, j, L) for l in L1 for j in L1
-                      for L in range(abs(l - j), min(l + j, total_Lmax) + 1) if (l + j - L) % 2 == 0]
-        self.n = h.n
-        self.nc = len(self.basis)
+        self.basis = natural_parity_channels(self.lmax, total_Lmax)
+        self.n, self.nc = product.n, len(self.basis)
         self.shape = (self.n, self.n, self.nc)
-        self.size = int(np.prod(self.shape))
-        self.grid, self.r, self.cut = h.grid, h.r, h.cut
-        for name in ('ptr', 'col', 'tv', 'rad'):
-            setattr(self, name, getattr(h, name))
-        U = np.zeros((h.nc, self.nc))
-        for c, (l, j, L) in enumerate(self.basis):
-            for a, ((ll, m), (jj, mm)) in enumerate(h.ch):
-                if l == ll and j == jj:
-                    U[a, c] = (-1) ** (l - j) * np.sqrt(2 * L + 1) * float(wigner_3j(l, j, L, m, mm, 0))
-        if np.linalg.norm(U.T @ U - np.eye(self.nc)) > 1e-11:
-            raise RuntimeError('CG transformation is not isometric')
+        self.size = self.n * self.n * self.nc
+        self.grid, self.r, self.cut = product.grid, product.r, product.cut
+        self.ptr, self.col, self.tv, self.rad = product.ptr, product.col, product.tv, product.rad
+        U = isometry(product.ch, [(l1, l2, L, 0) for l1, l2, L in self.basis])
+        check_isometry(U, 'coupled M = 0 channels', 1e-11)
         self.transform = U
-        zero_m = [h.ch.index(((l, 0), (j, 0))) for l, j, _ in self.basis]
-        self._diag = None
-        if hasattr(h, 'diag_parts'):
-            self.diag_parts = tuple(np.asfortranarray(p[:, zero_m]) for p in h.diag_parts)
+        # the diagonal is local in (l1, l2): take the parts of the (l1 0)(l2 0) product channel
+        source = [product.ch.index(((l1, 0), (l2, 0))) for l1, l2, _ in self.basis]
+        if hasattr(product, 'diag_parts'):
+            self.diag_parts = tuple(np.asfortranarray(part[:, source]) for part in product.diag_parts)
+            self._diag = None
         else:
-            self._diag = np.asfortranarray(np.stack([h.diag[:, :, c] for c in zero_m], axis=2))
-        self._project_edges(h, U)
-        self.exchange = np.array([self.basis.index((j, l, L)) for l, j, L in self.basis])
-        self.exchange_sign = np.array([(-1) ** (l + j - L) for l, j, L in self.basis])
-
-    @property
-    def diag(self):
-        if self._diag is None:
-            self._diag = separable_diagonal(*self.diag_parts)
-        return self._diag
-
-    def _project_edges(self, h, U):
-        nlam = h.rad.shape[2]
-        V = []
-        for lam in range(nlam):
-            A = np.zeros((h.nc, h.nc), complex)
-            for a in range(h.nc):
-                for k in range(h.vptr[a], h.vptr[a + 1]):
-                    if h.vl[k] == lam:
-                        A[a, h.vc[k]] += h.vcoef[k]
-            V.append(U.T @ A @ U)
-        D = np.zeros((2, h.nc, h.nc), complex)
-        for a in range(h.nc):
-            for k in range(h.dptr[a], h.dptr[a + 1]):
-                D[h.de[k] - 1, a, h.dc[k]] += h.dcoef[2, k]
-        D = np.array([U.T @ A @ U for A in D])
-        vp, vc, vl, vv = [0], [], [], []
-        dp, dc, de, dv, dl = [0], [], [], [], []
-        for a, (l, j, _) in enumerate(self.basis):
-            for b, (ll, jj, _) in enumerate(self.basis):
-                for lam, A in enumerate(V):
-                    if abs(A[a, b]) > 1e-13:
-                        vc.append(b); vl.append(lam); vv.append(A[a, b])
-                for e in range(2):
-                    if abs(D[e, a, b]) > 1e-13:
-                        dc.append(b); de.append(e + 1); dv.append([0, 0, D[e, a, b]])
-                        bra, ket = (l, j)[e], (ll, jj)[e]
-                        dl.append(bra * (bra + 1) - ket * (ket + 1))
-            vp.append(len(vc)); dp.append(len(dc))
-        for name, values in [('vptr', vp), ('vc', vc), ('vl', vl), ('dptr', dp), ('dc', dc), ('de', de)]:
-            setattr(self, name, np.array(values, np.int32))
-        self.vcoef = np.array(vv, complex)
-        self.dcoef = np.asfortranarray(np.array(dv, complex).reshape(-1, 3).T)
-        self.ldiff = np.array(dl, float)
+            self._diag = np.asfortranarray(product.diag[:, :, source])
+        self._install(project_tables(product, U, [c[:2] for c in self.basis], electron_major=False))
+        where = {c: k for k, c in enumerate(self.basis)}
+        self.exchange = np.array([where[l2, l1, L] for l1, l2, L in self.basis])
+        self.exchange_sign = np.array([1 - 2 * ((l1 + l2 - L) & 1) for l1, l2, L in self.basis])
 
     prepare_surface = Helium.prepare_surface
     flux = Helium.flux
 
     def apply(self, x, field=(0., 0., 0.), velocity=False):
-        if abs(field[0]) + abs(field[1]) > 1e-15:
-            raise ValueError('M=0 coupled basis only supports z polarization')
+        """H·psi through the C-ABI; the M = 0 channels admit only a z field."""
+        if max(abs(field[0]), abs(field[1])) > 1e-15:
+            raise ValueError('an M = 0 coupled basis takes only a z field; use BipolarHelium for x/y fields')
         return Helium.apply(self, x, field, velocity)
 
-    def expand(self, x):
-        u = np.asarray(x).reshape(self.n * self.n, self.nc, order='F')
-        return (u @ self.transform.T).ravel(order='F')
-
-    def project(self, x):
-        u = np.asarray(x).reshape(self.n * self.n, self.uncoupled.nc, order='F')
-        return (u @ self.transform).ravel(order='F')
-
     def ground(self, tol=1e-10, cache_dir=None):
+        """Ground state of the compressed total-L = 0 problem, placed in the (l, l, 0) channels."""
         from .ground_s import GroundS
         solver = GroundS(self.uncoupled)
-        E, g, res = solver.solve(tol, cache_dir, expand=False)
-        small = g.reshape(solver.shape, order='F')
-        out = np.zeros(self.shape, complex, order='F')
-        for l in range(self.lmax + 1):
-            out[:, :, self.basis.index((l, l, 0))] = small[:, :, l]
-        return E, out.ravel(order='F'), res
-
-    def exchange_error(self, x):
-        u = np.asarray(x).reshape(self.shape, order='F')
-        swapped = u.transpose(1, 0, 2)[:, :, self.exchange] * self.exchange_sign[None, None, :]
-        return float(np.linalg.norm(u - swapped))
+        energy, small, residual = solver.solve(tol, cache_dir, expand=False)
+        columns = {l: self.basis.index((l, l, 0)) for l in range(self.lmax + 1)}
+        return energy, self._embed_singlet(small.reshape(solver.shape, order='F'), columns), residual

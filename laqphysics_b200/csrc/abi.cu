@@ -352,6 +352,7 @@ extern "C" int he_create(he_handle *out, int n, int nc, int nt, const int *ptr, 
     h->separable = separable;
     h->has32 = (flags & 1) != 0;
     HE_CUDA_TRY(cudaGetDevice(&h->device));
+    if ((s = he_noalloc_prepare_device())) { delete h; g_status = s; return s; }
     std::vector<double> hinv(2 * (size_t)n), tdiag(2 * (size_t)n, 0.0);
     for (int i = 0; i < n; ++i) {
         const std::complex<double> v = 1.0 / (2.0 * std::complex<double>(r[2 * i], r[2 * i + 1]));

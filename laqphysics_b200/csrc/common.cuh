@@ -108,6 +108,10 @@ template <typename R> struct DeviceTables {
 
 void he_set_error(const char* what, const char* file, int line);
 
+// Looks up (and under lazy module loading, loads) the allocation-free entry point's static
+// scratch on the current device (noalloc.cu).
+int he_noalloc_prepare_device();
+
 // Raise a kernel's dynamic shared-memory limit on the current device, once per kernel,
 // device and size (the attribute call costs microseconds per launch otherwise).
 cudaError_t he_smem_limit(const void* kernel, size_t bytes);

@@ -7,15 +7,24 @@
 // must not stall on the allocator's implicit device synchronisation, and a library
 // embedded in another runtime that forbids device allocations outside its own
 // allocator.  he_vec_norms_noalloc serves them: its scratch is the file-scope device
-// array below, sized for NOALLOC_MAX_VECTORS vectors, which every GPU that loads this
-// library holds until the process exits.
+// array below, sized for NOALLOC_MAX_VECTORS vectors.
+//
+// When the array comes into being.  The array belongs to this file's CUDA module.  Under
+// CUDA's lazy module loading (the default since CUDA 12.2) the driver loads the module,
+// and allocates the array on that device, the first time the process touches it on a
+// device: the address lookup below.  That lookup happens (a) in he_create, for the device
+// an operator is created on, and (b) otherwise at the first he_vec_norms_noalloc call on a
+// device.  A caller that hands the device's memory to a pool allocator should therefore
+// create its operator, or make one he_vec_norms_noalloc call, before the pool takes the
+// memory; with CUDA_MODULE_LOADING=EAGER the array is allocated when the context is
+// created.  From then on the array stays allocated until the process exits and no call of
+// this entry point allocates device memory.  The address lookup of (b) must not run during
+// a stream capture, so that first call belongs before any capture on the device.
 //
 // The array is shared by all calls and keeps the last call's contents; every entry a
 // call reads is written earlier in the same call, so nothing needs clearing, but calls
 // that overlap on the GPU (e.g. on two streams) race on it and must be serialised by
-// the caller.  The first call on a device looks up the array's device address
-// (cudaGetSymbolAddress, with that device current); make that first call before any
-// stream capture begins on the device.
+// the caller.
 #include <mutex>
 
 #include "common.cuh"
@@ -90,6 +99,14 @@ __global__ void norms_finish_kernel(int count, double *scratch)
 }
 
 }  // namespace
+
+// Resolve the scratch array on the current device (loads this module there under lazy
+// loading); called by he_create so an operator's device holds the array from set-up on.
+int he_noalloc_prepare_device()
+{
+    double *unused = nullptr;
+    return scratch_address(&unused);
+}
 
 // norms[v] = ||x_v|| for v < count, x_v = x + v*ld (complex128 device vectors of n
 // elements); `norms` is host memory of count doubles.  Blocks the host until done.

@@ -190,3 +190,14 @@ extern "C" int he_krylov_combine_coef(he_krylov *k, int which, int m, const void
     HE_CUDA_TRY(cudaStreamSynchronize(s));
     return HE_OK;
 }
+
+// binaryVersion (major * 10 + minor) of a kernel of this library as the runtime loaded it
+// on the current device: 100 for code built for sm_100a.
+extern "C" int he_binary_version(int *version)
+{
+    if (!version) return he_fail(HE_ERR_ARG, "null argument", __FILE__, __LINE__);
+    cudaFuncAttributes attributes;
+    HE_CUDA_TRY(cudaFuncGetAttributes(&attributes, (const void *)sum_kernel));
+    *version = attributes.binaryVersion;
+    return HE_OK;
+}

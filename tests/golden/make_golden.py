@@ -1,9 +1,9 @@
 """Generate the golden fixtures in tests/golden/ from the reference implementation.
 
-Run in a container that has the reference sources (it reads them from
-/root/reference, or from $HELIUM_REFERENCE):
+Run where the reference sources are available, with $HELIUM_REFERENCE naming the
+reference checkout (the folder that holds its python/ directory):
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle && HELIUM_REFERENCE=<reference checkout> python tests/golden/make_golden.py
 
 The reference's Python imports its native Fortran library at import time
 (python/native.py:8).  No Fortran compiler exists here, so the library slot is
@@ -26,7 +26,9 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[1]
-REFERENCE = Path(os.environ.get('HELIUM_REFERENCE', '/root/reference'))
+if 'HELIUM_REFERENCE' not in os.environ:
+    sys.exit('set HELIUM_REFERENCE to the reference checkout (the folder holding python/)')
+REFERENCE = Path(os.environ['HELIUM_REFERENCE'])
 os.environ['HELIUM_LIBRARY'] = str(REPO / 'oracle' / '_build' / 'libhelium_oracle.so')
 os.environ.setdefault('OMP_NUM_THREADS', '4')
 sys.path.insert(0, str(REFERENCE / 'python'))

@@ -285,3 +285,13 @@ def test_host_stream_apply_matches_device_apply():
     ref = op.host(op.apply(xs[3].to(DEVICE).to(torch.complex64), f, True, precision='complex64'))
     np.testing.assert_array_equal(outs64[3].numpy(), ref)
     op.synchronize()
+
+
+def test_kernels_run_as_sm100a_binaries():
+    """cudaFuncGetAttributes(binaryVersion) of a library kernel as loaded on the B200."""
+    import ctypes as ct
+    from laqphysics_b200._lib import LIB
+    torch.zeros(1, device=DEVICE)
+    version = ct.c_int()
+    assert LIB.he_binary_version(ct.byref(version)) == 0, LIB.he_last_error().decode()
+    assert version.value == 100
