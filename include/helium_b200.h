@@ -267,6 +267,18 @@ int he_separable_create(he_separable_handle *out, int n, int nc, int nl, const d
 int he_separable_destroy(he_separable_handle h);
 int he_separable_apply(he_separable_handle h, const void *x, void *y, double alpha_re, double alpha_im,
                        double shift, void *stream);
+/* Products per K slice of the complex64 preconditioner's TF32 tensor-core GEMMs: 3 (each
+ * operand split into two TF32 parts, FP32-class accuracy; the default) or 1.  No
+ * counterpart in the reference (its complex64 preconditioner runs cuBLAS/torch CGEMM). */
+int he_separable_set_passes(he_separable_handle h, int passes);
+/* Tile shape of the complex128 GEMMs (outputs per CTA): 0 = 64 x 128, 1 = 64 x 96,
+ * 2 = 64 x 64, 3 = 32 x 64, -1 = 64 x 64 when that grid fills two CTAs per SM, else
+ * 32 x 64 (default); the project's autotuner
+ * (SeparablePreconditioner.autotune) times them per operator.  No counterpart in the
+ * reference. */
+int he_separable_set_tile(he_separable_handle h, int shape);
+/* HE_ERR_DEVICE once (then cleared) when a bounded pipeline wait of those GEMMs ran out. */
+int he_separable_status(he_separable_handle h);
 
 /* ------------------------------------------------------------------------------------
  * Online tSURFF (complex128).

@@ -77,6 +77,9 @@ SIGNATURES = {
     'he_separable_create': (I, [ct.POINTER(P), I, I, I, P, P, P, P, P, I]),
     'he_separable_destroy': (I, [P]),
     'he_separable_apply': (I, [P, P, P, D, D, D, P]),
+    'he_separable_set_passes': (I, [P, I]),
+    'he_separable_set_tile': (I, [P, I]),
+    'he_separable_status': (I, [P]),
     'he_surface_contract': (I, [ct.c_longlong, I, I, I, I, P, P, ct.c_longlong, ct.c_longlong, ct.c_longlong,
                                 P, P, P, P, P, P, P, P]),
     'he_volkov_add': (I, [I, I, I, I, I, P, P, P, P, P, P, D, P, D, D, I, P, P, P]),

@@ -21,7 +21,7 @@ INCLUDE = HERE.parent / 'include'
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 FLAGS = ['-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC', '--expt-relaxed-constexpr', '-Xcompiler', '-Wall']
 COMPILE_FLAGS = FLAGS
-LIBS = ['-lcublas', '-lnvrtc']
+LIBS = ['-lnvrtc', '-lcuda']
 
 
 def nvcc():

@@ -90,6 +90,31 @@ class SeparablePreconditioner:
                                           HE_C64 if self.flexible else HE_C128), 'he_separable_create')
         self.handle = handle
 
+    def autotune(self, repeats=3):
+        """Time the complex128 GEMM tile shapes (he_separable_set_tile 0..3) on this
+        operator and keep the fastest; returns {shape: ms per apply}.  complex64 has one
+        shape (128 x up to 256 tcgen05 tiles) and returns {}."""
+        if self.flexible:
+            return {}
+        n = self.engine.h.size
+        x = torch.randn(n, dtype=torch.complex128, device=self.engine.device)
+        alpha = .05 / (3 + 1j * SQRT3)
+        times = {}
+        for shape in range(4):
+            check(LIB.he_separable_set_tile(self.handle, shape), 'he_separable_set_tile')
+            self.apply(x, alpha, -2.)
+            start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record()
+            for _ in range(repeats):
+                self.apply(x, alpha, -2.)
+            stop.record()
+            stop.synchronize()
+            times[shape] = start.elapsed_time(stop) / repeats
+        best = min(times, key=times.get)
+        check(LIB.he_separable_set_tile(self.handle, best), 'he_separable_set_tile')
+        self.tile_times, self.tile = times, best
+        return times
+
     def apply(self, x, alpha, shift):
         y = torch.empty_like(x)
         alpha = complex(alpha)
