@@ -272,13 +272,31 @@ int he_separable_apply(he_separable_handle h, const void *x, void *y, double alp
  * counterpart in the reference (its complex64 preconditioner runs cuBLAS/torch CGEMM). */
 int he_separable_set_passes(he_separable_handle h, int passes);
 /* Tile shape of the complex128 GEMMs (outputs per CTA): 0 = 64 x 128, 1 = 64 x 96,
- * 2 = 64 x 64, 3 = 32 x 64, -1 = 64 x 64 when that grid fills two CTAs per SM, else
- * 32 x 64 (default); the project's autotuner
+ * 2 = 64 x 64, 3 = 32 x 64, 4 = 32 x 32, -1 = 64 x 64 when that grid fills two CTAs per
+ * SM, else 32 x 32 (default); the project's autotuner
  * (SeparablePreconditioner.autotune) times them per operator.  No counterpart in the
  * reference. */
 int he_separable_set_tile(he_separable_handle h, int shape);
 /* HE_ERR_DEVICE once (then cleared) when a bounded pipeline wait of those GEMMs ran out. */
 int he_separable_status(he_separable_handle h);
+
+/* ------------------------------------------------------------------------------------
+ * Device GMRES for one Pade system of CF4.  Replaces gmres (python/implicit.py:45-74) as
+ * called by pade_step (:76-89): solves (I + i alpha (H(field) - e_ref)) x = b (velocity
+ * gauge) from x0 = b, right preconditioned by `sep` (flexible GMRES when the workspace was
+ * created flexible, for a complex64 `sep`) or, with sep NULL, by the Jacobi diagonal
+ * 1 / (1 + i alpha (diag + shift)) of the device vector `diag`; restart length <= the
+ * workspace's maxdim, at most max_restarts cycles; precision HE_C64 applies H in complex64
+ * (inner solves of a mixed-precision solve; vectors stay complex128).  Least squares by
+ * Givens rotations, the check points (every 4 iterations, flexible 2, and the restart
+ * length), the true-residual acceptance and the restarts are decided on the device; the host
+ * reads the state once per enqueued segment.  HE_ERR_NOCONV with the reference's message
+ * 'GMRES did not converge: residual=..., iterations=...' when the cycles run out.
+ * ---------------------------------------------------------------------------------- */
+int he_gmres_shifted(he_krylov_handle k, he_handle op, he_separable_handle sep, const void *diag, const void *b,
+                     void *x, const double *field, double alpha_re, double alpha_im, double e_ref, double shift,
+                     double tol, int restart, int max_restarts, int precision, int *iterations, double *residual,
+                     void *stream);
 
 /* ------------------------------------------------------------------------------------
  * Online tSURFF (complex128).

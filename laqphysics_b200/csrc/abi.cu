@@ -491,6 +491,19 @@ extern "C" int he_apply_batched(he_handle h, int count, const void *psi, void *o
                                    static_cast<cudaStream_t>(stream));
 }
 
+namespace he {
+int apply_shifted_gated(he_handle h, const void *psi, void *out, const double *field, int velocity, double alpha_re,
+                        double alpha_im, double e_ref, int precision, const int *skip, cudaStream_t stream)
+{
+    const double ga_re = -alpha_im, ga_im = alpha_re;     // i*alpha
+    if (!field) return he_fail(HE_ERR_ARG, "null argument", __FILE__, __LINE__);
+    he::FieldBatch fb = single_field(field);
+    fb.skip = skip;
+    return apply_common(h, psi, out, fb, velocity, precision, 1.0 - ga_re * e_ref, -ga_im * e_ref, ga_re, ga_im,
+                        stream);
+}
+}  // namespace he
+
 extern "C" int he_apply_shifted(he_handle h, const void *psi, void *out, const double *field, int velocity,
                                 double alpha_re, double alpha_im, double e_ref, int precision, void *stream)
 {

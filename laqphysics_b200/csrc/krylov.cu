@@ -641,6 +641,7 @@ he_krylov::~he_krylov()
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (capture_stream) cudaStreamDestroy(capture_stream);
     if (host_status) cudaFreeHost(host_status);
+    he_gmres_buffers_free(gmres);
 }
 
 namespace {

@@ -29,6 +29,9 @@ constexpr int KRYLOV_FUSED = 16;      // CGS2 with a fused update + projection s
 
 }  // namespace he
 
+struct he_gmres_buffers;                          // gmres.cu: buffers of the device GMRES driver
+void he_gmres_buffers_free(he_gmres_buffers *b);
+
 struct he_krylov {
     int device = 0;
     size_t n = 0;                 // vector length (complex elements) of one instance
@@ -56,8 +59,15 @@ struct he_krylov {
     cudaGraphExec_t graph_exec = nullptr;
     long long hint_key = 0;           // configuration the dimension hint belongs to
     int dim_seen = 0;                 // largest converged dimension of solves with that configuration
+    he_gmres_buffers *gmres = nullptr;  // device GMRES buffers (gmres.cu), created on first use
     int kb() const { return blocks; }
     size_t hs() const { return (size_t)(maxdim + 1) * maxdim; }  // Hessenberg size per instance
     size_t ws() const { return (size_t)8 * (maxdim + 1) * (maxdim + 1); }   // dense scratch per instance
     ~he_krylov();
 };
+
+namespace he {
+// CGS2 of v against the first kc basis vectors: H column += projections, h = ||v|| into
+// *hsub and the status word (skipped once the status says done).
+int krylov_cgs2(he_krylov *k, int kc, double2 *v, double2 *hcol, double2 *hsub, cudaStream_t s, double happy_below);
+}  // namespace he

@@ -98,4 +98,10 @@ int apply_batched_gated(he_operator *h, int count, const void *psi, void *out, c
 // derivative of H(field) along `direction`), complex128, one instance; skipped while *skip != 0.
 int dipole_accumulate(he_operator *h, const double2 *psi, double2 *out, const double direction[3], const int *skip,
                       cudaStream_t stream);
+// out = psi + i alpha (H(field) psi - e_ref psi), kernels skipped while *skip != 0.
+int apply_shifted_gated(he_operator *h, const void *psi, void *out, const double *field, int velocity, double alpha_re,
+                        double alpha_im, double e_ref, int precision, const int *skip, cudaStream_t stream);
+// Separable preconditioner apply (separable.cu) whose kernels return at once while *gate != 0.
+int separable_apply_gated(he_separable *h, const double2 *x, double2 *y, double2 alpha, double shift,
+                          const int *gate, cudaStream_t s);
 }  // namespace he

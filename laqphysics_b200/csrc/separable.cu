@@ -49,9 +49,9 @@ namespace he {
 constexpr int DG_BK = 8;
 constexpr int DG_LD = DG_BK + 4;
 constexpr int DG_STAGES = 4;
-template <int WM, int WN> constexpr size_t dg_smem()
+template <int WM, int WN, int FM, int FN> constexpr size_t dg_smem()
 {
-    return (size_t)DG_STAGES * (32 * WM + 32 * WN) * DG_LD * sizeof(double2);
+    return (size_t)DG_STAGES * (8 * FM * WM + 8 * FN * WN) * DG_LD * sizeof(double2);
 }
 
 // Resolvent division fused into a product's store: out /= 1 + i alpha (e_row + e_col + shift),
@@ -89,12 +89,13 @@ __device__ __forceinline__ void cp16(void *smem, const void *gmem, bool ok)
 
 // out_c = (M_{sel[c]} X_c)^T for every channel c (grid.z): M row-major n x n (mats + l n^2),
 // X_c(k, j) = x[(c n + j) n + k], out_c(j, i) = out[(c n + i) n + j].
-template <int WM, int WN>
+template <int WM, int WN, int FM, int FN>
 __global__ void __launch_bounds__(32 * WM * WN, 1)
 sep_dgemm_kernel(int n, const double2 *__restrict__ mats, const int *__restrict__ sel, const double2 *__restrict__ x,
-                 double2 *__restrict__ out, Resolvent<double> rs)
+                 double2 *__restrict__ out, Resolvent<double> rs, const int *gate)
 {
-    constexpr int BM = 32 * WM, BN = 32 * WN, THREADS = 32 * WM * WN;
+    if (gate && *gate) return;
+    constexpr int BM = 8 * FM * WM, BN = 8 * FN * WN, THREADS = 32 * WM * WN;
     constexpr int A_ELEMS = BM * DG_LD, B_ELEMS = BN * DG_LD;
     extern __shared__ double2 dsm[];
     double2 *As = dsm, *Bs = dsm + DG_STAGES * A_ELEMS;
@@ -103,7 +104,7 @@ sep_dgemm_kernel(int n, const double2 *__restrict__ mats, const int *__restrict_
     const double2 *M = mats + (size_t)sel[c] * nn;
     const double2 *X = x + (size_t)c * nn;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int wm = (warp % WM) * 32, wn = (warp / WM) * 32;
+    const int wm = (warp % WM) * 8 * FM, wn = (warp / WM) * 8 * FN;
     const int nk = (n + DG_BK - 1) / DG_BK;
 
     auto load = [&](int kt, int stage) {
@@ -121,11 +122,11 @@ sep_dgemm_kernel(int n, const double2 *__restrict__ mats, const int *__restrict_
         }
     };
 
-    double cr[4][4][2], ci[4][4][2];
+    double cr[FM][FN][2], ci[FM][FN][2];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < FM; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) cr[a][b][0] = cr[a][b][1] = ci[a][b][0] = ci[a][b][1] = 0.0;
+        for (int b = 0; b < FN; ++b) cr[a][b][0] = cr[a][b][1] = ci[a][b][0] = ci[a][b][1] = 0.0;
 
 #pragma unroll
     for (int s = 0; s < DG_STAGES - 1; ++s) {
@@ -140,25 +141,25 @@ sep_dgemm_kernel(int n, const double2 *__restrict__ mats, const int *__restrict_
         const double2 *a = As + (kt % DG_STAGES) * A_ELEMS, *b = Bs + (kt % DG_STAGES) * B_ELEMS;
 #pragma unroll
         for (int kk = 0; kk < DG_BK; kk += 4) {
-            double2 fa[4], fb[4];
+            double2 fa[FM], fb[FN];
 #pragma unroll
-            for (int m = 0; m < 4; ++m) fa[m] = a[(wm + m * 8 + (lane >> 2)) * DG_LD + kk + (lane & 3)];
+            for (int m = 0; m < FM; ++m) fa[m] = a[(wm + m * 8 + (lane >> 2)) * DG_LD + kk + (lane & 3)];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) fb[q] = b[(wn + q * 8 + (lane >> 2)) * DG_LD + kk + (lane & 3)];
-            // the two halves of each complex product go 32 MMAs apart, so no MMA waits on
-            // the one before it
+            for (int q = 0; q < FN; ++q) fb[q] = b[(wn + q * 8 + (lane >> 2)) * DG_LD + kk + (lane & 3)];
+            // the two halves of each complex product go 2 FM FN MMAs apart, so no MMA waits
+            // on the one before it
 #pragma unroll
-            for (int m = 0; m < 4; ++m)
+            for (int m = 0; m < FM; ++m)
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
+                for (int q = 0; q < FN; ++q) {
                     dmma(cr[m][q][0], cr[m][q][1], fa[m].x, fb[q].x);
                     dmma(ci[m][q][0], ci[m][q][1], fa[m].x, fb[q].y);
                 }
 #pragma unroll
-            for (int m = 0; m < 4; ++m) {
+            for (int m = 0; m < FM; ++m) {
                 const double nai = -fa[m].y;
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
+                for (int q = 0; q < FN; ++q) {
                     dmma(cr[m][q][0], cr[m][q][1], nai, fb[q].y);
                     dmma(ci[m][q][0], ci[m][q][1], fa[m].y, fb[q].x);
                 }
@@ -169,11 +170,11 @@ sep_dgemm_kernel(int n, const double2 *__restrict__ mats, const int *__restrict_
 
     double2 *O = out + (size_t)c * nn;
 #pragma unroll
-    for (int m = 0; m < 4; ++m) {
+    for (int m = 0; m < FM; ++m) {
         const int i = i0 + wm + m * 8 + (lane >> 2);
         if (i >= n) continue;
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
+        for (int q = 0; q < FN; ++q)
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int j = j0 + wn + q * 8 + 2 * (lane & 3) + h;
@@ -208,6 +209,7 @@ struct TcArgs {
     double2 *y;                                  // complex128 output, ((c n + i) n + j)
     Resolvent<float> rs;
     int *err;
+    const int *gate;                             // non-zero at launch: return without work
 };
 
 __global__ void __launch_bounds__(TG_THREADS, 1)
@@ -215,6 +217,7 @@ sep_tf32_kernel(const __grid_constant__ CUtensorMap map_ah, const __grid_constan
                 const __grid_constant__ CUtensorMap map_xh, const __grid_constant__ CUtensorMap map_xl, TcArgs g)
 {
     using namespace sm100;
+    if (g.gate && *g.gate) return;               // uniform over the CTA, before any TMEM use
     extern __shared__ uint8_t tsm_raw[];
     const unsigned base_s = saddr(tsm_raw);
     uint8_t *tsm = tsm_raw + (((base_s + 1023u) & ~1023u) - base_s);  // 1024-byte aligned tiles
@@ -353,8 +356,9 @@ sep_tf32_kernel(const __grid_constant__ CUtensorMap map_ah, const __grid_constan
 
 // complex128 x -> TF32 hi/lo planes, row (c n + j) of the plane = column j of Psi_c.
 __global__ void split_tf32_kernel(size_t rows, int n, int ld, const double2 *__restrict__ x, float *__restrict__ hi,
-                                  float *__restrict__ lo)
+                                  float *__restrict__ lo, const int *gate)
 {
+    if (gate && *gate) return;
     const size_t total = rows * (size_t)n;
     for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < total; p += (size_t)gridDim.x * blockDim.x) {
         const size_t r = p / n;
@@ -462,56 +466,63 @@ void embed(const double *mats, int nl, int n, int ld, std::vector<float> &hi, st
             }
 }
 
-template <int WM, int WN>
-int dgemm_chain(he_separable *h, const double2 *x, double2 *y, double2 alpha, double shift, cudaStream_t s)
+template <int WM, int WN, int FM, int FN>
+int dgemm_chain(he_separable *h, const double2 *x, double2 *y, double2 alpha, double shift, const int *gate,
+                cudaStream_t s)
 {
     const int n = h->n;
     const double2 *S = static_cast<const double2 *>(h->S), *I = static_cast<const double2 *>(h->I);
     double2 *b0 = static_cast<double2 *>(h->buf[0]), *b1 = static_cast<double2 *>(h->buf[1]);
-    const void *kernel = (const void *)sep_dgemm_kernel<WM, WN>;
-    constexpr size_t smem = dg_smem<WM, WN>();
+    const void *kernel = (const void *)sep_dgemm_kernel<WM, WN, FM, FN>;
+    constexpr size_t smem = dg_smem<WM, WN, FM, FN>();
+    constexpr int BM = 8 * FM * WM, BN = 8 * FN * WN;
     HE_CUDA_TRY(he_smem_limit(kernel, smem));
-    const dim3 grid((n + 32 * WM - 1) / (32 * WM), (n + 32 * WN - 1) / (32 * WN), h->nc);
+    const dim3 grid((n + BM - 1) / BM, (n + BN - 1) / BN, h->nc);
     const int threads = 32 * WM * WN;
     Resolvent<double> none{nullptr, nullptr, nullptr, mk<double>(0, 0), 0.0, 0};
     Resolvent<double> rs{static_cast<const double2 *>(h->evals), h->l2, h->l1, alpha, shift, 1};
     // rows of the second product run over r2 (S_{l2}^-1), its columns over r1
-    sep_dgemm_kernel<WM, WN><<<grid, threads, smem, s>>>(n, I, h->l1, x, b0, none);
-    sep_dgemm_kernel<WM, WN><<<grid, threads, smem, s>>>(n, I, h->l2, b0, b1, rs);
-    sep_dgemm_kernel<WM, WN><<<grid, threads, smem, s>>>(n, S, h->l1, b1, b0, none);
-    sep_dgemm_kernel<WM, WN><<<grid, threads, smem, s>>>(n, S, h->l2, b0, y, none);
+    sep_dgemm_kernel<WM, WN, FM, FN><<<grid, threads, smem, s>>>(n, I, h->l1, x, b0, none, gate);
+    sep_dgemm_kernel<WM, WN, FM, FN><<<grid, threads, smem, s>>>(n, I, h->l2, b0, b1, rs, gate);
+    sep_dgemm_kernel<WM, WN, FM, FN><<<grid, threads, smem, s>>>(n, S, h->l1, b1, b0, none, gate);
+    sep_dgemm_kernel<WM, WN, FM, FN><<<grid, threads, smem, s>>>(n, S, h->l2, b0, y, none, gate);
     HE_CUDA_TRY(cudaGetLastError());
     return HE_OK;
 }
 
 // Default tile shape (measured on B200 at n = 560, nc = 43 and n = 132, nc = 17): 64 x 64
 // tiles at two CTAs per SM (8 warps per SM, the first CTA's store overlapping the second's
-// loads) once the grid fills a wave of them; 32 x 64 tiles for smaller grids, which keep more
-// SMs busy.  SeparablePreconditioner.autotune times all four shapes per operator.
-int apply_c128(he_separable *h, const double2 *x, double2 *y, double2 alpha, double shift, cudaStream_t s)
+// loads) once the grid fills a wave of them; below that, 32 x 32 tiles of four 16 x 16 warps,
+// which give small problems several warps per SM.  SeparablePreconditioner.autotune times
+// every shape per operator.
+int apply_c128(he_separable *h, const double2 *x, double2 *y, double2 alpha, double shift, const int *gate,
+               cudaStream_t s)
 {
     int shape = h->tile;
     if (shape < 0) {
         const long long ctas64 = (long long)((h->n + 63) / 64) * ((h->n + 63) / 64) * h->nc;
-        shape = ctas64 >= 2LL * sm_count(h->device) ? 2 : 3;
+        shape = ctas64 >= 2LL * sm_count(h->device) ? 2 : 4;
     }
     switch (shape) {
-    case 0: return dgemm_chain<2, 4>(h, x, y, alpha, shift, s);
-    case 1: return dgemm_chain<2, 3>(h, x, y, alpha, shift, s);
-    case 2: return dgemm_chain<2, 2>(h, x, y, alpha, shift, s);
-    default: return dgemm_chain<1, 2>(h, x, y, alpha, shift, s);
+    case 0: return dgemm_chain<2, 4, 4, 4>(h, x, y, alpha, shift, gate, s);
+    case 1: return dgemm_chain<2, 3, 4, 4>(h, x, y, alpha, shift, gate, s);
+    case 2: return dgemm_chain<2, 2, 4, 4>(h, x, y, alpha, shift, gate, s);
+    case 3: return dgemm_chain<1, 2, 4, 4>(h, x, y, alpha, shift, gate, s);
+    default: return dgemm_chain<2, 2, 2, 2>(h, x, y, alpha, shift, gate, s);
     }
 }
 
-int apply_c64(he_separable *h, const double2 *x, double2 *y, double2 alpha, double shift, cudaStream_t s)
+int apply_c64(he_separable *h, const double2 *x, double2 *y, double2 alpha, double shift, const int *gate,
+              cudaStream_t s)
 {
     const int n = h->n;
     HE_CUDA_TRY(he_smem_limit((const void *)sep_tf32_kernel, TG_SMEM));
-    split_tf32_kernel<<<4 * 148, 256, 0, s>>>((size_t)n * h->nc, n, h->ld, x, h->plane[0], h->plane[1]);
+    split_tf32_kernel<<<4 * 148, 256, 0, s>>>((size_t)n * h->nc, n, h->ld, x, h->plane[0], h->plane[1], gate);
     const dim3 grid((2 * n + TG_BM - 1) / TG_BM, h->ntn, h->nc);
     TcArgs g{};
     g.n = n; g.nc = h->nc; g.bn = h->bn; g.kt = h->kt; g.passes = h->passes; g.arows = 2 * n; g.ld = h->ld;
     g.err = h->err;
+    g.gate = gate;
     g.rs = Resolvent<float>{nullptr, nullptr, nullptr, mk<float>(0, 0), 0.f, 0};
     auto run = [&](const CUtensorMap *m, const int *sel, const CUtensorMap *in, int out_pair, int mode,
                    Resolvent<float> rs) {
@@ -577,8 +588,13 @@ extern "C" int he_separable_create(he_separable **out, int n, int nc, int nl, co
     } else {
         h->ld = (2 * n + 3) / 4 * 4;                       // 16-byte row stride for TMA
         h->kt = (2 * n + TG_BK - 1) / TG_BK;
+        // N tiles: as few as the 256 TMEM columns allow, more when the grid would leave SMs idle
+        const int mtiles = (2 * n + TG_BM - 1) / TG_BM;
         h->ntn = (n + TG_BN_MAX - 1) / TG_BN_MAX;
+        const int fill = (sm_count(h->device) + mtiles * nc - 1) / (mtiles * nc);
+        h->ntn = std::max(h->ntn, std::min(fill, std::max(1, n / 32)));
         h->bn = ((n + h->ntn - 1) / h->ntn + 15) / 16 * 16;
+        h->ntn = (n + h->bn - 1) / h->bn;
         std::vector<float2> ev((size_t)nl * n);
         for (size_t k = 0; k < ev.size(); ++k) ev[k] = make_float2((float)evals[2 * k], (float)evals[2 * k + 1]);
         if (e == cudaSuccess) e = copy(&h->evals, ev.data(), ev.size() * sizeof(float2));
@@ -627,10 +643,11 @@ extern "C" int he_separable_set_passes(he_separable *h, int passes)
 }
 
 // Tile shape of the complex128 GEMMs: 0 = 64 x 128, 1 = 64 x 96, 2 = 64 x 64, 3 = 32 x 64
-// outputs per CTA, -1 = the default rule of apply_c128.
+// (32 x 32 per warp), 4 = 32 x 32 (16 x 16 per warp) outputs per CTA, -1 = the default rule
+// of apply_c128.
 extern "C" int he_separable_set_tile(he_separable *h, int shape)
 {
-    if (!h || shape < -1 || shape > 3) return he_fail(HE_ERR_ARG, "tile shape must be -1..3", __FILE__, __LINE__);
+    if (!h || shape < -1 || shape > 4) return he_fail(HE_ERR_ARG, "tile shape must be -1..4", __FILE__, __LINE__);
     h->tile = shape;
     return HE_OK;
 }
@@ -654,8 +671,15 @@ extern "C" int he_separable_apply(he_separable *h, const void *x, void *y, doubl
 {
     if (!h || !x || !y || x == y) return he_fail(HE_ERR_ARG, "bad separable apply argument", __FILE__, __LINE__);
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const double2 alpha = mk<double>(alpha_re, alpha_im);
-    if (h->precision == HE_C128)
-        return apply_c128(h, static_cast<const double2 *>(x), static_cast<double2 *>(y), alpha, shift, s);
-    return apply_c64(h, static_cast<const double2 *>(x), static_cast<double2 *>(y), alpha, shift, s);
+    return he::separable_apply_gated(h, static_cast<const double2 *>(x), static_cast<double2 *>(y),
+                                     mk<double>(alpha_re, alpha_im), shift, nullptr, s);
+}
+
+// The same apply whose kernels return without work while *gate != 0 (the GMRES driver's
+// gate words; gate may be null).
+int he::separable_apply_gated(he_separable *h, const double2 *x, double2 *y, double2 alpha, double shift,
+                              const int *gate, cudaStream_t s)
+{
+    if (h->precision == HE_C128) return apply_c128(h, x, y, alpha, shift, gate, s);
+    return apply_c64(h, x, y, alpha, shift, gate, s);
 }

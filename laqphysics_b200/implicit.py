@@ -24,7 +24,7 @@ import numpy as np
 import torch
 from scipy.linalg import eig, inv
 
-from ._lib import LIB, HE_C128, HE_C64, check
+from ._lib import LIB, HE_C128, HE_C64, HE_ERR_NOCONV, check
 from .engine import _stream
 from .torch_backend import workspace
 
@@ -91,7 +91,7 @@ class SeparablePreconditioner:
         self.handle = handle
 
     def autotune(self, repeats=3):
-        """Time the complex128 GEMM tile shapes (he_separable_set_tile 0..3) on this
+        """Time the complex128 GEMM tile shapes (he_separable_set_tile 0..4) on this
         operator and keep the fastest; returns {shape: ms per apply}.  complex64 has one
         shape (128 x up to 256 tcgen05 tiles) and returns {}."""
         if self.flexible:
@@ -100,7 +100,7 @@ class SeparablePreconditioner:
         x = torch.randn(n, dtype=torch.complex128, device=self.engine.device)
         alpha = .05 / (3 + 1j * SQRT3)
         times = {}
-        for shape in range(4):
+        for shape in range(5):
             check(LIB.he_separable_set_tile(self.handle, shape), 'he_separable_set_tile')
             self.apply(x, alpha, -2.)
             start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -219,22 +219,74 @@ def gmres(apply, b, preconditioner, x0=None, tol=1e-11, restart=32, max_restarts
     raise RuntimeError(f'GMRES did not converge: residual={true:.3e}, iterations={iterations}')
 
 
+_DEVICE_SOLVES = [True]
+
+
+def device_solves(flag=True):
+    """Run the Pade solves of pade_step / cf4_step as whole device GMRES solves
+    (he_gmres_shifted: least squares, true-residual acceptance and restarts decided on the
+    device, one status read per enqueued segment) when the engine and preconditioner allow
+    it (the default), or through the host-driven :func:`gmres` loop."""
+    _DEVICE_SOLVES[0] = bool(flag)
+
+
+def _device_solver(engine, separable):
+    """The engine/preconditioner pair the device GMRES can run: this package's engine with its
+    own shifted operator, and the separable preconditioner or the Jacobi diagonal."""
+    from .engine import B200Hamiltonian
+    if not _DEVICE_SOLVES[0] or not isinstance(engine, B200Hamiltonian):
+        return False
+    if type(engine).apply_shifted is not B200Hamiltonian.apply_shifted:
+        return False
+    return separable is None or isinstance(separable, SeparablePreconditioner)
+
+
+def device_gmres(engine, b, field, alpha, reference_energy, separable, shift, tol=1e-11, restart=32,
+                 max_restarts=10, precision='complex128'):
+    """GMRES (python/implicit.py:45-74) for (I + i alpha (H(field) - E_ref)) s = b, right
+    preconditioned by ``separable`` (flexible when it is complex64) or, with ``separable``
+    None, by the Jacobi diagonal 1 / (1 + i alpha (diag + shift)); precision 'complex64'
+    applies H in complex64 (the inner solves of a mixed-precision Pade solve).  The whole
+    solve runs on the device (he_gmres_shifted); results, iteration counts and the
+    'GMRES did not converge' failure follow the reference's rules."""
+    flexible = bool(getattr(separable, 'flexible', False))
+    ws = workspace(b.numel(), restart, b.device, flexible)
+    x = torch.empty_like(b)
+    f = np.ascontiguousarray(field, dtype=np.float64)
+    alpha = complex(alpha)
+    iterations, residual = ct.c_int(), ct.c_double()
+    code = HE_C64 if precision == 'complex64' else HE_C128
+    status = LIB.he_gmres_shifted(ws.handle, engine.op.handle, separable.handle if separable is not None else None,
+                                  None if separable is not None else _vp(engine.diagonal), _vp(b), _vp(x),
+                                  f.ctypes.data, alpha.real, alpha.imag, float(reference_energy), float(shift),
+                                  float(tol), int(restart), int(max_restarts), code, ct.byref(iterations),
+                                  ct.byref(residual), _stream(b.device))
+    if status == HE_ERR_NOCONV:
+        raise RuntimeError(LIB.he_last_error().decode().split(' (')[0])
+    check(status, 'he_gmres_shifted')
+    return x, {'iterations': iterations.value, 'relative_residual': residual.value}
+
+
 INNER_TOLERANCE = 1e-5   # relative residual of each complex64 inner solve of a mixed Pade solve
 
 
-def defect_corrected_solve(A, A32, b, M, tol, flexible, restart, corrections=8):
+def defect_corrected_solve(A, A32, b, M, tol, flexible, restart, corrections=8, inner=None):
     """Solve A s = b to a complex128 relative residual <= tol by defect correction: each
     sweep solves A32 d = r by GMRES with the complex64 operator A32 (FP32 accumulation)
     to INNER_TOLERANCE, adds d to s and recomputes r = b - A s with the complex128
     operator.  Each sweep gains about five digits while that stays above the complex64
-    operator's own error, so a 1e-11 solve takes two or three sweeps.  Raises the
+    operator's own error, so a 1e-11 solve takes two or three sweeps.  ``inner(r, tol)``,
+    when given, replaces the host-driven inner GMRES (the device solver).  Raises the
     reference's 'GMRES did not converge' message when the sweeps run out."""
     s = torch.zeros_like(b)
     r = b
     bnorm = norm(b)
     iterations, relative = 0, 1.
     for sweep in range(corrections):
-        d, info = gmres(A32, r, M, tol=max(INNER_TOLERANCE, tol), flexible=flexible, restart=restart)
+        if inner is not None:
+            d, info = inner(r, max(INNER_TOLERANCE, tol))
+        else:
+            d, info = gmres(A32, r, M, tol=max(INNER_TOLERANCE, tol), flexible=flexible, restart=restart)
         iterations += info['iterations']
         s = axpby(1, s, 1, d, out=s)
         r = axpby(1, b, -1, A(s))
@@ -267,13 +319,22 @@ def pade_step(engine, x, field, dt, reference_energy=0., tol=1e-11, precision='c
             M = (lambda y, alpha=alpha: separable.apply(y, alpha, squared - reference_energy))
         else:
             M = _jacobi(engine.diagonal, alpha, squared - reference_energy)
+        restart = 16 if flexible else 32
+        on_device = _device_solver(engine, separable)
         if precision == 'mixed':
             def A32(y, alpha=alpha):
                 return engine.apply_shifted(y.to(torch.complex64), field, alpha, reference_energy,
                                             velocity=True).to(torch.complex128)
-            s, info = defect_corrected_solve(A, A32, x, M, tol, flexible, 16 if flexible else 32)
+
+            def inner(r, inner_tol, alpha=alpha):
+                return device_gmres(engine, r, field, alpha, reference_energy, separable, squared - reference_energy,
+                                    inner_tol, restart, precision='complex64')
+            s, info = defect_corrected_solve(A, A32, x, M, tol, flexible, restart, inner=inner if on_device else None)
+        elif on_device:
+            s, info = device_gmres(engine, x, field, alpha, reference_energy, separable, squared - reference_energy,
+                                   tol, restart)
         else:
-            s, info = gmres(A, x, M, tol=tol, flexible=flexible, restart=16 if flexible else 32)
+            s, info = gmres(A, x, M, tol=tol, flexible=flexible, restart=restart)
         x = axpby(2, s, -1, x)
         iterations += info['iterations']
         residual = max(residual, info['relative_residual'])

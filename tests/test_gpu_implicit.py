@@ -193,3 +193,51 @@ def test_separable_gemm_chain_matches_fp64(n, precision, passes, bound):
         assert err < bound, err
     finally:
         LIB.he_separable_destroy(handle)
+
+
+@pytest.mark.parametrize('preconditioner', ['complex128', 'complex64', 'jacobi'])
+def test_device_gmres_matches_host_driven_gmres(preconditioner):
+    """The device-driven GMRES (he_gmres_shifted: Givens least squares, true-residual
+    acceptance and restarts on the device) against the host-driven loop (lstsq on the host,
+    python/implicit.py:45-74's decisions) on the same Pade system: same iteration count, same
+    acceptance, solutions within 1e-12 relative L2, and both solve the system to tol."""
+    from laqphysics_b200.implicit import SeparablePreconditioner, device_gmres, gmres, _jacobi
+    g, h, op = _cf4_operator()
+    sep = None if preconditioner == 'jacobi' else SeparablePreconditioner(op, preconditioner)
+    flexible = bool(getattr(sep, 'flexible', False))
+    field = np.array([.02, .01, .03])
+    alpha = float(g['dt']) / 2 / (3 + 1j * np.sqrt(3))
+    eref, tol = float(g['e_ref']), 1e-12
+    shift = float(field @ field) - eref
+    b = op.state(g['x'])
+    restart = 16 if flexible else 32
+    x_dev, info_dev = device_gmres(op, b, field, alpha, eref, sep, shift, tol, restart)
+    A = lambda y: op.apply_shifted(y, field, alpha, eref, velocity=True)
+    M = (lambda y: sep.apply(y, alpha, shift)) if sep is not None else _jacobi(op.diagonal, alpha, shift)
+    x_host, info_host = gmres(A, b, M, tol=tol, flexible=flexible, restart=restart)
+    assert info_dev['iterations'] == info_host['iterations']
+    assert info_dev['relative_residual'] <= tol and info_host['relative_residual'] <= tol
+    a, r = op.host(x_dev), op.host(x_host)
+    assert np.linalg.norm(a - r) / np.linalg.norm(r) < 1e-12
+    res = op.host(b) - op.host(A(x_dev))
+    assert np.linalg.norm(res) <= 1.01 * tol * np.linalg.norm(op.host(b))
+
+
+def test_device_gmres_restarts_and_reports_non_convergence():
+    """Short restart lengths force several device cycles (restart from the accepted
+    candidate); a tolerance below what the cycles reach raises the reference's message."""
+    from laqphysics_b200.implicit import SeparablePreconditioner, device_gmres, gmres
+    g, h, op = _cf4_operator()
+    sep = SeparablePreconditioner(op)
+    field = np.array([.02, .01, .03])
+    alpha = float(g['dt']) / 2 / (3 + 1j * np.sqrt(3))
+    eref = float(g['e_ref'])
+    shift = float(field @ field) - eref
+    b = op.state(g['x'])
+    x_dev, info_dev = device_gmres(op, b, field, alpha, eref, sep, shift, 1e-12, restart=2, max_restarts=10)
+    A = lambda y: op.apply_shifted(y, field, alpha, eref, velocity=True)
+    x_host, info_host = gmres(A, b, lambda y: sep.apply(y, alpha, shift), tol=1e-12, restart=2, max_restarts=10)
+    assert info_dev['iterations'] == info_host['iterations'] > 2
+    assert np.linalg.norm(op.host(x_dev) - op.host(x_host)) <= 1e-12 * np.linalg.norm(op.host(x_host))
+    with pytest.raises(RuntimeError, match='GMRES did not converge'):
+        device_gmres(op, b, field, alpha, eref, sep, shift, 1e-16, restart=2, max_restarts=2)

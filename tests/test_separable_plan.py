@@ -9,9 +9,15 @@ import pytest
 TG_BM, TG_BK, TG_BN_MAX = 128, 32, 256
 
 
-def geometry(n):
+def geometry(n, nc, sms=148):
+    """he_separable_create's complex64 geometry: N tiles as few as the TMEM columns allow,
+    more when the grid would leave SMs idle."""
+    mtiles = -(-2 * n // TG_BM)
     ntn = -(-n // TG_BN_MAX)
+    fill = -(-sms // (mtiles * nc))
+    ntn = max(ntn, min(fill, max(1, n // 32)))
     bn = (-(-n // ntn) + 15) // 16 * 16
+    ntn = -(-n // bn)
     ld = (2 * n + 3) // 4 * 4
     return ntn, bn, ld, -(-2 * n // TG_BK)
 
@@ -22,10 +28,9 @@ def tf32(x):
     return ((b + np.uint32(0x1000)) & np.uint32(0xFFFFE000)).view(np.float32)
 
 
-@pytest.mark.parametrize('n', [7, 132, 150, 257, 300, 560])
-def test_epilogue_writes_every_output_once_in_bounds(n):
-    nc = 2
-    ntn, bn, ld, _ = geometry(n)
+@pytest.mark.parametrize('n, nc', [(7, 2), (132, 2), (132, 17), (150, 2), (257, 2), (300, 3), (560, 2), (560, 43)])
+def test_epilogue_writes_every_output_once_in_bounds(n, nc):
+    ntn, bn, ld, _ = geometry(n, nc)
     assert bn % 16 == 0 and 16 <= bn <= TG_BN_MAX and (ntn - 1) * bn < n <= ntn * bn
     assert ld % 4 == 0 and ld >= 2 * n
     hits = np.zeros((nc, n, n), int)
