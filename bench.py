@@ -40,13 +40,15 @@ def parse():
     p.add_argument('--impl', choices=['b200', 'reference'], default='b200')
     p.add_argument('--no-cpu-baseline', action='store_true')
     p.add_argument('--no-arnoldi', action='store_true', help='skip the Arnoldi steps/s leg')
+    p.add_argument('--cfg2-steps', type=int, default=4,
+                   help='steps of the mixed-precision config slice on the microbenchmark grid (0: skip)')
     p.add_argument('--path', type=int, default=1, choices=[0, 1, 2, 3],
                    help='H·psi kernel path of the microbenchmark operator (he_set_path; 1 = default fused kernels)')
     p.add_argument('--adjoint-steps', type=int, default=128, help='adjoint leg: Arnoldi steps (dt 0.005)')
     p.add_argument('--adjoint-knots', type=int, default=32, help='adjoint leg: field samples')
     p.add_argument('--adjoint-checkpoint', type=int, default=None,
                    help='adjoint leg: steps between kept states (default: every state resident in HBM)')
-    p.add_argument('--profile', choices=['c128', 'c64', 'arnoldi', 'arnoldi-split', 'batched', 'batched-attempt', 'cf4',
+    p.add_argument('--profile', choices=['c128', 'c64', 'arnoldi', 'arnoldi-split', 'batched', 'batched-attempt', 'cf4', 'cfg2',
                                          'adjoint', 'concurrent'],
                    default=None,
                    help='run only W+K applications of one precision (for ncu captures); prints no JSON')
@@ -414,6 +416,70 @@ def concurrent_leg(torch, device, count=8, steps=3):
     return out
 
 
+def cfg2_slice_leg(torch, device, steps=6):
+    """Bounded slice of the mixed-precision full propagation on the microbenchmark grid
+    (n = 560, nc = 43, real to 120 a.u.): sin^2 pulse omega 1.6 a.u., 20 cycles, peak
+    0.02 a.u., velocity gauge, Arnoldi order 16, dt 0.05, Krylov tolerance 1e-10, tSURFF at
+    R_s = 100 a.u. with the He+ n <= 3 channels (6 labels), default energy grid (397) and
+    32 polar directions.  `steps` steps from the middle of the pulse (t0 = 39.25 a.u.), started
+    from the ground state, a surface sample after every step (channel functions propagated
+    back from the slice's end; Volkov phases referenced to t0), in complex128 and in mixed
+    precision (complex64 H·psi inside the complex128 Krylov).  Reports steps/s, H·psi per
+    step, the slice's spectrum and state errors of the mixed run against the complex128 run,
+    and the projection to the full 1571-step run at the measured rates."""
+    from laqphysics_b200 import workloads
+    from laqphysics_b200.engine import B200Hamiltonian
+    from laqphysics_b200.ionic_adjoint import channel_functions
+    from laqphysics_b200.pulses import Pulse
+    from laqphysics_b200.surface3d import Ionic
+    from laqphysics_b200.surface_contract import SurfaceContractor
+    from laqphysics_b200.tsurff_run import run, spectrum_error
+    h, hreal = workloads.hpsi_microbench(), workloads.hpsi_microbench(ecs_angle=0.)
+    base = h.uncoupled
+    base.prepare_surface(100.)
+    h.prepare_surface(100.)
+    labels = [(1, 0, 0), (2, 0, 0), (2, 1, 0), (3, 0, 0), (3, 1, 0), (3, 2, 0)]
+    ion = Ionic(base, {0})
+    contractor = SurfaceContractor(base, ion, labels, labels, list(range(6)), True, h.transform, device)
+    pulse = Pulse(omega=1.6, cycles=20, field=.02)
+    avec = lambda t: np.array([0., 0., float(pulse.vector(t))])
+    dt = .05
+    t0 = round(pulse.duration / 2 / dt) * dt
+    t_ground = time.perf_counter()
+    _, g, _ = hreal.ground(tol=1e-9)
+    t_ground = time.perf_counter() - t_ground
+    ratio = np.sqrt(h.grid.weights / hreal.grid.weights)
+    psi0 = (g.reshape(h.shape, order='F') * ratio[:, None, None] * ratio[None, :, None]).ravel(order='F')
+    chi = channel_functions(ion, labels, avec, t0 + dt * np.arange(steps + 1), device)
+    engine = B200Hamiltonian(h, device)
+    config = {'M': 0}
+    out = {'workload': f'mixed-precision config slice: n={h.n} nc={h.nc} (N={h.size:,}), velocity gauge, Arnoldi order 16, '
+                       f'dt 0.05, tol 1e-10, {steps} steps from t0={t0:.2f} a.u. (mid-pulse, 20-cycle sin^2, '
+                       f'omega 1.6, 0.02 a.u.), ground-state start, tSURFF at R_s=100 with He+ n<=3 (6 labels)',
+           'steps': steps, 'ground_state_s': t_ground}
+    results = {}
+    for precision in ('complex128', 'mixed'):
+        applies = engine.apply_count
+        torch.cuda.synchronize(device)
+        start = time.perf_counter()
+        acc, psi, dim = run(engine, contractor, config, psi0, avec, dt, steps, chi, precision, tol=1e-10, maxdim=16,
+                            t0=t0)
+        torch.cuda.synchronize(device)
+        seconds = time.perf_counter() - start
+        results[precision] = (acc, psi)
+        out[precision] = {'steps_per_s': steps / seconds, 's_per_step': seconds / steps,
+                          'hpsi_per_step': (engine.apply_count - applies) / steps, 'mean_dimension': dim,
+                          'full_run_projection_h': 1571 * seconds / steps / 3600}
+    rel, per_label = spectrum_error(results['mixed'][0], results['complex128'][0])
+    a, b = results['mixed'][1], results['complex128'][1]
+    out['spectrum_rel_l2_mixed_vs_fp64'] = rel
+    out['angle_integrated_rel_max_mixed_vs_fp64'] = per_label
+    out['state_rel_l2_mixed_vs_fp64'] = float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+    out['norm_error_mixed_vs_fp64'] = abs(float(torch.linalg.vector_norm(a)) - float(torch.linalg.vector_norm(b)))
+    out['mixed_speedup'] = out['mixed']['steps_per_s'] / out['complex128']['steps_per_s']
+    return out
+
+
 def cf4_leg(torch, device, steps=10):
     """CF4 Magnus steps, each exponential a [2/2] Pade pair of shifted solves by right-
     preconditioned GMRES (the reference's implicit.py:45-109 path), on the Arnoldi grid
@@ -583,6 +649,9 @@ def main():
         return 0
     if args.profile == 'cf4':
         print(json.dumps(cf4_leg(torch, device, steps=args.steps)), flush=True)
+        return 0
+    if args.profile == 'cfg2':
+        print(json.dumps(cfg2_slice_leg(torch, device, steps=args.steps)), flush=True)
         return 0
     if args.profile == 'arnoldi-split':   # CUDA-event cost of one H·psi and of 12-iteration attempts
         from laqphysics_b200 import workloads
@@ -774,6 +843,8 @@ def main():
         line['spectrum'] = spectrum_leg(torch, device)
         line['cf4'] = cf4_leg(torch, device)
         line['concurrent'] = concurrent_leg(torch, device)
+        if args.cfg2_steps:
+            line['cfg2_slice'] = cfg2_slice_leg(torch, device, steps=args.cfg2_steps)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         os.environ.setdefault('OMP_NUM_THREADS', str(os.cpu_count()))

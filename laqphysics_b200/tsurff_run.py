@@ -25,19 +25,21 @@ def ionic_channel_functions(ion, unique, avec, dt, steps, device='cuda:0'):
     return channel_functions(ion, unique, avec, dt * np.arange(steps + 1), device)
 
 
-def run(engine, contractor, config, psi0, avec, dt, steps, chi, precision='complex128', tol=1e-10, maxdim=16):
-    """Propagate psi0 for `steps` velocity-gauge steps of dt, sampling the surface at every
-    step; returns (accumulator, final state, mean Krylov dimension)."""
+def run(engine, contractor, config, psi0, avec, dt, steps, chi, precision='complex128', tol=1e-10, maxdim=16, t0=0.):
+    """Propagate psi0 from t0 for `steps` velocity-gauge steps of dt, sampling the surface
+    at every step (chi[k] = channel functions at t0 + k dt); returns (accumulator, final
+    state, mean Krylov dimension)."""
     acc = VolkovAccumulator(contractor, config, avec, device=engine.device)
     sampler = SurfaceSampler(engine, contractor, acc)
     schedule = FieldSchedule(engine, avec, velocity=True, precision=precision)
     psi = psi0.clone() if torch.is_tensor(psi0) else engine.state(psi0)
-    sampler.record(0, 0.0, psi, avec(0.0), chi[0])
+    sampler.record(0, t0, psi, avec(t0), chi[0])
     dims = []
     for k in range(steps):
-        psi, info = step(schedule, psi, k * dt, dt, tol, maxdim)
+        psi, info = step(schedule, psi, t0 + k * dt, dt, tol, maxdim)
         dims.append(info['dimension'])
-        sampler.record(k + 1, (k + 1) * dt, psi, avec((k + 1) * dt), chi[k + 1])
+        t = t0 + (k + 1) * dt
+        sampler.record(k + 1, t, psi, avec(t), chi[k + 1])
     return acc, psi, float(np.mean(dims))
 
 
@@ -61,9 +63,11 @@ SMALL_CASE = {'radial': {'edges': [0, 1, 2, 3, 4, 6, 8, 10, 12], 'order': 4, 'ta
               'spectrum_energy': [.3, 2.3, 21], 'spectrum': {'theta_points': 4, 'phi_points': 1}}
 
 
-def build_case(config, device, dt=.02, after=1.0):
+def build_case(config, device, dt=.02, after=1.0, ground=None):
     """Engine, contractor, initial state (scaled ground state, python/run3d.py:134-136),
-    vector potential, step count (pulse + `after` a.u.) and channel functions of a config."""
+    vector potential, step count (pulse + `after` a.u.) and channel functions of a config.
+    ``ground``: the real-grid ground state to start from (default: solved here on the
+    device)."""
     from .engine import B200Hamiltonian
     from .pulses import Pulse
     from .surface3d import Ionic
@@ -83,7 +87,7 @@ def build_case(config, device, dt=.02, after=1.0):
     contractor = SurfaceContractor(base, ion, labels, unique, columns, True, h.transform, device)
     pulse = Pulse(**config['pulses'][0]['pulse'])
     avec = lambda t: np.array([0., 0., float(pulse.vector(t))])
-    _, g, _ = hreal.ground(tol=1e-10)
+    g = ground if ground is not None else hreal.ground(tol=1e-10)[1]
     ratio = np.sqrt(h.grid.weights / hreal.grid.weights)
     psi0 = (g.reshape(h.shape, order='F') * ratio[:, None, None] * ratio[None, :, None]).ravel(order='F')
     engine = B200Hamiltonian(h, device)

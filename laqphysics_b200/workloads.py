@@ -17,14 +17,14 @@ def coupled(edges, order, lmax, total_Lmax, ecs_angle=0., tail=0, alpha=1., cuto
     return CoupledHelium(Helium(grid, lmax, M=0, cutoff_radii=cutoff_radii), total_Lmax)
 
 
-def hpsi_microbench(tail=20):
+def hpsi_microbench(tail=20, ecs_angle=.35):
     """H·psi microbenchmark grid: 60 finite elements of order 9 (10 Lobatto nodes each,
     541 points) on [0, 120] a.u., then an infinite exterior-scaled Laguerre tail of
     ``tail`` points from 120 a.u. at theta = 0.35 (alpha = 1; the reference's irECS
     has no finite outer edge, so "box 150" maps to this tail).  Coupled channels
     l1, l2 <= 5, L <= 3, M = 0 -> nc = 43; origin removed -> n = 560 at tail = 20,
     N = n^2 nc = 13 484 800 amplitudes.  Coulomb cut between 80 and 95 a.u."""
-    return coupled(np.linspace(0, 120, 61), 9, 5, 3, ecs_angle=.35, tail=tail, cutoff_radii=(80., 95.))
+    return coupled(np.linspace(0, 120, 61), 9, 5, 3, ecs_angle=ecs_angle, tail=tail, cutoff_radii=(80., 95.))
 
 
 def arnoldi_small(tail=12):

@@ -401,6 +401,31 @@ def sharded_case():
     save('shards_values', values=values)
 
 
+def tsurff_run_case():
+    """A whole channel-resolved tSURFF run through the reference's own production driver
+    (python/run3d.py:_run_impl with the Torch backend on the CPU and online spectrum storage,
+    python/streaming_surface.py:OnlineSurface): the small case of laqphysics_b200.tsurff_run
+    with post_time 1 a.u., dt 0.02 (the driver rounds it to T / ceil(T / dt)), Krylov
+    dimension 16 and tolerance 1e-10.  Stores the spectrum file's arrays, the final state and
+    the time grid, so the device run can be compared with the reference's composition of
+    propagation, flux, ionic channel functions, contraction and Volkov integral."""
+    import run3d
+    sys.path.insert(0, str(REPO))
+    from laqphysics_b200.tsurff_run import SMALL_CASE
+    config = json.loads(json.dumps(SMALL_CASE))
+    config.update({'dt': .02, 'post_time': 1.0, 'krylov_dimension': 16, 'krylov_tolerance': 1e-10,
+                   'ground_tolerance': 1e-10, 'checkpoint_every': 100000, 'storage': {'mode': 'spectrum'}})
+    with tempfile.TemporaryDirectory() as out:
+        meta = run3d.run(config, out, backend='torch', device='cpu')
+        with np.load(Path(out) / 'spectrum.npz') as d:
+            spec = {k: d[k] for k in ('energy', 'theta', 'phi', 'solid_angle_weights', 'amplitudes', 'pes',
+                                      'angle_integrated', 'labels')}
+        with np.load(Path(out) / 'checkpoint.npz') as d:
+            psi, ground = d['psi'], d['ground']
+    save('tsurff_run', config=json.dumps(config), dt=meta['dt'], nsteps=meta['nsteps'], ground_energy=meta['ground_energy'],
+         psi=psi, ground=ground, **spec)
+
+
 if __name__ == '__main__':
     if len(sys.argv) > 1:          # named cases only, e.g. `make_golden.py sharded_case`
         for name in sys.argv[1:]:
@@ -421,3 +446,4 @@ if __name__ == '__main__':
     ground_case()
     pulses()
     sharded_case()
+    tsurff_run_case()
