@@ -167,6 +167,10 @@ int he_krylov_create_batched(he_krylov_handle *out, long long n, int maxdim, int
  * captured once on an internal stream and replayed on the caller's stream as one CUDA graph, updated in place
  * for new states, fields and step sizes; results are identical.  Off by default. */
 int he_krylov_set_graphs(he_krylov_handle k, int enable);
+/* Solves whose graph capture was invalidated (by work outside the solve) and were enqueued
+ * directly instead, and whether the workspace still captures: after three failed captures
+ * in a row it stops trying.  No counterpart in the reference. */
+int he_krylov_capture_fallbacks(he_krylov_handle k, int *fallbacks, int *graphs_on);
 /* Field derivative of one step: y = exp(-i dt B) x for the block operator
  * B = [[H(field), direction . d], [0, H(field)]] (length gauge, complex128) on x = [u; w], so
  * y = [e^{-i dt H} u + L w; e^{-i dt H} w] with L the derivative of e^{-i dt H(field)} along

@@ -70,6 +70,7 @@ SIGNATURES = {
     'he_krylov_scale': (I, [P, I, I, D, P]),
     'he_krylov_normalize': (I, [P, I, P]),
     'he_krylov_set_graphs': (I, [P, I]),
+    'he_krylov_capture_fallbacks': (I, [P, ct.POINTER(I), ct.POINTER(I)]),
     'he_expv_field_derivative': (I, [P, P, P, P, P, P, D, D, I, ct.POINTER(I), ct.POINTER(D), P]),
     'he_krylov_hessenberg': (I, [P, I, I, P, P]),
     'he_krylov_reset': (I, [P, P]),

@@ -77,8 +77,10 @@ namespace he {
 // Fields of a batch of instances that share one operator (passed by value to kernels):
 // instance b of a batched apply sees the field f[b][0..2]; a single apply has count 1.
 // skip (optional): a device flag that, when non-zero at launch, makes the banded kinetic and
-// generated mixing kernels return without work (the done word of a Krylov solve, so the
-// applies a fused solve enqueues past its convergence cost one empty launch each).
+// generated mixing kernels (the default path) return without work (the done word of a Krylov
+// solve, so the applies a fused solve enqueues past its convergence cost one empty launch
+// each).  The other kernel paths (he_set_path 0, 2, 3; he_set_mix 0) ignore it: there those
+// applies run in full and their results are discarded.
 constexpr int HE_BATCH_MAX = 64;
 struct FieldBatch {
     int count;

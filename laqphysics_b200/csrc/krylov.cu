@@ -700,6 +700,16 @@ extern "C" int he_krylov_set_graphs(he_krylov *k, int enable)
     return HE_OK;
 }
 
+// Solves whose graph capture failed and were enqueued directly (total), and whether the
+// workspace still captures (graphs are turned off after repeated failures in a row).
+extern "C" int he_krylov_capture_fallbacks(he_krylov *k, int *fallbacks, int *graphs_on)
+{
+    if (!k) return he_fail(HE_ERR_ARG, "null handle", __FILE__, __LINE__);
+    if (fallbacks) *fallbacks = k->capture_fallbacks;
+    if (graphs_on) *graphs_on = k->graphs ? 1 : 0;
+    return HE_OK;
+}
+
 extern "C" int he_krylov_destroy(he_krylov *k)
 {
     delete k;
@@ -1011,11 +1021,17 @@ int expv_impl(he_krylov *k, he_handle op, const void *x, void *y, const double *
             // The capture can be invalidated by work outside this solve (another host thread
             // loading its kernels, for instance): nothing captured has run, so drop it and
             // enqueue the solve directly.  A genuine error repeats there and is returned.
+            // Captures that fail again and again (not a one-off invalidation) stop costing a
+            // capture per solve: after KRYLOV_CAPTURE_RETRIES failures in a row the workspace
+            // turns graphs off; he_krylov_capture_fallbacks reports the counts.
             if (g) cudaGraphDestroy(g);
             g = nullptr;
             cudaGetLastError();
+            k->capture_fallbacks += 1;
+            if (++k->capture_failures_in_row >= KRYLOV_CAPTURE_RETRIES) k->graphs = false;
             rc = enqueue_expv(k, op, x, y, fields, velocity, dt, tol, maxdim, s, precision, direction, 0, first);
         } else {
+            k->capture_failures_in_row = 0;
             bool updated = false;
             if (k->graph_exec) {
                 cudaGraphExecUpdateResultInfo info;

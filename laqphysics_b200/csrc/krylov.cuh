@@ -26,6 +26,7 @@ constexpr int KRYLOV_THREADS = 256;
 constexpr int KRYLOV_TILE = 8;        // basis vectors per register tile
 constexpr int KRYLOV_MAXDIM = 64;
 constexpr int KRYLOV_FUSED = 16;      // CGS2 with a fused update + projection sweep up to this many vectors
+constexpr int KRYLOV_CAPTURE_RETRIES = 3;   // failed graph captures in a row before a workspace stops capturing
 
 }  // namespace he
 
@@ -59,6 +60,8 @@ struct he_krylov {
     cudaGraphExec_t graph_exec = nullptr;
     long long hint_key = 0;           // configuration the dimension hint belongs to
     int dim_seen = 0;                 // largest converged dimension of solves with that configuration
+    int capture_fallbacks = 0;        // solves whose capture failed and were enqueued directly
+    int capture_failures_in_row = 0;
     he_gmres_buffers *gmres = nullptr;  // device GMRES buffers (gmres.cu), created on first use
     int kb() const { return blocks; }
     size_t hs() const { return (size_t)(maxdim + 1) * maxdim; }  // Hessenberg size per instance

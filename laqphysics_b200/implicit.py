@@ -270,30 +270,53 @@ def device_gmres(engine, b, field, alpha, reference_energy, separable, shift, to
 INNER_TOLERANCE = 1e-5   # relative residual of each complex64 inner solve of a mixed Pade solve
 
 
-def defect_corrected_solve(A, A32, b, M, tol, flexible, restart, corrections=8, inner=None):
+def defect_corrected_solve(A, A32, b, M, tol, flexible, restart, corrections=8, inner=None, finish=None):
     """Solve A s = b to a complex128 relative residual <= tol by defect correction: each
     sweep solves A32 d = r by GMRES with the complex64 operator A32 (FP32 accumulation)
     to INNER_TOLERANCE, adds d to s and recomputes r = b - A s with the complex128
     operator.  Each sweep gains about five digits while that stays above the complex64
     operator's own error, so a 1e-11 solve takes two or three sweeps.  ``inner(r, tol)``,
-    when given, replaces the host-driven inner GMRES (the device solver).  Raises the
-    reference's 'GMRES did not converge' message when the sweeps run out."""
+    when given, replaces the host-driven inner GMRES (the device solver).
+
+    When an inner solve cannot reach its tolerance, or a sweep gains less than a factor 10
+    (the complex64 operator's own error reached), the remaining correction is solved in
+    complex128 from the current s (``finish(r, tol)``, default: GMRES with A), so the solve
+    still meets tol; info['fallback'] says so.  Raises the reference's 'GMRES did not
+    converge' message when that also fails."""
     s = torch.zeros_like(b)
     r = b
     bnorm = norm(b)
     iterations, relative = 0, 1.
+    if finish is None:
+        finish = lambda rhs, t: gmres(A, rhs, M, tol=t, flexible=flexible, restart=restart)
     for sweep in range(corrections):
-        if inner is not None:
-            d, info = inner(r, max(INNER_TOLERANCE, tol))
-        else:
-            d, info = gmres(A32, r, M, tol=max(INNER_TOLERANCE, tol), flexible=flexible, restart=restart)
+        try:
+            if inner is not None:
+                d, info = inner(r, max(INNER_TOLERANCE, tol))
+            else:
+                d, info = gmres(A32, r, M, tol=max(INNER_TOLERANCE, tol), flexible=flexible, restart=restart)
+        except RuntimeError as error:
+            if 'GMRES did not converge' not in str(error):
+                raise
+            break
         iterations += info['iterations']
         s = axpby(1, s, 1, d, out=s)
         r = axpby(1, b, -1, A(s))
-        relative = norm(r) / bnorm
+        previous, relative = relative, norm(r) / bnorm
         if relative <= tol:
-            return s, {'iterations': iterations, 'relative_residual': relative, 'corrections': sweep + 1}
-    raise RuntimeError(f'GMRES did not converge: residual={relative:.3e}, iterations={iterations}')
+            return s, {'iterations': iterations, 'relative_residual': relative, 'corrections': sweep + 1,
+                       'fallback': False}
+        if relative > .1 * previous:
+            break
+    # complex128 solve of the remaining correction A d = r, to tol relative to ||b||
+    rnorm = norm(r)
+    d, info = finish(r, tol * bnorm / rnorm)
+    iterations += info['iterations']
+    s = axpby(1, s, 1, d, out=s)
+    relative = norm(axpby(1, b, -1, A(s))) / bnorm
+    if relative > tol * 1.01:
+        raise RuntimeError(f'GMRES did not converge: residual={relative:.3e}, iterations={iterations}')
+    return s, {'iterations': iterations, 'relative_residual': relative, 'corrections': sweep + 1, 'fallback': True}
 
 
 @torch.no_grad()
@@ -306,7 +329,7 @@ def pade_step(engine, x, field, dt, reference_energy=0., tol=1e-11, precision='c
         raise ValueError("precision must be 'complex128' or 'mixed'")
     a2 = getattr(engine, 'a2_coefficient', 1.)
     squared = a2 * sum(float(a) ** 2 for a in field)
-    iterations, residual = 0, 0.
+    iterations, residual, corrections, fallbacks = 0, 0., 0, 0
     separable = getattr(engine, 'separable', None)
     flexible = getattr(separable, 'flexible', False)
     for root in (3 + 1j * SQRT3, 3 - 1j * SQRT3):
@@ -329,7 +352,14 @@ def pade_step(engine, x, field, dt, reference_energy=0., tol=1e-11, precision='c
             def inner(r, inner_tol, alpha=alpha):
                 return device_gmres(engine, r, field, alpha, reference_energy, separable, squared - reference_energy,
                                     inner_tol, restart, precision='complex64')
-            s, info = defect_corrected_solve(A, A32, x, M, tol, flexible, restart, inner=inner if on_device else None)
+
+            def finish(r, finish_tol, alpha=alpha):
+                return device_gmres(engine, r, field, alpha, reference_energy, separable, squared - reference_energy,
+                                    finish_tol, restart)
+            s, info = defect_corrected_solve(A, A32, x, M, tol, flexible, restart, inner=inner if on_device else None,
+                                             finish=finish if on_device else None)
+            corrections += info['corrections']
+            fallbacks += int(info['fallback'])
         elif on_device:
             s, info = device_gmres(engine, x, field, alpha, reference_energy, separable, squared - reference_energy,
                                    tol, restart)
@@ -338,7 +368,10 @@ def pade_step(engine, x, field, dt, reference_energy=0., tol=1e-11, precision='c
         x = axpby(2, s, -1, x)
         iterations += info['iterations']
         residual = max(residual, info['relative_residual'])
-    return x, {'linear_iterations': iterations, 'linear_residual': residual}
+    out = {'linear_iterations': iterations, 'linear_residual': residual}
+    if precision == 'mixed':
+        out.update(corrections=corrections, fallbacks=fallbacks)
+    return x, out
 
 
 @torch.no_grad()
@@ -347,6 +380,7 @@ def cf4_step(engine, x, avec, t, dt, reference_energy=0., tol=1e-11, depth=0, pr
     :func:`pade_step`."""
     fields = np.array([avec(t + C1 * dt), avec(t + C2 * dt)], float)
     iterations, residual, original = 0, 0., x
+    extra = {}
     a2 = getattr(engine, 'a2_coefficient', 1.)
     try:
         for w in ((A2, A1), (A1, A2)):
@@ -357,8 +391,11 @@ def cf4_step(engine, x, avec, t, dt, reference_energy=0., tol=1e-11, depth=0, pr
             x = axpby(phase, x, 0, x, out=x)
             iterations += info['linear_iterations']
             residual = max(residual, info['linear_residual'])
+            for key in ('corrections', 'fallbacks'):
+                if key in info:
+                    extra[key] = extra.get(key, 0) + info[key]
         return x, {'linear_iterations': iterations, 'linear_residual': residual, 'dimension': 0,
-                   'residual_estimate': None}
+                   'residual_estimate': None, **extra}
     except RuntimeError as error:
         if 'GMRES did not converge' not in str(error) or depth >= 6:
             raise

@@ -226,3 +226,20 @@ def test_applies_past_convergence_do_no_work(precision):
     t_apply = timed(lambda: apply(x), reps=20)
     # each extra iteration is a handful of empty launches, not an apply
     assert (t48 - t_small) / (48 - small) < 0.6 * t_apply, (t_small, t48, t_apply)
+
+
+def test_graph_capture_fallback_counter_starts_at_zero():
+    """Repeated solves replay as graphs without a capture fallback in a single thread."""
+    import ctypes as ct
+    from laqphysics_b200._lib import LIB
+    from laqphysics_b200.torch_backend import FieldOperator, exponential_action, workspace
+    from laqphysics_b200.workloads import coupled, seeded_state
+    h = coupled(np.linspace(0, 12, 7), 5, 2, 2, ecs_angle=.3, tail=8, cutoff_radii=(1., 1.8))
+    op = engine(h)
+    x = op.state(seeded_state(h.size, 4))
+    for _ in range(4):
+        exponential_action(FieldOperator(op, (0., 0., .05), False), x, .005, 1e-11, 16)
+    ws = workspace(h.size, 16, op.device)
+    fallbacks, graphs = ct.c_int(-1), ct.c_int(-1)
+    assert LIB.he_krylov_capture_fallbacks(ws.handle, ct.byref(fallbacks), ct.byref(graphs)) == 0
+    assert fallbacks.value == 0 and graphs.value == 1
