@@ -325,6 +325,17 @@ int he_volkov_add(int nlab, int nouter, int ns, int ne, int nang, const void *q,
                   void *stream);
 
 /* ------------------------------------------------------------------------------------
+ * Run diagnostics on the device.  Replaces the checkpoint diagnostics of
+ * python/run3d.py:212-224 (which copy the whole state to the host): out[0] = real-region
+ * norm sum |u(i,j,c)|^2 f_i f_j with f = interior weight / |weight|, out[1] + i out[2] =
+ * <g|psi> (0 when g is NULL), out[3] = exchange error ||u - P12 u|| with
+ * (P12 u)(i,j,c) = sign_c u(j,i,xc_c) (python/coupled_angular.py:80-82).  f (n doubles),
+ * xc (nc ints), sign (nc doubles) and the states are device memory; out is host memory.
+ * ---------------------------------------------------------------------------------- */
+int he_diagnostics(he_handle h, const void *psi, const void *g, const double *f, const int *xc, const double *sign,
+                   double *out, void *stream);
+
+/* ------------------------------------------------------------------------------------
  * Batched norms with no device allocation.  No counterpart in the reference: it serves
  * callers that cannot let a call allocate device memory (a process whose device memory
  * belongs to a pool allocator, a latency-critical loop that must not stall on the

@@ -86,6 +86,7 @@ SIGNATURES = {
                                 P, P, P, P, P, P, P, P]),
     'he_volkov_add': (I, [I, I, I, I, I, P, P, P, P, P, P, D, P, D, D, I, P, P, P]),
     'he_vec_norms_noalloc': (I, [ct.c_longlong, I, P, ct.c_longlong, P, P]),
+    'he_diagnostics': (I, [P, P, P, P, P, P, ct.POINTER(D), P]),
     'he_plan_build': (P, [I, I, P, P, P, I, P, P, P, P, I, I, P, P, P, P]),
     'he_plan_free': (None, [P]),
     'he_plan_array': (ct.c_longlong, [P, I, P]),

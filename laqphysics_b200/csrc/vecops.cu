@@ -201,3 +201,85 @@ extern "C" int he_binary_version(int *version)
     *version = attributes.binaryVersion;
     return HE_OK;
 }
+
+// ---------------------------------------------------------------------------------
+// Run diagnostics of python/run3d.py:212-224 on the device (no state copy to the host):
+//   real-region norm  sum |u(i,j,c)|^2 f_i f_j   (f = interior weight / |weight|),
+//   <g|psi> = sum conj(g) psi,
+//   exchange error^2  sum |u(i,j,c) - sign_c u(j,i,x_c)|^2   (x_c the exchanged channel).
+// ---------------------------------------------------------------------------------
+namespace he {
+__global__ void __launch_bounds__(KRYLOV_THREADS)
+diagnostics_kernel(int n, int nc, const double2 *__restrict__ psi, const double2 *__restrict__ g,
+                   const double *__restrict__ f, const int *__restrict__ xc, const double *__restrict__ sign,
+                   double *__restrict__ partial)
+{
+    const size_t nn = (size_t)n * n, total = nn * nc;
+    double norm = 0, ex = 0;
+    double2 ov = mk<double>(0, 0);
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < total; p += (size_t)gridDim.x * blockDim.x) {
+        const int c = (int)(p / nn);
+        const size_t q = p - (size_t)c * nn;
+        const int i = (int)(q % n), j = (int)(q / n);
+        const double2 u = psi[p];
+        norm += cabs2<double>(u) * f[i] * f[j];
+        if (g) ov = cfma_conj<double>(g[p], u, ov);
+        const double2 w = psi[(size_t)xc[c] * nn + (size_t)i * n + j];
+        const double s = sign[c];
+        ex += cabs2<double>(mk<double>(u.x - s * w.x, u.y - s * w.y));
+    }
+    double v[4] = {norm, ov.x, ov.y, ex};
+    __shared__ double red[4][KRYLOV_THREADS / 32];
+    for (int k = 0; k < 4; ++k) {
+        double s = v[k];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+        if ((threadIdx.x & 31) == 0) red[k][threadIdx.x >> 5] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        double t = 0;
+        for (int w = 0; w < KRYLOV_THREADS / 32; ++w) t += red[threadIdx.x][w];
+        partial[(size_t)threadIdx.x * KRYLOV_BLOCKS + blockIdx.x] = t;
+    }
+}
+
+__global__ void diagnostics_sum_kernel(const double *partial, double *out)
+{
+    const int k = threadIdx.x >> 5;     // one warp per quantity, fixed order
+    const double s = warp_fixed_sum(partial + (size_t)k * KRYLOV_BLOCKS, KRYLOV_BLOCKS, 1);
+    if ((threadIdx.x & 31) == 0) out[k] = s;
+}
+}  // namespace he
+
+// out[0] = real-region norm, out[1] + i out[2] = <g|psi> (0 when g is NULL), out[3] = exchange
+// error ||u - P12 u|| (host memory, 4 doubles).  f: n doubles, xc: nc ints, sign: nc doubles,
+// all device memory; psi, g: complex128 device states.  Blocks the host until done.
+extern "C" int he_diagnostics(he_handle h, const void *psi, const void *g, const double *f, const int *xc,
+                              const double *sign, double *out, void *stream)
+{
+    if (!h || !psi || !f || !xc || !sign || !out) return he_fail(HE_ERR_ARG, "bad diagnostics argument", __FILE__, __LINE__);
+    static thread_local double *scratch = nullptr, *host = nullptr;
+    static thread_local int scratch_device = -1;
+    int dev = 0;
+    HE_CUDA_TRY(cudaGetDevice(&dev));
+    if (!scratch || scratch_device != dev) {
+        if (scratch) cudaFree(scratch);
+        scratch = nullptr;
+        HE_CUDA_TRY(cudaMalloc(&scratch, (4 * KRYLOV_BLOCKS + 4) * sizeof(double)));
+        if (!host) HE_CUDA_TRY(cudaMallocHost(&host, 4 * sizeof(double)));
+        scratch_device = dev;
+    }
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    diagnostics_kernel<<<KRYLOV_BLOCKS, KRYLOV_THREADS, 0, s>>>(h->n, h->nc, static_cast<const double2 *>(psi),
+                                                                static_cast<const double2 *>(g), f, xc, sign, scratch);
+    diagnostics_sum_kernel<<<1, 128, 0, s>>>(scratch, scratch + 4 * KRYLOV_BLOCKS);
+    HE_CUDA_TRY(cudaGetLastError());
+    HE_CUDA_TRY(cudaMemcpyAsync(host, scratch + 4 * KRYLOV_BLOCKS, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    HE_CUDA_TRY(cudaStreamSynchronize(s));
+    out[0] = host[0];
+    out[1] = host[1];
+    out[2] = host[2];
+    out[3] = sqrt(host[3]);
+    return HE_OK;
+}

@@ -222,6 +222,30 @@ class B200Hamiltonian:
         torch.cuda.synchronize(self.device)
         self.device_status()
 
+    # --- run diagnostics (python/run3d.py:212-224) -------------------------------------
+    def diagnostics(self, x, ground=None):
+        """The driver's checkpoint diagnostics computed on the device (he_diagnostics),
+        without copying the state to the host: {'real_region_norm': sum |u|^2 f_i f_j with
+        f = interior weight / |weight| (the real-element mass fraction), 'ground_population':
+        |<g|psi>|^2 (ground: device state, or None), 'exchange_error': ||u - P12 u||}."""
+        self._check(x, torch.complex128)
+        if ground is not None:
+            self._check(ground, torch.complex128)
+        if not hasattr(self, '_diag_tables'):
+            g = self.h.grid
+            f = np.asarray(g.interior_weights / np.abs(g.weights), dtype=np.float64)
+            sign = np.asarray(getattr(self.h, 'exchange_sign', np.ones(self.nc)), dtype=np.float64)
+            self._diag_tables = (torch.as_tensor(f, device=self.device),
+                                 torch.as_tensor(np.asarray(self.h.exchange, dtype=np.int32), device=self.device),
+                                 torch.as_tensor(sign, device=self.device))
+        f, xc, sign = self._diag_tables
+        out = (ct.c_double * 4)()
+        vp = lambda t: ct.c_void_p(t.data_ptr())
+        check(LIB.he_diagnostics(self.op.handle, vp(x), vp(ground) if ground is not None else None, vp(f), vp(xc),
+                                 vp(sign), out, _stream(self.device)), 'he_diagnostics')
+        return {'real_region_norm': out[0], 'ground_population': out[1] ** 2 + out[2] ** 2 if ground is not None else None,
+                'exchange_error': out[3]}
+
     def _check(self, x, dtype):
         if x.device != self.device or x.dtype != dtype or not x.is_contiguous() or x.numel() != self.size:
             raise ValueError(f'state must be a contiguous {dtype} tensor of {self.size} elements on {self.device}')

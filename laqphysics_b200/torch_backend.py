@@ -278,20 +278,24 @@ def step_batched(engine, fields_at, x, t, dt, tol=1e-10, maxdim=48, velocity=Fal
 
 
 def step(apply_at, x, t, dt, tol=1e-10, maxdim=48, depth=0):
-    """Midpoint exponential step with recursive halving (python/torch_backend.py:160-167)."""
+    """Midpoint exponential step with recursive halving (python/torch_backend.py:160-167).
+    info['path'] lists the accepted exponentials in order as (t, dt, tol, dimension)."""
     try:
         if isinstance(apply_at, FieldSchedule):
             operator = apply_at.at(t + dt / 2)
         else:
             operator = lambda y: apply_at(t + dt / 2, y)
-        return exponential_action(operator, x, dt, tol, maxdim)
+        y, info = exponential_action(operator, x, dt, tol, maxdim)
+        info['path'] = [(t, dt, tol, info['dimension'])]
+        return y, info
     except RuntimeError as error:
         if 'Arnoldi did not converge' not in str(error) or depth >= 8:
             raise
         y, a = step(apply_at, x, t, dt / 2, tol / 2, maxdim, depth + 1)
         y, b = step(apply_at, y, t + dt / 2, dt / 2, tol / 2, maxdim, depth + 1)
         return y, {'dimension': max(a['dimension'], b['dimension']),
-                   'residual_estimate': a['residual_estimate'] + b['residual_estimate'], 'subdivided': True}
+                   'residual_estimate': a['residual_estimate'] + b['residual_estimate'], 'subdivided': True,
+                   'path': a['path'] + b['path']}
 
 
 __all__ = ['TorchHamiltonian', 'B200Hamiltonian', 'exponential_action', 'step', 'step_batched', 'FieldOperator',

@@ -50,3 +50,25 @@ def step(apply_at, x, t, dt, tol=1e-11, maxdim=60, depth=0):
         y, b = step(apply_at, y, t + dt / 2, dt / 2, tol / 2, maxdim, depth + 1)
         return y, {'dimension': max(a['dimension'], b['dimension']),
                    'residual_estimate': a['residual_estimate'] + b['residual_estimate'], 'subdivided': True}
+
+
+def exponential_action_fixed(apply, x, dt, m):
+    """The same Krylov exponential with the dimension given instead of chosen: m CGS2
+    Arnoldi vectors, y = Q_m expm(-i dt H_m)[:, 0] beta, and the error estimate
+    |dt h_{m+1,m} c_m| the adaptive version would have compared with its tolerance (used to
+    replay another implementation's step decisions on the same dimensions)."""
+    beta = np.linalg.norm(x)
+    Q = np.empty((len(x), m + 1), complex, order='F')
+    H = np.zeros((m + 1, m), complex)
+    Q[:, 0] = x / beta
+    for j in range(m):
+        v = apply(Q[:, j])
+        for _ in range(2):
+            proj = Q[:, :j + 1].conj().T @ v
+            H[:j + 1, j] += proj
+            v = v - Q[:, :j + 1] @ proj
+        H[j + 1, j] = np.linalg.norm(v)
+        if j + 1 < m:
+            Q[:, j + 1] = v / H[j + 1, j]
+    c = expm(-1j * dt * H[:m, :m])[:, 0] * beta
+    return Q[:, :m] @ c, float(abs(dt * H[m, m - 1] * c[-1]))

@@ -295,3 +295,26 @@ def test_kernels_run_as_sm100a_binaries():
     version = ct.c_int()
     assert LIB.he_binary_version(ct.byref(version)) == 0, LIB.he_last_error().decode()
     assert version.value == 100
+
+
+@pytest.mark.parametrize('basis', ['coupled', 'product'])
+def test_device_run_diagnostics_match_the_driver_formulas(basis):
+    """B200Hamiltonian.diagnostics (he_diagnostics) against python/run3d.py:212-224's host
+    formulas on the host copy: real-region norm with the interior mass fraction, ground
+    population |<g|psi>|^2 and the exchange error (coupled: with the (-1)^(l1+l2-L) sign)."""
+    from laqphysics_b200.fedvr import make_grid
+    from laqphysics_b200.helium3d import Helium
+    from laqphysics_b200.workloads import coupled, seeded_state
+    if basis == 'coupled':
+        h = coupled(np.linspace(0, 12, 7), 5, 2, 2, ecs_angle=.3, tail=8, cutoff_radii=(1., 1.8))
+    else:
+        h = Helium(make_grid(np.linspace(0, 12, 7), 5, ecs_angle=.3, tail=8), 1, M=None, cutoff_radii=(1., 1.8))
+    op = engine(h)
+    x, gs = seeded_state(h.size, 5), seeded_state(h.size, 6)
+    d = op.diagnostics(op.state(x), op.state(gs))
+    u = x.reshape(h.shape, order='F')
+    f = h.grid.interior_weights / abs(h.grid.weights)
+    norm = float(np.sum(abs(u) ** 2 * f[:, None, None] * f[None, :, None]))
+    assert abs(d['real_region_norm'] - norm) <= 1e-13 * norm
+    assert abs(d['ground_population'] - abs(np.vdot(gs, x)) ** 2) <= 1e-13
+    assert abs(d['exchange_error'] - h.exchange_error(x)) <= 1e-12 * h.exchange_error(x)
