@@ -44,11 +44,12 @@ def parse():
                    help='steps of the mixed-precision config slice on the microbenchmark grid (0: skip)')
     p.add_argument('--path', type=int, default=1, choices=[0, 1, 2, 3],
                    help='H·psi kernel path of the microbenchmark operator (he_set_path; 1 = default fused kernels)')
-    p.add_argument('--adjoint-steps', type=int, default=128, help='adjoint leg: Arnoldi steps (dt 0.005)')
-    p.add_argument('--adjoint-knots', type=int, default=32, help='adjoint leg: field samples')
+    p.add_argument('--adjoint-steps', type=int, default=2048, help='adjoint leg: Arnoldi steps (dt 0.005)')
+    p.add_argument('--adjoint-knots', type=int, default=512, help='adjoint leg: field samples')
     p.add_argument('--adjoint-checkpoint', type=int, default=None,
                    help='adjoint leg: steps between kept states (default: every state resident in HBM)')
     p.add_argument('--profile', choices=['c128', 'c64', 'arnoldi', 'arnoldi-split', 'batched', 'batched-attempt', 'cf4', 'cfg2',
+                                         'pump-probe', 'preconditioner',
                                          'adjoint', 'concurrent'],
                    default=None,
                    help='run only W+K applications of one precision (for ncu captures); prints no JSON')
@@ -254,12 +255,15 @@ def batched_leg(torch, device, steps, count=32):
     dt, tol, maxdim = .02, 1e-10, 12
     x0 = engine.state(psi0).repeat(count).reshape(count, -1).contiguous()
     out = {'workload': f'{count} instances, Arnoldi grid n=132 nc=17, length gauge, maxdim 12, dt 0.02',
-           'count': count}
+           'count': count, 'steps': steps}
     finals = {}
+    warm = None
     for precision in ('complex128', 'mixed'):
         x = x0.clone()
         for i in range(3):
             x, _ = step_batched(engine, fields_at, x, i * dt, dt, tol, maxdim, precision=precision)
+        if precision == 'complex128':
+            warm = x.clone()
         torch.cuda.synchronize(device)
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         dims = []
@@ -275,22 +279,27 @@ def batched_leg(torch, device, steps, count=32):
         out[precision] = {'instance_steps_per_s': count * steps / (ms * 1e-3), 'ms_per_step': ms / steps,
                           'mean_dimension': float(np.mean(dims)),
                           'hpsi_per_instance_step': (engine.apply_count - applies0) / (count * steps)}
-    # the same instances stepped one at a time by the plain FP64 engine (same start, same
-    # fields, same first steps), for the like-for-like speed-up of batching
+    # like for like: the same instances over the same steps (3 .. 3+steps, from the same
+    # complex128 states), stepped one at a time by the plain FP64 engine
     from laqphysics_b200.torch_backend import FieldSchedule, step
-    single_steps = 3
     torch.cuda.synchronize(device)
+    applies0 = engine.apply_count
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     start.record()
+    singles = []
     for b in range(count):
         schedule = FieldSchedule(engine, lambda t, b=b: fields_at(t)[b], velocity=False)
-        xb = x0[b].contiguous()
-        for i in range(single_steps):
+        xb = warm[b].contiguous()
+        for i in range(3, 3 + steps):
             xb, _ = step(schedule, xb, i * dt, dt, tol, maxdim)
+        singles.append(xb)
     stop.record()
     torch.cuda.synchronize(device)
-    out['single_fp64_same_instances'] = {'instance_steps_per_s': count * single_steps / (start.elapsed_time(stop) * 1e-3),
-                                         'steps_per_instance': single_steps}
+    out['single_fp64_same_instances'] = {
+        'instance_steps_per_s': count * steps / (start.elapsed_time(stop) * 1e-3), 'steps_per_instance': steps,
+        'hpsi_per_instance_step': (engine.apply_count - applies0) / (count * steps),
+        'rel_l2_vs_batched_complex128': float(torch.max(torch.linalg.vector_norm(torch.stack(singles) - finals['complex128'], dim=1)
+                                                        / torch.linalg.vector_norm(finals['complex128'], dim=1)))}
     for precision in ('complex128', 'mixed'):
         out[precision]['speedup_vs_single_fp64_same_instances'] = (
             out[precision]['instance_steps_per_s'] / out['single_fp64_same_instances']['instance_steps_per_s'])
@@ -307,7 +316,8 @@ def adjoint_leg(torch, device, steps=128, knots=32, checkpoint=None):
     (two pulses, peak 0.02 a.u.); objective = He+(n = 2) channel yield with the second
     electron beyond 5 a.u. (adjoint.ChannelYield).
     Reports the forward and backward times and their ratio with every state resident (the
-    default) and with states kept every 32 steps (segments recomputed)."""
+    default) and with states kept every 64 steps (segments recomputed).  The defaults are the
+    adjoint configuration's stated size: 2048 steps, 512 field samples, checkpoint 64."""
     from laqphysics_b200 import workloads
     from laqphysics_b200.adjoint import Propagation, check_complex_symmetric
     from laqphysics_b200.engine import B200Hamiltonian
@@ -340,12 +350,12 @@ def adjoint_leg(torch, device, steps=128, knots=32, checkpoint=None):
         return prop, J, grad, t1 - t0, t2 - t1
 
     prop, J, grad, fwd, bwd = run(checkpoint)
-    _, _, grad32, fwd32, bwd32 = run(32)
+    _, _, grad32, fwd32, bwd32 = run(64)
     return {'workload': f'adjoint gradient: l1,l2<=4 L<=2 (nc={h.nc}, n={h.n}), {steps} Arnoldi steps dt 0.005, '
                         f'{knots} field samples, objective: He+(n=2) yield, second electron beyond 5 a.u.',
             'checkpoint': prop.checkpoint, 'objective': J, 'forward_ms': fwd * 1e3, 'backward_ms': bwd * 1e3,
             'backward_over_forward': bwd / fwd, 'gradient_norm': float(np.linalg.norm(grad)),
-            'checkpoint_32': {'forward_ms': fwd32 * 1e3, 'backward_ms': bwd32 * 1e3,
+            'checkpoint_64': {'forward_ms': fwd32 * 1e3, 'backward_ms': bwd32 * 1e3,
                               'backward_over_forward': bwd32 / fwd32,
                               'gradient_rel_diff': float(np.linalg.norm(grad32 - grad) / np.linalg.norm(grad))}}
 
@@ -416,6 +426,91 @@ def concurrent_leg(torch, device, count=8, steps=3):
     return out
 
 
+def pump_probe_leg(torch, device, count=32, steps=2):
+    """The batched pump-probe configuration's shape at a size that fits one GPU for 32
+    instances at once: bipolar all-M channels (l1, l2 <= 3 or 4 alternating, total L <= 1),
+    10 or 12 finite elements of order 9 on [0, 25] a.u. + 8-point ECS tail, circular (sigma+)
+    probe pulses (omega 1.6 a.u., 6 cycles) with seeded delays 0-800 a.u. and peak fields
+    0.005-0.03 a.u., CF4 + Pade/GMRES steps dt 0.05 (tol 1e-10) from the ground state, in the
+    middle of each instance's probe.  The stated 40-60 elements x order 10 with l <= 6 and
+    every total L would need up to 2.4 GB per state and ~78 GB of FGMRES basis per instance.
+    Three ways: the plain FP64 engine (complex128 preconditioner, GMRES(32)) one instance
+    after another; complex64 preconditioners (FGMRES(16)) one after another; and all 32
+    instances stepped together (laqphysics_b200.concurrent: own engine, stream and host thread
+    each, complex64 preconditioners)."""
+    from dataclasses import replace
+    from laqphysics_b200.bipolar import BipolarHelium
+    from laqphysics_b200.concurrent import ConcurrentStepper
+    from laqphysics_b200.engine import B200Hamiltonian
+    from laqphysics_b200.fedvr import make_grid
+    from laqphysics_b200.implicit import SeparablePreconditioner, cf4_step
+    from laqphysics_b200.pulses import Pulse
+    from laqphysics_b200.torch_backend import FieldSchedule
+    shapes = {}
+    for lmax, elements in ((3, 10), (4, 12)):
+        grid = lambda angle: make_grid(np.linspace(0, 25, elements + 1), 9, ecs_angle=angle, tail=8)
+        h = BipolarHelium(grid(.3), lmax=lmax, total_Lmax=1, M=None, cutoff_radii=(18., 22.))
+        hreal = BipolarHelium(grid(0.), lmax=lmax, total_Lmax=1, M=None, cutoff_radii=(18., 22.))
+        E0, g, _ = hreal.ground(tol=1e-9)
+        ratio = np.sqrt(h.grid.weights / hreal.grid.weights)
+        psi0 = (g.reshape(h.shape, order='F') * ratio[:, None, None] * ratio[None, :, None]).ravel(order='F')
+        shapes[lmax] = (h, psi0, E0)
+    rng = np.random.default_rng(33)
+    delays, peaks = rng.uniform(0, 800, count), rng.uniform(.005, .03, count)
+    probe = Pulse(omega=1.6, cycles=6, field=1.)
+    avecs, engines, states, e_ref, sizes = [], [], [], [], []
+    for k in range(count):
+        h, psi0, E0 = shapes[3 + k % 2]
+        pk = replace(probe, field=float(peaks[k]), start=float(delays[k]))
+        skew = replace(pk, cep=pk.cep - np.pi / 2)
+        t_mid = delays[k] + probe.duration / 2
+        avecs.append(lambda t, pk=pk, skew=skew, t0=t_mid: np.array([pk.vector(t + t0), skew.vector(t + t0), 0.])
+                     / np.sqrt(2))
+        engine = B200Hamiltonian(h, device)
+        engines.append(engine)
+        states.append(engine.state(psi0))
+        e_ref.append(E0)
+        sizes.append(h.size)
+    dt, tol = .05, 1e-10
+    out = {'workload': f'{count} bipolar all-M instances (nc = {min(s[0].nc for s in shapes.values())}..'
+                       f'{max(s[0].nc for s in shapes.values())}, N = {min(sizes):,}..{max(sizes):,}), sigma+ probes, '
+                       f'{steps} CF4 steps each, dt 0.05', 'count': count, 'steps': steps}
+
+    def alone(precision):
+        for e in engines:
+            e.separable = SeparablePreconditioner(e, precision)
+        for e, av, x, er in zip(engines, avecs, states, e_ref):     # warm-up
+            cf4_step(e, x, av, 0., dt, er, tol)
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        finals = []
+        for e, av, x, er in zip(engines, avecs, states, e_ref):
+            for i in range(steps):
+                x, _ = cf4_step(e, x, av, i * dt, dt, er, tol)
+            finals.append(x)
+        torch.cuda.synchronize(device)
+        return count * steps / (time.perf_counter() - t0), finals
+
+    fp64, ref = alone('complex128')
+    c64, _ = alone('complex64')
+    stepper = ConcurrentStepper([FieldSchedule(e, av, velocity=True) for e, av in zip(engines, avecs)], device)
+    stepper.cf4(states, avecs, 0., dt, e_ref, tol)                  # warm-up
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    xs = states
+    for i in range(steps):
+        xs, _ = stepper.cf4(xs, avecs, i * dt, dt, e_ref, tol)
+    torch.cuda.synchronize(device)
+    together = count * steps / (time.perf_counter() - t0)
+    stepper.close()
+    err = max(float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)) for a, b in zip(xs, ref))
+    out.update(plain_fp64_one_after_another_instance_steps_per_s=fp64,
+               complex64_preconditioner_one_after_another_instance_steps_per_s=c64,
+               concurrent_complex64_preconditioner_instance_steps_per_s=together,
+               speedup_vs_plain_fp64=together / fp64, state_rel_l2_vs_plain_fp64_max=err)
+    return out
+
+
 def cfg2_slice_leg(torch, device, steps=6):
     """Bounded slice of the mixed-precision full propagation on the microbenchmark grid
     (n = 560, nc = 43, real to 120 a.u.): sin^2 pulse omega 1.6 a.u., 20 cycles, peak
@@ -477,6 +572,45 @@ def cfg2_slice_leg(torch, device, steps=6):
     out['state_rel_l2_mixed_vs_fp64'] = float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
     out['norm_error_mixed_vs_fp64'] = abs(float(torch.linalg.vector_norm(a)) - float(torch.linalg.vector_norm(b)))
     out['mixed_speedup'] = out['mixed']['steps_per_s'] / out['complex128']['steps_per_s']
+    return out
+
+
+def preconditioner_leg(torch, device):
+    """The separable preconditioner's GEMM chain on the microbenchmark grid (n = 560, nc = 43,
+    l <= 5: 241 GFLOP of complex GEMM per apply, 32 n^3 nc) in both precisions, against the
+    same count of torch.bmm calls (cuBLAS Z/CGEMM) on the same box: complex128 on the FP64
+    tensor cores (DMMA), complex64 on tcgen05 (TF32, split operands, 3 MMAs per K slice)."""
+    from laqphysics_b200 import workloads
+    from laqphysics_b200.engine import B200Hamiltonian
+    from laqphysics_b200.implicit import SeparablePreconditioner
+    h = workloads.hpsi_microbench()
+    engine = B200Hamiltonian(h, device)
+    x = engine.state(workloads.seeded_state(h.size, 7))
+    flops = 32.0 * h.n ** 3 * h.nc
+    out = {'workload': f'separable preconditioner, n={h.n} nc={h.nc}: 4 complex n^3 GEMMs per channel + resolvent',
+           'gflop_per_apply': flops / 1e9}
+
+    def timed(fn, reps=5):
+        fn()
+        torch.cuda.synchronize(device)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize(device)
+        return a.elapsed_time(b) / reps
+
+    for precision, dtype in (('complex128', torch.complex128), ('complex64', torch.complex64)):
+        pre = SeparablePreconditioner(engine, precision)
+        ms = timed(lambda: pre.apply(x, .05 / (3 + 1j * np.sqrt(3)), -2.))
+        A = torch.randn(h.nc, h.n, h.n, dtype=dtype, device=device)
+        B = torch.randn(h.nc, h.n, h.n, dtype=dtype, device=device)
+        ref = timed(lambda: [torch.bmm(A, B) for _ in range(4)])
+        out[precision] = {'ms_per_apply': ms, 'tflops': flops / (ms * 1e-3) / 1e12,
+                          'cublas_bmm_x4_ms': ref, 'cublas_tflops': flops / (ref * 1e-3) / 1e12,
+                          'speedup_vs_cublas': ref / ms}
+        del pre
     return out
 
 
@@ -645,10 +779,16 @@ def main():
         arnoldi_leg(torch, device, steps=args.steps, cpu_steps=0)
         return 0
     if args.profile == 'batched':
-        batched_leg(torch, device, steps=args.steps)
+        print(json.dumps(batched_leg(torch, device, steps=args.steps)), flush=True)
         return 0
     if args.profile == 'cf4':
         print(json.dumps(cf4_leg(torch, device, steps=args.steps)), flush=True)
+        return 0
+    if args.profile == 'pump-probe':
+        print(json.dumps(pump_probe_leg(torch, device)), flush=True)
+        return 0
+    if args.profile == 'preconditioner':
+        print(json.dumps(preconditioner_leg(torch, device)), flush=True)
         return 0
     if args.profile == 'cfg2':
         print(json.dumps(cfg2_slice_leg(torch, device, steps=args.steps)), flush=True)
@@ -842,7 +982,9 @@ def main():
         line['adjoint'] = adjoint_leg(torch, device, args.adjoint_steps, args.adjoint_knots, args.adjoint_checkpoint)
         line['spectrum'] = spectrum_leg(torch, device)
         line['cf4'] = cf4_leg(torch, device)
+        line['preconditioner'] = preconditioner_leg(torch, device)
         line['concurrent'] = concurrent_leg(torch, device)
+        line['pump_probe'] = pump_probe_leg(torch, device)
         if args.cfg2_steps:
             line['cfg2_slice'] = cfg2_slice_leg(torch, device, steps=args.cfg2_steps)
 
