@@ -471,20 +471,23 @@ extern "C" int he_gmres_shifted(he_krylov *k, he_handle op, he_separable *sep, c
         int first = restart;
         if (gb->iters_seen > 0) first = std::min(restart, (gb->iters_seen + cadence - 1) / cadence * cadence);
         while (j < restart) {
-            const int end = j == 0 ? first : restart;
+            // a solve that outruns the hint continues in doubling segments
+            const int end = j == 0 ? first : std::min(restart, j + std::max(cadence, j));
             if ((rc = enqueue_iterations(v, j, end))) return rc;
             if ((rc = read_state(v))) return rc;
             j = end;
             if (gb->host->solved || gb->host_status->done) break;
         }
         if (gb->host->solved) {
+            // the hint follows first cycles that converged; a solve that restarts runs its
+            // first cycle to the restart length in two segments anyway, and must not make
+            // every later solve enqueue whole cycles
             const int in_cycle = gb->host->m;
             if (cycle == 0 && in_cycle > gb->iters_seen) gb->iters_seen = in_cycle;
             if (iterations) *iterations = gb->host->iterations;
             if (residual) *residual = gb->host->true_residual;
             return HE_OK;
         }
-        gb->iters_seen = restart;
     }
     if (iterations) *iterations = gb->host->iterations;
     if (residual) *residual = gb->host->true_residual;
