@@ -49,7 +49,7 @@ def parse():
     p.add_argument('--adjoint-checkpoint', type=int, default=None,
                    help='adjoint leg: steps between kept states (default: every state resident in HBM)')
     p.add_argument('--profile', choices=['c128', 'c64', 'arnoldi', 'arnoldi-split', 'batched', 'batched-attempt', 'cf4', 'cfg2',
-                                         'pump-probe', 'preconditioner',
+                                         'pump-probe', 'preconditioner', 'spectrum',
                                          'adjoint', 'concurrent'],
                    default=None,
                    help='run only W+K applications of one precision (for ncu captures); prints no JSON')
@@ -715,6 +715,32 @@ def spectrum_leg(torch, device):
     out['angle_integrated_rel_max_mixed_vs_fp64'] = per_label
     out['state_rel_l2_mixed_vs_fp64'] = float(torch.linalg.vector_norm(p32 - p64) / torch.linalg.vector_norm(p64))
     out['norm_error_mixed_vs_fp64'] = float(abs(torch.linalg.vector_norm(p32) - torch.linalg.vector_norm(p64)))
+    out['surface_sample'] = sample_timing(torch, device, engine, contractor, avec, p64, chi)
+    return out
+
+
+def sample_timing(torch, device, engine, contractor, avec, state, chi, count=200):
+    """One surface sample (flux frame, contraction, Volkov update) as one launch
+    (he_sample_record) and as three (he_flux, he_surface_contract, he_volkov_add): device
+    time per sample (CUDA events over `count` samples) and host time per call."""
+    from laqphysics_b200.streaming_surface import SurfaceSampler, VolkovAccumulator
+    from laqphysics_b200.tsurff_run import SMALL_CASE
+    out = {}
+    for name, fused in (('one_launch', True), ('three_launches', False)):
+        sampler = SurfaceSampler(engine, contractor, VolkovAccumulator(contractor, SMALL_CASE, avec, device=device),
+                                 fused=fused)
+        for i in range(5):
+            sampler.record(i, .02 * i, state, avec(.02 * i), chi[i])
+        torch.cuda.synchronize(device)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        a.record()
+        for i in range(5, 5 + count):
+            sampler.record(i, .02 * i, state, avec(.02 * i), chi[i % len(chi)])
+        b.record()
+        host = (time.perf_counter() - t0) / count
+        torch.cuda.synchronize(device)
+        out[name] = {'us_per_sample': a.elapsed_time(b) * 1e3 / count, 'host_us_per_call': host * 1e6}
     return out
 
 
@@ -792,6 +818,9 @@ def main():
         return 0
     if args.profile == 'cfg2':
         print(json.dumps(cfg2_slice_leg(torch, device, steps=args.steps)), flush=True)
+        return 0
+    if args.profile == 'spectrum':
+        print(json.dumps(spectrum_leg(torch, device)), flush=True)
         return 0
     if args.profile == 'arnoldi-split':   # CUDA-event cost of one H·psi and of 12-iteration attempts
         from laqphysics_b200 import workloads

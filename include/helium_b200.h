@@ -325,6 +325,33 @@ int he_volkov_add(int nlab, int nouter, int ns, int ne, int nang, const void *q,
                   void *stream);
 
 /* ------------------------------------------------------------------------------------
+ * One surface sample in one launch.  Replaces the per-sample chain of
+ * python/streaming_surface.py:252-255 (flux frame python/helium3d.py:52-77 ->
+ * SurfaceContractor.__call__ python/surface_contract.py:41-56 -> VolkovAccumulator.add
+ * python/streaming_surface.py:54-64) with one cooperative launch: the frame of he_flux
+ * (same arithmetic, written to `frame` as (c, s, r)), q of he_surface_contract (partial
+ * sums per CTA, added in CTA order: reproducible, equal to he_surface_contract's q up to
+ * summation order) written to `q`, and the Volkov update of he_volkov_add.
+ * he_sample_create keeps the given device tables (stencil window J/JP, the contraction
+ * entry lists, the Volkov tests/harmonics/energy/k/unit; the caller keeps them alive) and
+ * allocates the per-CTA partial sums; ns <= 16 surface rows and nlab*nouter*ns <= 1024
+ * (else HE_ERR_SHAPE).  The CTAs wait for each other's partial sums with a bounded poll:
+ * when it runs out the sample is incomplete and he_sample_status reports HE_ERR_DEVICE
+ * (once).  he_sample_grid: CTAs per launch.
+ * ---------------------------------------------------------------------------------- */
+typedef struct he_sample *he_sample_handle;
+int he_sample_create(he_sample_handle *out, he_handle op, int ns, int lo, int width, const void *J, const void *JP,
+                     int nunique, int nlab, int nouter, const int *eptr, const int *ecol, const int *einner,
+                     const double *ecoef, const int *eouter, const int *column, int ne, int nang, const void *tests,
+                     const void *harmonics, const double *energy, const double *k, const double *unit);
+int he_sample_record(he_sample_handle h, const void *psi, const void *chi, const double *field, double time,
+                     const double *int_a, double int_a2, double d, int first, void *frame, void *q, void *amplitude,
+                     void *previous, void *stream);
+int he_sample_grid(he_sample_handle h);
+int he_sample_status(he_sample_handle h);
+int he_sample_destroy(he_sample_handle h);
+
+/* ------------------------------------------------------------------------------------
  * Run diagnostics on the device.  Replaces the checkpoint diagnostics of
  * python/run3d.py:212-224 (which copy the whole state to the host): out[0] = real-region
  * norm sum |u(i,j,c)|^2 f_i f_j with f = interior weight / |weight|, out[1] + i out[2] =

@@ -85,6 +85,11 @@ SIGNATURES = {
     'he_surface_contract': (I, [ct.c_longlong, I, I, I, I, P, P, ct.c_longlong, ct.c_longlong, ct.c_longlong,
                                 P, P, P, P, P, P, P, P]),
     'he_volkov_add': (I, [I, I, I, I, I, P, P, P, P, P, P, D, P, D, D, I, P, P, P]),
+    'he_sample_create': (I, [P, P, I, I, I, P, P, I, I, I, P, P, P, P, P, P, I, I, P, P, P, P, P]),
+    'he_sample_record': (I, [P, P, P, P, D, P, D, D, I, P, P, P, P, P]),
+    'he_sample_grid': (I, [P]),
+    'he_sample_status': (I, [P]),
+    'he_sample_destroy': (I, [P]),
     'he_vec_norms_noalloc': (I, [ct.c_longlong, I, P, ct.c_longlong, P, P]),
     'he_diagnostics': (I, [P, P, P, P, P, P, ct.POINTER(D), P]),
     'he_plan_build': (P, [I, I, P, P, P, I, P, P, P, P, I, I, P, P, P, P]),

@@ -9,7 +9,11 @@
 //                        current[j,e,a] = i sqrt(2) phase(e,a) sum_l harmonics[l,a]
 //                                         sum_s q[j,l,s] tests[l,e,s],
 //                        phase = exp(i (E t + k (u_a . int A) + int A^2 / 2))
-//                        — python/streaming_surface.py:54-64 (and its GPU twin :97-109).
+//                        — python/streaming_surface.py:54-64 (and its GPU twin :97-109);
+//   he_sample_record     one surface sample in ONE launch: the flux frame of the state
+//                        (he_flux's arithmetic), the contraction and the Volkov update —
+//                        the chain python/streaming_surface.py:252-255 runs per sample.
+#include <algorithm>
 #include <cmath>
 
 #include "common.cuh"
@@ -60,6 +64,43 @@ surface_contract_kernel(long long n, int nunique, int nouter, int ns, const doub
     }
 }
 
+// Volkov item idx = (label j, energy e, direction a): current = i sqrt(2) phase sum_l
+// harm[l, a] sum_s q[j, l, s] tests[l, e, s]; trapezoid update of the amplitude.
+__device__ __forceinline__ void volkov_item(long long idx, int nouter, int ns, int ne, int nang,
+                                            const double2 *__restrict__ q, const double2 *__restrict__ tests,
+                                            const double2 *__restrict__ harm, const double *__restrict__ energy,
+                                            const double *__restrict__ k, const double *__restrict__ unit, double time,
+                                            double ax, double ay, double az, double a2, double d, int first,
+                                            double2 *__restrict__ amplitude, double2 *__restrict__ previous)
+{
+    const int a = (int)(idx % nang);
+    const int e = (int)((idx / nang) % ne);
+    const int j = (int)(idx / ((long long)nang * ne));
+    double2 sum = mk<double>(0, 0);
+    for (int l = 0; l < nouter; ++l) {
+        double2 radial = mk<double>(0, 0);
+        const double2 *ql = q + ((size_t)j * nouter + l) * ns;
+        const double2 *tl = tests + ((size_t)l * ne + e) * ns;
+        for (int s = 0; s < ns; ++s) radial = cfma<double>(ql[s], tl[s], radial);
+        sum = cfma<double>(radial, harm[(size_t)l * nang + a], sum);
+    }
+    const double disp = unit[3 * a] * ax + unit[3 * a + 1] * ay + unit[3 * a + 2] * az;
+    const double arg = energy[e] * time + k[e] * disp + a2 / 2;
+    double sn, cs;
+    sincos(arg, &sn, &cs);
+    // current = i sqrt(2) sum * exp(i arg)
+    const double2 ph = mk<double>(cs, sn);
+    const double2 t = cmul<double>(sum, ph);
+    const double r2 = sqrt(2.0);
+    const double2 cur = mk<double>(-r2 * t.y, r2 * t.x);
+    const size_t o = (size_t)idx;
+    if (!first) {
+        const double2 prev = previous[o];
+        amplitude[o] = rfma<double>(d / 2, cadd<double>(prev, cur), amplitude[o]);
+    }
+    previous[o] = cur;
+}
+
 __global__ void __launch_bounds__(SURF_THREADS)
 volkov_add_kernel(int nlab, int nouter, int ns, int ne, int nang, const double2 *__restrict__ q,
                   const double2 *__restrict__ tests, const double2 *__restrict__ harm, const double *__restrict__ energy,
@@ -69,34 +110,142 @@ volkov_add_kernel(int nlab, int nouter, int ns, int ne, int nang, const double2 
 {
     const long long total = (long long)nlab * ne * nang;
     for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
-         idx += (long long)gridDim.x * blockDim.x) {
-        const int a = (int)(idx % nang);
-        const int e = (int)((idx / nang) % ne);
-        const int j = (int)(idx / ((long long)nang * ne));
-        double2 sum = mk<double>(0, 0);
-        for (int l = 0; l < nouter; ++l) {
-            double2 radial = mk<double>(0, 0);
-            const double2 *ql = q + ((size_t)j * nouter + l) * ns;
-            const double2 *tl = tests + ((size_t)l * ne + e) * ns;
-            for (int s = 0; s < ns; ++s) radial = cfma<double>(ql[s], tl[s], radial);
-            sum = cfma<double>(radial, harm[(size_t)l * nang + a], sum);
+         idx += (long long)gridDim.x * blockDim.x)
+        volkov_item(idx, nouter, ns, ne, nang, q, tests, harm, energy, k, unit, time, ax, ay, az, a2, d, first,
+                    amplitude, previous);
+}
+
+// ---- one launch per surface sample -------------------------------------------------
+// A cooperative grid (every CTA resident) in three phases:
+//  1. tiles of 32 radial rows x 8 channels: the flux frame rows of the tile (written out,
+//     and kept in shared memory), then the tile's share of every q entry (warp w owns the
+//     entries w, w + 8, ...; lanes run over the tile's rows), summed per CTA;
+//  2. each CTA stores its partial q, arrives on a counter and waits (bounded) for all;
+//  3. every CTA sums the partials in CTA order (the same sum in every CTA, so q is
+//     reproducible bit for bit), CTA 0 stores q, and the CTAs share the Volkov items.
+constexpr int SAMPLE_THREADS = 256, SAMPLE_TA = 32, SAMPLE_TC = SAMPLE_THREADS / SAMPLE_TA;
+constexpr int SAMPLE_NS_MAX = 16, SAMPLE_NQ_MAX = 1024;
+constexpr int SAMPLE_WAIT_LIMIT = 1 << 22;   // polls of the arrival counter (about a second)
+
+struct SampleArgs {
+    DeviceTables<double> t;                  // n, nc and the dipole edges of the operator
+    const double2 *psi;
+    double2 *frame;                          // (c, s, r): frame[r + n (s + ns c)], as he_flux
+    int ns, lo, width;
+    const double2 *J, *JP;
+    double f0, f1, f2;
+    const double2 *chi;
+    int nunique, nlab, nouter;
+    const int *eptr, *ecol, *einner, *eouter, *column;
+    const double *ecoef;
+    double2 *q;
+    int ne, nang;
+    const double2 *tests, *harm;
+    const double *energy, *k, *unit;
+    double time, ax, ay, az, a2, d;
+    int first;
+    double2 *amplitude, *previous;
+    double2 *partial;                        // gridDim.x x nq
+    unsigned *arrived;                       // zeroed before the launch
+    int *err;
+};
+
+__global__ void __launch_bounds__(SAMPLE_THREADS) surface_sample_kernel(const __grid_constant__ SampleArgs g)
+{
+    extern __shared__ __align__(16) unsigned char sample_smem[];
+    __shared__ int lost;
+    const int n = g.t.n, nc = g.t.nc, ns = g.ns;
+    const int nq = g.nlab * g.nouter * ns;
+    double2 *F = reinterpret_cast<double2 *>(sample_smem);          // [ns][SAMPLE_TC][SAMPLE_TA]
+    double2 *Q = F + (size_t)ns * SAMPLE_THREADS;                   // [nq]
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int al = tid % SAMPLE_TA, cl = tid / SAMPLE_TA;
+    const size_t nn = (size_t)n * n;
+    const int tiles_a = (n + SAMPLE_TA - 1) / SAMPLE_TA, tiles = tiles_a * ((nc + SAMPLE_TC - 1) / SAMPLE_TC);
+    if (tid == 0) lost = 0;
+    for (int i = tid; i < nq; i += SAMPLE_THREADS) Q[i] = mk<double>(0, 0);
+    __syncthreads();
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int a0 = (tile % tiles_a) * SAMPLE_TA, c0 = (tile / tiles_a) * SAMPLE_TC;
+        const int a = a0 + al, c = c0 + cl;
+        if (a < n && c < nc) {
+            const double2 *pc = g.psi + nn * c + a;
+            for (int s = 0; s < ns; ++s) {
+                double2 acc = mk<double>(0, 0);
+                for (int q = 0; q < g.width; ++q)
+                    acc = cfma<double>(ldg<double>(g.J + (size_t)s * g.width + q), pc[(size_t)n * (g.lo + q)], acc);
+                for (int k = __ldg(g.t.dptr + c), e = __ldg(g.t.dptr + c + 1); k < e; ++k) {
+                    if (__ldg(g.t.de + k) != 2) continue;
+                    const double2 *dk = g.t.dcoef + 3 * (size_t)k;
+                    double2 coef = cscale<double>(g.f0, ldg<double>(dk));
+                    coef = rfma<double>(g.f1, ldg<double>(dk + 1), coef);
+                    coef = rfma<double>(g.f2, ldg<double>(dk + 2), coef);
+                    if (sqrt(cabs2<double>(coef)) <= 1e-15) continue;
+                    const double2 *ps = g.psi + nn * __ldg(g.t.dc + k) + a;
+                    double2 part = mk<double>(0, 0);
+                    for (int q = 0; q < g.width; ++q)
+                        part = cfma<double>(ldg<double>(g.JP + (size_t)s * g.width + q), ps[(size_t)n * (g.lo + q)], part);
+                    acc = cfma<double>(coef, part, acc);
+                }
+                F[(s * SAMPLE_TC + cl) * SAMPLE_TA + al] = acc;
+                g.frame[a + (size_t)n * (s + (size_t)ns * c)] = acc;
+            }
+        } else {
+            for (int s = 0; s < ns; ++s) F[(s * SAMPLE_TC + cl) * SAMPLE_TA + al] = mk<double>(0, 0);
         }
-        const double disp = unit[3 * a] * ax + unit[3 * a + 1] * ay + unit[3 * a + 2] * az;
-        const double arg = energy[e] * time + k[e] * disp + a2 / 2;
-        double sn, cs;
-        sincos(arg, &sn, &cs);
-        // current = i sqrt(2) sum * exp(i arg)
-        const double2 ph = mk<double>(cs, sn);
-        const double2 t = cmul<double>(sum, ph);
-        const double r2 = sqrt(2.0);
-        const double2 cur = mk<double>(-r2 * t.y, r2 * t.x);
-        const size_t o = (size_t)idx;
-        if (!first) {
-            const double2 prev = previous[o];
-            amplitude[o] = rfma<double>(d / 2, cadd<double>(prev, cur), amplitude[o]);
+        __syncthreads();
+        for (int qi = warp; qi < nq; qi += SAMPLE_THREADS / 32) {
+            const int s = qi % ns, o = (qi / ns) % g.nouter, j = qi / (ns * g.nouter);
+            const size_t col = (size_t)g.column[j];
+            double2 acc = mk<double>(0, 0);
+            for (int e = g.eptr[j]; e < g.eptr[j + 1]; ++e) {
+                const int ce = g.ecol[e];
+                if (g.eouter[e] != o || ce < c0 || ce >= c0 + SAMPLE_TC) continue;
+                double2 part = mk<double>(0, 0);
+                if (a0 + lane < n)
+                    part = cfma_conj<double>(g.chi[((size_t)g.einner[e] * n + a0 + lane) * g.nunique + col],
+                                             F[(s * SAMPLE_TC + (ce - c0)) * SAMPLE_TA + lane], part);
+                acc = rfma<double>(g.ecoef[e], part, acc);
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                acc.x += __shfl_down_sync(0xffffffffu, acc.x, off);
+                acc.y += __shfl_down_sync(0xffffffffu, acc.y, off);
+            }
+            if (lane == 0) Q[qi] = cadd<double>(Q[qi], acc);
         }
-        previous[o] = cur;
+        __syncthreads();
     }
+    for (int i = tid; i < nq; i += SAMPLE_THREADS) g.partial[(size_t)blockIdx.x * nq + i] = Q[i];
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        atomicAdd(g.arrived, 1u);
+        bool ok = false;
+        for (int k = 0; k < SAMPLE_WAIT_LIMIT && !ok; ++k) {
+            ok = *reinterpret_cast<volatile unsigned *>(g.arrived) >= gridDim.x;
+            if (!ok) __nanosleep(256);
+        }
+        __threadfence();
+        if (!ok) {
+            lost = 1;
+            atomicExch(g.err, 1);
+        }
+    }
+    __syncthreads();
+    if (lost) return;
+    for (int i = tid; i < nq; i += SAMPLE_THREADS) {
+        double2 v = mk<double>(0, 0);
+        for (int b = 0; b < (int)gridDim.x; ++b) v = cadd<double>(v, __ldcg(g.partial + (size_t)b * nq + i));
+        Q[i] = v;
+        if (blockIdx.x == 0) g.q[i] = v;
+    }
+    __syncthreads();
+    const long long total = (long long)g.nlab * g.ne * g.nang;
+    for (long long idx = blockIdx.x * (long long)SAMPLE_THREADS + tid; idx < total;
+         idx += (long long)gridDim.x * SAMPLE_THREADS)
+        volkov_item(idx, g.nouter, ns, g.ne, g.nang, Q, g.tests, g.harm, g.energy, g.k, g.unit, g.time, g.ax, g.ay,
+                    g.az, g.a2, g.d, g.first, g.amplitude, g.previous);
 }
 
 }  // namespace he
@@ -133,5 +282,120 @@ extern "C" int he_volkov_add(int nlab, int nouter, int ns, int ne, int nang, con
         static_cast<const double2 *>(harmonics), energy, k, unit, time, int_a[0], int_a[1], int_a[2], int_a2, d, first,
         static_cast<double2 *>(amplitude), static_cast<double2 *>(previous));
     HE_CUDA_TRY(cudaGetLastError());
+    return HE_OK;
+}
+
+// ---- fused surface sample ------------------------------------------------------------
+struct he_sample {
+    int device = 0;
+    he::SampleArgs args{};                   // the tables; per-sample fields are set by he_sample_record
+    int grid = 0;
+    size_t smem = 0;
+    double2 *partial = nullptr;
+    unsigned *arrived = nullptr;
+    int *err = nullptr;
+    ~he_sample()
+    {
+        cudaFree(partial);
+        cudaFree(arrived);
+        cudaFree(err);
+    }
+};
+
+extern "C" int he_sample_create(he_sample **out, he_handle op, int ns, int lo, int width, const void *J,
+                                const void *JP, int nunique, int nlab, int nouter, const int *eptr, const int *ecol,
+                                const int *einner, const double *ecoef, const int *eouter, const int *column, int ne,
+                                int nang, const void *tests, const void *harmonics, const double *energy,
+                                const double *k, const double *unit)
+{
+    if (!out || !op || !J || !JP || !eptr || !ecol || !einner || !ecoef || !eouter || !column || !tests || !harmonics ||
+        !energy || !k || !unit || nunique < 1 || nlab < 1 || nouter < 1 || ne < 1 || nang < 1)
+        return he_fail(HE_ERR_ARG, "bad surface sample argument", __FILE__, __LINE__);
+    if (ns < 1 || ns > SAMPLE_NS_MAX || width < 1 || lo < 0 || lo + width > op->n)
+        return he_fail(HE_ERR_SHAPE, "surface stencil outside the grid or more than 16 surface rows", __FILE__,
+                       __LINE__);
+    const int nq = nlab * nouter * ns;
+    if (nq > SAMPLE_NQ_MAX)
+        return he_fail(HE_ERR_SHAPE, "more than 1024 contracted surface values per sample", __FILE__, __LINE__);
+    *out = nullptr;
+    int device = 0;
+    HE_CUDA_TRY(cudaGetDevice(&device));
+    he_sample *h = new he_sample();
+    h->device = device;
+    SampleArgs &a = h->args;
+    a.t = op->t64;
+    a.ns = ns; a.lo = lo; a.width = width;
+    a.J = static_cast<const double2 *>(J); a.JP = static_cast<const double2 *>(JP);
+    a.nunique = nunique; a.nlab = nlab; a.nouter = nouter;
+    a.eptr = eptr; a.ecol = ecol; a.einner = einner; a.eouter = eouter; a.column = column; a.ecoef = ecoef;
+    a.ne = ne; a.nang = nang;
+    a.tests = static_cast<const double2 *>(tests); a.harm = static_cast<const double2 *>(harmonics);
+    a.energy = energy; a.k = k; a.unit = unit;
+    h->smem = ((size_t)ns * SAMPLE_THREADS + nq) * sizeof(double2);
+    const int tiles = ((op->n + SAMPLE_TA - 1) / SAMPLE_TA) * ((op->nc + SAMPLE_TC - 1) / SAMPLE_TC);
+    const long long items = ((long long)nlab * ne * nang + SAMPLE_THREADS - 1) / SAMPLE_THREADS;
+    const cudaError_t limit = he_smem_limit(reinterpret_cast<const void *>(surface_sample_kernel), h->smem);
+    if (limit != cudaSuccess) {
+        he_set_error(cudaGetErrorString(limit), __FILE__, __LINE__);
+        delete h;
+        return HE_ERR_CUDA;
+    }
+    const int resident = resident_ctas(reinterpret_cast<const void *>(surface_sample_kernel), SAMPLE_THREADS, h->smem) *
+                         sm_count(h->device);
+    h->grid = (int)std::max<long long>(1, std::min<long long>(resident, std::max<long long>(tiles, items)));
+    auto fail = [&](cudaError_t e) {
+        he_set_error(cudaGetErrorString(e), __FILE__, __LINE__);
+        delete h;
+        return HE_ERR_CUDA;
+    };
+    cudaError_t e = cudaMalloc(&h->partial, (size_t)h->grid * nq * sizeof(double2));
+    if (e == cudaSuccess) e = cudaMalloc(&h->arrived, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMalloc(&h->err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(h->err, 0, sizeof(int));
+    if (e != cudaSuccess) return fail(e);
+    a.partial = h->partial; a.arrived = h->arrived; a.err = h->err;
+    *out = h;
+    return HE_OK;
+}
+
+extern "C" int he_sample_record(he_sample *h, const void *psi, const void *chi, const double *field, double time,
+                                const double *int_a, double int_a2, double d, int first, void *frame, void *q,
+                                void *amplitude, void *previous, void *stream)
+{
+    if (!h || !psi || !chi || !field || !int_a || !frame || !q || !amplitude || !previous)
+        return he_fail(HE_ERR_ARG, "null surface sample argument", __FILE__, __LINE__);
+    SampleArgs a = h->args;
+    a.psi = static_cast<const double2 *>(psi);
+    a.chi = static_cast<const double2 *>(chi);
+    a.f0 = field[0]; a.f1 = field[1]; a.f2 = field[2];
+    a.time = time; a.ax = int_a[0]; a.ay = int_a[1]; a.az = int_a[2]; a.a2 = int_a2; a.d = d; a.first = first;
+    a.frame = static_cast<double2 *>(frame);
+    a.q = static_cast<double2 *>(q);
+    a.amplitude = static_cast<double2 *>(amplitude);
+    a.previous = static_cast<double2 *>(previous);
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    HE_CUDA_TRY(he_smem_limit(reinterpret_cast<const void *>(surface_sample_kernel), h->smem));
+    HE_CUDA_TRY(cudaMemsetAsync(h->arrived, 0, sizeof(unsigned), s));
+    void *params[] = {&a};
+    HE_CUDA_TRY(cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(surface_sample_kernel), dim3(h->grid),
+                                            dim3(SAMPLE_THREADS), params, h->smem, s));
+    return HE_OK;
+}
+
+extern "C" int he_sample_grid(he_sample *h) { return h ? h->grid : 0; }
+
+extern "C" int he_sample_status(he_sample *h)
+{
+    if (!h) return he_fail(HE_ERR_ARG, "null surface sample", __FILE__, __LINE__);
+    int v = 0;
+    HE_CUDA_TRY(cudaMemcpy(&v, h->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (!v) return HE_OK;
+    HE_CUDA_TRY(cudaMemset(h->err, 0, sizeof(int)));
+    return he_fail(HE_ERR_DEVICE, "surface sample: the wait for every CTA's partial sums ran out", __FILE__, __LINE__);
+}
+
+extern "C" int he_sample_destroy(he_sample *h)
+{
+    delete h;
     return HE_OK;
 }

@@ -10,7 +10,8 @@ Restates, with the reference's call surface:
   ``add`` runs one device launch per surface sample, the amplitude never leaves the
   device until ``payload``/``write``;
 * ``SurfaceSampler``: flux frame -> ionic contraction -> Volkov accumulation for one
-  surface sample, entirely on the device (no host copy of the frame).
+  surface sample, entirely on the device (no host copy of the frame), by default in one
+  launch (``FusedSample``).
 """
 import ctypes as ct
 
@@ -73,9 +74,9 @@ class VolkovAccumulator:
         self.time = 0.
         self.index = -1
 
-    @torch.no_grad()
-    def add(self, index, time, q):
-        """Accumulate one sample; q: (labels, outer, ns) complex128 (device tensor or numpy)."""
+    def _advance(self, index, time):
+        """Trapezoid bookkeeping of a new sample (int A, int A^2 up to `time`): returns the
+        step d and whether this is the first sample."""
         if index != self.index + 1:
             raise ValueError('nonsequential spectrum samples')
         if self.index >= 0:
@@ -85,6 +86,16 @@ class VolkovAccumulator:
             self.intA2 += d * (np.dot(before, before) + np.dot(after, after)) / 2
         else:
             d = 0.
+        return float(d), int(self.index < 0)
+
+    def _commit(self, index, time):
+        self.time = float(time)
+        self.index = int(index)
+
+    @torch.no_grad()
+    def add(self, index, time, q):
+        """Accumulate one sample; q: (labels, outer, ns) complex128 (device tensor or numpy)."""
+        d, first = self._advance(index, time)
         if not torch.is_tensor(q):
             q = torch.as_tensor(np.ascontiguousarray(q, dtype=complex), device=self.device)
         q = q.contiguous()
@@ -93,11 +104,10 @@ class VolkovAccumulator:
         vp = lambda t: ct.c_void_p(t.data_ptr())
         check(LIB.he_volkov_add(nlab, len(self.outerstates), q.shape[2], ne, nang, vp(q), vp(self._tests),
                                 vp(self._harm), vp(self._energy), vp(self._k), vp(self._unit), float(time),
-                                intA.ctypes.data, float(self.intA2), float(d), int(self.index < 0), vp(self.amplitude),
+                                intA.ctypes.data, float(self.intA2), float(d), first, vp(self.amplitude),
                                 vp(self.previous), ct.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)),
               'he_volkov_add')
-        self.time = float(time)
-        self.index = int(index)
+        self._commit(index, time)
 
     def payload(self):
         return {'amplitude': self.amplitude.cpu().numpy(), 'previous_integrand': self.previous.cpu().numpy(),
@@ -130,26 +140,80 @@ class VolkovAccumulator:
 TorchVolkovAccumulator = VolkovAccumulator
 
 
+class FusedSample:
+    """The device tables of one surface sample launch (he_sample_create): the engine's flux
+    stencil window, the contractor's entry lists and the accumulator's Volkov tables."""
+
+    def __init__(self, engine, contractor, accumulator):
+        flux = engine.surface
+        nlab, nouter, ns = contractor.shape
+        if flux.ns != ns:
+            raise ValueError('surface stencil rows and contraction rows differ')
+        nlab_acc, ne, nang = accumulator.amplitude.shape
+        vp = lambda t: ct.c_void_p(t.data_ptr())
+        handle = ct.c_void_p()
+        check(LIB.he_sample_create(ct.byref(handle), engine.op.handle, ns, flux.lo, flux.width, vp(flux.J),
+                                   vp(flux.JP), len(contractor.unique), nlab, nouter, vp(contractor._eptr),
+                                   vp(contractor._ecol), vp(contractor._einner), vp(contractor._ecoef),
+                                   vp(contractor._eouter), vp(contractor._column), ne, nang, vp(accumulator._tests),
+                                   vp(accumulator._harm), vp(accumulator._energy), vp(accumulator._k),
+                                   vp(accumulator._unit)), 'he_sample_create')
+        self.handle = handle
+        self.grid = LIB.he_sample_grid(handle)
+        self.tables = (flux, contractor, accumulator)   # the device arrays the handle reads
+
+    def status(self):
+        check(LIB.he_sample_status(self.handle), 'he_sample_status')
+
+    def __del__(self):
+        if getattr(self, 'handle', None):
+            LIB.he_sample_destroy(self.handle)
+            self.handle = None
+
+
 class SurfaceSampler:
     """One tSURFF surface sample on the device: flux frame (engine), ionic contraction
-    with the device channel functions chi, Volkov accumulation.  Optional storage in the
-    reference's sharded layout (surface_storage.ShardedArray): `projected` keeps q of every
-    sample (storage mode 'projected', python/streaming_surface.py:255), `raw` the flux frame
-    (mode 'raw_shards', python/run3d.py:139-141)."""
+    with the device channel functions chi, Volkov accumulation.  By default the three run
+    as one launch (``FusedSample``, he_sample_record); ``fused=False`` runs them as three
+    (he_flux, he_surface_contract, he_volkov_add).  Optional storage in the reference's
+    sharded layout (surface_storage.ShardedArray): `projected` keeps q of every sample
+    (storage mode 'projected', python/streaming_surface.py:255), `raw` the flux frame (mode
+    'raw_shards', python/run3d.py:139-141)."""
 
-    def __init__(self, engine, contractor, accumulator, projected=None, raw=None):
+    def __init__(self, engine, contractor, accumulator, projected=None, raw=None, fused=True):
         self.engine, self.contractor, self.accumulator = engine, contractor, accumulator
         self.projected, self.raw = projected, raw
+        self.fused = FusedSample(engine, contractor, accumulator) if fused else None
 
     @torch.no_grad()
     def record(self, index, time, state, field, chi):
-        frame = self.engine.surface.frame(state, field)
-        if self.raw is not None:
-            self.raw[index] = frame
         if not torch.is_tensor(chi):
             chi = torch.as_tensor(np.ascontiguousarray(chi, dtype=complex), device=self.engine.device)
-        q = self.contractor.contract(chi, frame)
-        self.accumulator.add(index, time, q)
+        if self.fused is None:
+            frame = self.engine.surface.frame(state, field)
+            q = self.contractor.contract(chi, frame)
+            self.accumulator.add(index, time, q)
+        else:
+            frame, q = self._record_fused(index, time, state, field, chi)
+        if self.raw is not None:
+            self.raw[index] = frame
         if self.projected is not None:
             self.projected[index] = q
         return q
+
+    def _record_fused(self, index, time, state, field, chi):
+        e, acc = self.engine, self.accumulator
+        e._check(state, torch.complex128)
+        ns = self.contractor.shape[2]
+        frame = torch.empty((e.nc, ns, e.n), dtype=torch.complex128, device=e.device)
+        q = torch.empty(self.contractor.shape, dtype=torch.complex128, device=e.device)
+        chi = chi.contiguous()
+        d, first = acc._advance(index, time)
+        f = np.ascontiguousarray(field, dtype=np.float64)
+        intA = np.ascontiguousarray(acc.intA, dtype=np.float64)
+        vp = lambda t: ct.c_void_p(t.data_ptr())
+        check(LIB.he_sample_record(self.fused.handle, vp(state), vp(chi), f.ctypes.data, float(time), intA.ctypes.data,
+                                   float(acc.intA2), d, first, vp(frame), vp(q), vp(acc.amplitude), vp(acc.previous),
+                                   ct.c_void_p(torch.cuda.current_stream(e.device).cuda_stream)), 'he_sample_record')
+        acc._commit(index, time)
+        return frame.permute(2, 1, 0), q

@@ -25,12 +25,13 @@ def ionic_channel_functions(ion, unique, avec, dt, steps, device='cuda:0'):
     return channel_functions(ion, unique, avec, dt * np.arange(steps + 1), device)
 
 
-def run(engine, contractor, config, psi0, avec, dt, steps, chi, precision='complex128', tol=1e-10, maxdim=16, t0=0.):
+def run(engine, contractor, config, psi0, avec, dt, steps, chi, precision='complex128', tol=1e-10, maxdim=16, t0=0.,
+        fused=True):
     """Propagate psi0 from t0 for `steps` velocity-gauge steps of dt, sampling the surface
-    at every step (chi[k] = channel functions at t0 + k dt); returns (accumulator, final
-    state, mean Krylov dimension)."""
+    at every step (chi[k] = channel functions at t0 + k dt; one launch per sample unless
+    fused=False); returns (accumulator, final state, mean Krylov dimension)."""
     acc = VolkovAccumulator(contractor, config, avec, device=engine.device)
-    sampler = SurfaceSampler(engine, contractor, acc)
+    sampler = SurfaceSampler(engine, contractor, acc, fused=fused)
     schedule = FieldSchedule(engine, avec, velocity=True, precision=precision)
     psi = psi0.clone() if torch.is_tensor(psi0) else engine.state(psi0)
     sampler.record(0, t0, psi, avec(t0), chi[0])

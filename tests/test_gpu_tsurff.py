@@ -20,23 +20,23 @@ CONFIG = {'radial': {'edges': [0, 1, 2, 4, 6, 8], 'order': 3, 'tail': 6, 'ecs_an
           'spectrum_energy': [.2, 1.2, 7], 'spectrum': {'theta_points': 4, 'phi_points': 1}}
 
 
-def _setup():
+def _setup(config=CONFIG):
     from laqphysics_b200.pulses import Pulse
     from laqphysics_b200.surface3d import Ionic
     from laqphysics_b200.surface_contract import SurfaceContractor
     from laqphysics_b200.workloads import coupled
-    rc = CONFIG['radial']
-    h = coupled(rc['edges'], rc['order'], CONFIG['lmax'], CONFIG['total_Lmax'], ecs_angle=rc['ecs_angle'],
-                tail=rc['tail'], cutoff_radii=tuple(CONFIG['cutoff_radii']))
+    rc = config['radial']
+    h = coupled(rc['edges'], rc['order'], config['lmax'], config['total_Lmax'], ecs_angle=rc['ecs_angle'],
+                tail=rc['tail'], cutoff_radii=tuple(config['cutoff_radii']))
     base = h.uncoupled
-    base.prepare_surface(CONFIG['surface'])
-    h.prepare_surface(CONFIG['surface'])
-    labels = [tuple(x) for x in CONFIG['ionic_channels']]
+    base.prepare_surface(config['surface'])
+    h.prepare_surface(config['surface'])
+    labels = [tuple(x) for x in config['ionic_channels']]
     unique = list(dict.fromkeys((n, l, abs(m)) for n, l, m in labels))
     columns = [unique.index((n, l, abs(m))) for n, l, m in labels]
     ion = Ionic(base, {m for n, l, m in unique})
     contractor = SurfaceContractor(base, ion, labels, unique, columns, True, h.transform, DEVICE)
-    pulse = Pulse(**CONFIG['pulses'][0]['pulse'])
+    pulse = Pulse(**config['pulses'][0]['pulse'])
     avec = lambda t: np.array([0., 0., float(pulse.vector(t))])
     return h, base, ion, contractor, avec
 
@@ -131,3 +131,38 @@ def test_sampler_keeps_projected_and_raw_history_in_shards(tmp_path):
     for i, t in enumerate(g['times'][:count]):
         np.testing.assert_allclose(flux[i], h.flux(seeded_state(h.size, 100 + i), avec(t)), rtol=1e-12, atol=1e-14)
     np.testing.assert_array_equal(ShardedArray(tmp_path / 'run' / 'projected')[:], np.array(qs))
+
+
+def test_one_launch_sample_equals_the_three_launch_chain():
+    """he_sample_record (flux frame, contraction and Volkov update in one cooperative launch
+    whose CTAs wait for each other's partial sums) against he_flux -> he_surface_contract ->
+    he_volkov_add on the same device states and channel functions: frames bit for bit, q
+    and amplitudes to rounding (q sums per CTA in a different order), on a grid of several
+    CTAs; the bounded wait reports no time-out."""
+    from laqphysics_b200.engine import B200Hamiltonian
+    from laqphysics_b200.streaming_surface import SurfaceSampler, VolkovAccumulator
+    from laqphysics_b200.workloads import seeded_state
+    config = dict(CONFIG, radial={'edges': list(range(0, 21, 2)), 'order': 6, 'tail': 8, 'ecs_angle': .3},
+                  lmax=2, total_Lmax=2, cutoff_radii=[10, 14], surface=16., spectrum_energy=[.2, 3., 240],
+                  spectrum={'theta_points': 16, 'phi_points': 1})
+    h, base, ion, contractor, avec = _setup(config)
+    op = B200Hamiltonian(h, DEVICE)
+    raw1, raw3 = {}, {}
+    one = SurfaceSampler(op, contractor, VolkovAccumulator(contractor, config, avec, device=DEVICE), raw=raw1)
+    three = SurfaceSampler(op, contractor, VolkovAccumulator(contractor, config, avec, device=DEVICE), raw=raw3,
+                           fused=False)
+    assert one.fused.grid > 1 and three.fused is None
+    rng = np.random.default_rng(3)
+    chi = torch.as_tensor(rng.normal(size=(ion.na * h.n, len(contractor.unique))) +
+                          1j * rng.normal(size=(ion.na * h.n, len(contractor.unique))), device=DEVICE)
+    for i in range(6):
+        t = .25 * i
+        state = op.state(seeded_state(h.size, 40 + i))
+        q1 = one.record(i, t, state, avec(t), chi)
+        q3 = three.record(i, t, state, avec(t), chi)
+        assert torch.equal(raw1[i], raw3[i])
+        scale = float(torch.max(torch.abs(q3)))
+        assert float(torch.max(torch.abs(q1 - q3))) <= 1e-14 * scale
+    a1, a3 = one.accumulator.amplitude, three.accumulator.amplitude
+    assert float(torch.max(torch.abs(a1 - a3))) <= 1e-13 * float(torch.max(torch.abs(a3)))
+    one.fused.status()
