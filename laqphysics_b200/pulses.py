@@ -16,6 +16,7 @@ sin^2 x = 1/2 - cos 2x / 2 and sin^4 x = 3/8 - cos 2x / 2 + cos 4x / 8.  For an 
 number (>= 2) of cycles the analytic final A is zero for any CEP; the value is set to
 exactly zero after the pulse so that no rounding residue acts as an impulse.
 """
+import math
 from dataclasses import dataclass
 
 import numpy as np
@@ -61,6 +62,8 @@ class Pulse:
 
     def vector(self, t):
         """A(t) = -int_start^t E(t') dt' in closed form (phasor integrals above)."""
+        if isinstance(t, (float, int)):
+            return self._vector_scalar(float(t))
         u = self._elapsed(t)
         b = 2 * np.pi / self.duration
         total = 0.
@@ -73,6 +76,20 @@ class Pulse:
         if whole >= 2 and abs(self.cycles - whole) < 1e-12:
             A = np.where(np.asarray(t) >= self.start + self.duration, 0., A)
         return A
+
+    def _vector_scalar(self, t):
+        """vector() for one time with the math module (a time-step loop calls it every step):
+        sinc(w u / 2 pi) = sin(x) / x with x = w u / 2."""
+        u = min(max(t - self.start, 0.), self.duration)
+        b = 2 * math.pi / self.duration
+        total = 0.
+        for weight, shift in _PHASORS:
+            x = (self.omega + shift * b) * u / 2
+            total += weight * u * (math.sin(x) / x if x != 0 else 1.) * math.cos(self.cep + x)
+        whole = round(self.cycles)
+        if whole >= 2 and abs(self.cycles - whole) < 1e-12 and t >= self.start + self.duration:
+            return 0.
+        return -self.field * total
 
     def _cosine_series_integral(self, t, coefficients):
         """int_0^u sum_k a_k cos(k b s) ds with u = elapsed time, b = 2 pi / T."""

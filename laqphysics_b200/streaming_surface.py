@@ -71,6 +71,7 @@ class VolkovAccumulator:
         self._unit = dev(self.unit, torch.float64)
         self.intA = np.zeros(3)
         self.intA2 = 0.
+        self._last_a = None   # (time, A(time)) of the latest sample
         self.time = 0.
         self.index = -1
 
@@ -81,7 +82,11 @@ class VolkovAccumulator:
             raise ValueError('nonsequential spectrum samples')
         if self.index >= 0:
             d = time - self.time
-            before, after = np.asarray(self.avec(self.time), float), np.asarray(self.avec(time), float)
+            cached = self._last_a
+            before = cached[1] if cached is not None and cached[0] == self.time else \
+                np.asarray(self.avec(self.time), float)
+            after = np.asarray(self.avec(time), float)
+            self._last_a = (float(time), after)
             self.intA = self.intA + d * (before + after) / 2
             self.intA2 += d * (np.dot(before, before) + np.dot(after, after)) / 2
         else:
@@ -118,6 +123,7 @@ class VolkovAccumulator:
         self.amplitude, self.previous = dev(data['amplitude']), dev(data['previous_integrand'])
         self.intA = np.array(data['intA'], float)
         self.intA2, self.time, self.index = float(data['intA2']), float(data['time']), int(data['sample_index'])
+        self._last_a = None
 
     def spectrum(self):
         """(pes, angle-integrated) as in the reference's write(): |b|^2 k and its solid-angle sum."""

@@ -94,3 +94,6 @@ def test_pulses_match_reference():
         p = Pulse(**json.loads(str(g[f'p{k}'])))
         np.testing.assert_allclose(p.electric(g['t']), g[f'p{k}_E'], rtol=1e-14, atol=1e-16)
         np.testing.assert_allclose(p.vector(g['t']), g[f'p{k}_A'], rtol=1e-13, atol=1e-16)
+        # the scalar path of a time-step loop agrees with the array path
+        scalar = np.array([p.vector(float(t)) for t in g['t']])
+        np.testing.assert_allclose(scalar, g[f'p{k}_A'], rtol=1e-13, atol=1e-16)
