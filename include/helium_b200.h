@@ -302,6 +302,20 @@ int he_gmres_shifted(he_krylov_handle k, he_handle op, he_separable_handle sep, 
                      double tol, int restart, int max_restarts, int precision, int *iterations, double *residual,
                      void *stream);
 
+/* One CF4 step (python/implicit.py:91-109): y = the state x after dt, from the vector
+ * potentials at the two Gauss points (fields: 2 x 3 host doubles, A(t + C1 dt) then
+ * A(t + C2 dt), C1,2 = 1/2 -+ sqrt(3)/6).  Each of the two exponentials (field weights
+ * (A2, A1) and (A1, A2), A1,2 = (3 -+ 2 sqrt 3)/12) is a [2/2] Pade pair of
+ * he_gmres_shifted solves in complex128 with alpha = (dt/2)/(3 +- i sqrt 3), shift
+ * a2 |A_eff|^2 - e_ref and the same preconditioner rule, followed by the phase
+ * exp(-i dt (a2 (w . |A|^2 - |A_eff|^2 / 2) + e_ref / 2)).  x is not modified (x != y);
+ * on HE_ERR_NOCONV ('GMRES did not converge') y is undefined and the caller halves dt as
+ * python/implicit.py:104-109 does.  iterations: GMRES iterations of the four solves;
+ * residual: the largest true relative residual. */
+int he_cf4_step(he_krylov_handle k, he_handle op, he_separable_handle sep, const void *diag, const void *x, void *y,
+                const double *fields, double dt, double e_ref, double a2, double tol, int restart, int max_restarts,
+                int *iterations, double *residual, void *stream);
+
 /* ------------------------------------------------------------------------------------
  * Online tSURFF (complex128).
  * he_surface_contract replaces SurfaceContractor.__call__ (python/surface_contract.py:41-56):

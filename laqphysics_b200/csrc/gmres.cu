@@ -297,13 +297,14 @@ struct he_gmres_buffers {
     GmresHeader *host = nullptr;          // pinned mirror of the header
     KrylovStatus *host_status = nullptr;
     double2 *t = nullptr, *z = nullptr, *c = nullptr, *d = nullptr, *cand = nullptr;
+    double2 *step = nullptr;              // he_cf4_step: the solution of the current Pade solve
     float2 *s32[2] = {nullptr, nullptr};
     size_t n = 0;
     long long hint_key = 0;
     int iters_seen = 0;                   // most iterations a cycle of that configuration needed
     ~he_gmres_buffers()
     {
-        cudaFree(state); cudaFree(t); cudaFree(z); cudaFree(c); cudaFree(d); cudaFree(cand);
+        cudaFree(state); cudaFree(t); cudaFree(z); cudaFree(c); cudaFree(d); cudaFree(cand); cudaFree(step);
         cudaFree(s32[0]); cudaFree(s32[1]);
         if (host) cudaFreeHost(host);
         if (host_status) cudaFreeHost(host_status);
@@ -495,4 +496,68 @@ extern "C" int he_gmres_shifted(he_krylov *k, he_handle op, he_separable *sep, c
     snprintf(msg, sizeof(msg), "GMRES did not converge: residual=%.3e, iterations=%d", gb->host->true_residual,
              gb->host->iterations);
     return he_fail(HE_ERR_NOCONV, msg, __FILE__, __LINE__);
+}
+
+extern "C" int he_vec_axpby(long long n, double a_re, double a_im, const void *x, double b_re, double b_im,
+                            const void *y, void *out, void *stream);
+
+// One commutator-free fourth-order Magnus step (python/implicit.py:91-109): two
+// exponentials with the field weights (A2, A1) and (A1, A2) of the Gauss-point vector
+// potentials, each a [2/2] Pade pair of shifted solves (I + i alpha (H(A_eff) - e_ref)) s = x,
+// alpha = (dt / 2) / (3 +- i sqrt 3), x <- 2 s - x (python/implicit.py:76-89), each solve the
+// device GMRES above, followed by the phase exp(-i dt (a2 (w . |A|^2 - |A_eff|^2 / 2) + e_ref / 2)).
+extern "C" int he_cf4_step(he_krylov *k, he_handle op, he_separable *sep, const void *diag, const void *x, void *y,
+                           const double *fields, double dt, double e_ref, double a2, double tol, int restart,
+                           int max_restarts, int *iterations, double *residual, void *stream)
+{
+    if (!k || !op || !x || !y || !fields || x == y || (!sep && !diag))
+        return he_fail(HE_ERR_ARG, "bad CF4 step argument", __FILE__, __LINE__);
+    if ((size_t)op->n * op->n * op->nc != k->n) return he_fail(HE_ERR_SHAPE, "workspace size != operator size", __FILE__, __LINE__);
+    he_gmres_buffers *gb = nullptr;
+    int rc = buffers(k, HE_C128, &gb);
+    if (rc) return rc;
+    if (!gb->step) HE_CUDA_TRY(cudaMalloc(&gb->step, k->n * sizeof(double2)));
+    const double sqrt3 = std::sqrt(3.0);
+    const double A1 = (3 - 2 * sqrt3) / 12, A2 = (3 + 2 * sqrt3) / 12;
+    const double weights[2][2] = {{A2, A1}, {A1, A2}};
+    double sumsq[2];
+    for (int a = 0; a < 2; ++a) sumsq[a] = fields[3 * a] * fields[3 * a] + fields[3 * a + 1] * fields[3 * a + 1] +
+                                           fields[3 * a + 2] * fields[3 * a + 2];
+    const long long n = (long long)k->n;
+    int total = 0;
+    double worst = 0;
+    const void *src = x;
+    for (int e = 0; e < 2; ++e) {
+        const double *w = weights[e];
+        double eff[3], effsq = 0;
+        for (int j = 0; j < 3; ++j) {
+            eff[j] = 2 * (w[0] * fields[j] + w[1] * fields[3 + j]);
+            effsq += eff[j] * eff[j];
+        }
+        const double correction = a2 * (w[0] * sumsq[0] + w[1] * sumsq[1] - .5 * effsq);
+        const double shift = a2 * effsq - e_ref;
+        for (int r = 0; r < 2; ++r) {
+            // alpha = (dt / 2) / (3 + i sigma sqrt 3) = (dt / 2) (3 - i sigma sqrt 3) / 12
+            const double sigma = r == 0 ? 1 : -1;
+            const double alpha_re = dt / 2 * 3 / 12, alpha_im = -sigma * dt / 2 * sqrt3 / 12;
+            int it = 0;
+            double res = 0;
+            rc = he_gmres_shifted(k, op, sep, diag, src, gb->step, eff, alpha_re, alpha_im, e_ref, shift, tol, restart,
+                                  max_restarts, HE_C128, &it, &res, stream);
+            total += it;
+            if (res > worst) worst = res;
+            if (rc) {
+                if (iterations) *iterations = total;
+                if (residual) *residual = worst;
+                return rc;
+            }
+            if ((rc = he_vec_axpby(n, 2, 0, gb->step, -1, 0, src, y, stream))) return rc;
+            src = y;
+        }
+        const double theta = -dt * (correction + e_ref / 2);
+        if ((rc = he_vec_axpby(n, std::cos(theta), std::sin(theta), y, 0, 0, y, y, stream))) return rc;
+    }
+    if (iterations) *iterations = total;
+    if (residual) *residual = worst;
+    return HE_OK;
 }

@@ -220,6 +220,14 @@ def gmres(apply, b, preconditioner, x0=None, tol=1e-11, restart=32, max_restarts
 
 
 _DEVICE_SOLVES = [True]
+_DEVICE_STEPS = [True]
+
+
+def device_steps(flag=True):
+    """Run a complex128 CF4 step as one C-ABI call (he_cf4_step: the four Pade solves, the
+    state updates and the phases enqueued by the library) when the device solves apply (the
+    default), or compose it here from :func:`device_gmres` calls; both run the same solves."""
+    _DEVICE_STEPS[0] = bool(flag)
 
 
 def device_solves(flag=True):
@@ -265,6 +273,29 @@ def device_gmres(engine, b, field, alpha, reference_energy, separable, shift, to
         raise RuntimeError(LIB.he_last_error().decode().split(' (')[0])
     check(status, 'he_gmres_shifted')
     return x, {'iterations': iterations.value, 'relative_residual': residual.value}
+
+
+def device_cf4(engine, x, fields, dt, reference_energy, tol):
+    """One complex128 CF4 step through he_cf4_step (python/implicit.py:91-109): fields are
+    the vector potentials at t + C1 dt and t + C2 dt.  Raises the reference's 'GMRES did not
+    converge' message when a solve fails, so :func:`cf4_step` halves dt as the reference does."""
+    separable = getattr(engine, 'separable', None)
+    flexible = bool(getattr(separable, 'flexible', False))
+    restart = 16 if flexible else 32
+    engine._check(x, torch.complex128)
+    ws = workspace(x.numel(), restart, x.device, flexible)
+    y = torch.empty_like(x)
+    f = np.ascontiguousarray(fields, dtype=np.float64)
+    iterations, residual = ct.c_int(), ct.c_double()
+    status = LIB.he_cf4_step(ws.handle, engine.op.handle, separable.handle if separable is not None else None,
+                             None if separable is not None else _vp(engine.diagonal), _vp(x), _vp(y), f.ctypes.data,
+                             float(dt), float(reference_energy), float(getattr(engine, 'a2_coefficient', 1.)),
+                             float(tol), restart, 10, ct.byref(iterations), ct.byref(residual), _stream(x.device))
+    if status == HE_ERR_NOCONV:
+        raise RuntimeError(LIB.he_last_error().decode().split(' (')[0])
+    check(status, 'he_cf4_step')
+    return y, {'linear_iterations': iterations.value, 'linear_residual': residual.value, 'dimension': 0,
+               'residual_estimate': None}
 
 
 INNER_TOLERANCE = 1e-5   # relative residual of each complex64 inner solve of a mixed Pade solve
@@ -383,6 +414,9 @@ def cf4_step(engine, x, avec, t, dt, reference_energy=0., tol=1e-11, depth=0, pr
     extra = {}
     a2 = getattr(engine, 'a2_coefficient', 1.)
     try:
+        separable = getattr(engine, 'separable', None)
+        if precision == 'complex128' and _DEVICE_STEPS[0] and _device_solver(engine, separable):
+            return device_cf4(engine, x, fields, dt, reference_energy, tol)
         for w in ((A2, A1), (A1, A2)):
             effective = 2 * np.einsum('a,aj->j', w, fields)
             correction = a2 * (np.dot(w, np.sum(fields ** 2, axis=1)) - .5 * np.dot(effective, effective))

@@ -271,3 +271,31 @@ def test_mixed_cf4_reports_its_corrections():
     A = lambda t: np.array([.02 * np.cos(t), .01 * np.sin(t), .03])
     y, info = cf4_step(op, op.state(g['x']), A, 0, float(g['dt']), float(g['e_ref']), tol=1e-12, precision='mixed')
     assert info['corrections'] >= 4 and info['fallbacks'] == 0 and info['linear_residual'] <= 1e-12
+
+
+@pytest.mark.parametrize('preconditioner', ['complex128', 'complex64', None])
+def test_whole_cf4_step_call_equals_the_composed_step(preconditioner):
+    """he_cf4_step (the four Pade solves, the state updates and both phases in one C-ABI
+    call) against the same step composed here from device GMRES solves: the same GMRES
+    iterations, states equal to rounding, the input state untouched; a tolerance no solve
+    can reach raises the reference's 'GMRES did not converge' from the whole-step call."""
+    from laqphysics_b200.implicit import C1, C2, SeparablePreconditioner, cf4_step, device_cf4, device_steps
+    g, h, op = _cf4_operator()
+    op.separable = SeparablePreconditioner(op, preconditioner) if preconditioner else None
+    A = lambda t: np.array([.02 * np.cos(t), .01 * np.sin(t), .03])
+    dt, e_ref, tol = float(g['dt']), float(g['e_ref']), float(g['tol'])
+    x = op.state(g['x'])
+    keep = x.clone()
+    y1, i1 = cf4_step(op, x, A, 0, dt, e_ref, tol=tol)
+    try:
+        device_steps(False)
+        y0, i0 = cf4_step(op, x, A, 0, dt, e_ref, tol=tol)
+    finally:
+        device_steps(True)
+    assert torch.equal(x, keep)
+    assert i1['linear_iterations'] == i0['linear_iterations'] > 0
+    assert float(torch.linalg.vector_norm(y1 - y0) / torch.linalg.vector_norm(y0)) < 1e-13
+    np.testing.assert_allclose(op.host(y1), g['y128'], rtol=1e-9, atol=1e-10)
+    fields = np.array([A(C1 * dt), A(C2 * dt)])
+    with pytest.raises(RuntimeError, match='GMRES did not converge'):
+        device_cf4(op, x, fields, dt, e_ref, 1e-17)
