@@ -311,7 +311,9 @@ int he_gmres_shifted(he_krylov_handle k, he_handle op, he_separable_handle sep, 
  * exp(-i dt (a2 (w . |A|^2 - |A_eff|^2 / 2) + e_ref / 2)).  x is not modified (x != y);
  * on HE_ERR_NOCONV ('GMRES did not converge') y is undefined and the caller halves dt as
  * python/implicit.py:104-109 does.  iterations: GMRES iterations of the four solves;
- * residual: the largest true relative residual. */
+ * residual: the largest true relative residual.  The workspace k (as for he_gmres_shifted:
+ * flexible for a complex64 preconditioner, restart <= its maxdim) also holds the step's
+ * scratch vector, so concurrent steps need one workspace each. */
 int he_cf4_step(he_krylov_handle k, he_handle op, he_separable_handle sep, const void *diag, const void *x, void *y,
                 const double *fields, double dt, double e_ref, double a2, double tol, int restart, int max_restarts,
                 int *iterations, double *residual, void *stream);
@@ -351,7 +353,9 @@ int he_volkov_add(int nlab, int nouter, int ns, int ne, int nang, const void *q,
  * allocates the per-CTA partial sums; ns <= 16 surface rows and nlab*nouter*ns <= 1024
  * (else HE_ERR_SHAPE).  The CTAs wait for each other's partial sums with a bounded poll:
  * when it runs out the sample is incomplete and he_sample_status reports HE_ERR_DEVICE
- * (once).  he_sample_grid: CTAs per launch.
+ * (once).  he_sample_grid: CTAs per launch.  The operator and the tables must outlive the
+ * handle; the handle's partial sums serve one he_sample_record at a time (records on
+ * several streams need one handle each).
  * ---------------------------------------------------------------------------------- */
 typedef struct he_sample *he_sample_handle;
 int he_sample_create(he_sample_handle *out, he_handle op, int ns, int lo, int width, const void *J, const void *JP,
