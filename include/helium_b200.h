@@ -371,6 +371,9 @@ int he_sample_record(he_sample_handle h, const void *psi, const void *chi, const
                      const double *int_a, double int_a2, double d, int first, void *frame, void *q, void *amplitude,
                      void *previous, void *stream);
 int he_sample_grid(he_sample_handle h);
+/* Test hook: later records wait for `extra` CTA arrivals that never come, so the bounded
+ * wait runs out (about a second) and he_sample_status reports HE_ERR_DEVICE; 0 restores. */
+int he_sample_set_wait_extra(he_sample_handle h, unsigned extra);
 int he_sample_status(he_sample_handle h);
 int he_sample_destroy(he_sample_handle h);
 

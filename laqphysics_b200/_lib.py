@@ -90,6 +90,7 @@ SIGNATURES = {
     'he_sample_create': (I, [P, P, I, I, I, P, P, I, I, I, P, P, P, P, P, P, I, I, P, P, P, P, P]),
     'he_sample_record': (I, [P, P, P, P, D, P, D, D, I, P, P, P, P, P]),
     'he_sample_grid': (I, [P]),
+    'he_sample_set_wait_extra': (I, [P, ct.c_uint]),
     'he_sample_status': (I, [P]),
     'he_sample_destroy': (I, [P]),
     'he_vec_norms_noalloc': (I, [ct.c_longlong, I, P, ct.c_longlong, P, P]),

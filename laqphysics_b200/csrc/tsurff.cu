@@ -125,7 +125,7 @@ volkov_add_kernel(int nlab, int nouter, int ns, int ne, int nang, const double2 
 //     reproducible bit for bit), CTA 0 stores q, and the CTAs share the Volkov items.
 constexpr int SAMPLE_THREADS = 256, SAMPLE_TA = 32, SAMPLE_TC = SAMPLE_THREADS / SAMPLE_TA;
 constexpr int SAMPLE_NS_MAX = 16, SAMPLE_NQ_MAX = 1024;
-constexpr int SAMPLE_WAIT_LIMIT = 1 << 22;   // polls of the arrival counter (about a second)
+constexpr int SAMPLE_WAIT_LIMIT = 1 << 20;   // polls of the arrival counter (about a second)
 
 struct SampleArgs {
     DeviceTables<double> t;                  // n, nc and the dipole edges of the operator
@@ -147,6 +147,7 @@ struct SampleArgs {
     double2 *amplitude, *previous;
     double2 *partial;                        // gridDim.x x nq
     unsigned *arrived;                       // zeroed before the launch
+    unsigned extra;                          // arrivals awaited beyond the grid (0; a test hook)
     int *err;
 };
 
@@ -223,7 +224,7 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) surface_sample_kernel(const __
         atomicAdd(g.arrived, 1u);
         bool ok = false;
         for (int k = 0; k < SAMPLE_WAIT_LIMIT && !ok; ++k) {
-            ok = *reinterpret_cast<volatile unsigned *>(g.arrived) >= gridDim.x;
+            ok = *reinterpret_cast<volatile unsigned *>(g.arrived) >= gridDim.x + g.extra;
             if (!ok) __nanosleep(256);
         }
         __threadfence();
@@ -383,6 +384,15 @@ extern "C" int he_sample_record(he_sample *h, const void *psi, const void *chi, 
 }
 
 extern "C" int he_sample_grid(he_sample *h) { return h ? h->grid : 0; }
+
+// Test hook: the CTAs of later records wait for `extra` arrivals beyond the grid, which never
+// come, so their bounded wait runs out (he_sample_status then reports it); 0 restores.
+extern "C" int he_sample_set_wait_extra(he_sample *h, unsigned extra)
+{
+    if (!h) return he_fail(HE_ERR_ARG, "null surface sample", __FILE__, __LINE__);
+    h->args.extra = extra;
+    return HE_OK;
+}
 
 extern "C" int he_sample_status(he_sample *h)
 {

@@ -166,3 +166,32 @@ def test_one_launch_sample_equals_the_three_launch_chain():
     a1, a3 = one.accumulator.amplitude, three.accumulator.amplitude
     assert float(torch.max(torch.abs(a1 - a3))) <= 1e-13 * float(torch.max(torch.abs(a3)))
     one.fused.status()
+
+
+def test_sample_wait_that_runs_out_reports_and_leaves_the_device_usable():
+    """The one-launch sample's only inter-CTA wait is bounded: with the test hook making the
+    CTAs wait for an arrival that never comes, the record returns, he_sample_status reports
+    HE_ERR_DEVICE once, and the next records on the same device give the three-launch
+    chain's q again."""
+    from laqphysics_b200._lib import LIB
+    from laqphysics_b200.engine import B200Hamiltonian
+    from laqphysics_b200.streaming_surface import SurfaceSampler, VolkovAccumulator
+    from laqphysics_b200.workloads import seeded_state
+    g = golden('volkov')
+    h, base, ion, contractor, avec = _setup()
+    op = B200Hamiltonian(h, DEVICE)
+    state = op.state(seeded_state(h.size, 7))
+    stalled = SurfaceSampler(op, contractor, VolkovAccumulator(contractor, CONFIG, avec, device=DEVICE))
+    assert LIB.he_sample_set_wait_extra(stalled.fused.handle, 1) == 0
+    stalled.record(0, 0., state, avec(0.), g['chi'][0])
+    torch.cuda.synchronize()
+    with pytest.raises(RuntimeError, match='ran out'):
+        stalled.fused.status()
+    stalled.fused.status()                       # reported once
+    one = SurfaceSampler(op, contractor, VolkovAccumulator(contractor, CONFIG, avec, device=DEVICE))
+    three = SurfaceSampler(op, contractor, VolkovAccumulator(contractor, CONFIG, avec, device=DEVICE), fused=False)
+    for i, t in enumerate(g['times'][:3]):
+        q1 = one.record(i, t, state, avec(t), g['chi'][i])
+        q3 = three.record(i, t, state, avec(t), g['chi'][i])
+        assert float(torch.max(torch.abs(q1 - q3))) <= 1e-14 * float(torch.max(torch.abs(q3)))
+    one.fused.status()
