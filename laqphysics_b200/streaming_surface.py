@@ -19,7 +19,7 @@ import numpy as np
 import torch
 from scipy.special import sph_harm_y, spherical_jn
 
-from ._lib import LIB, check
+from ._lib import HE_ERR_SHAPE, LIB, HeliumError, check
 
 
 def directions(config):
@@ -180,8 +180,8 @@ class FusedSample:
 class SurfaceSampler:
     """One tSURFF surface sample on the device: flux frame (engine), ionic contraction
     with the device channel functions chi, Volkov accumulation.  By default the three run
-    as one launch (``FusedSample``, he_sample_record); ``fused=False`` runs them as three
-    (he_flux, he_surface_contract, he_volkov_add).  Optional storage in the reference's
+    as one launch (``FusedSample``, he_sample_record); ``fused=False``, or a surface beyond
+    that launch's limits, runs them as three (he_flux, he_surface_contract, he_volkov_add).  Optional storage in the reference's
     sharded layout (surface_storage.ShardedArray): `projected` keeps q of every sample
     (storage mode 'projected', python/streaming_surface.py:255), `raw` the flux frame (mode
     'raw_shards', python/run3d.py:139-141)."""
@@ -189,7 +189,15 @@ class SurfaceSampler:
     def __init__(self, engine, contractor, accumulator, projected=None, raw=None, fused=True):
         self.engine, self.contractor, self.accumulator = engine, contractor, accumulator
         self.projected, self.raw = projected, raw
-        self.fused = FusedSample(engine, contractor, accumulator) if fused else None
+        self.fused = None
+        if fused:
+            try:
+                self.fused = FusedSample(engine, contractor, accumulator)
+            except HeliumError as error:
+                # beyond the one-launch limits (more than 16 surface rows or 1024 contracted
+                # values per sample): the three launches serve any size
+                if error.status != HE_ERR_SHAPE:
+                    raise
 
     @torch.no_grad()
     def record(self, index, time, state, field, chi):
