@@ -302,10 +302,11 @@ int he_gmres_shifted(he_krylov_handle k, he_handle op, he_separable_handle sep, 
                      double tol, int restart, int max_restarts, int precision, int *iterations, double *residual,
                      void *stream);
 
-/* Diagnostic: the iterations the first segment of the next he_gmres_shifted solve on k
- * enqueues (the most a converged first cycle of the same configuration needed; 0: the whole
- * restart length) and, in *key when key != NULL, the configuration it belongs to. */
-int he_gmres_segment_hint(he_krylov_handle k, long long *key);
+/* Diagnostic: in *iterations, the iterations the first segment of the next
+ * he_gmres_shifted solve on k enqueues (the most a converged first cycle of the same
+ * configuration needed; 0: the whole restart length) and, in *key when key != NULL, the
+ * configuration it belongs to. */
+int he_gmres_segment_hint(he_krylov_handle k, int *iterations, long long *key);
 
 /* One CF4 step (python/implicit.py:91-109): y = the state x after dt, from the vector
  * potentials at the two Gauss points (fields: 2 x 3 host doubles, A(t + C1 dt) then

@@ -500,12 +500,13 @@ extern "C" int he_gmres_shifted(he_krylov *k, he_handle op, he_separable *sep, c
 
 // Iterations the first segment of the next solve on this workspace enqueues (0: a whole
 // cycle), and the configuration key the hint belongs to.
-extern "C" int he_gmres_segment_hint(he_krylov *k, long long *key)
+extern "C" int he_gmres_segment_hint(he_krylov *k, int *iterations, long long *key)
 {
-    if (!k) return he_fail(HE_ERR_ARG, "null workspace", __FILE__, __LINE__);
+    if (!k || !iterations) return he_fail(HE_ERR_ARG, "null GMRES hint argument", __FILE__, __LINE__);
     const he_gmres_buffers *gb = k->gmres;
+    *iterations = gb ? gb->iters_seen : 0;
     if (key) *key = gb ? gb->hint_key : 0;
-    return gb ? gb->iters_seen : 0;
+    return HE_OK;
 }
 
 extern "C" int he_vec_axpby(long long n, double a_re, double a_im, const void *x, double b_re, double b_im,

@@ -94,3 +94,23 @@ def test_native_tensor_apply_validates_field_shape():
     h = Tables(golden('apply_ecs'))
     with pytest.raises(ValueError, match='three Cartesian'):
         tensor_apply(h, np.zeros(h.size, complex), field=(0., 1.))
+
+
+def test_step_and_sample_entries_reject_bad_arguments_on_the_host():
+    """he_cf4_step, he_gmres_shifted and the surface-sample entries check their pointers
+    and sizes before any device work: HE_ERR_ARG with a message, no CUDA call needed."""
+    from laqphysics_b200._lib import HE_ERR_ARG, LIB
+    i, d = ct.c_int(), ct.c_double()
+    fields = np.zeros(6)
+    assert LIB.he_cf4_step(None, None, None, None, None, None, fields.ctypes.data, .05, 0., 1., 1e-10, 16, 10,
+                           ct.byref(i), ct.byref(d), None) == HE_ERR_ARG
+    assert b'CF4' in LIB.he_last_error()
+    assert LIB.he_gmres_shifted(None, None, None, None, None, None, fields.ctypes.data, .01, 0., 0., 0., 1e-10, 16, 10,
+                                0, ct.byref(i), ct.byref(d), None) == HE_ERR_ARG
+    assert LIB.he_sample_create(ct.byref(ct.c_void_p()), None, 1, 0, 1, None, None, 1, 1, 1, None, None, None, None,
+                                None, None, 1, 1, None, None, None, None, None) == HE_ERR_ARG
+    assert LIB.he_sample_record(None, None, None, None, 0., None, 0., 0., 1, None, None, None, None, None) == HE_ERR_ARG
+    assert LIB.he_sample_status(None) == HE_ERR_ARG
+    assert LIB.he_sample_set_wait_extra(None, 1) == HE_ERR_ARG
+    assert LIB.he_sample_grid(None) == 0
+    assert LIB.he_gmres_segment_hint(None, ct.byref(i), None) == HE_ERR_ARG
