@@ -382,7 +382,13 @@ int enqueue_iterations(const Solve &v, int j0, int j1)
         double2 *zj = k->flexible ? k->Z + (size_t)j * k->n : v.gb->z;
         if ((rc = apply_M(v, qj, zj, done))) break;
         if ((rc = apply_A(v, zj, q1, done))) break;
-        if ((rc = krylov_cgs2(k, j + 1, q1, k->H + (size_t)j * ld, k->H + (size_t)j * ld + j + 1, v.s, 1e-14))) break;
+        // CGS2: up to 16 basis vectors as the fused sweeps (projection; update + second
+        // projection + h; the second update and 1/h after the rotation step), beyond as
+        // separate projection / update launches
+        const bool fused = j + 1 <= KRYLOV_FUSED;
+        if (fused) rc = krylov_cgs2_fused(k, j + 1, q1, j, v.s, 1e-14);
+        else rc = krylov_cgs2(k, j + 1, q1, k->H + (size_t)j * ld, k->H + (size_t)j * ld + j + 1, v.s, 1e-14);
+        if (rc) break;
         const bool checkpoint = (j + 1) % cadence == 0 || j + 1 == v.restart;
         gm_givens_kernel<<<1, 32, 0, v.s>>>(k->H, ld, j, v.restart, checkpoint, v.tol, k->status, gs);
         if (checkpoint) {     // the candidate test (runs only when the rotation step asked for it)
@@ -398,7 +404,13 @@ int enqueue_iterations(const Solve &v, int j0, int j1)
             gm_decide_kernel<<<1, 32, 0, v.s>>>(k->norm_partial, GM_BLOCKS, v.restart, v.tol, k->status, gs);
             gm_accept_kernel<<<kGrid, kThreads, 0, v.s>>>(k->n, v.gb->cand, v.x, gs);
         }
-        if (j + 1 < v.restart) gm_scale_kernel<<<kGrid, kThreads, 0, v.s>>>(k->n, q1, k->status);
+        if (j + 1 < v.restart) {
+            if (fused) {
+                if ((rc = krylov_next(k, j + 1, q1, v.s))) break;
+            } else {
+                gm_scale_kernel<<<kGrid, kThreads, 0, v.s>>>(k->n, q1, k->status);
+            }
+        }
         HE_CUDA_TRY(cudaGetLastError());
     }
     return rc;

@@ -397,6 +397,7 @@ __device__ void expm_pade13(double2 *A, double2 *R, double2 *work, int m)
 __device__ __noinline__ void arnoldi_check_block(const double2 *__restrict__ H, int ld, int j, int maxdim, double dt, double tol,
                                     double2 *__restrict__ coef, double2 *__restrict__ work, KrylovStatus *st)
 {
+    if (tol < 0) return;   // a GMRES iteration: the sweeps without the exponential's check
     const int m = j + 1;
     const bool happy = st->happy;
     const bool check = happy || (j >= 3 && ((j + 1) % 4 == 0 || j + 1 == maxdim));
@@ -884,7 +885,7 @@ dim3 sweep_grid(const he_krylov *k, const void *kernel)
 // sized to the basis (4, 8, 12 or 16 vectors).
 template <int KT>
 void launch_fused_sweeps(he_krylov *k, int kc, double2 *v, const float2 *src32, int j, int maxdim, double dt,
-                         double tol, cudaStream_t s)
+                         double tol, cudaStream_t s, double happy_below)
 {
     const int ld = k->maxdim + 1;
     arnoldi_project_kernel<KT><<<sweep_grid(k, reinterpret_cast<const void *>(arnoldi_project_kernel<KT>)), kBlock, 0, s>>>(k->Q, k->n, k->qs(), kc, v, src32, k->partial, ld, k->ticket,
@@ -892,16 +893,16 @@ void launch_fused_sweeps(he_krylov *k, int kc, double2 *v, const float2 *src32, 
     arnoldi_reorth_kernel<KT><<<sweep_grid(k, reinterpret_cast<const void *>(arnoldi_reorth_kernel<KT>)), kBlock, 0, s>>>(
         k->Q, k->n, k->qs(), kc, k->z, v, k->partial, ld, k->ticket,
                                                          k->H, k->hs(), j, maxdim, dt, tol, k->coef, k->work, k->ws(),
-                                                         k->status, 1e-13);
+                                                         k->status, happy_below);
 }
 
 int fused_sweeps(he_krylov *k, int kc, double2 *v, const float2 *src32, int j, int maxdim, double dt, double tol,
-                 cudaStream_t s)
+                 cudaStream_t s, double happy_below = 1e-13)
 {
-    if (kc <= 4) launch_fused_sweeps<4>(k, kc, v, src32, j, maxdim, dt, tol, s);
-    else if (kc <= 8) launch_fused_sweeps<8>(k, kc, v, src32, j, maxdim, dt, tol, s);
-    else if (kc <= 12) launch_fused_sweeps<12>(k, kc, v, src32, j, maxdim, dt, tol, s);
-    else launch_fused_sweeps<KRYLOV_FUSED>(k, kc, v, src32, j, maxdim, dt, tol, s);
+    if (kc <= 4) launch_fused_sweeps<4>(k, kc, v, src32, j, maxdim, dt, tol, s, happy_below);
+    else if (kc <= 8) launch_fused_sweeps<8>(k, kc, v, src32, j, maxdim, dt, tol, s, happy_below);
+    else if (kc <= 12) launch_fused_sweeps<12>(k, kc, v, src32, j, maxdim, dt, tol, s, happy_below);
+    else launch_fused_sweeps<KRYLOV_FUSED>(k, kc, v, src32, j, maxdim, dt, tol, s, happy_below);
     HE_CUDA_TRY(cudaGetLastError());
     return HE_OK;
 }
@@ -1074,6 +1075,26 @@ int expv_impl(he_krylov *k, he_handle op, const void *x, void *y, const double *
     return HE_OK;
 }
 }  // namespace
+
+namespace he {
+// The first two sweeps of a fused CGS2 iteration for GMRES (no exponential check): H[:, j]
+// gets the projections of v against Q_0..Q_{kc-1} and H[j+1, j] = h, v is updated once and
+// the second projection stays in the workspace for krylov_next.  kc <= KRYLOV_FUSED.
+int krylov_cgs2_fused(he_krylov *k, int kc, double2 *v, int j, cudaStream_t s, double happy_below)
+{
+    if (kc > KRYLOV_FUSED) return he_fail(HE_ERR_ARG, "fused CGS2 holds at most 16 vectors", __FILE__, __LINE__);
+    return fused_sweeps(k, kc, v, nullptr, j, k->maxdim, 0.0, -1.0, s, happy_below);
+}
+
+// The third sweep: v <- (v - Q z') / h, the next basis vector (nothing once the solve is done).
+int krylov_next(he_krylov *k, int kc, double2 *v, cudaStream_t s)
+{
+    arnoldi_next_kernel<<<sweep_grid(k, reinterpret_cast<const void *>(arnoldi_next_kernel)), kBlock, 0, s>>>(
+        k->Q, k->n, k->qs(), kc, k->z, k->maxdim + 1, v, nullptr, k->status);
+    HE_CUDA_TRY(cudaGetLastError());
+    return HE_OK;
+}
+}  // namespace he
 
 extern "C" int he_expv(he_krylov *k, he_handle op, const void *x, void *y, const double *field, int velocity,
                        double dt, double tol, int maxdim, int *dimension, double *estimate, void *stream)

@@ -73,4 +73,6 @@ namespace he {
 // CGS2 of v against the first kc basis vectors: H column += projections, h = ||v|| into
 // *hsub and the status word (skipped once the status says done).
 int krylov_cgs2(he_krylov *k, int kc, double2 *v, double2 *hcol, double2 *hsub, cudaStream_t s, double happy_below);
+int krylov_cgs2_fused(he_krylov *k, int kc, double2 *v, int j, cudaStream_t s, double happy_below);
+int krylov_next(he_krylov *k, int kc, double2 *v, cudaStream_t s);
 }  // namespace he
