@@ -190,7 +190,10 @@ class SurfaceSampler:
         self.engine, self.contractor, self.accumulator = engine, contractor, accumulator
         self.projected, self.raw = projected, raw
         self.fused = None
-        if fused:
+        # the one launch recomputes SurfaceFlux's frame; an engine with another surface
+        # object keeps the three launches, which call its own frame()
+        from .surface import SurfaceFlux
+        if fused and type(getattr(engine, 'surface', None)) is SurfaceFlux:
             try:
                 self.fused = FusedSample(engine, contractor, accumulator)
             except HeliumError as error:
