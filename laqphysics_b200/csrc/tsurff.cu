@@ -120,11 +120,14 @@ volkov_add_kernel(int nlab, int nouter, int ns, int ne, int nang, const double2 
 //  1. tiles of 32 radial rows x 8 channels: the flux frame rows of the tile (written out,
 //     and kept in shared memory), then the tile's share of every q entry (warp w owns the
 //     entries w, w + 8, ...; lanes run over the tile's rows), summed per CTA;
-//  2. each CTA stores its partial q, arrives on a counter and waits (bounded) for all;
-//  3. every CTA sums the partials in CTA order (the same sum in every CTA, so q is
-//     reproducible bit for bit), CTA 0 stores q, and the CTAs share the Volkov items.
+//  2. each CTA that had tiles stores its partial q; all arrive on a counter and wait
+//     (bounded) for all;
+//  3. each q entry is summed once over those partials in CTA order (reproducible bit for
+//     bit) by the CTA it falls to and stored; a second wait on the same counter; every CTA
+//     reads q and the CTAs share the Volkov items.
 constexpr int SAMPLE_THREADS = 256, SAMPLE_TA = 32, SAMPLE_TC = SAMPLE_THREADS / SAMPLE_TA;
 constexpr int SAMPLE_NS_MAX = 16, SAMPLE_NQ_MAX = 1024;
+constexpr int SAMPLE_SC = 8;                     // surface rows held in registers at a time
 constexpr int SAMPLE_WAIT_LIMIT = 1 << 20;   // polls of the arrival counter (about a second)
 
 struct SampleArgs {
@@ -151,10 +154,33 @@ struct SampleArgs {
     int *err;
 };
 
+// Arrive on the counter and wait (thread 0, bounded) until it reaches `target`; false, with
+// the error word set, when the wait ran out.  Every thread of the CTA calls it.
+__device__ bool sample_grid_wait(unsigned *arrived, unsigned target, int *err, volatile int &lost)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(arrived, 1u);
+        bool ok = false;
+        for (int k = 0; k < SAMPLE_WAIT_LIMIT && !ok; ++k) {
+            ok = *reinterpret_cast<volatile unsigned *>(arrived) >= target;
+            if (!ok) __nanosleep(256);
+        }
+        __threadfence();
+        if (!ok) {
+            lost = 1;
+            atomicExch(err, 1);
+        }
+    }
+    __syncthreads();
+    return !lost;
+}
+
 __global__ void __launch_bounds__(SAMPLE_THREADS) surface_sample_kernel(const __grid_constant__ SampleArgs g)
 {
     extern __shared__ __align__(16) unsigned char sample_smem[];
-    __shared__ int lost;
+    __shared__ volatile int lost;
     const int n = g.t.n, nc = g.t.nc, ns = g.ns;
     const int nq = g.nlab * g.nouter * ns;
     double2 *F = reinterpret_cast<double2 *>(sample_smem);          // [ns][SAMPLE_TC][SAMPLE_TA]
@@ -169,12 +195,20 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) surface_sample_kernel(const __
     for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const int a0 = (tile % tiles_a) * SAMPLE_TA, c0 = (tile / tiles_a) * SAMPLE_TC;
         const int a = a0 + al, c = c0 + cl;
-        if (a < n && c < nc) {
-            const double2 *pc = g.psi + nn * c + a;
-            for (int s = 0; s < ns; ++s) {
-                double2 acc = mk<double>(0, 0);
-                for (int q = 0; q < g.width; ++q)
-                    acc = cfma<double>(ldg<double>(g.J + (size_t)s * g.width + q), pc[(size_t)n * (g.lo + q)], acc);
+        // flux frame rows of (a, c), eight surface rows at a time: each psi value of the
+        // window is read once per chunk; per row the operations of flux_kernel, in its order
+        for (int s0 = 0; s0 < ns; s0 += SAMPLE_SC) {
+            double2 acc[SAMPLE_SC];
+#pragma unroll
+            for (int u = 0; u < SAMPLE_SC; ++u) acc[u] = mk<double>(0, 0);
+            if (a < n && c < nc) {
+                const double2 *pc = g.psi + nn * c + a;
+                for (int q = 0; q < g.width; ++q) {
+                    const double2 x = pc[(size_t)n * (g.lo + q)];
+#pragma unroll
+                    for (int u = 0; u < SAMPLE_SC; ++u)
+                        if (s0 + u < ns) acc[u] = cfma<double>(ldg<double>(g.J + (size_t)(s0 + u) * g.width + q), x, acc[u]);
+                }
                 for (int k = __ldg(g.t.dptr + c), e = __ldg(g.t.dptr + c + 1); k < e; ++k) {
                     if (__ldg(g.t.de + k) != 2) continue;
                     const double2 *dk = g.t.dcoef + 3 * (size_t)k;
@@ -183,64 +217,83 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) surface_sample_kernel(const __
                     coef = rfma<double>(g.f2, ldg<double>(dk + 2), coef);
                     if (sqrt(cabs2<double>(coef)) <= 1e-15) continue;
                     const double2 *ps = g.psi + nn * __ldg(g.t.dc + k) + a;
-                    double2 part = mk<double>(0, 0);
-                    for (int q = 0; q < g.width; ++q)
-                        part = cfma<double>(ldg<double>(g.JP + (size_t)s * g.width + q), ps[(size_t)n * (g.lo + q)], part);
-                    acc = cfma<double>(coef, part, acc);
+                    double2 part[SAMPLE_SC];
+#pragma unroll
+                    for (int u = 0; u < SAMPLE_SC; ++u) part[u] = mk<double>(0, 0);
+                    for (int q = 0; q < g.width; ++q) {
+                        const double2 y = ps[(size_t)n * (g.lo + q)];
+#pragma unroll
+                        for (int u = 0; u < SAMPLE_SC; ++u)
+                            if (s0 + u < ns)
+                                part[u] = cfma<double>(ldg<double>(g.JP + (size_t)(s0 + u) * g.width + q), y, part[u]);
+                    }
+#pragma unroll
+                    for (int u = 0; u < SAMPLE_SC; ++u)
+                        if (s0 + u < ns) acc[u] = cfma<double>(coef, part[u], acc[u]);
                 }
-                F[(s * SAMPLE_TC + cl) * SAMPLE_TA + al] = acc;
-                g.frame[a + (size_t)n * (s + (size_t)ns * c)] = acc;
-            }
-        } else {
-            for (int s = 0; s < ns; ++s) F[(s * SAMPLE_TC + cl) * SAMPLE_TA + al] = mk<double>(0, 0);
-        }
-        __syncthreads();
-        for (int qi = warp; qi < nq; qi += SAMPLE_THREADS / 32) {
-            const int s = qi % ns, o = (qi / ns) % g.nouter, j = qi / (ns * g.nouter);
-            const size_t col = (size_t)g.column[j];
-            double2 acc = mk<double>(0, 0);
-            for (int e = g.eptr[j]; e < g.eptr[j + 1]; ++e) {
-                const int ce = g.ecol[e];
-                if (g.eouter[e] != o || ce < c0 || ce >= c0 + SAMPLE_TC) continue;
-                double2 part = mk<double>(0, 0);
-                if (a0 + lane < n)
-                    part = cfma_conj<double>(g.chi[((size_t)g.einner[e] * n + a0 + lane) * g.nunique + col],
-                                             F[(s * SAMPLE_TC + (ce - c0)) * SAMPLE_TA + lane], part);
-                acc = rfma<double>(g.ecoef[e], part, acc);
+#pragma unroll
+                for (int u = 0; u < SAMPLE_SC; ++u)
+                    if (s0 + u < ns) g.frame[a + (size_t)n * (s0 + u + (size_t)ns * c)] = acc[u];
             }
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                acc.x += __shfl_down_sync(0xffffffffu, acc.x, off);
-                acc.y += __shfl_down_sync(0xffffffffu, acc.y, off);
+            for (int u = 0; u < SAMPLE_SC; ++u)
+                if (s0 + u < ns) F[((s0 + u) * SAMPLE_TC + cl) * SAMPLE_TA + al] = acc[u];
+        }
+        __syncthreads();
+        // contraction partials of this tile: warp w owns the (label, outer) pairs w, w + 8, ...
+        // and with them the q entries of all their surface rows; each entry of a pair is read
+        // once per chunk of eight rows
+        for (int jo = warp; jo < g.nlab * g.nouter; jo += SAMPLE_THREADS / 32) {
+            const int j = jo / g.nouter, o = jo % g.nouter;
+            const size_t col = (size_t)g.column[j];
+            for (int s0 = 0; s0 < ns; s0 += SAMPLE_SC) {
+                double2 acc[SAMPLE_SC];
+#pragma unroll
+                for (int u = 0; u < SAMPLE_SC; ++u) acc[u] = mk<double>(0, 0);
+                for (int e = g.eptr[j]; e < g.eptr[j + 1]; ++e) {
+                    const int ce = g.ecol[e];
+                    if (g.eouter[e] != o || ce < c0 || ce >= c0 + SAMPLE_TC) continue;
+                    const double w = g.ecoef[e];
+                    const double2 x = a0 + lane < n ? g.chi[((size_t)g.einner[e] * n + a0 + lane) * g.nunique + col]
+                                                    : mk<double>(0, 0);
+#pragma unroll
+                    for (int u = 0; u < SAMPLE_SC; ++u) {
+                        if (s0 + u >= ns) continue;
+                        double2 part = mk<double>(0, 0);
+                        if (a0 + lane < n)
+                            part = cfma_conj<double>(x, F[((s0 + u) * SAMPLE_TC + (ce - c0)) * SAMPLE_TA + lane], part);
+                        acc[u] = rfma<double>(w, part, acc[u]);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < SAMPLE_SC; ++u) {
+                    if (s0 + u >= ns) continue;
+                    double2 v = acc[u];
+#pragma unroll
+                    for (int off = 16; off > 0; off >>= 1) {
+                        v.x += __shfl_down_sync(0xffffffffu, v.x, off);
+                        v.y += __shfl_down_sync(0xffffffffu, v.y, off);
+                    }
+                    if (lane == 0) Q[jo * ns + s0 + u] = cadd<double>(Q[jo * ns + s0 + u], v);
+                }
             }
-            if (lane == 0) Q[qi] = cadd<double>(Q[qi], acc);
         }
         __syncthreads();
     }
-    for (int i = tid; i < nq; i += SAMPLE_THREADS) g.partial[(size_t)blockIdx.x * nq + i] = Q[i];
-    __syncthreads();
-    if (tid == 0) {
-        __threadfence();
-        atomicAdd(g.arrived, 1u);
-        bool ok = false;
-        for (int k = 0; k < SAMPLE_WAIT_LIMIT && !ok; ++k) {
-            ok = *reinterpret_cast<volatile unsigned *>(g.arrived) >= gridDim.x + g.extra;
-            if (!ok) __nanosleep(256);
-        }
-        __threadfence();
-        if (!ok) {
-            lost = 1;
-            atomicExch(g.err, 1);
-        }
-    }
-    __syncthreads();
-    if (lost) return;
-    for (int i = tid; i < nq; i += SAMPLE_THREADS) {
+    // CTAs past the last tile hold no partial sums
+    const int with_tiles = (int)gridDim.x < tiles ? (int)gridDim.x : tiles;
+    if ((int)blockIdx.x < with_tiles)
+        for (int i = tid; i < nq; i += SAMPLE_THREADS) g.partial[(size_t)blockIdx.x * nq + i] = Q[i];
+    // every CTA's partials, then each q entry summed once (in CTA order, by the CTA and
+    // thread it falls to), then every CTA reads q
+    if (!sample_grid_wait(g.arrived, gridDim.x + g.extra, g.err, lost)) return;
+    for (int i = (int)blockIdx.x + (int)gridDim.x * tid; i < nq; i += (int)gridDim.x * SAMPLE_THREADS) {
         double2 v = mk<double>(0, 0);
-        for (int b = 0; b < (int)gridDim.x; ++b) v = cadd<double>(v, __ldcg(g.partial + (size_t)b * nq + i));
-        Q[i] = v;
-        if (blockIdx.x == 0) g.q[i] = v;
+        for (int b = 0; b < with_tiles; ++b) v = cadd<double>(v, __ldcg(g.partial + (size_t)b * nq + i));
+        g.q[i] = v;
     }
+    if (!sample_grid_wait(g.arrived, 2 * gridDim.x + g.extra, g.err, lost)) return;
+    for (int i = tid; i < nq; i += SAMPLE_THREADS) Q[i] = __ldcg(g.q + i);
     __syncthreads();
     const long long total = (long long)g.nlab * g.ne * g.nang;
     for (long long idx = blockIdx.x * (long long)SAMPLE_THREADS + tid; idx < total;
