@@ -119,7 +119,8 @@ volkov_add_kernel(int nlab, int nouter, int ns, int ne, int nang, const double2 
 // A cooperative grid (every CTA resident) in three phases:
 //  1. tiles of 32 radial rows x 8 channels: the flux frame rows of the tile (written out,
 //     and kept in shared memory), then the tile's share of every q entry (warp w owns the
-//     entries w, w + 8, ...; lanes run over the tile's rows), summed per CTA;
+//     (label, outer state) pairs w, w + 8, ... with all their surface rows; lanes run over
+//     the tile's radial rows), summed per CTA;
 //  2. each CTA that had tiles stores its partial q; all arrive on a counter and wait
 //     (bounded) for all;
 //  3. each q entry is summed once over those partials in CTA order (reproducible bit for
