@@ -320,6 +320,11 @@ int he_gmres_segment_hint(he_krylov_handle k, int *iterations, long long *key);
  * residual: the largest true relative residual.  The workspace k (as for he_gmres_shifted:
  * flexible for a complex64 preconditioner, restart <= its maxdim) also holds the step's
  * scratch vector, so concurrent steps need one workspace each. */
+/* The host arithmetic of he_cf4_step (no device work): out[5 e .. 5 e + 4] for exponential
+ * e = 0, 1 = the effective field (3), the preconditioner shift a2 |A_eff|^2 - e_ref and the
+ * phase angle -dt (a2 (w . |A|^2 - |A_eff|^2 / 2) + e_ref / 2); out[10..13] = the two Pade
+ * alphas (re, im).  out: 14 host doubles. */
+int he_cf4_coefficients(const double *fields, double dt, double e_ref, double a2, double *out);
 int he_cf4_step(he_krylov_handle k, he_handle op, he_separable_handle sep, const void *diag, const void *x, void *y,
                 const double *fields, double dt, double e_ref, double a2, double tol, int restart, int max_restarts,
                 int *iterations, double *residual, void *stream);

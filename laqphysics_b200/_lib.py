@@ -82,6 +82,7 @@ SIGNATURES = {
     'he_separable_set_tile': (I, [P, I]),
     'he_gmres_shifted': (I, [P, P, P, P, P, P, P, D, D, D, D, D, I, I, I, ct.POINTER(I), ct.POINTER(D), P]),
     'he_cf4_step': (I, [P, P, P, P, P, P, P, D, D, D, D, I, I, ct.POINTER(I), ct.POINTER(D), P]),
+    'he_cf4_coefficients': (I, [P, D, D, D, P]),
     'he_gmres_segment_hint': (I, [P, ct.POINTER(I), ct.POINTER(ct.c_longlong)]),
     'he_separable_status': (I, [P]),
     'he_surface_contract': (I, [ct.c_longlong, I, I, I, I, P, P, ct.c_longlong, ct.c_longlong, ct.c_longlong,

@@ -521,6 +521,41 @@ extern "C" int he_gmres_segment_hint(he_krylov *k, int *iterations, long long *k
     return HE_OK;
 }
 
+// Host arithmetic of a CF4 step (python/implicit.py:91-109, :76-89) from the vector
+// potentials at the two Gauss points (fields: 2 x 3).  out[5 e .. 5 e + 4] for exponential
+// e = 0, 1 (field weights (A2, A1), (A1, A2)): the effective field (3), the preconditioner
+// shift a2 |A_eff|^2 - e_ref, and the phase angle -dt (a2 (w . |A|^2 - |A_eff|^2 / 2) +
+// e_ref / 2); out[10 + 2 r], out[11 + 2 r]: alpha = (dt / 2) / (3 + i sigma_r sqrt 3), sigma
+// = +1, -1.
+extern "C" int he_cf4_coefficients(const double *fields, double dt, double e_ref, double a2, double *out)
+{
+    if (!fields || !out) return he_fail(HE_ERR_ARG, "null CF4 coefficient argument", __FILE__, __LINE__);
+    const double sqrt3 = std::sqrt(3.0);
+    const double A1 = (3 - 2 * sqrt3) / 12, A2 = (3 + 2 * sqrt3) / 12;
+    const double weights[2][2] = {{A2, A1}, {A1, A2}};
+    double sumsq[2];
+    for (int a = 0; a < 2; ++a) sumsq[a] = fields[3 * a] * fields[3 * a] + fields[3 * a + 1] * fields[3 * a + 1] +
+                                           fields[3 * a + 2] * fields[3 * a + 2];
+    for (int e = 0; e < 2; ++e) {
+        const double *w = weights[e];
+        double *o = out + 5 * e, effsq = 0;
+        for (int j = 0; j < 3; ++j) {
+            o[j] = 2 * (w[0] * fields[j] + w[1] * fields[3 + j]);
+            effsq += o[j] * o[j];
+        }
+        const double correction = a2 * (w[0] * sumsq[0] + w[1] * sumsq[1] - .5 * effsq);
+        o[3] = a2 * effsq - e_ref;
+        o[4] = -dt * (correction + e_ref / 2);
+    }
+    for (int r = 0; r < 2; ++r) {
+        // (dt / 2) / (3 + i sigma sqrt 3) = (dt / 2) (3 - i sigma sqrt 3) / 12
+        const double sigma = r == 0 ? 1 : -1;
+        out[10 + 2 * r] = dt / 2 * 3 / 12;
+        out[11 + 2 * r] = -sigma * dt / 2 * sqrt3 / 12;
+    }
+    return HE_OK;
+}
+
 extern "C" int he_vec_axpby(long long n, double a_re, double a_im, const void *x, double b_re, double b_im,
                             const void *y, void *out, void *stream);
 
@@ -528,7 +563,8 @@ extern "C" int he_vec_axpby(long long n, double a_re, double a_im, const void *x
 // exponentials with the field weights (A2, A1) and (A1, A2) of the Gauss-point vector
 // potentials, each a [2/2] Pade pair of shifted solves (I + i alpha (H(A_eff) - e_ref)) s = x,
 // alpha = (dt / 2) / (3 +- i sqrt 3), x <- 2 s - x (python/implicit.py:76-89), each solve the
-// device GMRES above, followed by the phase exp(-i dt (a2 (w . |A|^2 - |A_eff|^2 / 2) + e_ref / 2)).
+// device GMRES above, followed by the phase exp(-i dt (a2 (w . |A|^2 - |A_eff|^2 / 2) + e_ref / 2))
+// (the coefficients of he_cf4_coefficients).
 extern "C" int he_cf4_step(he_krylov *k, he_handle op, he_separable *sep, const void *diag, const void *x, void *y,
                            const double *fields, double dt, double e_ref, double a2, double tol, int restart,
                            int max_restarts, int *iterations, double *residual, void *stream)
@@ -540,33 +576,19 @@ extern "C" int he_cf4_step(he_krylov *k, he_handle op, he_separable *sep, const 
     int rc = buffers(k, HE_C128, &gb);
     if (rc) return rc;
     if (!gb->step) HE_CUDA_TRY(cudaMalloc(&gb->step, k->n * sizeof(double2)));
-    const double sqrt3 = std::sqrt(3.0);
-    const double A1 = (3 - 2 * sqrt3) / 12, A2 = (3 + 2 * sqrt3) / 12;
-    const double weights[2][2] = {{A2, A1}, {A1, A2}};
-    double sumsq[2];
-    for (int a = 0; a < 2; ++a) sumsq[a] = fields[3 * a] * fields[3 * a] + fields[3 * a + 1] * fields[3 * a + 1] +
-                                           fields[3 * a + 2] * fields[3 * a + 2];
+    double co[14];
+    if ((rc = he_cf4_coefficients(fields, dt, e_ref, a2, co))) return rc;
     const long long n = (long long)k->n;
     int total = 0;
     double worst = 0;
     const void *src = x;
     for (int e = 0; e < 2; ++e) {
-        const double *w = weights[e];
-        double eff[3], effsq = 0;
-        for (int j = 0; j < 3; ++j) {
-            eff[j] = 2 * (w[0] * fields[j] + w[1] * fields[3 + j]);
-            effsq += eff[j] * eff[j];
-        }
-        const double correction = a2 * (w[0] * sumsq[0] + w[1] * sumsq[1] - .5 * effsq);
-        const double shift = a2 * effsq - e_ref;
+        const double *eff = co + 5 * e, shift = co[5 * e + 3], theta = co[5 * e + 4];
         for (int r = 0; r < 2; ++r) {
-            // alpha = (dt / 2) / (3 + i sigma sqrt 3) = (dt / 2) (3 - i sigma sqrt 3) / 12
-            const double sigma = r == 0 ? 1 : -1;
-            const double alpha_re = dt / 2 * 3 / 12, alpha_im = -sigma * dt / 2 * sqrt3 / 12;
             int it = 0;
             double res = 0;
-            rc = he_gmres_shifted(k, op, sep, diag, src, gb->step, eff, alpha_re, alpha_im, e_ref, shift, tol, restart,
-                                  max_restarts, HE_C128, &it, &res, stream);
+            rc = he_gmres_shifted(k, op, sep, diag, src, gb->step, eff, co[10 + 2 * r], co[11 + 2 * r], e_ref, shift, tol,
+                                  restart, max_restarts, HE_C128, &it, &res, stream);
             total += it;
             if (res > worst) worst = res;
             if (rc) {
@@ -577,7 +599,6 @@ extern "C" int he_cf4_step(he_krylov *k, he_handle op, he_separable *sep, const 
             if ((rc = he_vec_axpby(n, 2, 0, gb->step, -1, 0, src, y, stream))) return rc;
             src = y;
         }
-        const double theta = -dt * (correction + e_ref / 2);
         if ((rc = he_vec_axpby(n, std::cos(theta), std::sin(theta), y, 0, 0, y, y, stream))) return rc;
     }
     if (iterations) *iterations = total;

@@ -114,3 +114,28 @@ def test_step_and_sample_entries_reject_bad_arguments_on_the_host():
     assert LIB.he_sample_set_wait_extra(None, 1) == HE_ERR_ARG
     assert LIB.he_sample_grid(None) == 0
     assert LIB.he_gmres_segment_hint(None, ct.byref(i), None) == HE_ERR_ARG
+
+
+@pytest.mark.parametrize('a2, e_ref', [(1., -2.9), (.5, 0.), (1., .37)])
+def test_cf4_step_host_arithmetic_matches_the_python_step(a2, e_ref):
+    """he_cf4_coefficients (the arithmetic he_cf4_step runs on the host) against the
+    formulas of implicit.cf4_step / pade_step (python/implicit.py:91-109, :76-89): effective
+    fields, preconditioner shifts, phase angles and the two Pade alphas."""
+    from laqphysics_b200._lib import HE_OK, LIB
+    from laqphysics_b200.implicit import A1, A2, C1, C2, SQRT3
+    rng = np.random.default_rng(11)
+    fields = np.ascontiguousarray(rng.normal(scale=.05, size=(2, 3)))
+    dt = .05
+    out = np.zeros(14)
+    assert LIB.he_cf4_coefficients(fields.ctypes.data, dt, e_ref, a2, out.ctypes.data) == HE_OK
+    for e, w in enumerate(((A2, A1), (A1, A2))):
+        effective = 2 * np.einsum('a,aj->j', w, fields)
+        correction = a2 * (np.dot(w, np.sum(fields ** 2, axis=1)) - .5 * np.dot(effective, effective))
+        shift = a2 * sum(float(a) ** 2 for a in effective) - e_ref
+        np.testing.assert_allclose(out[5 * e:5 * e + 3], effective, rtol=1e-15, atol=1e-18)
+        np.testing.assert_allclose(out[5 * e + 3], shift, rtol=1e-14, atol=1e-16)
+        np.testing.assert_allclose(out[5 * e + 4], -dt * (correction + e_ref / 2), rtol=1e-13, atol=1e-17)
+    for r, root in enumerate((3 + 1j * SQRT3, 3 - 1j * SQRT3)):
+        alpha = (dt / 2) / root
+        np.testing.assert_allclose(out[10 + 2 * r] + 1j * out[11 + 2 * r], alpha, rtol=1e-15)
+    assert C1 < C2
